@@ -1,0 +1,130 @@
+"""Seeded synthetic Macaulay matrices and dense blocks.
+
+No public benchmark suite exists for this path: the reference ships input
+systems without timings.  These generators stand in for the workloads,
+with the shapes, sizes and value distributions the benchmark configurations
+name.  Every generator is a pure function of its arguments and seed
+(numpy PCG64).
+
+* :func:`staircase` -- the standalone A|B/C|D matrix: ``nru = ncl`` known
+  pivots (row i has lead i, coefficient 1), ``nrl`` rows to reduce with
+  leads uniform in ``[0, ncl)``; each row holds a fraction U[dmin, dmax] of
+  all columns, half in the left block inside a band right of its lead and
+  half in the right block around column ``ncl + lead * ncr / ncl``
+  (banded along the pivot staircase), coefficients uniform in [1, p-1],
+  every row monic.  Rows are sorted by (lead, length) like
+  ``sort_matrix_rows`` (src/order.c:98-131), with the known pivot first
+  for its lead.
+* :func:`random_macaulay` -- small irregular matrices for parity tests
+  (sparse, with duplicated leads, empty-ish right blocks, rank deficiency).
+* :func:`dense_lowrank` -- D = L * R mod p with L n x r, R r x n (rank <= r).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .matrix import MacaulayMatrix
+
+
+def _band_sample(rng: np.random.Generator, lo: int, hi: int, k: int) -> np.ndarray:
+    """k distinct integers from [lo, hi) (fewer if the range is short)."""
+    n = hi - lo
+    if n <= 0 or k <= 0:
+        return np.zeros(0, dtype=np.int64)
+    k = min(k, n)
+    if k * 3 >= n:
+        return lo + rng.permutation(n)[:k]
+    out = np.unique(rng.integers(lo, hi, size=int(k * 1.3) + 8))
+    while out.shape[0] < k:
+        out = np.unique(np.concatenate([out, rng.integers(lo, hi, size=k)]))
+    return rng.permutation(out)[:k]
+
+
+def staircase(nru: int = 20000, nrl: int = 5000, ncr: int = 20000, p: int = 65521,
+              dmin: float = 0.02, dmax: float = 0.05, band: float = 4.0,
+              seed: int = 1, laopt: int = 1) -> MacaulayMatrix:
+    """The banded A|B/C|D matrix described in the module docstring.
+
+    ``band`` is the ratio of a band's width to the number of entries drawn
+    in it (4 -> about a quarter of the band is filled)."""
+    rng = np.random.default_rng(seed)
+    ncl = nru
+    nc = ncl + ncr
+    leads = np.concatenate([np.arange(nru), rng.integers(0, ncl, size=nrl)])
+    nnz = np.maximum(2, np.round(rng.uniform(dmin, dmax, size=nru + nrl) * nc)).astype(np.int64)
+    rows_c, rows_v = [], []
+    for i in range(nru + nrl):
+        lead = int(leads[i])
+        na = int(nnz[i] // 2)
+        nb = int(nnz[i] - na)
+        wa = max(1, int(band * na))
+        a = _band_sample(rng, lead + 1, min(ncl, lead + 1 + wa), na - 1)
+        center = ncl + (lead * ncr) // max(ncl, 1)
+        wb = max(1, int(band * nb))
+        b = _band_sample(rng, max(ncl, center - wb // 2), min(nc, center + wb - wb // 2), nb)
+        c = np.concatenate([[lead], rng.permutation(np.concatenate([a, b]))])
+        v = np.concatenate([[1], rng.integers(1, p, size=c.shape[0] - 1)])
+        rows_c.append(c)
+        rows_v.append(v)
+    lens = np.array([r.shape[0] for r in rows_c], dtype=np.int64)
+    is_lower = np.concatenate([np.zeros(nru, bool), np.ones(nrl, bool)])
+    order = np.lexsort((lens, is_lower, leads))  # known pivot first per lead
+    ptr = np.zeros(nru + nrl + 1, dtype=np.int64)
+    np.cumsum(lens[order], out=ptr[1:])
+    cols = np.concatenate([rows_c[i] for i in order]).astype(np.int32)
+    vals = np.concatenate([rows_v[i] for i in order]).astype(np.int32)
+    return MacaulayMatrix(p, ncl, ncr, ptr, cols, vals, laopt)
+
+
+def random_macaulay(nru: int, nrl: int, ncr: int, p: int, density: float = 0.1,
+                    seed: int = 0, laopt: int = 1, dup_rows: int = 0,
+                    right_only_frac: float = 0.0) -> MacaulayMatrix:
+    """Irregular matrix satisfying the mat_t contract.
+
+    ``dup_rows`` lower rows are exact multiples-free copies of known pivots
+    (they reduce to zero); ``right_only_frac`` of the lower rows have no
+    left entries besides their lead."""
+    rng = np.random.default_rng(seed)
+    ncl = nru
+    nc = ncl + ncr
+    rows = []
+    for i in range(nru):
+        k = max(0, int(rng.binomial(nc - i - 1, density)))
+        c = np.concatenate([[i], _band_sample(rng, i + 1, nc, k)])
+        v = np.concatenate([[1], rng.integers(1, p, size=c.shape[0] - 1)])
+        rows.append((i, 0, c, v))
+    for j in range(nrl):
+        lead = int(rng.integers(0, max(ncl, 1)))
+        if j < dup_rows:
+            c, v = rows[lead][2].copy(), rows[lead][3].copy()
+        else:
+            lo = ncl if rng.random() < right_only_frac else lead + 1
+            k = max(0, int(rng.binomial(nc - lo, density)))
+            c = np.concatenate([[lead], _band_sample(rng, lo, nc, k)])
+            v = np.concatenate([[1], rng.integers(1, p, size=c.shape[0] - 1)])
+        rows.append((lead, 1, c, v))
+    rows.sort(key=lambda r: (r[0], r[1], r[2].shape[0]))
+    lens = np.array([r[2].shape[0] for r in rows], dtype=np.int64)
+    ptr = np.zeros(len(rows) + 1, dtype=np.int64)
+    np.cumsum(lens, out=ptr[1:])
+    cols = np.concatenate([r[2] for r in rows]).astype(np.int32) if rows else np.zeros(0, np.int32)
+    vals = np.concatenate([r[3] for r in rows]).astype(np.int32) if rows else np.zeros(0, np.int32)
+    return MacaulayMatrix(p, ncl, ncr, ptr, cols, vals, laopt)
+
+
+def dense_lowrank(n_rows: int, n_cols: int, rank: int, p: int, seed: int = 0) -> np.ndarray:
+    """Residue matrix L * R mod p (int64) of rank <= ``rank``, L and R uniform.
+
+    Exact: the products are split into 16-bit halves of R so every partial
+    sum stays far below 2^63."""
+    rng = np.random.default_rng(seed)
+    L = rng.integers(0, p, size=(n_rows, rank), dtype=np.int64)
+    R = rng.integers(0, p, size=(rank, n_cols), dtype=np.int64)
+    out = np.zeros((n_rows, n_cols), dtype=np.int64)
+    r_lo, r_hi = R & 0xFFFF, R >> 16
+    step = max(1, int((1 << 62) // (max(p - 1, 1) << 16)))
+    for k0 in range(0, rank, step):
+        lo = (L[:, k0:k0 + step] @ r_lo[k0:k0 + step, :]) % p
+        hi = (L[:, k0:k0 + step] @ r_hi[k0:k0 + step, :]) % p
+        out = (out + lo + ((hi << 16) % p)) % p
+    return out
