@@ -1,0 +1,307 @@
+"""Benchmark: exact GF(p) Macaulay-matrix reductions per second on one B200.
+
+Workload (one "step" = one full reduction of one matrix): the standalone
+A|B/C|D matrix of 20,000 known pivots (upper-triangular A with unit
+diagonal), 5,000 rows to reduce and 40,000 columns (20,000 | 20,000), row
+density U[2%, 5%] banded along the pivot staircase, coefficients uniform mod
+65521, uint32 column indices -- seeded synthetic data (gb_b200.synth.staircase,
+seed 1).  The input (about 230 MB of CSR) is larger than the 126 MB L2, so
+consecutive steps do not hit in L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  `value` is device-timed (CUDA events on the
+library's launching stream, inputs resident in HBM); `e2e` goes through the
+public C entry point gbgpu_reduce with the CSR in pinned host memory
+(H2D + reduction + D2H of the answer each step).  `--impl reference` times the
+reference's own CPU la (oracle/_ref, all host threads) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+CONFIG = {"nru": 20000, "nrl": 5000, "ncr": 20000, "p": 65521, "dmin": 0.02, "dmax": 0.05,
+          "seed": 1}
+METRIC = "GF(p) matrix reductions/s (20000x5000 A|B/C|D, 40000 cols, p=65521, bit-exact)"
+UNIT = "matrices/s"
+
+
+def workload_name():
+    c = CONFIG
+    return (f"staircase A|B/C|D nru={c['nru']} nrl={c['nrl']} ncl={c['nru']} ncr={c['ncr']} "
+            f"density U[{c['dmin']},{c['dmax']}] p={c['p']}")
+
+
+def make_matrix():
+    from gb_b200 import synth
+    c = CONFIG
+    return synth.staircase(c["nru"], c["nrl"], c["ncr"], c["p"], c["dmin"], c["dmax"],
+                           seed=c["seed"])
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l]
+            os.unlink(self.path)
+        except OSError:
+            return out
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+        if mx:
+            out["sm_max_mhz"] = max(mx)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(sm)
+        return out
+
+
+def algorithmic_bytes_schur(mat, work_entries: int, ncr: int) -> int:
+    """Algorithmic bytes of the known-pivot reduction of the C|D rows:
+    read of the rows to reduce (4 + 4 len + cb len each), the pivot entries
+    applied (W (4 + cb)), the dense right-block rows written (4 ncr each).
+    cb = ceil(log2(p) / 8) bytes per coefficient."""
+    cb = max(1, (int(mat.p - 1).bit_length() + 7) // 8)
+    leads = mat.leads()
+    first = np.zeros(mat.nr, dtype=bool)
+    _, idx = np.unique(leads, return_index=True)
+    first[idx] = True
+    lens = np.diff(mat.row_ptr)[~first]
+    rows_in = int(np.sum(4 + 4 * lens + cb * lens))
+    return rows_in + work_entries * (4 + cb) + int(lens.shape[0]) * ncr * 4
+
+
+def cpu_reference(mat, steps: int, budget_s: float = 20.0):
+    """The reference's own la (oracle/_ref, la option 1, all host threads) on
+    a bounded sample: all known pivots and a stride-selected subset of the
+    C|D rows.  Matrices/s is extrapolated linearly in the number of C|D rows
+    (the dense tail grows faster, so this favours the CPU)."""
+    import oracle
+    threads = os.cpu_count() or 1
+    nrl = mat.nr - mat.ncl
+    frac = 0.01
+    # calibrate the sample so one call takes a few seconds
+    while True:
+        keep = np.arange(0, nrl, max(1, int(round(1 / frac))))
+        sub = mat.subset(keep)
+        _, secs = oracle.ref_la(sub, 1, nthreads=threads)
+        if secs > budget_s / max(steps, 1) / 4 or frac >= 1.0:
+            break
+        frac = min(1.0, frac * 2)
+    times = [secs]
+    for _ in range(max(steps, 1) - 1):
+        _, secs = oracle.ref_la(sub, 1, nthreads=threads)
+        times.append(secs)
+    t = statistics.median(times)
+    share = keep.shape[0] / nrl
+    return {"value": share / t, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": (f"reference la option 1 (oracle/_ref, {threads} OpenMP threads) on all "
+                       f"{mat.ncl} known pivots + {keep.shape[0]} of {nrl} C|D rows "
+                       f"(every {int(round(1 / frac))}th), median of {len(times)} calls "
+                       f"{t:.3f}s, extrapolated linearly to all {nrl} rows")}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    mat = make_matrix()
+    cb = cpu_reference(mat, args.steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": workload_name(), "la_option": 1,
+                       "l2": "input larger than L2"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gbgpu")
+    ap.add_argument("--form", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from gb_b200 import _lib, la
+
+    lib = _lib.load()
+    mat = make_matrix()  # every rank reduces its own replica (weak scaling)
+
+    # ---- device-resident timing ------------------------------------------
+    plan = la.Plan(mat, form=args.form, device=local)
+    for _ in range(max(args.warmup, 3)):
+        plan.run()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    launches0 = lib.gbgpu_kernel_launches()
+    step_ms, schur_ms, stats = [], [], None
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            plan.run()
+            stats = plan.stats()
+            step_ms.append(stats["ms_total"])
+            schur_ms.append(stats["ms_schur"])
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    launches = lib.gbgpu_kernel_launches() - launches0
+    ms = float(np.mean(step_ms))
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    answer = plan.result()
+    work_sparse = _work_counters(plan)
+    plan.close()
+
+    # ---- end to end through gbgpu_reduce with pinned host buffers ---------
+    ptr_h = torch.from_numpy(mat.row_ptr).pin_memory()
+    cols_h = torch.from_numpy(mat.cols).pin_memory()
+    vals_h = torch.from_numpy(mat.vals).pin_memory()
+    csr = _lib.Csr(mat.p, mat.laopt, mat.nr, mat.ncl, mat.ncr, ptr_h.data_ptr(),
+                   cols_h.data_ptr(), vals_h.data_ptr())
+    opt = _lib.Options(args.form, local, 1, 0, None)
+    e2e_steps = max(2, min(args.steps, 5))
+    out = _lib.Rows()
+    _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
+    lib.gbgpu_rows_free(C.byref(out))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d2h = 0
+    for _ in range(e2e_steps):
+        out = _lib.Rows()
+        _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
+        d2h = (out.np + 1) * 8 + out.nnz * 8
+        lib.gbgpu_rows_free(C.byref(out))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
+
+    value = ws * 1000.0 / ms
+    sch = float(np.mean(schur_ms))
+    alg = algorithmic_bytes_schur(mat, work_sparse, mat.ncr)
+    peaks = _peaks()
+    achieved = alg / (sch * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (mod p, exact)",
+        "data": "synthetic (seeded, gb_b200.synth.staircase)",
+        "config": {"workload": workload_name(), "form": "plain" if args.form in (0, 1) else "tensor",
+                   "l2": "inputs (CSR ~230 MB) larger than L2; no flush needed",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+        "e2e": {"value": ws / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_reduce_sparse", "achieved": achieved,
+                     "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+                     "peak_source": peaks[1], "traffic": None,
+                     "alg_bytes_per_launch": alg, "launch_ms": sch},
+        "stages_ms": {k: stats[k] for k in ("ms_schur", "ms_echelon", "ms_rref", "ms_compact")},
+        "rank": answer.np, "out_nnz": answer.nnz, "wall_s_timed": wall,
+    }
+    line["clocks"] = clk.summary()
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_reference(mat, 3)
+        except Exception as e:  # reference build absent on this host
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def _work_counters(plan) -> int:
+    """Pivot entries applied by the known-pivot step in the last run (the W
+    of the algorithmic-bytes formula; equal to the oracle's count)."""
+    return int(plan.stats()["work_schur"])
+
+
+def _peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+if __name__ == "__main__":
+    main()

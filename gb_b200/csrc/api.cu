@@ -1,0 +1,668 @@
+// api.cu -- host orchestration and the C ABI declared in include/gbgpu.h.
+//
+// A plan owns the device copy of one matrix and every work buffer of one
+// reduction (stream-ordered allocations from the device's default memory
+// pool, which keeps freed blocks cached between F4 rounds).  Runs are
+// enqueued on the plan's stream; the echelon's claiming rounds read one
+// counter back per round, everything else stays on the device until the
+// answer is copied out.
+#include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <sys/time.h>
+#include <vector>
+
+#include "../../include/gbgpu.h"
+#include "common.cuh"
+#include "internal.h"
+#include "kernels.h"
+
+namespace gbgpu {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void set_error(const std::string& s) { g_last_error = s; }
+void count_launch(long long n) { g_launches += n; }
+
+#define GB_CUDA(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+            return GBGPU_ECUDA;                                                    \
+        }                                                                          \
+    } while (0)
+
+#define GB_LAUNCH(...)                                                             \
+    do {                                                                           \
+        __VA_ARGS__;                                                               \
+        cudaError_t e_ = cudaGetLastError();                                       \
+        if (e_ != cudaSuccess) {                                                   \
+            set_error(std::string("launch: ") + cudaGetErrorString(e_));           \
+            return GBGPU_ECUDA;                                                    \
+        }                                                                          \
+        ++launches;                                                                \
+    } while (0)
+
+static int grid_for(int64_t n, int threads, int cap = 148 * 16) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+int device_init(int device, DeviceInfo* info) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        set_error("no CUDA device");
+        return GBGPU_ENODEV;
+    }
+    if (device < 0 || device >= n) {
+        set_error("device ordinal out of range");
+        return GBGPU_ENODEV;
+    }
+    GB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    GB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error("libgbgpu is built for sm_100 (B200) only");
+        return GBGPU_ENODEV;
+    }
+    info->sms = prop.multiProcessorCount;
+    info->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    // keep freed blocks in the stream-ordered pool between reductions
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    return GBGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+struct Plan {
+    int device = 0;
+    DeviceInfo dev{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int mode = 0;  // 0: linear_algebra, 1: interreduction
+    int form = GBGPU_FORM_PLAIN;
+    int check = 1;
+    int32_t p = 0, nr = 0, ncl = 0, ncr = 0, nc = 0, n_work = 0;
+    int64_t nnz = 0;
+    std::vector<void*> bufs;
+
+    // inputs
+    int64_t* row_ptr = nullptr;
+    int32_t* cols = nullptr;
+    uint32_t* vals = nullptr;
+    // classification
+    int32_t* piv_row = nullptr;
+    uint8_t* flag = nullptr;
+    int32_t* work = nullptr;
+    int32_t* n_sel = nullptr;
+    uint32_t* err = nullptr;
+    int32_t* counters = nullptr;  // [0] queue, [1] n_cand, [2] n_losers, [3] n_next, [4] queue2
+    int64_t* work_count = nullptr;
+    // reduced rows
+    int64_t ld = 0;
+    uint32_t* D = nullptr;
+    uint32_t* R = nullptr;
+    int32_t* lead = nullptr;
+    uint32_t* gacc = nullptr;
+    int grid_sparse = 0;
+    bool smem_sparse = true, smem_dense = true;
+    // echelon
+    int32_t* piv_of_col = nullptr;
+    int32_t* claim = nullptr;
+    int32_t* cand = nullptr;
+    int32_t* losers = nullptr;
+    // compaction
+    int32_t* pflag = nullptr;
+    int32_t* ppos = nullptr;
+    int32_t* pivcol = nullptr;
+    int64_t* counts = nullptr;
+    int64_t* offs = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int32_t* out_cols = nullptr;
+    int32_t* out_vals = nullptr;
+    int64_t out_cap = 0;
+    // answer
+    int32_t np = 0;
+    int64_t onnz = 0;
+    uint32_t errbits = 0;
+    gbgpu_stats stats{};
+    cudaEvent_t ev[6] = {};
+    long long launches = 0;
+
+    template <class T>
+    int alloc(T** p, size_t count) {
+        void* q = nullptr;
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        cudaError_t e = cudaMallocAsync(&q, bytes, stream);
+        if (e != cudaSuccess) {
+            set_error(std::string("device allocation: ") + cudaGetErrorString(e));
+            return GBGPU_ENOMEM;
+        }
+        bufs.push_back(q);
+        *p = (T*)q;
+        return GBGPU_OK;
+    }
+    ~Plan() {
+        for (void* q : bufs) cudaFreeAsync(q, stream);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+static int err_to_status(uint32_t bits, std::string* msg) {
+    if (!bits) return GBGPU_OK;
+    std::string s = "input breaks the mat_t contract:";
+    if (bits & kErrEmptyRow) s += " empty row;";
+    if (bits & kErrLeadRange) s += " lead outside the left block;";
+    if (bits & kErrColRange) s += " column out of range or repeated lead;";
+    if (bits & kErrCoefRange) s += " coefficient outside [1,p);";
+    if (bits & kErrNotMonic) s += " row not monic;";
+    if (bits & kErrMissingPivot) s += " left column without known pivot;";
+    if (bits & kErrDupLead) s += " repeated lead in interreduction input;";
+    *msg = s;
+    return GBGPU_EINVAL;
+}
+
+static int plan_setup(Plan* P, const gbgpu_options* opt) {
+    gbgpu_options o{};
+    if (opt) o = *opt;
+    P->device = o.device;
+    int rc = device_init(P->device, &P->dev);
+    if (rc) return rc;
+    P->form = o.form == GBGPU_FORM_AUTO ? GBGPU_FORM_PLAIN : o.form;
+    P->check = 1;  // the contract check is cheap and guards every later index
+    if (o.stream) {
+        P->stream = (cudaStream_t)o.stream;
+    } else {
+        GB_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+        P->own_stream = true;
+    }
+    for (auto& e : P->ev) GB_CUDA(cudaEventCreate(&e));
+    return GBGPU_OK;
+}
+
+static int plan_alloc(Plan* P) {
+    int rc;
+#define A(ptr, n) \
+    if ((rc = P->alloc(&P->ptr, (size_t)(n)))) return rc
+    A(row_ptr, P->nr + 1);
+    A(cols, P->nnz);
+    A(vals, P->nnz);
+    A(piv_row, P->nc);
+    A(flag, P->nr);
+    A(work, P->nr);
+    A(n_sel, 1);
+    A(err, 1);
+    A(counters, 8);
+    A(work_count, 2);
+    const int32_t width = P->mode == 0 ? P->ncr : P->nc;
+    P->ld = ((int64_t)width + 3) & ~(int64_t)3;
+    A(D, (size_t)P->n_work * P->ld);
+    A(lead, P->n_work);
+    if (P->mode == 0) {
+        A(R, (size_t)P->n_work * P->ld);
+        A(claim, P->ncr);
+        A(cand, P->n_work);
+        A(losers, P->n_work);
+    }
+    A(piv_of_col, width);
+    A(pflag, width);
+    A(ppos, width);
+    A(pivcol, width);
+    A(counts, width + 1);
+    A(offs, width + 1);
+    // shared memory budget for the dense accumulators
+    const int64_t smem_cap = std::min<int64_t>(P->dev.smem_optin - 1024, 200 * 1024);
+    P->smem_sparse = (int64_t)P->nc * 4 <= smem_cap;
+    P->smem_dense = (int64_t)P->ncr * 4 <= smem_cap;
+    P->grid_sparse = std::max(1, std::min<int>(P->n_work, P->dev.sms * (P->smem_sparse ? 1 : 2)));
+    if (P->smem_sparse) {
+        // two CTAs per SM when two accumulators fit
+        if ((int64_t)P->nc * 4 * 2 <= P->dev.smem_optin - 4096)
+            P->grid_sparse = std::max(1, std::min<int>(P->n_work, P->dev.sms * 2));
+    } else {
+        A(gacc, (size_t)P->grid_sparse * (((size_t)P->nc + 31) & ~(size_t)31));
+    }
+    // cub temporaries: selection over rows, scans over columns
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cub::CountingInputIterator<int32_t> it(0);
+    cub::DeviceSelect::Flagged(nullptr, b1, it, P->flag, P->work, P->n_sel, P->nr, P->stream);
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, P->pflag, P->ppos, width, P->stream);
+    cub::DeviceScan::ExclusiveSum(nullptr, b3, P->counts, P->offs, width + 1, P->stream);
+    P->cub_bytes = std::max(b1, std::max(b2, b3));
+    A(cub_tmp, P->cub_bytes);
+#undef A
+    return GBGPU_OK;
+}
+
+template <class T>
+static void set_smem(T kernel, int bytes) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <class F>
+static int run_plain(Plan* P, const F& f) {
+    cudaStream_t s = P->stream;
+    long long& launches = P->launches;
+    const int T = 256;
+    const int32_t width = P->mode == 0 ? P->ncr : P->nc;
+
+    GB_CUDA(cudaEventRecord(P->ev[0], s));
+    GB_CUDA(cudaMemsetAsync(P->err, 0, sizeof(uint32_t), s));
+    GB_CUDA(cudaMemsetAsync(P->counters, 0, 8 * sizeof(int32_t), s));
+    GB_CUDA(cudaMemsetAsync(P->work_count, 0, 2 * sizeof(int64_t), s));
+    const int32_t lead_bound = P->mode == 0 ? P->ncl : P->nc;
+    GB_LAUNCH(k_check_rows<<<grid_for((int64_t)P->nr * 32, T), T, 0, s>>>(
+        P->nr, P->row_ptr, P->cols, P->vals, lead_bound, P->nc, (uint32_t)P->p, P->err));
+    GB_LAUNCH(k_fill_i32<<<grid_for(P->nc, T), T, 0, s>>>(P->piv_row, P->nc, INT_MAX));
+    GB_LAUNCH(k_classify<<<grid_for(P->nr, T), T, 0, s>>>(P->nr, P->row_ptr, P->cols, P->nc,
+                                                          P->piv_row));
+    GB_LAUNCH(k_mark_lower<<<grid_for(P->nr, T), T, 0, s>>>(P->nr, P->row_ptr, P->cols, P->nc,
+                                                            P->piv_row, P->flag, P->err,
+                                                            P->mode == 1));
+    if (P->mode == 0)
+        GB_LAUNCH(k_check_pivots<<<grid_for(P->ncl, T), T, 0, s>>>(P->ncl, P->piv_row, P->err));
+    GB_CUDA(cudaMemcpyAsync(&P->errbits, P->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    if (P->errbits) {
+        std::string msg;
+        int rc = err_to_status(P->errbits, &msg);
+        set_error(msg);
+        return rc;
+    }
+    // rows to reduce: the C|D rows in row order (all rows for interreduction)
+    if (P->mode == 0) {
+        cub::CountingInputIterator<int32_t> it(0);
+        size_t bytes = P->cub_bytes;
+        GB_CUDA(cub::DeviceSelect::Flagged(P->cub_tmp, bytes, it, P->flag, P->work, P->n_sel,
+                                           P->nr, s));
+        ++launches;
+    } else {
+        // every row, in row order; row i of the output buffer is input row i,
+        // so the pivot table of the compaction is the lead table itself
+        GB_LAUNCH(k_iota<<<grid_for(P->nr, T), T, 0, s>>>(P->work, P->nr));
+        GB_LAUNCH(k_pivtab<<<grid_for(P->nc, T), T, 0, s>>>(P->nc, P->piv_row, P->piv_of_col));
+    }
+    GB_CUDA(cudaEventRecord(P->ev[1], s));
+
+    // ---- known-pivot reduction ----------------------------------------
+    SparseReduceArgs sa{};
+    sa.row_ptr = P->row_ptr;
+    sa.cols = P->cols;
+    sa.vals = P->vals;
+    sa.piv_row = P->piv_row;
+    sa.piv_limit = P->mode == 0 ? P->ncl : P->nc;
+    sa.skip_lead = P->mode == 1;
+    sa.work = P->work;
+    sa.n_work = P->n_work;
+    sa.nc = P->nc;
+    sa.emit_from = P->mode == 0 ? P->ncl : 0;
+    sa.emit_width = width;
+    sa.out_ld = P->ld;
+    sa.acc_stride = ((int64_t)P->nc + 31) & ~(int64_t)31;
+    sa.out = P->D;
+    sa.out_lead = P->lead;
+    sa.gacc = P->gacc;
+    sa.queue = P->counters + 0;
+    sa.work_count = P->work_count + 0;
+    if (P->n_work > 0) {
+        if (P->smem_sparse) {
+            const int bytes = P->nc * 4;
+            set_smem(k_reduce_sparse<F, true>, bytes);
+            GB_LAUNCH(k_reduce_sparse<F, true><<<P->grid_sparse, kReduceThreads, bytes, s>>>(sa, f));
+        } else {
+            GB_LAUNCH(k_reduce_sparse<F, false><<<P->grid_sparse, kReduceThreads, 0, s>>>(sa, f));
+        }
+    }
+    GB_CUDA(cudaEventRecord(P->ev[2], s));
+
+    const uint32_t* final_rows = P->D;
+    if (P->mode == 0) {
+        // ---- echelon rounds on the dense right block ------------------------
+        GB_LAUNCH(k_fill_i32<<<grid_for(P->ncr, T), T, 0, s>>>(P->piv_of_col, P->ncr, -1));
+        GB_LAUNCH(k_collect_nonzero<<<grid_for(P->n_work, T), T, 0, s>>>(
+            P->n_work, P->lead, P->cand, P->counters + 1));
+        int32_t n_cand = 0;
+        GB_CUDA(cudaMemcpyAsync(&n_cand, P->counters + 1, 4, cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+        P->stats.dense_rows = n_cand;
+        const int dense_grid = std::max(1, P->dev.sms * (P->smem_dense && P->ncr * 8 <= P->dev.smem_optin - 4096 ? 2 : 1));
+        const int dense_bytes = P->smem_dense ? P->ncr * 4 : 0;
+        if (P->smem_dense) set_smem(k_reduce_dense<F, true>, dense_bytes);
+        int rounds = 0;
+        int32_t* cand = P->cand;
+        int32_t* nxt = P->losers;
+        while (n_cand > 0) {
+            ++rounds;
+            GB_LAUNCH(k_fill_i32<<<grid_for(P->ncr, T), T, 0, s>>>(P->claim, P->ncr, INT_MAX));
+            GB_LAUNCH(k_claim<<<grid_for(n_cand, T), T, 0, s>>>(cand, P->counters + 1, P->lead,
+                                                                P->claim));
+            GB_CUDA(cudaMemsetAsync(P->counters + 2, 0, 3 * sizeof(int32_t), s));
+            GB_LAUNCH(k_promote<F><<<grid_for((int64_t)n_cand * 32, T), T, 0, s>>>(
+                cand, P->counters + 1, P->lead, P->claim, P->piv_of_col, P->D, P->ld, P->ncr,
+                nxt, P->counters + 2, f));
+            int32_t n_lost = 0;
+            GB_CUDA(cudaMemcpyAsync(&n_lost, P->counters + 2, 4, cudaMemcpyDeviceToHost, s));
+            GB_CUDA(cudaStreamSynchronize(s));
+            if (n_lost == 0) break;
+            DenseReduceArgs da{};
+            da.src = P->D;
+            da.dst = P->D;
+            da.ld = P->ld;
+            da.ncr = P->ncr;
+            da.mode = kUntilFree;
+            da.piv_of_col = P->piv_of_col;
+            da.work = nxt;
+            da.n_work = P->counters + 2;
+            da.lead = P->lead;
+            da.next = cand;
+            da.n_next = P->counters + 3;
+            da.queue = P->counters + 4;
+            da.work_count = P->work_count + 1;
+            const int g = std::min(dense_grid, n_lost);
+            if (P->smem_dense)
+                GB_LAUNCH(k_reduce_dense<F, true><<<g, kReduceThreads, dense_bytes, s>>>(da, f));
+            else
+                GB_LAUNCH(k_reduce_dense<F, false><<<g, kReduceThreads, 0, s>>>(da, f));
+            // survivors become the next candidates
+            GB_CUDA(cudaMemcpyAsync(P->counters + 1, P->counters + 3, 4, cudaMemcpyDeviceToDevice, s));
+            GB_CUDA(cudaMemcpyAsync(&n_cand, P->counters + 3, 4, cudaMemcpyDeviceToHost, s));
+            GB_CUDA(cudaStreamSynchronize(s));
+        }
+        P->stats.echelon_rounds = rounds;
+        GB_CUDA(cudaEventRecord(P->ev[3], s));
+
+        // ---- back substitution: reduced row echelon form --------------------
+        GB_LAUNCH(k_pivot_flags<<<grid_for(P->ncr, T), T, 0, s>>>(P->ncr, P->piv_of_col, 1,
+                                                                   P->pflag));
+        size_t bytes = P->cub_bytes;
+        GB_CUDA(cub::DeviceScan::ExclusiveSum(P->cub_tmp, bytes, P->pflag, P->ppos, P->ncr, s));
+        ++launches;
+        GB_LAUNCH(k_pivot_list<<<grid_for(P->ncr, T), T, 0, s>>>(P->ncr, P->pflag, P->ppos, 1,
+                                                                  P->pivcol));
+        int32_t last_pos = 0, last_flag = 0;
+        if (P->ncr > 0) {
+            GB_CUDA(cudaMemcpyAsync(&last_pos, P->ppos + P->ncr - 1, 4, cudaMemcpyDeviceToHost, s));
+            GB_CUDA(cudaMemcpyAsync(&last_flag, P->pflag + P->ncr - 1, 4, cudaMemcpyDeviceToHost, s));
+        }
+        GB_CUDA(cudaStreamSynchronize(s));
+        P->np = last_pos + last_flag;
+        if (P->np > 0) {
+            // work list: the pivot rows (row index of each pivot column)
+            GB_LAUNCH(k_gather_rows<<<grid_for(P->np, T), T, 0, s>>>(P->np, P->pivcol,
+                                                                     P->piv_of_col, P->cand,
+                                                                     P->counters + 1));
+            GB_CUDA(cudaMemsetAsync(P->counters + 4, 0, sizeof(int32_t), s));
+            DenseReduceArgs da{};
+            da.src = P->D;
+            da.dst = P->R;
+            da.ld = P->ld;
+            da.ncr = P->ncr;
+            da.mode = kFull;
+            da.piv_of_col = P->piv_of_col;
+            da.work = P->cand;
+            da.n_work = P->counters + 1;
+            da.lead = P->lead;
+            da.queue = P->counters + 4;
+            da.work_count = P->work_count + 1;
+            const int g = std::min(dense_grid, (int)P->np);
+            if (P->smem_dense)
+                GB_LAUNCH(k_reduce_dense<F, true><<<g, kReduceThreads, dense_bytes, s>>>(da, f));
+            else
+                GB_LAUNCH(k_reduce_dense<F, false><<<g, kReduceThreads, 0, s>>>(da, f));
+        }
+        final_rows = P->R;
+        GB_CUDA(cudaEventRecord(P->ev[4], s));
+    } else {
+        GB_LAUNCH(k_pivot_flags<<<grid_for(P->nc, T), T, 0, s>>>(P->nc, P->piv_of_col, 0, P->pflag));
+        size_t bytes = P->cub_bytes;
+        GB_CUDA(cub::DeviceScan::ExclusiveSum(P->cub_tmp, bytes, P->pflag, P->ppos, P->nc, s));
+        ++launches;
+        GB_LAUNCH(k_pivot_list<<<grid_for(P->nc, T), T, 0, s>>>(P->nc, P->pflag, P->ppos, 0,
+                                                                 P->pivcol));
+        P->np = P->nr;
+        GB_CUDA(cudaEventRecord(P->ev[3], s));
+        GB_CUDA(cudaEventRecord(P->ev[4], s));
+    }
+
+    // ---- compaction -----------------------------------------------------------
+    const int32_t shift = P->mode == 0 ? P->ncl : 0;
+    P->onnz = 0;
+    if (P->np > 0) {
+        GB_LAUNCH(k_row_nnz<<<grid_for((int64_t)P->np * 32, T), T, 0, s>>>(
+            P->np, P->pivcol, P->piv_of_col, final_rows, P->ld, width, P->counts));
+        GB_CUDA(cudaMemsetAsync(P->counts + P->np, 0, sizeof(int64_t), s));
+        size_t bytes = P->cub_bytes;
+        GB_CUDA(cub::DeviceScan::ExclusiveSum(P->cub_tmp, bytes, P->counts, P->offs, P->np + 1, s));
+        ++launches;
+        GB_CUDA(cudaMemcpyAsync(&P->onnz, P->offs + P->np, 8, cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+        if (P->onnz > P->out_cap) {
+            int rc;
+            if ((rc = P->alloc(&P->out_cols, (size_t)P->onnz))) return rc;
+            if ((rc = P->alloc(&P->out_vals, (size_t)P->onnz))) return rc;
+            P->out_cap = P->onnz;
+        }
+        GB_LAUNCH(k_row_write<<<grid_for((int64_t)P->np * 32, T), T, 0, s>>>(
+            P->np, P->pivcol, P->piv_of_col, final_rows, P->ld, width, P->offs, shift,
+            P->out_cols, P->out_vals));
+    }
+    GB_CUDA(cudaEventRecord(P->ev[5], s));
+    return GBGPU_OK;
+}
+
+int plan_run(Plan* P) {
+    P->launches = 0;
+    int rc;
+    if ((uint32_t)P->p < 65536u)
+        rc = run_plain(P, FieldSmall::make((uint32_t)P->p));
+    else
+        rc = run_plain(P, FieldMont::make((uint32_t)P->p));
+    count_launch(P->launches);
+    if (rc) return rc;
+    GB_CUDA(cudaEventSynchronize(P->ev[5]));
+    int64_t wc[2] = {0, 0};
+    GB_CUDA(cudaMemcpyAsync(wc, P->work_count, sizeof(wc), cudaMemcpyDeviceToHost, P->stream));
+    GB_CUDA(cudaStreamSynchronize(P->stream));
+    P->stats.work_schur = wc[0];
+    P->stats.work_dense = wc[1];
+    float ms[5] = {0, 0, 0, 0, 0};
+    cudaEventElapsedTime(&ms[0], P->ev[0], P->ev[5]);
+    cudaEventElapsedTime(&ms[1], P->ev[1], P->ev[2]);
+    cudaEventElapsedTime(&ms[2], P->ev[2], P->ev[3]);
+    cudaEventElapsedTime(&ms[3], P->ev[3], P->ev[4]);
+    cudaEventElapsedTime(&ms[4], P->ev[4], P->ev[5]);
+    P->stats.ms_total = ms[0];
+    P->stats.ms_schur = ms[1];
+    P->stats.ms_echelon = ms[2];
+    P->stats.ms_rref = ms[3];
+    P->stats.ms_compact = ms[4];
+    P->stats.rows_reduced = P->n_work;
+    P->stats.rank = P->np;
+    P->stats.kernel_launches = P->launches;
+    return GBGPU_OK;
+}
+
+int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** out) {
+    *out = nullptr;
+    if (!m || m->p < 2 || m->nr < 0 || m->ncl < 0 || m->ncr < 0 ||
+        (int64_t)m->ncl + m->ncr > INT_MAX / 2) {
+        set_error("bad matrix header");
+        return GBGPU_EINVAL;
+    }
+    if (m->nr > 0 && (!m->row_ptr || !m->cols || !m->vals)) {
+        set_error("null CSR array");
+        return GBGPU_EINVAL;
+    }
+    Plan* P = new (std::nothrow) Plan();
+    if (!P) return GBGPU_ENOMEM;
+    int rc = plan_setup(P, opt);
+    if (rc) {
+        delete P;
+        return rc;
+    }
+    P->mode = mode;
+    P->p = m->p;
+    P->nr = m->nr;
+    P->ncl = m->ncl;
+    P->ncr = m->ncr;
+    P->nc = m->ncl + m->ncr;
+    P->nnz = m->nr > 0 ? m->row_ptr[m->nr] : 0;
+    if (m->nr > 0 && (m->row_ptr[0] != 0 || P->nnz < 0)) {
+        delete P;
+        set_error("row_ptr must start at 0");
+        return GBGPU_EINVAL;
+    }
+    // rows to reduce: C|D rows (nr - ncl when the contract holds) or all rows
+    P->n_work = mode == 0 ? std::max(0, m->nr - m->ncl) : m->nr;
+    if ((rc = plan_alloc(P))) {
+        delete P;
+        return rc;
+    }
+    cudaError_t e1 = cudaMemcpyAsync(P->row_ptr, m->row_ptr, sizeof(int64_t) * (P->nr + 1),
+                                     cudaMemcpyHostToDevice, P->stream);
+    cudaError_t e2 = cudaMemcpyAsync(P->cols, m->cols, sizeof(int32_t) * P->nnz,
+                                     cudaMemcpyHostToDevice, P->stream);
+    cudaError_t e3 = cudaMemcpyAsync(P->vals, m->vals, sizeof(int32_t) * P->nnz,
+                                     cudaMemcpyHostToDevice, P->stream);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+        set_error("host to device copy failed");
+        delete P;
+        return GBGPU_ECUDA;
+    }
+    *out = P;
+    return GBGPU_OK;
+}
+
+int plan_result(Plan* P, gbgpu_rows* out) {
+    memset(out, 0, sizeof(*out));
+    GB_CUDA(cudaStreamSynchronize(P->stream));
+    out->np = P->np;
+    out->nnz = P->onnz;
+    out->row_ptr = (int64_t*)malloc(sizeof(int64_t) * (P->np + 1));
+    out->cols = (int32_t*)malloc(sizeof(int32_t) * std::max<int64_t>(P->onnz, 1));
+    out->vals = (int32_t*)malloc(sizeof(int32_t) * std::max<int64_t>(P->onnz, 1));
+    if (!out->row_ptr || !out->cols || !out->vals) {
+        gbgpu_rows_free(out);
+        return GBGPU_ENOMEM;
+    }
+    out->row_ptr[0] = 0;
+    if (P->np > 0) {
+        GB_CUDA(cudaMemcpyAsync(out->row_ptr, P->offs, sizeof(int64_t) * (P->np + 1),
+                                cudaMemcpyDeviceToHost, P->stream));
+        if (P->onnz > 0) {
+            GB_CUDA(cudaMemcpyAsync(out->cols, P->out_cols, sizeof(int32_t) * P->onnz,
+                                    cudaMemcpyDeviceToHost, P->stream));
+            GB_CUDA(cudaMemcpyAsync(out->vals, P->out_vals, sizeof(int32_t) * P->onnz,
+                                    cudaMemcpyDeviceToHost, P->stream));
+        }
+        GB_CUDA(cudaStreamSynchronize(P->stream));
+    }
+    return GBGPU_OK;
+}
+
+void plan_destroy(Plan* P) { delete P; }
+const gbgpu_stats& plan_stats(const Plan* P) { return P->stats; }
+
+}  // namespace gbgpu
+
+// ===========================================================================
+// C ABI
+using namespace gbgpu;
+
+extern "C" {
+
+struct gbgpu_plan {
+    Plan* impl;
+};
+
+int gbgpu_plan_create(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_plan** plan) {
+    if (!plan) return GBGPU_EINVAL;
+    Plan* P = nullptr;
+    int rc = plan_create(m, opt, 0, &P);
+    if (rc) return rc;
+    *plan = new gbgpu_plan{P};
+    return GBGPU_OK;
+}
+
+int gbgpu_plan_run(gbgpu_plan* plan) {
+    if (!plan) return GBGPU_EINVAL;
+    return plan_run(plan->impl);
+}
+
+int gbgpu_plan_result(gbgpu_plan* plan, gbgpu_rows* out) {
+    if (!plan || !out) return GBGPU_EINVAL;
+    return plan_result(plan->impl, out);
+}
+
+int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {
+    if (!plan || !stats) return GBGPU_EINVAL;
+    *stats = plan_stats(plan->impl);
+    return GBGPU_OK;
+}
+
+void gbgpu_plan_destroy(gbgpu_plan* plan) {
+    if (!plan) return;
+    plan_destroy(plan->impl);
+    delete plan;
+}
+
+int gbgpu_reduce(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows* out) {
+    if (!out) return GBGPU_EINVAL;
+    memset(out, 0, sizeof(*out));
+    Plan* P = nullptr;
+    int rc = plan_create(m, opt, 0, &P);
+    if (rc) return rc;
+    rc = plan_run(P);
+    if (!rc) rc = plan_result(P, out);
+    plan_destroy(P);
+    return rc;
+}
+
+int gbgpu_interreduce(int32_t p, int32_t nr, int32_t nc, const int64_t* row_ptr,
+                      const int32_t* cols, const int32_t* vals, const gbgpu_options* opt,
+                      gbgpu_rows* out) {
+    if (!out) return GBGPU_EINVAL;
+    memset(out, 0, sizeof(*out));
+    gbgpu_csr m{p, 2, nr, 0, nc, row_ptr, cols, vals};
+    Plan* P = nullptr;
+    int rc = plan_create(&m, opt, 1, &P);
+    if (rc) return rc;
+    rc = plan_run(P);
+    if (!rc) rc = plan_result(P, out);
+    plan_destroy(P);
+    return rc;
+}
+
+void gbgpu_rows_free(gbgpu_rows* rows) {
+    if (!rows) return;
+    free(rows->row_ptr);
+    free(rows->cols);
+    free(rows->vals);
+    memset(rows, 0, sizeof(*rows));
+}
+
+const char* gbgpu_last_error(void) { return g_last_error.c_str(); }
+int64_t gbgpu_kernel_launches(void) { return g_launches.load(); }
+
+}  // extern "C"

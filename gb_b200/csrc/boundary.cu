@@ -1,0 +1,248 @@
+// boundary.cu -- the drop-in replacements for gb's linear-algebra function
+// pointers (src/data.h:269-279) over the mirrored mat_t / bs_t / stat_t, and
+// the batched flat entry point.
+//
+// Ownership follows the reference exactly (src/la_ff_16.c:601-735,
+// :737-835, :1322-1392, :1605-1673): input rows are freed by the callee,
+// bs coefficient arrays are only read (interreduction frees the basis
+// elements like free_basis_elements, src/basis.c:25-57), output rows and
+// coefficient arrays are malloc'ed host blocks the basis later adopts and
+// frees (src/convert.c:137-280).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <sys/time.h>
+#include <vector>
+
+#include "../../include/gbgpu.h"
+#include "internal.h"
+
+using namespace gbgpu;
+
+namespace {
+
+double cpu_seconds() { return (double)clock() / CLOCKS_PER_SEC; }
+double wall_seconds() {
+    struct timeval t;
+    gettimeofday(&t, nullptr);
+    return (double)t.tv_sec + 1e-6 * (double)t.tv_usec;
+}
+
+// ff_bits as src/io.c:815-828 selects it; the stat_t field is used when set
+int coef_bits(const gbgpu_stat_t* st) {
+    if (st->ff_bits == 8 || st->ff_bits == 16 || st->ff_bits == 32) return st->ff_bits;
+    if (st->fc < 128) return 8;
+    if (st->fc < 32768) return 16;
+    return 32;
+}
+
+int32_t load_cf(const void* const* tab, int bits, int32_t idx, int64_t j) {
+    if (bits == 8) return (int32_t)((const int8_t* const*)tab)[idx][j];
+    if (bits == 16) return (int32_t)((const int16_t* const*)tab)[idx][j];
+    return ((const int32_t* const*)tab)[idx][j];
+}
+
+const void* const* bs_table(const gbgpu_bs_t* bs, int bits) {
+    if (bits == 8) return (const void* const*)bs->cf_8;
+    if (bits == 16) return (const void* const*)bs->cf_16;
+    return (const void* const*)bs->cf_32;
+}
+
+// mat->r rows -> flat CSR (coefficients from `tab`, reduced into [0, p))
+void gather_rows(gbgpu_hm_t* const* rows, int32_t nr, const void* const* tab, int bits,
+                 int32_t p, std::vector<int64_t>& ptr, std::vector<int32_t>& cols,
+                 std::vector<int32_t>& vals) {
+    ptr.assign((size_t)nr + 1, 0);
+    for (int32_t i = 0; i < nr; ++i) ptr[i + 1] = ptr[i] + rows[i][2];
+    cols.resize((size_t)std::max<int64_t>(ptr[nr], 1));
+    vals.resize((size_t)std::max<int64_t>(ptr[nr], 1));
+    for (int32_t i = 0; i < nr; ++i) {
+        const gbgpu_hm_t* r = rows[i];
+        const int64_t off = ptr[i];
+        memcpy(&cols[off], r + 3, sizeof(int32_t) * (size_t)r[2]);
+        for (int64_t j = 0; j < r[2]; ++j) {
+            int32_t v = load_cf(tab, bits, r[0], j) % p;
+            vals[off + j] = v < 0 ? v + p : v;
+        }
+    }
+}
+
+// CSR answer -> malloc'ed reference rows and coefficient arrays
+int store_rows(gbgpu_mat_t* mat, int bits, const gbgpu_rows& out) {
+    const int32_t np = out.np;
+    gbgpu_hm_t** r = (gbgpu_hm_t**)malloc(sizeof(gbgpu_hm_t*) * (size_t)std::max(np, 1));
+    void** cf = (void**)malloc(sizeof(void*) * (size_t)std::max(np, 1));
+    if (!r || !cf) return GBGPU_ENOMEM;
+    const size_t esz = bits == 8 ? 1 : bits == 16 ? 2 : 4;
+    for (int32_t l = 0; l < np; ++l) {
+        const int64_t b = out.row_ptr[l], len = out.row_ptr[l + 1] - b;
+        gbgpu_hm_t* row = (gbgpu_hm_t*)malloc(sizeof(gbgpu_hm_t) * (size_t)(len + 3));
+        void* c = malloc(esz * (size_t)std::max<int64_t>(len, 1));
+        if (!row || !c) return GBGPU_ENOMEM;
+        row[0] = l;
+        row[1] = (gbgpu_hm_t)(len % 4);
+        row[2] = (gbgpu_hm_t)len;
+        memcpy(row + 3, out.cols + b, sizeof(int32_t) * (size_t)len);
+        for (int64_t j = 0; j < len; ++j) {
+            const int32_t v = out.vals[b + j];
+            if (bits == 8) ((int8_t*)c)[j] = (int8_t)v;
+            else if (bits == 16) ((int16_t*)c)[j] = (int16_t)v;
+            else ((int32_t*)c)[j] = v;
+        }
+        r[l] = row;
+        cf[l] = c;
+    }
+    free(mat->r);
+    mat->r = r;
+    if (bits == 8) {
+        free(mat->cf_8);
+        mat->cf_8 = (int8_t**)cf;
+    } else if (bits == 16) {
+        free(mat->cf_16);
+        mat->cf_16 = (int16_t**)cf;
+    } else {
+        free(mat->cf_32);
+        mat->cf_32 = (int32_t**)cf;
+    }
+    mat->np = np;
+    return GBGPU_OK;
+}
+
+gbgpu_options shim_options() {
+    gbgpu_options o{};
+    o.form = GBGPU_FORM_AUTO;
+    const char* dev = getenv("GBGPU_DEVICE");
+    o.device = dev ? atoi(dev) : 0;
+    o.check = 1;
+    return o;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gbgpu_linear_algebra_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_stat_t* st) {
+    if (!mat || !bs || !st) return GBGPU_EINVAL;
+    const double ct0 = cpu_seconds(), rt0 = wall_seconds();
+    const int bits = coef_bits(st);
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> cols, vals;
+    gather_rows(mat->r, mat->nr, bs_table(bs, bits), bits, st->fc, ptr, cols, vals);
+    gbgpu_csr m{st->fc, st->laopt, mat->nr, mat->ncl, mat->ncr, ptr.data(), cols.data(),
+                vals.data()};
+    gbgpu_options o = shim_options();
+    gbgpu_rows out{};
+    int rc = gbgpu_reduce(&m, &o, &out);
+    if (rc) return rc;
+    // the la functions free their input rows (src/la_ff_16.c:665, :688-691, :804)
+    for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
+    rc = store_rows(mat, bits, out);
+    gbgpu_rows_free(&out);
+    if (rc) return rc;
+    // the sparse options also reset the row count (src/la_ff_16.c:734)
+    const int32_t lo = st->laopt;
+    if (!(lo == 1 || lo == 42 || lo == 43)) mat->nr = mat->sz = mat->np;
+    st->la_ctime += cpu_seconds() - ct0;
+    st->la_rtime += wall_seconds() - rt0;
+    st->num_zerored += (mat->nrl - mat->np);
+    if (st->info_level > 1) {
+        printf("%7d new %7d zero", mat->np, mat->nrl - mat->np);
+        fflush(stdout);
+    }
+    return GBGPU_OK;
+}
+
+void gbgpu_linear_algebra(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_stat_t* st) {
+    const int rc = gbgpu_linear_algebra_status(mat, bs, st);
+    if (rc) {
+        fprintf(stderr, "gbgpu_linear_algebra failed (%d): %s\n", rc, gbgpu_last_error());
+        exit(1);
+    }
+}
+
+int gbgpu_interreduce_matrix_rows_status(gbgpu_mat_t* mat, gbgpu_bs_t* bs,
+                                         const gbgpu_stat_t* st) {
+    if (!mat || !bs || !st) return GBGPU_EINVAL;
+    if (st->info_level > 1) printf("                        ");
+    const int bits = coef_bits(st);
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> cols, vals;
+    gather_rows(mat->r, mat->nr, bs_table(bs, bits), bits, st->fc, ptr, cols, vals);
+    gbgpu_options o = shim_options();
+    gbgpu_rows out{};
+    int rc = gbgpu_interreduce(st->fc, mat->nr, mat->nc, ptr.data(), cols.data(), vals.data(),
+                               &o, &out);
+    if (rc) return rc;
+    // free_basis_elements (src/basis.c:25-57): the basis gives up its elements
+    const void* const* tab = bs_table(bs, bits);
+    for (int32_t i = 0; i < bs->ld; ++i) {
+        free(((void**)tab)[i]);
+        free(bs->hm[i]);
+    }
+    bs->ld = 0;
+    for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
+    rc = store_rows(mat, bits, out);
+    gbgpu_rows_free(&out);
+    return rc;
+}
+
+void gbgpu_interreduce_matrix_rows(gbgpu_mat_t* mat, gbgpu_bs_t* bs, const gbgpu_stat_t* st) {
+    const int rc = gbgpu_interreduce_matrix_rows_status(mat, bs, st);
+    if (rc) {
+        fprintf(stderr, "gbgpu_interreduce_matrix_rows failed (%d): %s\n", rc,
+                gbgpu_last_error());
+        exit(1);
+    }
+}
+
+int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
+                       gbgpu_rows* outs, int32_t* status) {
+    if (n < 0 || (n > 0 && (!ms || !outs || !status))) return GBGPU_EINVAL;
+    std::vector<Plan*> plans((size_t)n, nullptr);
+    // every matrix gets its own stream so independent reductions overlap
+    for (int32_t i = 0; i < n; ++i) {
+        memset(&outs[i], 0, sizeof(gbgpu_rows));
+        gbgpu_options o{};
+        if (opt) o = *opt;
+        o.stream = nullptr;
+        status[i] = plan_create(&ms[i], &o, 0, &plans[i]);
+    }
+    for (int32_t i = 0; i < n; ++i)
+        if (!status[i]) status[i] = plan_run(plans[i]);
+    for (int32_t i = 0; i < n; ++i) {
+        if (!status[i]) status[i] = plan_result(plans[i], &outs[i]);
+        if (plans[i]) plan_destroy(plans[i]);
+    }
+    return GBGPU_OK;
+}
+
+int gbgpu_layout(int64_t* out, int32_t n) {
+    const int64_t v[] = {
+        (int64_t)sizeof(gbgpu_mat_t),
+        (int64_t)offsetof(gbgpu_mat_t, r), (int64_t)offsetof(gbgpu_mat_t, cf_8),
+        (int64_t)offsetof(gbgpu_mat_t, cf_16), (int64_t)offsetof(gbgpu_mat_t, cf_32),
+        (int64_t)offsetof(gbgpu_mat_t, sz), (int64_t)offsetof(gbgpu_mat_t, np),
+        (int64_t)offsetof(gbgpu_mat_t, nr), (int64_t)offsetof(gbgpu_mat_t, nc),
+        (int64_t)offsetof(gbgpu_mat_t, nru), (int64_t)offsetof(gbgpu_mat_t, nrl),
+        (int64_t)offsetof(gbgpu_mat_t, ncl), (int64_t)offsetof(gbgpu_mat_t, ncr),
+        (int64_t)sizeof(gbgpu_bs_t),
+        (int64_t)offsetof(gbgpu_bs_t, ld), (int64_t)offsetof(gbgpu_bs_t, hm),
+        (int64_t)offsetof(gbgpu_bs_t, cf_8), (int64_t)offsetof(gbgpu_bs_t, cf_16),
+        (int64_t)offsetof(gbgpu_bs_t, cf_32),
+        (int64_t)sizeof(gbgpu_stat_t),
+        (int64_t)offsetof(gbgpu_stat_t, la_ctime), (int64_t)offsetof(gbgpu_stat_t, la_rtime),
+        (int64_t)offsetof(gbgpu_stat_t, num_zerored), (int64_t)offsetof(gbgpu_stat_t, fc),
+        (int64_t)offsetof(gbgpu_stat_t, laopt), (int64_t)offsetof(gbgpu_stat_t, nthrds),
+        (int64_t)offsetof(gbgpu_stat_t, ff_bits), (int64_t)offsetof(gbgpu_stat_t, info_level),
+    };
+    const int32_t k = (int32_t)(sizeof(v) / sizeof(v[0]));
+    for (int32_t i = 0; i < k && i < n; ++i) out[i] = v[i];
+    return k;
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+// internal.h -- host-side declarations shared by the library's translation units.
+#pragma once
+#include <string>
+
+#include "../../include/gbgpu.h"
+
+namespace gbgpu {
+
+struct DeviceInfo {
+    int sms;
+    int smem_optin;
+};
+
+struct Plan;
+
+void set_error(const std::string& s);
+void count_launch(long long n);
+int device_init(int device, DeviceInfo* info);
+
+// mode 0: linear_algebra (reduce C|D rows by the known pivots, then reduced
+// echelon form of the right block); mode 1: full interreduction of rows with
+// distinct leads.
+int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** out);
+int plan_run(Plan* P);
+int plan_result(Plan* P, gbgpu_rows* out);
+void plan_destroy(Plan* P);
+const gbgpu_stats& plan_stats(const Plan* P);
+
+}  // namespace gbgpu

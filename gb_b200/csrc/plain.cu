@@ -1,0 +1,393 @@
+// plain.cu -- the plain (CUDA-core) form of the GF(p) Macaulay reduction.
+//
+// Pipeline (host side in api.cu):
+//   1. k_check / k_classify / k_mark_lower: input contract, the known pivot of
+//      every lead (first row with that lead, src/la_ff_16.c:762-772) and the
+//      list of C|D rows.
+//   2. k_reduce_sparse: each C|D row is reduced by the known A|B pivots (the
+//      sparse A^-1 step of src/la_ff_16.c:289-351 / :102-190) by one CTA with
+//      a dense accumulator of the row in shared memory (global scratch when the
+//      row does not fit); the D part is written out dense.
+//   3. echelon rounds on the dense D' rows: every nonzero row claims its lead
+//      column, one winner per column becomes a normalised pivot, the others
+//      are reduced by the pivots until their lead is a free column
+//      (src/la_ff_16.c:873-989 without the CAS retry loop).
+//   4. k_reduce_dense in full mode: every pivot row is reduced by the echelon
+//      pivots of all later columns, which gives the reduced row echelon form
+//      (the result of interreduce_dense_matrix, src/la_ff_16.c:837-871).
+//   5. compaction into CSR rows in descending lead order
+//      (convert_to_sparse_matrix_rows, src/la_ff_16.c:1322-1392).
+//
+// Exactness: every value is a residue in [0, p) after every update (field.cuh).
+#include <climits>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gbgpu {
+
+// ---------------------------------------------------------------------------
+// 1. classification and input checks
+__global__ void k_check_rows(int32_t nr, const int64_t* __restrict__ row_ptr,
+                             const int32_t* __restrict__ cols,
+                             const uint32_t* __restrict__ vals, int32_t lead_bound,
+                             int32_t nc, uint32_t p, uint32_t* err) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < nr; i += nwarps) {
+        const int64_t b = row_ptr[i], e = row_ptr[i + 1];
+        uint32_t bad = 0;
+        if (e <= b) {
+            bad |= kErrEmptyRow;
+        } else {
+            const int32_t lead = cols[b];
+            if (lead < 0 || lead >= lead_bound) bad |= kErrLeadRange;
+            if (vals[b] != 1u) bad |= kErrNotMonic;
+            for (int64_t k = b + lane; k < e; k += 32) {
+                const int32_t c = cols[k];
+                const uint32_t v = vals[k];
+                if (c < lead || c >= nc || (k > b && c == lead)) bad |= kErrColRange;
+                if (v == 0u || v >= p) bad |= kErrCoefRange;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        if (lane == 0 && bad) atomicOr(err, bad);
+    }
+}
+
+__global__ void k_fill_i32(int32_t* a, int64_t n, int32_t v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+// piv_row[c] = smallest row index whose lead is c (INT_MAX if none).
+__global__ void k_classify(int32_t nr, const int64_t* __restrict__ row_ptr,
+                           const int32_t* __restrict__ cols, int32_t table_size,
+                           int32_t* piv_row) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x) {
+        const int64_t b = row_ptr[i];
+        if (row_ptr[i + 1] <= b) continue;
+        const int32_t lead = cols[b];
+        if (lead >= 0 && lead < table_size) atomicMin(&piv_row[lead], i);
+    }
+}
+
+// flag[i] = 1 for rows that are not the known pivot of their lead.
+__global__ void k_mark_lower(int32_t nr, const int64_t* __restrict__ row_ptr,
+                             const int32_t* __restrict__ cols, int32_t table_size,
+                             const int32_t* __restrict__ piv_row, uint8_t* flag,
+                             uint32_t* err, int32_t dup_is_error) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x) {
+        const int64_t b = row_ptr[i];
+        uint8_t f = 0;
+        if (row_ptr[i + 1] > b) {
+            const int32_t lead = cols[b];
+            if (lead >= 0 && lead < table_size) f = piv_row[lead] != i;
+        }
+        flag[i] = f;
+        if (f && dup_is_error) atomicOr(err, kErrDupLead);
+    }
+}
+
+__global__ void k_iota(int32_t* a, int32_t n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        a[i] = i;
+}
+
+// pivot table with -1 for columns that lead no row
+__global__ void k_pivtab(int32_t n, const int32_t* __restrict__ piv_row, int32_t* piv_of_col) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        piv_of_col[i] = piv_row[i] == INT_MAX ? -1 : piv_row[i];
+}
+
+// out[i] = pivot row of the i-th pivot column; *n_out = n
+__global__ void k_gather_rows(int32_t n, const int32_t* __restrict__ pivcol,
+                              const int32_t* __restrict__ piv_of_col, int32_t* out,
+                              int32_t* n_out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = piv_of_col[pivcol[i]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = n;
+}
+
+// every column below ncl needs a known pivot
+__global__ void k_check_pivots(int32_t ncl, const int32_t* __restrict__ piv_row, uint32_t* err) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncl; c += gridDim.x * blockDim.x)
+        if (piv_row[c] == INT_MAX) atomicOr(err, kErrMissingPivot);
+}
+
+// ---------------------------------------------------------------------------
+// 2. reduction of sparse rows by sparse pivot rows
+//
+// One CTA per row (persistent CTAs pull rows from a queue in order, so CTAs
+// that run together sweep nearby pivot rows and share them in L2).  The row
+// lives in a dense accumulator acc[0, nc).  Each step finds the first column
+// after the last one handled whose value is nonzero and which has a pivot,
+// then subtracts m * (pivot row) with m = acc[col] (pivot rows are monic).
+// The lead entry of the pivot row is not applied; acc[col] is cleared.
+template <class F, bool SMEM>
+__global__ void __launch_bounds__(kReduceThreads)
+k_reduce_sparse(SparseReduceArgs a, F f) {
+    extern __shared__ __align__(16) uint32_t s_acc[];
+    __shared__ int s_scratch[kReduceThreads / 32];
+    __shared__ int s_work;
+    uint32_t* acc = SMEM ? s_acc : a.gacc + (size_t)blockIdx.x * a.acc_stride;
+    const int tid = threadIdx.x, nt = blockDim.x;
+
+    for (;;) {
+        if (tid == 0) s_work = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int w = s_work;
+        __syncthreads();
+        if (w >= a.n_work) break;
+        const int32_t r = a.work[w];
+        const int64_t rb = a.row_ptr[r], re = a.row_ptr[r + 1];
+        const int32_t lead = a.cols[rb];
+
+        for (int c = lead + tid; c < a.nc; c += nt) acc[c] = 0u;
+        __syncthreads();
+        for (int64_t k = rb + tid; k < re; k += nt) acc[a.cols[k]] = a.vals[k];
+        __syncthreads();
+
+        int last = lead - 1 + a.skip_lead;  // columns <= last are done
+        for (;;) {
+            // scan windows of nt columns after `last`
+            int found = INT_MAX;
+            uint32_t m = 0;
+            for (int base = last + 1; base < a.piv_limit; base += nt) {
+                const int c = base + tid;
+                int cand = INT_MAX;
+                if (c < a.piv_limit && acc[c] != 0u && a.piv_row[c] != INT_MAX) cand = c;
+                found = block_min(cand, s_scratch);
+                if (found != INT_MAX) break;
+            }
+            if (found == INT_MAX) break;
+            m = f.prep(acc[found]);
+            const int32_t pr = a.piv_row[found];
+            const int64_t pb = a.row_ptr[pr] + 1, pe = a.row_ptr[pr + 1];
+            __syncthreads();  // every thread read acc[found] before it is cleared
+            for (int64_t k = pb + tid; k < pe; k += nt) {
+                const int32_t c = a.cols[k];
+                acc[c] = f.mulsub(acc[c], m, a.vals[k]);
+            }
+            if (tid == 0) acc[found] = 0u;
+            if (tid == 0) atomicAdd((unsigned long long*)a.work_count,
+                                    (unsigned long long)(pe - pb + 1));
+            last = found;
+            __syncthreads();
+        }
+
+        // write the window [emit_from, emit_from + emit_width) and its lead
+        uint32_t* out = a.out + (size_t)w * a.out_ld;
+        int first = INT_MAX;
+        for (int k = tid; k < a.emit_width; k += nt) {
+            const uint32_t v = acc[a.emit_from + k];
+            out[k] = v;
+            if (v != 0u && k < first) first = k;
+        }
+        first = block_min(first, s_scratch);
+        if (tid == 0) a.out_lead[w] = first == INT_MAX ? -1 : first;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3./4. reduction of dense rows by dense (echelon) pivot rows
+//
+// mode kUntilFree: reduce row r (in place in `rows`) by the pivots of its
+//   nonzero columns, left to right, until its first nonzero column has no
+//   pivot (its new lead) or the row is zero (lead -1).  Survivors are pushed
+//   onto `next` for the next claiming round.
+// mode kFull: reduce pivot row r of `src` by the pivots of every later
+//   nonzero column and write the result to `dst` (reduced echelon form).
+template <class F, bool SMEM>
+__global__ void __launch_bounds__(kReduceThreads)
+k_reduce_dense(DenseReduceArgs a, F f) {
+    extern __shared__ __align__(16) uint32_t s_acc[];
+    __shared__ int s_scratch[kReduceThreads / 32];
+    __shared__ int s_work;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int ncr = a.ncr;
+
+    for (;;) {
+        if (tid == 0) s_work = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int w = s_work;
+        __syncthreads();
+        if (w >= *a.n_work) break;
+        const int32_t r = a.work[w];
+        const int32_t lead = a.lead[r];
+        const uint32_t* src = a.src + (size_t)r * a.ld;
+        uint32_t* dst = a.dst + (size_t)r * a.ld;
+        uint32_t* acc = SMEM ? s_acc : dst;
+        if (SMEM || src != dst) {
+            for (int c = lead + tid; c < ncr; c += nt) acc[c] = src[c];
+            __syncthreads();
+        }
+        int last = a.mode == kFull ? lead : lead - 1;
+        int new_lead = -1;
+        for (;;) {
+            int found = INT_MAX;
+            for (int base = last + 1; base < ncr; base += nt) {
+                const int c = base + tid;
+                int cand = INT_MAX;
+                if (c < ncr && acc[c] != 0u) {
+                    if (a.mode == kUntilFree || a.piv_of_col[c] >= 0) cand = c;
+                }
+                found = block_min(cand, s_scratch);
+                if (found != INT_MAX) break;
+            }
+            if (found == INT_MAX) break;
+            const int32_t pr = a.piv_of_col[found];
+            if (pr < 0) {  // kUntilFree only: a free column is the new lead
+                new_lead = found;
+                break;
+            }
+            const uint32_t m = f.prep(acc[found]);
+            const uint32_t* prow = a.src + (size_t)pr * a.ld;
+            __syncthreads();
+            for (int c = found + 1 + tid; c < ncr; c += nt) {
+                const uint32_t v = prow[c];
+                if (v != 0u) acc[c] = f.mulsub(acc[c], m, v);
+            }
+            if (tid == 0) acc[found] = 0u;
+            if (tid == 0) atomicAdd((unsigned long long*)a.work_count,
+                                    (unsigned long long)(ncr - found));
+            last = found;
+            __syncthreads();
+        }
+        if (SMEM) {
+            for (int c = lead + tid; c < ncr; c += nt) dst[c] = acc[c];
+        }
+        if (a.mode == kUntilFree && tid == 0) {
+            a.lead[r] = new_lead;
+            if (new_lead >= 0) a.next[atomicAdd(a.n_next, 1)] = r;
+        }
+        __syncthreads();
+    }
+}
+
+// claim[lead] = smallest candidate row with that lead
+__global__ void k_claim(const int32_t* __restrict__ cand, const int32_t* n_cand,
+                        const int32_t* __restrict__ lead, int32_t* claim) {
+    const int n = *n_cand;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t r = cand[i];
+        atomicMin(&claim[lead[r]], r);
+    }
+}
+
+// winners become pivots (normalised by a warp each), losers are listed
+template <class F>
+__global__ void k_promote(const int32_t* __restrict__ cand, const int32_t* n_cand,
+                          const int32_t* __restrict__ lead, int32_t* claim, int32_t* piv_of_col,
+                          uint32_t* rows, int64_t ld, int32_t ncr, int32_t* losers,
+                          int32_t* n_losers, F f) {
+    const int n = *n_cand;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < n; i += nwarps) {
+        const int32_t r = cand[i];
+        const int32_t c = lead[r];
+        if (claim[c] == r) {
+            uint32_t* row = rows + (size_t)r * ld;
+            const uint32_t inv = inverse_mod(row[c], f.p);
+            for (int j = c + 1 + lane; j < ncr; j += 32) row[j] = f.mulmod(row[j], inv);
+            __syncwarp();
+            if (lane == 0) {
+                row[c] = 1u;
+                piv_of_col[c] = r;
+            }
+        } else if (lane == 0) {
+            losers[atomicAdd(n_losers, 1)] = r;
+        }
+    }
+}
+
+// rows with lead >= 0 -> candidate list (first round)
+__global__ void k_collect_nonzero(int32_t n, const int32_t* __restrict__ lead, int32_t* out,
+                                  int32_t* n_out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (lead[i] >= 0) out[atomicAdd(n_out, 1)] = i;
+}
+
+// ---------------------------------------------------------------------------
+// 5. compaction: output row k is the pivot of the k-th pivot column, in
+// descending (linear_algebra) or ascending (interreduction) column order
+__global__ void k_pivot_flags(int32_t ncr, const int32_t* __restrict__ piv_of_col,
+                              int32_t desc, int32_t* flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncr; i += gridDim.x * blockDim.x)
+        flag[i] = piv_of_col[desc ? ncr - 1 - i : i] >= 0;
+}
+
+// pos = exclusive scan of flag; writes the pivot column of output row k
+__global__ void k_pivot_list(int32_t ncr, const int32_t* __restrict__ flag,
+                             const int32_t* __restrict__ pos, int32_t desc, int32_t* pivcol) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncr; i += gridDim.x * blockDim.x)
+        if (flag[i]) pivcol[pos[i]] = desc ? ncr - 1 - i : i;
+}
+
+// nnz of each reduced pivot row (one warp per row)
+__global__ void k_row_nnz(int32_t np, const int32_t* __restrict__ pivcol,
+                          const int32_t* __restrict__ piv_of_col, const uint32_t* __restrict__ rows,
+                          int64_t ld, int32_t ncr, int64_t* counts) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < np; i += nwarps) {
+        const int32_t c0 = pivcol[i];
+        const uint32_t* row = rows + (size_t)piv_of_col[c0] * ld;
+        int64_t cnt = 0;
+        for (int j = c0 + lane; j < ncr; j += 32) cnt += row[j] != 0u;
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0) counts[i] = cnt;
+    }
+}
+
+// write CSR rows: columns shifted by col_shift, order preserved by a warp
+// ballot prefix over each 32-column chunk
+__global__ void k_row_write(int32_t np, const int32_t* __restrict__ pivcol,
+                            const int32_t* __restrict__ piv_of_col,
+                            const uint32_t* __restrict__ rows, int64_t ld, int32_t ncr,
+                            const int64_t* __restrict__ offs, int32_t col_shift,
+                            int32_t* out_cols, int32_t* out_vals) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < np; i += nwarps) {
+        const int32_t c0 = pivcol[i];
+        const uint32_t* row = rows + (size_t)piv_of_col[c0] * ld;
+        int64_t o = offs[i];
+        for (int base = c0; base < ncr; base += 32) {
+            const int j = base + lane;
+            const uint32_t v = j < ncr ? row[j] : 0u;
+            const unsigned bal = __ballot_sync(0xffffffffu, v != 0u);
+            if (v != 0u) {
+                const int64_t at = o + __popc(bal & ((1u << lane) - 1u));
+                out_cols[at] = j + col_shift;
+                out_vals[at] = (int32_t)v;
+            }
+            o += __popc(bal);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// explicit instantiations
+template __global__ void k_reduce_sparse<FieldSmall, true>(SparseReduceArgs, FieldSmall);
+template __global__ void k_reduce_sparse<FieldSmall, false>(SparseReduceArgs, FieldSmall);
+template __global__ void k_reduce_sparse<FieldMont, true>(SparseReduceArgs, FieldMont);
+template __global__ void k_reduce_sparse<FieldMont, false>(SparseReduceArgs, FieldMont);
+template __global__ void k_reduce_dense<FieldSmall, true>(DenseReduceArgs, FieldSmall);
+template __global__ void k_reduce_dense<FieldSmall, false>(DenseReduceArgs, FieldSmall);
+template __global__ void k_reduce_dense<FieldMont, true>(DenseReduceArgs, FieldMont);
+template __global__ void k_reduce_dense<FieldMont, false>(DenseReduceArgs, FieldMont);
+template __global__ void k_promote<FieldSmall>(const int32_t*, const int32_t*, const int32_t*,
+                                               int32_t*, int32_t*, uint32_t*, int64_t, int32_t,
+                                               int32_t*, int32_t*, FieldSmall);
+template __global__ void k_promote<FieldMont>(const int32_t*, const int32_t*, const int32_t*,
+                                              int32_t*, int32_t*, uint32_t*, int64_t, int32_t,
+                                              int32_t*, int32_t*, FieldMont);
+
+}  // namespace gbgpu

@@ -1,0 +1,210 @@
+/* gbgpu.h -- C ABI of the B200 GF(p) linear-algebra library (libgbgpu.so).
+ *
+ * The library performs the linear-algebra step of gb's F4 (ederc/gb v0.16):
+ * the exact reduction over GF(p) of one Macaulay matrix, for primes below
+ * 2^31 (the 8-, 16-, 17- and 31-bit paths of src/la_ff_8.c, src/la_ff_16.c,
+ * src/la_ff_32.c), on one NVIDIA B200.  There is no CPU fallback: every entry
+ * point fails with GBGPU_ENODEV when no usable sm_100 device is present.
+ *
+ * Two layers:
+ *   1. Drop-in replacements for the reference's function pointers
+ *      linear_algebra / interreduce_matrix_rows (src/data.h:269-279), over
+ *      layout-compatible mirrors of mat_t, bs_t and stat_t.
+ *   2. A flat CSR interface (plain pointers and sizes) for standalone and
+ *      batched matrices, with a device-resident plan for repeated runs.
+ *
+ * Answer of one reduction: the rows of the reduced row echelon form of the
+ * matrix's row space restricted to {x : x vanishes on the left block}, i.e.
+ * the new pivots of src/la_ff_16.c:702-727 / :1343-1390: lead coefficient 1,
+ * columns ascending (all >= ncl), rows in descending lead order.  The answer
+ * does not depend on the la option; options 1, 2, 42, 43 and 44 return the
+ * same rows in the reference too.
+ */
+#ifndef GBGPU_H
+#define GBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define GBGPU_OK 0
+#define GBGPU_EINVAL (-22)  /* input breaks the mat_t contract          */
+#define GBGPU_ENOMEM (-12)  /* host or device allocation failed         */
+#define GBGPU_ENODEV (-19)  /* no sm_100 device / CUDA error at init    */
+#define GBGPU_ECUDA (-5)    /* a CUDA call failed                       */
+#define GBGPU_ETIMEDOUT (-110) /* a device-side bounded wait gave up     */
+#define GBGPU_ERANGE (-34)  /* size beyond a documented limit           */
+
+/* ---- 1. drop-in boundary -------------------------------------------- */
+/* Layout mirrors of the reference structs (src/data.h:117-211).  Only the
+ * members the linear algebra reads or writes are named; the byte layout is
+ * identical (checked by the test-suite against the reference build). */
+typedef int32_t gbgpu_hm_t;   /* hm_t  (src/data.h:59-60) */
+typedef int32_t gbgpu_len_t;  /* len_t (src/data.h:64)    */
+
+typedef struct gbgpu_bs_t {   /* bs_t, src/data.h:117-135 */
+    int32_t ld, sz, lo, mltdeg;
+    int32_t *lmps;
+    int32_t *lm;
+    int32_t lml;
+    int8_t *red;
+    gbgpu_hm_t **hm;
+    int8_t **cf_8;
+    int16_t **cf_16;
+    int32_t **cf_32;
+    void **cf_qq;
+} gbgpu_bs_t;
+
+typedef struct gbgpu_mat_t {  /* mat_t, src/data.h:137-155 */
+    gbgpu_hm_t **r;
+    int8_t **cf_8;
+    int16_t **cf_16;
+    int32_t **cf_32;
+    void **cf_qq;
+    void **cf_ab_qq;
+    gbgpu_len_t sz, np, nr, nc, nru, nrl, ncl, ncr;
+} gbgpu_mat_t;
+
+typedef struct gbgpu_stat_t { /* stat_t, src/data.h:157-211 */
+    double round_ctime, select_ctime, symbol_ctime, la_ctime, update_ctime,
+        convert_ctime, overall_ctime, reduce_gb_ctime, rht_ctime;
+    double round_rtime, select_rtime, symbol_rtime, la_rtime, update_rtime,
+        convert_rtime, overall_rtime, reduce_gb_rtime, rht_rtime;
+    int64_t num_pairsred, num_gb_crit, num_redundant_old, num_redundant,
+        num_rht, num_rowsred, num_zerored;
+    int32_t ngens, nvars, mnsel, homogeneous, fc, mo, laopt, init_hts,
+        nthrds, reset_ht, current_rd, current_deg;
+    int64_t max_bht_size, max_sht_size, max_uht_size, nterms_basis;
+    int32_t size_basis, ff_bits, reduce_gb;
+    int32_t info_level, gen_pbm_file;
+} gbgpu_stat_t;
+
+/* Replaces `linear_algebra(mat, bs, st)` at src/f4.c:306 for every la option
+ * (the function-pointer table of src/io.c:581-780).  Same contract as the
+ * reference (src/la_ff_16.c:1430-1507): reads mat->r rows and bs->cf_X
+ * coefficient arrays, frees the input rows, sets mat->np / mat->r /
+ * mat->cf_X with malloc'ed output rows (row[0] = index into mat->cf_X,
+ * row[1] = len % 4, row[2] = len), updates st->la_ctime / la_rtime /
+ * num_zerored.  The reference's function returns void and cannot fail; this
+ * one prints the GBGPU_* status and exits on error, since it has no CPU
+ * fallback. */
+void gbgpu_linear_algebra(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
+                          gbgpu_stat_t *st);
+
+/* Replaces `interreduce_matrix_rows(mat, bs, st)` at src/f4.c:137
+ * (src/la_ff_16.c:1605-1673 and twins): fully interreduces rows with
+ * distinct leads, frees the basis elements like free_basis_elements
+ * (src/basis.c:25-57), stores the reduced rows in mat->r in ascending lead
+ * order and sets mat->np = mat->nr. */
+void gbgpu_interreduce_matrix_rows(gbgpu_mat_t *mat, gbgpu_bs_t *bs,
+                                   const gbgpu_stat_t *st);
+
+/* Same as the two above but returning a status instead of exiting. */
+int gbgpu_linear_algebra_status(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
+                                gbgpu_stat_t *st);
+int gbgpu_interreduce_matrix_rows_status(gbgpu_mat_t *mat, gbgpu_bs_t *bs,
+                                         const gbgpu_stat_t *st);
+
+/* ---- 2. flat CSR interface ------------------------------------------ */
+typedef struct gbgpu_csr {
+    int32_t p;        /* prime, 2 <= p < 2^31                           */
+    int32_t laopt;    /* reference la option (1, 2, 42, 43, 44); informational */
+    int32_t nr;       /* rows                                           */
+    int32_t ncl;      /* left-block columns (= number of known pivots)  */
+    int32_t ncr;      /* right-block columns                            */
+    const int64_t *row_ptr; /* [nr + 1], host or device (see flags)      */
+    const int32_t *cols;    /* [nnz]; first entry of a row = its lead     */
+    const int32_t *vals;    /* [nnz]; residues in [1, p), lead = 1        */
+} gbgpu_csr;
+
+/* Reduced rows in host memory allocated by the library with malloc. */
+typedef struct gbgpu_rows {
+    int32_t np;
+    int64_t nnz;
+    int64_t *row_ptr; /* [np + 1] */
+    int32_t *cols;    /* [nnz]    */
+    int32_t *vals;    /* [nnz]    */
+} gbgpu_rows;
+
+/* Algorithm selection. */
+#define GBGPU_FORM_AUTO 0
+#define GBGPU_FORM_PLAIN 1  /* sparse rows on CUDA cores                */
+#define GBGPU_FORM_TENSOR 2 /* blocked, int8 tensor-core modular GEMMs  */
+
+typedef struct gbgpu_options {
+    int32_t form;       /* GBGPU_FORM_*                                  */
+    int32_t device;     /* CUDA device ordinal                           */
+    int32_t check;      /* 1: validate the input contract on the device  */
+    int32_t reserved;
+    void *stream;       /* cudaStream_t to run on; NULL = library stream */
+} gbgpu_options;
+
+/* Work counters and timings of the last run of a plan. */
+typedef struct gbgpu_stats {
+    double ms_total;        /* device time of the whole reduction (events)   */
+    double ms_schur;        /* known-pivot reduction of the C|D rows         */
+    double ms_echelon;      /* echelon of the reduced right block            */
+    double ms_rref;         /* back substitution to reduced echelon form     */
+    double ms_compact;      /* output compaction                             */
+    int64_t rows_reduced;   /* C|D rows                                      */
+    int64_t dense_rows;     /* nonzero rows after the known-pivot step       */
+    int64_t rank;           /* np                                            */
+    int64_t echelon_rounds; /* pivot-claiming rounds of the echelon          */
+    int64_t kernel_launches;/* kernels launched by the last run              */
+    int64_t work_schur;     /* known-pivot entries applied (sum of pivot row
+                               lengths over every pivot application)        */
+    int64_t work_dense;     /* dense-pivot entries applied in the echelon and
+                               back substitution                            */
+} gbgpu_stats;
+
+/* One-shot: host CSR in, host rows out (H2D, reduction, D2H). */
+int gbgpu_reduce(const gbgpu_csr *m, const gbgpu_options *opt,
+                 gbgpu_rows *out);
+
+/* Full interreduction of rows with distinct leads over nc columns (the
+ * reference's interreduce_matrix_rows on a flat matrix); ascending leads. */
+int gbgpu_interreduce(int32_t p, int32_t nr, int32_t nc,
+                      const int64_t *row_ptr, const int32_t *cols,
+                      const int32_t *vals, const gbgpu_options *opt,
+                      gbgpu_rows *out);
+
+void gbgpu_rows_free(gbgpu_rows *rows);
+
+/* Device-resident plan: the matrix is uploaded once; each run reduces it
+ * again from the uploaded copy (inputs are never modified). */
+typedef struct gbgpu_plan gbgpu_plan;
+
+int gbgpu_plan_create(const gbgpu_csr *m, const gbgpu_options *opt,
+                      gbgpu_plan **plan);
+/* Enqueue one reduction on the plan's stream; returns after enqueueing
+ * (the echelon's claiming rounds read one counter back per round). */
+int gbgpu_plan_run(gbgpu_plan *plan);
+/* Block until the last run finished and copy its answer to host memory. */
+int gbgpu_plan_result(gbgpu_plan *plan, gbgpu_rows *out);
+int gbgpu_plan_stats(const gbgpu_plan *plan, gbgpu_stats *stats);
+void gbgpu_plan_destroy(gbgpu_plan *plan);
+
+/* Batched reduction of n independent matrices (different sizes and primes)
+ * in one pass: status[i] receives each matrix's own status, so one bad
+ * matrix does not fail the others.  Returns GBGPU_OK if the batch ran. */
+int gbgpu_reduce_batch(int32_t n, const gbgpu_csr *ms,
+                       const gbgpu_options *opt, gbgpu_rows *outs,
+                       int32_t *status);
+
+/* ---- misc ------------------------------------------------------------ */
+/* Fills out[0..n) with sizeof/offsetof values of the mirrored structs in
+ * the order the test-suite compares; returns how many it knows. */
+int gbgpu_layout(int64_t *out, int32_t n);
+/* Short description of the last error on this thread. */
+const char *gbgpu_last_error(void);
+/* Kernels launched since load (all entry points), for accounting. */
+int64_t gbgpu_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GBGPU_H */

@@ -104,30 +104,36 @@ def _take(free, n: int, ptr, cols, vals) -> ReducedRows:
     return ReducedRows(optr, oc, ov)
 
 
-def oracle_la(mat: MacaulayMatrix, laopt: Optional[int] = None) -> Tuple[ReducedRows, int]:
+def oracle_la(mat: MacaulayMatrix, laopt: Optional[int] = None, with_work: bool = False):
     """The oracle's answer for one Macaulay matrix and its work count W
-    (pivot-row entries applied, single-threaded order)."""
+    (pivot-row entries applied, single-threaded order).  With ``with_work``
+    W is split as (known pivots, new pivots)."""
     lib = _load_oracle()
     npv = C.c_int32()
     ptr, cols, vals = _PI64(), _PI32(), _PI32()
-    work = C.c_int64()
+    work = (C.c_int64 * 2)()
     rc = lib.oracle_la_csr(mat.p, mat.laopt if laopt is None else laopt, mat.nr, mat.ncl,
                            mat.ncr, mat.row_ptr, mat.cols, mat.vals, C.byref(npv),
-                           C.byref(ptr), C.byref(cols), C.byref(vals), C.byref(work))
+                           C.byref(ptr), C.byref(cols), C.byref(vals),
+                           C.cast(work, _PI64))
     if rc != 0:
         raise ValueError(f"oracle rejected the matrix (rc={rc})")
-    return _take(lib.oracle_free, npv.value, ptr, cols, vals), work.value
+    rows = _take(lib.oracle_free, npv.value, ptr, cols, vals)
+    if with_work:
+        return rows, (work[0], work[1])
+    return rows, work[0] + work[1]
 
 
 def oracle_interreduce(p: int, nc: int, rows: ReducedRows) -> Tuple[ReducedRows, int]:
     lib = _load_oracle()
     ptr, cols, vals = _PI64(), _PI32(), _PI32()
-    work = C.c_int64()
+    work = (C.c_int64 * 2)()
     rc = lib.oracle_interreduce_csr(p, rows.np, nc, rows.row_ptr, rows.cols, rows.vals,
-                                    C.byref(ptr), C.byref(cols), C.byref(vals), C.byref(work))
+                                    C.byref(ptr), C.byref(cols), C.byref(vals),
+                                    C.cast(work, _PI64))
     if rc != 0:
         raise ValueError(f"oracle rejected the rows (rc={rc})")
-    return _take(lib.oracle_free, rows.np, ptr, cols, vals), work.value
+    return _take(lib.oracle_free, rows.np, ptr, cols, vals), work[0] + work[1]
 
 
 def oracle_normalize(row: np.ndarray, p: int) -> np.ndarray:

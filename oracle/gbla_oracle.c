@@ -78,7 +78,8 @@ typedef struct {
     int64_t p;
     int64_t p2;
     int lazy; /* p < 2^17: lazy-add family */
-    int64_t work;
+    int32_t ncl;     /* pivots of columns below ncl are the known ones */
+    int64_t work[2]; /* entries applied: [0] known pivots, [1] new pivots */
 } ofield_t;
 
 static void ofield_init(ofield_t *f, int32_t p)
@@ -86,7 +87,8 @@ static void ofield_init(ofield_t *f, int32_t p)
     f->p = p;
     f->p2 = (int64_t)p * p;
     f->lazy = p < (1 << 17);
-    f->work = 0;
+    f->ncl = 0;
+    f->work[0] = f->work[1] = 0;
 }
 
 /* dr[c] += mul * cf, with mul the multiplier that cancels a residue `m`. */
@@ -134,7 +136,7 @@ static orow_t oreduce_sparse(ofield_t *f, int64_t *dr, orow_t *const *pivs,
         const orow_t *pr = pivs[i];
         const int64_t m = dr[i];
         for (j = 0; j < pr->len; ++j) oaxpy(f, dr, pr->cols[j], m, pr->cfs[j]);
-        f->work += pr->len;
+        f->work[i < f->ncl ? 0 : 1] += pr->len;
         dr[i] = 0;
     }
     if (k == 0) return out;
@@ -221,6 +223,7 @@ static int osplit(int32_t p, int32_t nr, int32_t ncols, int32_t lead_bound,
             bad |= r.cols[j] <= lead || r.cols[j] >= ncols;
         }
         for (j = 0; j < r.len; ++j) bad |= r.cfs[j] <= 0 || r.cfs[j] >= p;
+        bad |= r.cfs[0] != 1; /* F4 rows are monic (src/basis.c:252) */
         if (bad) {
             free(r.cols);
             free(r.cfs);
@@ -331,7 +334,7 @@ static odrow_t oreduce_dense(ofield_t *f, int64_t *dr, int32_t pc,
         const int64_t m = dr[i];
         const int32_t *pv = nps[i]->v;
         for (j = i; j < ncr; ++j) oaxpy(f, dr, j, m, pv[j - i]);
-        f->work += ncr - i;
+        f->work[1] += ncr - i;
     }
     if (np == -1) return out;
     out.start = np;
@@ -376,7 +379,7 @@ static int oracle_sparse_dense(ofield_t *f, int32_t nr, int32_t ncl,
             const int64_t m = dr[c];
             int64_t k;
             for (k = 0; k < pr->len; ++k) oaxpy(f, dr, pr->cols[k], m, pr->cfs[k]);
-            f->work += pr->len;
+            f->work[0] += pr->len;
             dr[c] = 0;
         }
         int32_t *row = (int32_t *)calloc((size_t)ncr + 1, sizeof(int32_t));
@@ -500,6 +503,7 @@ int oracle_la_csr(int32_t p, int32_t laopt, int32_t nr, int32_t ncl,
     int rc;
     if (p < 2 || nr < 0 || ncl < 0 || ncr < 0) return ORACLE_EINVAL;
     ofield_init(&f, p);
+    f.ncl = ncl;
     /* option 1 is the sparse/dense split; every other option is answered by
      * the exact sparse echelon (the probabilistic options 42/43/44 return the
      * same reduced rows, src/io.c:630-650 maps unknown options to 2) */
@@ -510,7 +514,10 @@ int oracle_la_csr(int32_t p, int32_t laopt, int32_t nr, int32_t ncl,
         rc = oracle_sparse_echelon(&f, nr, ncl, ncr, row_ptr, cols, vals,
                                    out_np, optr, ocols, ovals);
     }
-    if (work) *work = f.work;
+    if (work) {
+        work[0] = f.work[0];
+        work[1] = f.work[1];
+    }
     return rc;
 }
 
@@ -554,7 +561,10 @@ int oracle_interreduce_csr(int32_t p, int32_t nr, int32_t nc,
     free(dup);
     free(pivs);
     free(dr);
-    if (work) *work = f.work;
+    if (work) {
+        work[0] = f.work[0];
+        work[1] = f.work[1];
+    }
     return rc;
 }
 

@@ -1,0 +1,103 @@
+"""CPU tests of the boundary: the C-ABI library loads and exports every entry
+point include/gbgpu.h declares, the mirrored structs have the reference's
+byte layout, and the host-side containers/generators keep the contract.
+No compute call is made here (there is no GPU on the CPU runner)."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from gb_b200 import _lib, la, synth
+from gb_b200.matrix import MacaulayMatrix, ff_bits, kernel_family
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                      "gbgpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", " ", src, flags=re.S)
+    names = re.findall(r"\b(gbgpu_[a-z_0-9]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_header_lists_match_binding():
+    assert declared_functions() == sorted(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (\w+)", out))
+    for name in declared_functions():
+        assert name in exported, name
+        assert getattr(lib, name) is not None
+
+
+def test_library_is_sm100a_only():
+    out = subprocess.run(["cuobjdump", "--list-elf", _lib.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    assert "sm_100a" in out
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+def test_mirrored_struct_layout_matches_reference():
+    want = oracle.ref_layout()
+    got = la.layout()
+    assert got.tolist() == want.tolist()
+
+
+def test_ff_bits_and_family_follow_reference_dispatch():
+    assert [ff_bits(p) for p in (2, 101, 127, 128, 251, 32003, 32768, 65521, 2147483647)] == \
+        [8, 8, 8, 16, 16, 16, 32, 32, 32]
+    assert kernel_family(65521) == "17_bit" and kernel_family(131071) == "17_bit" \
+        and kernel_family(2147483647) == "31_bit"
+
+
+def test_staircase_generator_contract():
+    m = synth.staircase(300, 80, 300, 65521, seed=2)
+    m.validate()
+    nru, nrl = m.split_counts()
+    assert (nru, nrl) == (300, 80)
+    lens = np.diff(m.row_ptr)
+    dens = lens / m.nc
+    assert dens.min() >= 0.015 and dens.max() <= 0.055
+    # deterministic
+    m2 = synth.staircase(300, 80, 300, 65521, seed=2)
+    assert np.array_equal(m.cols, m2.cols) and np.array_equal(m.vals, m2.vals)
+
+
+def test_validate_catches_contract_violations():
+    m = synth.random_macaulay(10, 6, 12, 101, seed=4)
+    m.validate()
+    bad = MacaulayMatrix(m.p, m.ncl, m.ncr, m.row_ptr, m.cols.copy(), m.vals)
+    bad.cols[-1] = m.nc  # column out of range
+    with pytest.raises(ValueError):
+        bad.validate()
+    bad = MacaulayMatrix(m.p, m.ncl, m.ncr, m.row_ptr, m.cols, m.vals.copy())
+    bad.vals[-1] = m.p  # coefficient out of range
+    with pytest.raises(ValueError):
+        bad.validate()
+
+
+def test_dense_lowrank_rank():
+    D = synth.dense_lowrank(12, 15, 5, 101, seed=1)
+    # rank over GF(101) by plain elimination
+    A = D.copy() % 101
+    r = 0
+    for c in range(A.shape[1]):
+        piv = next((i for i in range(r, A.shape[0]) if A[i, c] % 101), None)
+        if piv is None:
+            continue
+        A[[r, piv]] = A[[piv, r]]
+        inv = pow(int(A[r, c]), 99, 101)
+        A[r] = (A[r] * inv) % 101
+        for i in range(A.shape[0]):
+            if i != r and A[i, c]:
+                A[i] = (A[i] - A[i, c] * A[r]) % 101
+        r += 1
+    assert r == 5

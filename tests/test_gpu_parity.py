@@ -1,0 +1,174 @@
+"""GPU parity tests: libgbgpu.so (called through its C ABI) against the oracle
+and the reference's captured answers, bit-exact (integer work: no tolerance).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from gb_b200 import _lib, la, synth
+from gb_b200.matrix import MacaulayMatrix, ReducedRows
+from tests.helpers import all_captures, as_rows, f4_cases
+
+pytestmark = pytest.mark.gpu
+
+CAPTURES = all_captures()
+FORMS = [_lib.FORM_PLAIN]
+
+
+def check_same(got: ReducedRows, want: ReducedRows):
+    assert got.equals(want), got.first_difference(want)
+
+
+@pytest.mark.parametrize("name,k,cap", CAPTURES, ids=[f"{n}-{k}" for n, k, _ in CAPTURES])
+def test_gpu_matches_reference_capture(name, k, cap):
+    if cap.kind == 0:
+        for form in FORMS:
+            check_same(la.linear_algebra(cap.mat, form=form), cap.answer)
+    else:
+        got = la.interreduce_matrix_rows(cap.mat.p, cap.mat.nc, as_rows(cap.mat))
+        check_same(got, cap.answer)
+
+
+PRIMES = [2, 3, 101, 127, 251, 32003, 65521, 65537, 131071, 1000003, 2147483647]
+
+
+@pytest.mark.parametrize("p", PRIMES)
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_gpu_matches_oracle_random(p, seed):
+    m = synth.random_macaulay(40, 60, 50, p, density=0.08, seed=seed, dup_rows=5,
+                              right_only_frac=0.3)
+    want, _ = oracle.oracle_la(m)
+    for form in FORMS:
+        check_same(la.linear_algebra(m, form=form), want)
+
+
+@pytest.mark.parametrize("p", [251, 32003, 65521, 2147483647])
+def test_gpu_matches_oracle_staircase(p):
+    m = synth.staircase(1500, 400, 1500, p, seed=7)
+    want, _ = oracle.oracle_la(m, 1)
+    for form in FORMS:
+        check_same(la.linear_algebra(m, form=form), want)
+
+
+def test_gpu_wide_matrix_global_accumulators():
+    # nc and ncr beyond the shared-memory accumulator: global scratch path
+    m = synth.random_macaulay(400, 40, 60000, 65521, density=0.0015, seed=11, dup_rows=3)
+    want, _ = oracle.oracle_la(m)
+    check_same(la.linear_algebra(m), want)
+    m = synth.random_macaulay(300, 30, 70000, 2147483647, density=0.001, seed=12)
+    want, _ = oracle.oracle_la(m)
+    check_same(la.linear_algebra(m), want)
+
+
+def test_gpu_edge_cases():
+    # no rows to reduce
+    m = synth.random_macaulay(20, 0, 10, 101, seed=1)
+    want, _ = oracle.oracle_la(m)
+    assert want.np == 0
+    check_same(la.linear_algebra(m), want)
+    # every lower row is a copy of a known pivot: everything reduces to zero
+    m = synth.random_macaulay(20, 12, 10, 32003, seed=2, dup_rows=12)
+    got = la.linear_algebra(m)
+    assert got.np == 0
+    # empty right block
+    m = synth.random_macaulay(15, 10, 0, 65521, seed=3, density=0.3)
+    got = la.linear_algebra(m)
+    assert got.np == 0
+    # one right column
+    m = synth.random_macaulay(15, 10, 1, 65521, seed=4, density=0.3)
+    want, _ = oracle.oracle_la(m)
+    check_same(la.linear_algebra(m), want)
+    # many rows colliding on few leads, rank-deficient right block
+    m = synth.random_macaulay(3, 80, 20, 7, seed=5, density=0.5)
+    want, _ = oracle.oracle_la(m)
+    check_same(la.linear_algebra(m), want)
+
+
+def _expect_einval(m):
+    with pytest.raises(_lib.GbgpuError) as ei:
+        la.linear_algebra(m)
+    assert ei.value.code == _lib.GBGPU_EINVAL
+
+
+def test_gpu_rejects_contract_violations():
+    m = synth.random_macaulay(10, 8, 12, 101, seed=6)
+    bad = MacaulayMatrix(m.p, m.ncl, m.ncr, m.row_ptr, m.cols, m.vals.copy())
+    bad.vals[0] = 2
+    _expect_einval(bad)  # not monic
+    _expect_einval(MacaulayMatrix(m.p, m.ncl + 1, m.ncr - 1, m.row_ptr, m.cols, m.vals))
+    bad = MacaulayMatrix(m.p, m.ncl, m.ncr, m.row_ptr, m.cols, m.vals.copy())
+    bad.vals[-1] = m.p
+    _expect_einval(bad)  # coefficient out of range
+    bad = MacaulayMatrix(m.p, m.ncl, m.ncr, m.row_ptr, m.cols.copy(), m.vals)
+    bad.cols[-1] = m.nc + 5
+    _expect_einval(bad)  # column out of range
+    # the library still works after rejecting input
+    want, _ = oracle.oracle_la(m)
+    check_same(la.linear_algebra(m), want)
+
+
+def test_gpu_batch_isolates_failures():
+    mats = [synth.random_macaulay(30, 20, 30, p, seed=s, density=0.1)
+            for s, p in enumerate([101, 32003, 65521, 2147483647, 251])]
+    bad = MacaulayMatrix(mats[2].p, mats[2].ncl, mats[2].ncr, mats[2].row_ptr, mats[2].cols,
+                         mats[2].vals.copy())
+    bad.vals[0] = 3
+    mats[2] = bad
+    outs, status = la.reduce_batch(mats)
+    assert status[2] == _lib.GBGPU_EINVAL and outs[2] is None
+    for i in (0, 1, 3, 4):
+        assert status[i] == 0
+        want, _ = oracle.oracle_la(mats[i])
+        check_same(outs[i], want)
+
+
+def test_gpu_plan_reruns_identically():
+    m = synth.staircase(800, 200, 800, 65521, seed=9)
+    want, _ = oracle.oracle_la(m)
+    plan = la.Plan(m)
+    for _ in range(3):
+        plan.run()
+        check_same(plan.result(), want)
+    st = plan.stats()
+    assert st["rank"] == want.np and st["rows_reduced"] == 200
+    assert st["ms_total"] > 0 and st["kernel_launches"] > 0
+    plan.close()
+
+
+def test_gpu_interreduce_random():
+    rng = np.random.default_rng(5)
+    for p in (101, 65521, 2147483647):
+        leads = np.sort(rng.choice(300, size=120, replace=False))
+        ptr, cols, vals = [0], [], []
+        for l in leads:
+            k = min(15, 299 - l)
+            tail = np.sort(rng.choice(np.arange(l + 1, 300), size=k, replace=False)) if k else []
+            cols += [int(l)] + list(map(int, tail))
+            vals += [1] + rng.integers(1, p, size=len(tail)).tolist()
+            ptr.append(len(cols))
+        perm = rng.permutation(len(leads))  # any row order
+        rows = ReducedRows(np.array(ptr), np.array(cols), np.array(vals))
+        sel = [np.arange(rows.row_ptr[i], rows.row_ptr[i + 1]) for i in perm]
+        lens = np.array([len(s) for s in sel])
+        rows_p = ReducedRows(np.concatenate([[0], np.cumsum(lens)]),
+                             rows.cols[np.concatenate(sel)], rows.vals[np.concatenate(sel)])
+        want, _ = oracle.oracle_interreduce(p, 300, rows)
+        check_same(la.interreduce_matrix_rows(p, 300, rows_p), want)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("case", f4_cases(), ids=[c["name"] for c in f4_cases()])
+def test_f4_with_gpu_linear_algebra_matches_golden(case):
+    """gb's own F4 (host code of the reference build) with both linear-algebra
+    call sites pointed at libgbgpu.so reproduces the golden basis."""
+    la_fn = la.function_address("gbgpu_linear_algebra")
+    ir_fn = la.function_address("gbgpu_interreduce_matrix_rows")
+    lens, cfs, exps = oracle.ref_f4(case, la_fn=la_fn, ir_fn=ir_fn)
+    exp = case["expected"]
+    assert lens.shape[0] == exp["bld"]
+    assert int(lens.sum()) == exp["nterms"]
+    assert lens.tolist() == exp["tlen"]
+    assert cfs.tolist() == exp["tcf"]
+    assert exps.tolist() == exp["texp"]
