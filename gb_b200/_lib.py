@@ -64,7 +64,7 @@ EXPORTS = [
     "gbgpu_interreduce_matrix_rows_status", "gbgpu_reduce", "gbgpu_interreduce",
     "gbgpu_rows_free", "gbgpu_plan_create", "gbgpu_plan_run", "gbgpu_plan_result",
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
-    "gbgpu_last_error", "gbgpu_kernel_launches",
+    "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
 ]
 
 _lib = None
@@ -93,6 +93,10 @@ def load(path: str = LIB_PATH):
     lib.gbgpu_reduce_batch.argtypes = [C.c_int32, C.POINTER(Csr), C.POINTER(Options),
                                        C.POINTER(Rows), _PI32]
     lib.gbgpu_layout.argtypes = [_PI64, C.c_int32]
+    dense = [C.c_int32] * 4 + [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                               C.c_int64, C.POINTER(Options)]
+    lib.gbgpu_dense_submul.argtypes = dense
+    lib.gbgpu_dense_submul_host.argtypes = dense
     lib.gbgpu_last_error.restype = C.c_char_p
     lib.gbgpu_kernel_launches.restype = C.c_int64
     _lib = lib

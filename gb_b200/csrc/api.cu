@@ -48,12 +48,31 @@ void count_launch(long long n) { g_launches += n; }
     do {                                                                           \
         __VA_ARGS__;                                                               \
         cudaError_t e_ = cudaGetLastError();                                       \
+        if (debug_trace()) fprintf(stderr, "gbgpu launch %s: %s\n", #__VA_ARGS__,  \
+                                   cudaGetErrorString(e_));                        \
         if (e_ != cudaSuccess) {                                                   \
             set_error(std::string("launch: ") + cudaGetErrorString(e_));           \
             return GBGPU_ECUDA;                                                    \
         }                                                                          \
         ++launches;                                                                \
     } while (0)
+
+#define GB_CALL(expr)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (expr);                                                   \
+        if (debug_trace()) fprintf(stderr, "gbgpu launch %s: %s\n", #expr,          \
+                                   cudaGetErrorString(e_));                        \
+        if (e_ != cudaSuccess) {                                                   \
+            set_error(std::string("launch: ") + cudaGetErrorString(e_));           \
+            return GBGPU_ECUDA;                                                    \
+        }                                                                          \
+        ++launches;                                                                \
+    } while (0)
+
+static bool debug_trace() {
+    static const bool on = getenv("GBGPU_DEBUG") != nullptr;
+    return on;
+}
 
 static int grid_for(int64_t n, int threads, int cap = 148 * 16) {
     int64_t g = (n + threads - 1) / threads;
@@ -255,11 +274,6 @@ static int plan_alloc(Plan* P) {
     return GBGPU_OK;
 }
 
-template <class T>
-static void set_smem(T kernel, int bytes) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-
 template <class F>
 static int run_plain(Plan* P, const F& f) {
     cudaStream_t s = P->stream;
@@ -267,6 +281,11 @@ static int run_plain(Plan* P, const F& f) {
     const int T = 256;
     const int32_t width = P->mode == 0 ? P->ncr : P->nc;
 
+    {
+        cudaError_t stale = cudaGetLastError();
+        if (stale != cudaSuccess && debug_trace())
+            fprintf(stderr, "gbgpu: stale error before run: %s\n", cudaGetErrorString(stale));
+    }
     GB_CUDA(cudaEventRecord(P->ev[0], s));
     GB_CUDA(cudaMemsetAsync(P->err, 0, sizeof(uint32_t), s));
     GB_CUDA(cudaMemsetAsync(P->counters, 0, 8 * sizeof(int32_t), s));
@@ -325,15 +344,8 @@ static int run_plain(Plan* P, const F& f) {
     sa.gacc = P->gacc;
     sa.queue = P->counters + 0;
     sa.work_count = P->work_count + 0;
-    if (P->n_work > 0) {
-        if (P->smem_sparse) {
-            const int bytes = P->nc * 4;
-            set_smem(k_reduce_sparse<F, true>, bytes);
-            GB_LAUNCH(k_reduce_sparse<F, true><<<P->grid_sparse, kReduceThreads, bytes, s>>>(sa, f));
-        } else {
-            GB_LAUNCH(k_reduce_sparse<F, false><<<P->grid_sparse, kReduceThreads, 0, s>>>(sa, f));
-        }
-    }
+    if (P->n_work > 0)
+        GB_CALL(launch_reduce_sparse(sa, f, P->grid_sparse, P->smem_sparse, P->nc * 4, s));
     GB_CUDA(cudaEventRecord(P->ev[2], s));
 
     const uint32_t* final_rows = P->D;
@@ -348,7 +360,6 @@ static int run_plain(Plan* P, const F& f) {
         P->stats.dense_rows = n_cand;
         const int dense_grid = std::max(1, P->dev.sms * (P->smem_dense && P->ncr * 8 <= P->dev.smem_optin - 4096 ? 2 : 1));
         const int dense_bytes = P->smem_dense ? P->ncr * 4 : 0;
-        if (P->smem_dense) set_smem(k_reduce_dense<F, true>, dense_bytes);
         int rounds = 0;
         int32_t* cand = P->cand;
         int32_t* nxt = P->losers;
@@ -358,9 +369,9 @@ static int run_plain(Plan* P, const F& f) {
             GB_LAUNCH(k_claim<<<grid_for(n_cand, T), T, 0, s>>>(cand, P->counters + 1, P->lead,
                                                                 P->claim));
             GB_CUDA(cudaMemsetAsync(P->counters + 2, 0, 3 * sizeof(int32_t), s));
-            GB_LAUNCH(k_promote<F><<<grid_for((int64_t)n_cand * 32, T), T, 0, s>>>(
-                cand, P->counters + 1, P->lead, P->claim, P->piv_of_col, P->D, P->ld, P->ncr,
-                nxt, P->counters + 2, f));
+            GB_CALL(launch_promote(grid_for((int64_t)n_cand * 32, T), T, s, cand, P->counters + 1,
+                                   P->lead, P->claim, P->piv_of_col, P->D, P->ld, P->ncr, nxt,
+                                   P->counters + 2, f));
             int32_t n_lost = 0;
             GB_CUDA(cudaMemcpyAsync(&n_lost, P->counters + 2, 4, cudaMemcpyDeviceToHost, s));
             GB_CUDA(cudaStreamSynchronize(s));
@@ -380,10 +391,7 @@ static int run_plain(Plan* P, const F& f) {
             da.queue = P->counters + 4;
             da.work_count = P->work_count + 1;
             const int g = std::min(dense_grid, n_lost);
-            if (P->smem_dense)
-                GB_LAUNCH(k_reduce_dense<F, true><<<g, kReduceThreads, dense_bytes, s>>>(da, f));
-            else
-                GB_LAUNCH(k_reduce_dense<F, false><<<g, kReduceThreads, 0, s>>>(da, f));
+            GB_CALL(launch_reduce_dense(da, f, g, P->smem_dense, dense_bytes, s));
             // survivors become the next candidates
             GB_CUDA(cudaMemcpyAsync(P->counters + 1, P->counters + 3, 4, cudaMemcpyDeviceToDevice, s));
             GB_CUDA(cudaMemcpyAsync(&n_cand, P->counters + 3, 4, cudaMemcpyDeviceToHost, s));
@@ -426,10 +434,7 @@ static int run_plain(Plan* P, const F& f) {
             da.queue = P->counters + 4;
             da.work_count = P->work_count + 1;
             const int g = std::min(dense_grid, (int)P->np);
-            if (P->smem_dense)
-                GB_LAUNCH(k_reduce_dense<F, true><<<g, kReduceThreads, dense_bytes, s>>>(da, f));
-            else
-                GB_LAUNCH(k_reduce_dense<F, false><<<g, kReduceThreads, 0, s>>>(da, f));
+            GB_CALL(launch_reduce_dense(da, f, g, P->smem_dense, dense_bytes, s));
         }
         final_rows = P->R;
         GB_CUDA(cudaEventRecord(P->ev[4], s));

@@ -62,17 +62,22 @@ __global__ void k_pivtab(int32_t n, const int32_t* piv_row, int32_t* piv_of_col)
 __global__ void k_gather_rows(int32_t n, const int32_t* pivcol, const int32_t* piv_of_col,
                               int32_t* out, int32_t* n_out);
 
-template <class F, bool SMEM>
-__global__ void k_reduce_sparse(SparseReduceArgs a, F f);
-template <class F, bool SMEM>
-__global__ void k_reduce_dense(DenseReduceArgs a, F f);
+// templated kernels are launched through these host functions, defined in
+// the translation unit that defines the kernels
+template <class F>
+cudaError_t launch_reduce_sparse(const SparseReduceArgs& a, const F& f, int grid, bool smem,
+                                 int smem_bytes, cudaStream_t s);
+template <class F>
+cudaError_t launch_reduce_dense(const DenseReduceArgs& a, const F& f, int grid, bool smem,
+                                int smem_bytes, cudaStream_t s);
+template <class F>
+cudaError_t launch_promote(int grid, int threads, cudaStream_t s, const int32_t* cand,
+                           const int32_t* n_cand, const int32_t* lead, int32_t* claim,
+                           int32_t* piv_of_col, uint32_t* rows, int64_t ld, int32_t ncr,
+                           int32_t* losers, int32_t* n_losers, const F& f);
 
 __global__ void k_claim(const int32_t* cand, const int32_t* n_cand, const int32_t* lead,
                         int32_t* claim);
-template <class F>
-__global__ void k_promote(const int32_t* cand, const int32_t* n_cand, const int32_t* lead,
-                          int32_t* claim, int32_t* piv_of_col, uint32_t* rows, int64_t ld,
-                          int32_t ncr, int32_t* losers, int32_t* n_losers, F f);
 __global__ void k_collect_nonzero(int32_t n, const int32_t* lead, int32_t* out, int32_t* n_out);
 __global__ void k_pivot_flags(int32_t ncr, const int32_t* piv_of_col, int32_t desc,
                               int32_t* flag);

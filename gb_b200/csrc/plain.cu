@@ -374,20 +374,58 @@ __global__ void k_row_write(int32_t np, const int32_t* __restrict__ pivcol,
 }
 
 // ---------------------------------------------------------------------------
-// explicit instantiations
-template __global__ void k_reduce_sparse<FieldSmall, true>(SparseReduceArgs, FieldSmall);
-template __global__ void k_reduce_sparse<FieldSmall, false>(SparseReduceArgs, FieldSmall);
-template __global__ void k_reduce_sparse<FieldMont, true>(SparseReduceArgs, FieldMont);
-template __global__ void k_reduce_sparse<FieldMont, false>(SparseReduceArgs, FieldMont);
-template __global__ void k_reduce_dense<FieldSmall, true>(DenseReduceArgs, FieldSmall);
-template __global__ void k_reduce_dense<FieldSmall, false>(DenseReduceArgs, FieldSmall);
-template __global__ void k_reduce_dense<FieldMont, true>(DenseReduceArgs, FieldMont);
-template __global__ void k_reduce_dense<FieldMont, false>(DenseReduceArgs, FieldMont);
-template __global__ void k_promote<FieldSmall>(const int32_t*, const int32_t*, const int32_t*,
-                                               int32_t*, int32_t*, uint32_t*, int64_t, int32_t,
-                                               int32_t*, int32_t*, FieldSmall);
-template __global__ void k_promote<FieldMont>(const int32_t*, const int32_t*, const int32_t*,
-                                              int32_t*, int32_t*, uint32_t*, int64_t, int32_t,
-                                              int32_t*, int32_t*, FieldMont);
+// host launchers: every kernel is launched from this translation unit
+template <class F>
+cudaError_t launch_reduce_sparse(const SparseReduceArgs& a, const F& f, int grid, bool smem,
+                                 int smem_bytes, cudaStream_t s) {
+    if (smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_reduce_sparse<F, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem_bytes);
+        if (e != cudaSuccess) return e;
+        k_reduce_sparse<F, true><<<grid, kReduceThreads, smem_bytes, s>>>(a, f);
+    } else {
+        k_reduce_sparse<F, false><<<grid, kReduceThreads, 0, s>>>(a, f);
+    }
+    return cudaGetLastError();
+}
+
+template <class F>
+cudaError_t launch_reduce_dense(const DenseReduceArgs& a, const F& f, int grid, bool smem,
+                                int smem_bytes, cudaStream_t s) {
+    if (smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_reduce_dense<F, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem_bytes);
+        if (e != cudaSuccess) return e;
+        k_reduce_dense<F, true><<<grid, kReduceThreads, smem_bytes, s>>>(a, f);
+    } else {
+        k_reduce_dense<F, false><<<grid, kReduceThreads, 0, s>>>(a, f);
+    }
+    return cudaGetLastError();
+}
+
+template <class F>
+cudaError_t launch_promote(int grid, int threads, cudaStream_t s, const int32_t* cand,
+                           const int32_t* n_cand, const int32_t* lead, int32_t* claim,
+                           int32_t* piv_of_col, uint32_t* rows, int64_t ld, int32_t ncr,
+                           int32_t* losers, int32_t* n_losers, const F& f) {
+    k_promote<F><<<grid, threads, 0, s>>>(cand, n_cand, lead, claim, piv_of_col, rows, ld, ncr,
+                                          losers, n_losers, f);
+    return cudaGetLastError();
+}
+
+#define GBGPU_INSTANTIATE(F)                                                                   \
+    template cudaError_t launch_reduce_sparse<F>(const SparseReduceArgs&, const F&, int, bool, \
+                                                 int, cudaStream_t);                            \
+    template cudaError_t launch_reduce_dense<F>(const DenseReduceArgs&, const F&, int, bool,   \
+                                                int, cudaStream_t);                             \
+    template cudaError_t launch_promote<F>(int, int, cudaStream_t, const int32_t*,             \
+                                           const int32_t*, const int32_t*, int32_t*, int32_t*, \
+                                           uint32_t*, int64_t, int32_t, int32_t*, int32_t*,    \
+                                           const F&);
+GBGPU_INSTANTIATE(FieldSmall)
+GBGPU_INSTANTIATE(FieldMont)
+#undef GBGPU_INSTANTIATE
 
 }  // namespace gbgpu

@@ -1,0 +1,596 @@
+// tc_gemm.cu -- exact modular GEMM  D <- (D - A B) mod p  on the int8 tensor
+// cores of sm_100a (tcgen05.mma kind::i8, TMA, TMEM), and its plain CUDA-core
+// twin.
+//
+// Residues (uint32 in [0, p), p < 2^31 odd) are split into L unsigned bytes,
+// a = sum_i a_i 2^(8i) with L = 1 (p < 2^8), 2 (< 2^16), 3 (< 2^24), 4.  Then
+//   A B = sum_w 2^(8w) S_w,   S_w = sum_{i+j=w} A_i B_j,   w = 0 .. 2L-2,
+// and every S_w is a u8 x u8 -> s32 tensor-core product accumulated in TMEM.
+// At most L limb pairs share a weight, each product is <= 255^2, so a K panel
+// of at most floor((2^31-1) / (L 255^2)) columns keeps every S_w below 2^31
+// (kPanelBytes below).  After each panel the epilogue folds the weights,
+//   v = sum_w REDC(S_w * (2^(8w) R mod p))   (Montgomery, R = 2^32),
+// and updates D <- D - v mod p in place, so no partial sum ever leaves [0, p).
+// The result is bit-identical to any exact evaluation of (D - A B) mod p.
+//
+// Pipeline (one CTA per 128 x BN output tile, 192 threads):
+//   warp 0      TMA producer: L A-limb tiles (128 x 128 B) and L B-limb tiles
+//               (BN x 128 B) per 128-byte K step into a STAGES-deep ring,
+//               128-byte swizzle (the canonical K-major UMMA layout);
+//   warp 1      TMEM allocation and MMA issue (one elected thread), stage
+//               release through tcgen05.commit;
+//   warps 2..5  epilogue: tcgen05.ld of the 2L-1 weight accumulators of its
+//               32-lane TMEM quarter, fold, read-modify-write of D.
+// Every mbarrier wait is bounded (clock64 budget); on expiry the CTA records
+// GBGPU_ETIMEDOUT in *err, drains its in-flight copies and frees its TMEM.
+// No cluster multicast is used anywhere.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+
+#include "../../include/gbgpu.h"
+#include "field.cuh"
+#include "internal.h"
+#include "tc_gemm.h"
+
+namespace gbgpu {
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of parity `parity` to complete, at most `budget` cycles.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long budget) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > budget) return false;
+    }
+    return true;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// 32 consecutive TMEM columns of this warp's 32 lanes (one row per thread)
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+        "[%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// K-major operand tile with 128-byte swizzle: rows of 128 bytes, 8-row
+// groups 1024 bytes apart (SBO), LBO unused (1), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+template <int L>
+struct TcCfg {
+    static constexpr int BM = 128;
+    static constexpr int BK = 128;  // bytes of K per stage (one swizzle row)
+    static constexpr int BN = L == 1 ? 256 : (L == 2 ? 128 : 64);
+    static constexpr int NW = 2 * L - 1;
+    static constexpr int A_BYTES = BM * BK;
+    static constexpr int B_BYTES = BN * BK;
+    static constexpr int STAGE_BYTES = L * (A_BYTES + B_BYTES);
+    static constexpr int STAGES = L == 1 ? 4 : (L == 2 ? 3 : (L == 3 ? 3 : 2));
+    static constexpr int TMEM_COLS = NW * BN <= 256 ? 256 : 512;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    // K bytes per panel: L * 255^2 * K < 2^31
+    static constexpr int PANEL_KB = L == 1 ? 256 : (L == 2 ? 128 : (L == 3 ? 85 : 64));
+    static constexpr uint32_t IDESC = (2u << 4)                      // D = s32
+                                      | (0u << 7) | (0u << 10)       // A, B = u8
+                                      | ((uint32_t)(BN >> 3) << 17)  // N
+                                      | ((uint32_t)(BM >> 4) << 24); // M
+};
+
+struct TcParams {
+    uint32_t* D;
+    int64_t ldd;
+    int32_t M, N, Mp, Np, nkb;
+    uint32_t p, pneg_inv;
+    uint32_t cw[7];  // 2^(8w) R mod p
+    int32_t* err;
+    long long budget;
+};
+
+template <int L>
+__global__ void __launch_bounds__(192, 1)
+k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+            const TcParams prm) {
+    using C = TcCfg<L>;
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte aligned tile region (shared-window address)
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - raw);
+    uint64_t* bars = (uint64_t*)(gbase + C::STAGES * C::STAGE_BYTES);
+    // bars: full[STAGES], empty[STAGES], tmem_full, tmem_empty; then tmem slot, abort flag
+    const uint32_t bar0 = smem_u32(bars);
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (C::STAGES + s); };
+    const uint32_t tfull_bar = bar0 + 8u * (2 * C::STAGES);
+    const uint32_t tempty_bar = bar0 + 8u * (2 * C::STAGES + 1);
+    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 2 * C::STAGES + 2);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
+    const int nkb = prm.nkb;
+    const int npanels = (nkb + C::PANEL_KB - 1) / C::PANEL_KB;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(tfull_bar, 1);
+        mbar_init(tempty_bar, 4);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32((const void*)tmem_slot)),
+                     "r"((uint32_t)C::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- producer ----
+            int issued = 0;
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb % C::STAGES;
+                const uint32_t ph = (kb / C::STAGES) & 1;
+                if (*abort_flag || !mbar_wait(empty_bar(s), ph ^ 1, prm.budget)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                mbar_expect_tx(full_bar(s), C::STAGE_BYTES);
+                const uint32_t st = base + s * C::STAGE_BYTES;
+                for (int l = 0; l < L; ++l)
+                    tma_load_2d(st + l * C::A_BYTES, &mapA, kb * C::BK, l * prm.Mp + m0,
+                                full_bar(s));
+                for (int l = 0; l < L; ++l)
+                    tma_load_2d(st + L * C::A_BYTES + l * C::B_BYTES, &mapB, kb * C::BK,
+                                l * prm.Np + n0, full_bar(s));
+                issued = kb + 1;
+            }
+            // on abort, let the copies already issued land before the CTA exits
+            for (int kb = issued > C::STAGES ? issued - C::STAGES : 0; kb < issued; ++kb)
+                mbar_wait(full_bar(kb % C::STAGES), (kb / C::STAGES) & 1, prm.budget);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer ----
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb % C::STAGES;
+                const uint32_t ph = (kb / C::STAGES) & 1;
+                const int pk = kb % C::PANEL_KB;
+                const int panel = kb / C::PANEL_KB;
+                if (pk == 0 && panel > 0) {
+                    // accumulators are free once the epilogue read the last panel
+                    if (*abort_flag || !mbar_wait(tempty_bar, (panel - 1) & 1, prm.budget)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                }
+                if (*abort_flag || !mbar_wait(full_bar(s), ph, prm.budget)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t st = base + s * C::STAGE_BYTES;
+#pragma unroll
+                for (int i = 0; i < L; ++i) {
+#pragma unroll
+                    for (int j = 0; j < L; ++j) {
+                        const int w = i + j;
+                        const bool first_pair = (i == (w > L - 1 ? w - (L - 1) : 0));
+#pragma unroll
+                        for (int kk = 0; kk < C::BK / 32; ++kk) {
+                            const uint64_t ad =
+                                umma_desc_sw128(st + i * C::A_BYTES + kk * 32);
+                            const uint64_t bd = umma_desc_sw128(
+                                st + L * C::A_BYTES + j * C::B_BYTES + kk * 32);
+                            const uint32_t acc = (pk == 0 && kk == 0 && first_pair) ? 0u : 1u;
+                            tc_mma_i8(tmem + (uint32_t)(w * C::BN), ad, bd, C::IDESC, acc);
+                        }
+                    }
+                }
+                tc_commit(empty_bar(s));
+                if (pk == C::PANEL_KB - 1 || kb == nkb - 1) tc_commit(tfull_bar);
+            }
+        }
+    } else {
+        // ---- epilogue: warps 2..5, TMEM lane quarter (warp % 4) ----
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        const int gm = m0 + row;
+        const uint32_t p = prm.p;
+        for (int panel = 0; panel < npanels; ++panel) {
+            bool ok = true;
+            if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar, panel & 1, prm.budget);
+            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+            if (!ok) {
+                if (lane == 0) *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            for (int c0 = 0; c0 < C::BN; c0 += 32) {
+                uint32_t v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = 0;
+#pragma unroll
+                for (int w = 0; w < C::NW; ++w) {
+                    uint32_t a[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * C::BN + c0), a);
+                    const uint32_t cw = prm.cw[w];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const uint64_t T = (uint64_t)a[j] * cw;
+                        const uint32_t qq = (uint32_t)T * prm.pneg_inv;
+                        uint32_t r = (uint32_t)((T + (uint64_t)qq * p) >> 32);
+                        r = r >= p ? r - p : r;
+                        const uint32_t sum = v[j] + r;
+                        v[j] = sum >= p ? sum - p : sum;
+                    }
+                }
+                if (gm < prm.M) {
+                    uint32_t* drow = prm.D + (size_t)gm * prm.ldd;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int gn = n0 + c0 + j;
+                        if (gn < prm.N) {
+                            const uint32_t d = drow[gn];
+                            drow[gn] = d >= v[j] ? d - v[j] : d + (p - v[j]);
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty_bar);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(prm.err, GBGPU_ETIMEDOUT);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"((uint32_t)C::TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded
+__global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int32_t M, int32_t K,
+                             int32_t Mp, int32_t Kp, int32_t L, uint8_t* __restrict__ out) {
+    const int64_t total = (int64_t)Mp * (Kp / 4);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t m = (int32_t)(t / (Kp / 4));
+        const int32_t k = (int32_t)(t % (Kp / 4)) * 4;
+        uint32_t v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = (m < M && k + i < K) ? A[(size_t)m * lda + k + i] : 0u;
+        for (int l = 0; l < L; ++l) {
+            const uint32_t packed = ((v[0] >> (8 * l)) & 255u) | (((v[1] >> (8 * l)) & 255u) << 8) |
+                                    (((v[2] >> (8 * l)) & 255u) << 16) |
+                                    (((v[3] >> (8 * l)) & 255u) << 24);
+            *(uint32_t*)(out + ((size_t)l * Mp + m) * Kp + k) = packed;
+        }
+    }
+}
+
+// transposing split: out[l][n][k] = byte l of B[k][n]
+__global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int32_t K, int32_t N,
+                             int32_t Np, int32_t Kp, int32_t L, uint8_t* __restrict__ out) {
+    __shared__ uint32_t tile[32][33];
+    const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    for (int r = ty; r < 32; r += 8) {
+        const int k = k0 + r, n = n0 + tx;
+        tile[r][tx] = (k < K && n < N) ? B[(size_t)k * ldb + n] : 0u;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int n = n0 + r, k = k0 + tx;
+        if (n < Np && k < Kp) {
+            const uint32_t v = tile[tx][r];
+            for (int l = 0; l < L; ++l) out[((size_t)l * Np + n) * Kp + k] = (uint8_t)(v >> (8 * l));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// plain CUDA-core modular GEMM: 64 x 64 tile per 256 threads, 4 x 4 per thread;
+// b is split into 16-bit halves so 2^16 products fit the u64 partial sums.
+__global__ void __launch_bounds__(256)
+k_plain_submul(const uint32_t* __restrict__ A, int64_t lda, const uint32_t* __restrict__ B,
+               int64_t ldb, uint32_t* D, int64_t ldd, int32_t M, int32_t N, int32_t K,
+               FieldMont f) {
+    __shared__ uint32_t sA[16][64 + 1];
+    __shared__ uint32_t sB[16][64 + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    uint64_t lo[4][4], hi[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) lo[i][j] = hi[i][j] = 0;
+    int since = 0;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+            const int kk = t & 15, mm = t >> 4;
+            const int m = m0 + mm, k = k0 + kk;
+            sA[kk][mm] = (m < M && k < K) ? A[(size_t)m * lda + k] : 0u;
+            const int nn = t & 63, kr = t >> 6;
+            const int n = n0 + nn, k2 = k0 + kr;
+            sB[kr][nn] = (n < N && k2 < K) ? B[(size_t)k2 * ldb + n] : 0u;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < 16; ++kk) {
+            uint32_t a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sA[kk][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = sB[kk][tx * 4 + j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    lo[i][j] += (uint64_t)a[i] * (b[j] & 0xFFFFu);
+                    hi[i][j] += (uint64_t)a[i] * (b[j] >> 16);
+                }
+        }
+        __syncthreads();
+        since += 16;
+        if (since >= 32768) {  // keep the partial sums far from 2^64
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    lo[i][j] %= f.p;
+                    hi[i][j] %= f.p;
+                }
+            since = 0;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int m = m0 + ty * 4 + i;
+        if (m >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = n0 + tx * 4 + j;
+            if (n >= N) continue;
+            const uint64_t h = (hi[i][j] % f.p) << 16;
+            const uint32_t v = (uint32_t)((lo[i][j] % f.p + h % f.p) % f.p);
+            const uint32_t d = D[(size_t)m * ldd + n];
+            D[(size_t)m * ldd + n] = d >= v ? d - v : d + (f.p - v);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+static int make_map(CUtensorMap* map, const void* base, int64_t inner, int64_t rows,
+                    int box_inner, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("cuTensorMapEncodeTiled unavailable");
+        return GBGPU_ENODEV;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)inner};
+    cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed");
+        return GBGPU_ECUDA;
+    }
+    return GBGPU_OK;
+}
+
+int limbs_for(uint32_t p) {
+    if (p < (1u << 8)) return 1;
+    if (p < (1u << 16)) return 2;
+    if (p < (1u << 24)) return 3;
+    return 4;
+}
+
+template <int L>
+static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t* err,
+                  long long* launches) {
+    using Cfg = TcCfg<L>;
+    const int32_t Mp = (g.M + Cfg::BM - 1) / Cfg::BM * Cfg::BM;
+    const int32_t Np = (g.N + Cfg::BN - 1) / Cfg::BN * Cfg::BN;
+    const int32_t Kp = (g.K + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
+    uint8_t* Ap = planes;
+    uint8_t* Bp = planes + (size_t)L * Mp * Kp;
+    {
+        const int64_t total = (int64_t)Mp * (Kp / 4);
+        const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+        k_split_rows<<<grid, 256, 0, s>>>(g.A, g.lda, g.M, g.K, Mp, Kp, L, Ap);
+        dim3 gb((Np + 31) / 32, (Kp + 31) / 32);
+        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.K, g.N, Np, Kp, L, Bp);
+        *launches += 2;
+    }
+    CUtensorMap ma, mb;
+    int rc = make_map(&ma, Ap, Kp, (int64_t)L * Mp, Cfg::BK, Cfg::BM);
+    if (rc) return rc;
+    rc = make_map(&mb, Bp, Kp, (int64_t)L * Np, Cfg::BK, Cfg::BN);
+    if (rc) return rc;
+    TcParams prm{};
+    prm.D = g.D;
+    prm.ldd = g.ldd;
+    prm.M = g.M;
+    prm.N = g.N;
+    prm.Mp = Mp;
+    prm.Np = Np;
+    prm.nkb = Kp / Cfg::BK;
+    const FieldMont f = FieldMont::make(g.p);
+    prm.p = g.p;
+    prm.pneg_inv = f.pneg_inv;
+    const uint64_t R = ((uint64_t)1 << 32) % g.p;
+    uint64_t pw = 1;
+    for (int w = 0; w < 7; ++w) {
+        prm.cw[w] = (uint32_t)((pw % g.p) * R % g.p);
+        pw = (pw << 8) % g.p;
+    }
+    prm.err = err;
+    prm.budget = 4000000000LL;  // about 2 s at 2 GHz per wait
+    cudaError_t e = cudaFuncSetAttribute(k_tc_submul<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Cfg::SMEM_BYTES);
+    if (e != cudaSuccess) {
+        set_error(std::string("tc smem attribute: ") + cudaGetErrorString(e));
+        return GBGPU_ECUDA;
+    }
+    dim3 grid(Np / Cfg::BN, Mp / Cfg::BM);
+    k_tc_submul<L><<<grid, 192, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
+    ++*launches;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("tc launch: ") + cudaGetErrorString(e));
+        return GBGPU_ECUDA;
+    }
+    return GBGPU_OK;
+}
+
+size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K) {
+    const int L = limbs_for(p);
+    const int BN = L == 1 ? 256 : (L == 2 ? 128 : 64);
+    const size_t Mp = (size_t)(M + 127) / 128 * 128, Np = (size_t)(N + BN - 1) / BN * BN;
+    const size_t Kp = (size_t)(K + 127) / 128 * 128;
+    return (size_t)L * (Mp + Np) * Kp;
+}
+
+int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
+              long long* launches) {
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return GBGPU_OK;
+    if ((g.p & 1u) == 0 || g.p < 3) {
+        set_error("tensor-core path needs an odd prime");
+        return GBGPU_EINVAL;
+    }
+    uint8_t* planes = (uint8_t*)workspace;
+    switch (limbs_for(g.p)) {
+        case 1: return tc_run<1>(g, planes, s, err, launches);
+        case 2: return tc_run<2>(g, planes, s, err, launches);
+        case 3: return tc_run<3>(g, planes, s, err, launches);
+        default: return tc_run<4>(g, planes, s, err, launches);
+    }
+}
+
+int plain_submul(const TcGemmArgs& g, cudaStream_t s, long long* launches) {
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return GBGPU_OK;
+    dim3 grid((g.N + 63) / 64, (g.M + 63) / 64);
+    FieldMont f{};
+    f.p = g.p;
+    k_plain_submul<<<grid, 256, 0, s>>>(g.A, g.lda, g.B, g.ldb, g.D, g.ldd, g.M, g.N, g.K, f);
+    ++*launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("plain gemm launch: ") + cudaGetErrorString(e));
+        return GBGPU_ECUDA;
+    }
+    return GBGPU_OK;
+}
+
+}  // namespace gbgpu

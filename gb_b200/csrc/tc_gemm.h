@@ -1,0 +1,30 @@
+// tc_gemm.h -- exact modular GEMM D <- (D - A B) mod p (device pointers).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace gbgpu {
+
+struct TcGemmArgs {
+    uint32_t p;
+    int32_t M, N, K;
+    const uint32_t* A;  // M x K, row-major, residues
+    int64_t lda;
+    const uint32_t* B;  // K x N, row-major, residues
+    int64_t ldb;
+    uint32_t* D;        // M x N, row-major, residues, updated in place
+    int64_t ldd;
+};
+
+int limbs_for(uint32_t p);
+// bytes of device workspace the tensor-core path needs for the limb planes
+size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K);
+// tensor-core path (odd p); enqueues on s, *err receives GBGPU_ETIMEDOUT if a
+// bounded wait expired
+int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
+              long long* launches);
+// CUDA-core path (any p)
+int plain_submul(const TcGemmArgs& g, cudaStream_t s, long long* launches);
+
+}  // namespace gbgpu

@@ -195,6 +195,26 @@ int gbgpu_reduce_batch(int32_t n, const gbgpu_csr *ms,
                        const gbgpu_options *opt, gbgpu_rows *outs,
                        int32_t *status);
 
+/* ---- 3. dense exact modular GEMM -------------------------------------- */
+/* D <- (D - A B) mod p for residue matrices (uint32 in [0, p), row-major,
+ * leading dimensions in elements): A is M x K, B is K x N, D is M x N.  The
+ * Schur update D - C A^-1 B of the A|B/C|D split and the trailing updates of
+ * the dense echelon are this operation (the dense steps of
+ * src/la_ff_16.c:353-409 / :837-989 done blockwise).  GBGPU_FORM_TENSOR (the
+ * AUTO choice for odd p) runs it on the int8 tensor cores with the residues
+ * split into 8-bit limbs, GBGPU_FORM_PLAIN on CUDA cores; both are exact.
+ * Pointers are device memory; runs on opt->stream (NULL: the legacy default
+ * stream) and returns when the result is complete. */
+int gbgpu_dense_submul(int32_t p, int32_t M, int32_t N, int32_t K,
+                       const uint32_t *A, int64_t lda, const uint32_t *B,
+                       int64_t ldb, uint32_t *D, int64_t ldd,
+                       const gbgpu_options *opt);
+/* Same with host arrays (copied in and out). */
+int gbgpu_dense_submul_host(int32_t p, int32_t M, int32_t N, int32_t K,
+                            const uint32_t *A, int64_t lda, const uint32_t *B,
+                            int64_t ldb, uint32_t *D, int64_t ldd,
+                            const gbgpu_options *opt);
+
 /* ---- misc ------------------------------------------------------------ */
 /* Fills out[0..n) with sizeof/offsetof values of the mirrored structs in
  * the order the test-suite compares; returns how many it knows. */
