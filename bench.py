@@ -45,11 +45,13 @@ def workload_name():
             f"density U[{c['dmin']},{c['dmax']}] p={c['p']}")
 
 
-def make_matrix():
+def make_matrix(scale: float = 1.0):
+    """The benchmark matrix; `scale` < 1 shrinks every dimension (profiling
+    captures of a small case only; bench lines always use scale 1)."""
     from gb_b200 import synth
     c = CONFIG
-    return synth.staircase(c["nru"], c["nrl"], c["ncr"], c["p"], c["dmin"], c["dmax"],
-                           seed=c["seed"])
+    return synth.staircase(int(c["nru"] * scale), int(c["nrl"] * scale), int(c["ncr"] * scale),
+                           c["p"], c["dmin"], c["dmax"], seed=c["seed"])
 
 
 def dist_env():
@@ -185,7 +187,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gbgpu")
     ap.add_argument("--form", type=int, default=0)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="shrink the workload (profiling captures only)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -200,7 +205,7 @@ def main():
     from gb_b200 import _lib, la
 
     lib = _lib.load()
-    mat = make_matrix()  # every rank reduces its own replica (weak scaling)
+    mat = make_matrix(args.scale)  # every rank reduces its own replica (weak scaling)
 
     # ---- device-resident timing ------------------------------------------
     plan = la.Plan(mat, form=args.form, device=local)
@@ -231,26 +236,7 @@ def main():
     plan.close()
 
     # ---- end to end through gbgpu_reduce with pinned host buffers ---------
-    ptr_h = torch.from_numpy(mat.row_ptr).pin_memory()
-    cols_h = torch.from_numpy(mat.cols).pin_memory()
-    vals_h = torch.from_numpy(mat.vals).pin_memory()
-    csr = _lib.Csr(mat.p, mat.laopt, mat.nr, mat.ncl, mat.ncr, ptr_h.data_ptr(),
-                   cols_h.data_ptr(), vals_h.data_ptr())
-    opt = _lib.Options(args.form, local, 1, 0, None)
-    e2e_steps = max(2, min(args.steps, 5))
-    out = _lib.Rows()
-    _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
-    lib.gbgpu_rows_free(C.byref(out))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    d2h = 0
-    for _ in range(e2e_steps):
-        out = _lib.Rows()
-        _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
-        d2h = (out.np + 1) * 8 + out.nnz * 8
-        lib.gbgpu_rows_free(C.byref(out))
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
+    e2e_s, h2d, d2h = _e2e(lib, mat, args, local) if not args.no_e2e else (float("nan"), 0, 0)
 
     value = ws * 1000.0 / ms
     sch = float(np.mean(schur_ms))
@@ -276,6 +262,8 @@ def main():
         "rank": answer.np, "out_nnz": answer.nnz, "wall_s_timed": wall,
     }
     line["clocks"] = clk.summary()
+    if args.scale != 1.0:
+        line["config"]["scale"] = args.scale
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_reference(mat, 3)
@@ -286,6 +274,34 @@ def main():
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def _e2e(lib, mat, args, device):
+    """Seconds per reduction through gbgpu_reduce (H2D from pinned host memory,
+    reduction, D2H of the answer), and the bytes moved each way per step."""
+    import torch
+    from gb_b200 import _lib
+    ptr_h = torch.from_numpy(mat.row_ptr).pin_memory()
+    cols_h = torch.from_numpy(mat.cols).pin_memory()
+    vals_h = torch.from_numpy(mat.vals).pin_memory()
+    csr = _lib.Csr(mat.p, mat.laopt, mat.nr, mat.ncl, mat.ncr, ptr_h.data_ptr(),
+                   cols_h.data_ptr(), vals_h.data_ptr())
+    opt = _lib.Options(args.form, device, 1, 0, None)
+    steps = max(2, min(args.steps, 5))
+    out = _lib.Rows()
+    _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
+    lib.gbgpu_rows_free(C.byref(out))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d2h = 0
+    for _ in range(steps):
+        out = _lib.Rows()
+        _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
+        d2h = (out.np + 1) * 8 + out.nnz * 8
+        lib.gbgpu_rows_free(C.byref(out))
+    e2e_s = (time.perf_counter() - t0) / steps
+    h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
+    return e2e_s, h2d, d2h
 
 
 def _work_counters(plan) -> int:
