@@ -19,7 +19,7 @@ GBGPU_ECUDA = -5
 GBGPU_ETIMEDOUT = -110
 GBGPU_ERANGE = -34
 
-FORM_AUTO, FORM_PLAIN, FORM_TENSOR = 0, 1, 2
+FORM_AUTO, FORM_PLAIN, FORM_TENSOR, FORM_BLOCKED_PLAIN = 0, 1, 2, 3
 
 _PI64 = C.POINTER(C.c_int64)
 _PI32 = C.POINTER(C.c_int32)

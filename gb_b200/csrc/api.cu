@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/gbgpu.h"
+#include "blocked.h"
 #include "common.cuh"
 #include "internal.h"
 #include "kernels.h"
@@ -117,6 +118,8 @@ struct Plan {
     bool own_stream = false;
     int mode = 0;  // 0: linear_algebra, 1: interreduction
     int form = GBGPU_FORM_PLAIN;
+    int requested_form = GBGPU_FORM_AUTO;
+    bool blocked = false;  // blocked (dense block) algorithm instead of sparse rows
     int check = 1;
     int32_t p = 0, nr = 0, ncl = 0, ncr = 0, nc = 0, n_work = 0;
     int64_t nnz = 0;
@@ -208,7 +211,7 @@ static int plan_setup(Plan* P, const gbgpu_options* opt) {
     P->device = o.device;
     int rc = device_init(P->device, &P->dev);
     if (rc) return rc;
-    P->form = o.form == GBGPU_FORM_AUTO ? GBGPU_FORM_PLAIN : o.form;
+    P->requested_form = o.form;
     P->check = 1;  // the contract check is cheap and guards every later index
     if (o.stream) {
         P->stream = (cudaStream_t)o.stream;
@@ -236,13 +239,35 @@ static int plan_alloc(Plan* P) {
     A(work_count, 2);
     const int32_t width = P->mode == 0 ? P->ncr : P->nc;
     P->ld = ((int64_t)width + 3) & ~(int64_t)3;
-    A(D, (size_t)P->n_work * P->ld);
-    A(lead, P->n_work);
-    if (P->mode == 0) {
-        A(R, (size_t)P->n_work * P->ld);
-        A(claim, P->ncr);
-        A(cand, P->n_work);
-        A(losers, P->n_work);
+    // algorithm: the blocked form runs its dense steps as exact modular GEMMs
+    // (int8 tensor cores for odd p); AUTO picks it for matrices large enough
+    // to feed them, the sparse-row form for the small ones
+    const bool odd = (P->p & 1) && P->p >= 3;
+    if (P->mode == 1) {
+        P->blocked = false;
+        P->form = GBGPU_FORM_PLAIN;
+    } else if (P->requested_form == GBGPU_FORM_PLAIN) {
+        P->blocked = false;
+        P->form = GBGPU_FORM_PLAIN;
+    } else if (P->requested_form == GBGPU_FORM_TENSOR) {
+        P->blocked = true;
+        P->form = odd ? GBGPU_FORM_TENSOR : GBGPU_FORM_PLAIN;
+    } else if (P->requested_form == GBGPU_FORM_BLOCKED_PLAIN) {
+        P->blocked = true;
+        P->form = GBGPU_FORM_PLAIN;
+    } else {
+        P->blocked = odd && P->n_work >= 128 && P->ncr >= 128;
+        P->form = P->blocked ? GBGPU_FORM_TENSOR : GBGPU_FORM_PLAIN;
+    }
+    if (!P->blocked) {
+        A(D, (size_t)P->n_work * P->ld);
+        A(lead, P->n_work);
+        if (P->mode == 0) {
+            A(R, (size_t)P->n_work * P->ld);
+            A(claim, P->ncr);
+            A(cand, P->n_work);
+            A(losers, P->n_work);
+        }
     }
     A(piv_of_col, width);
     A(pflag, width);
@@ -259,7 +284,7 @@ static int plan_alloc(Plan* P) {
         // two CTAs per SM when two accumulators fit
         if ((int64_t)P->nc * 4 * 2 <= P->dev.smem_optin - 4096)
             P->grid_sparse = std::max(1, std::min<int>(P->n_work, P->dev.sms * 2));
-    } else {
+    } else if (!P->blocked) {
         A(gacc, (size_t)P->grid_sparse * (((size_t)P->nc + 31) & ~(size_t)31));
     }
     // cub temporaries: selection over rows, scans over columns
@@ -275,7 +300,7 @@ static int plan_alloc(Plan* P) {
 }
 
 template <class F>
-static int run_plain(Plan* P, const F& f) {
+static int run_form(Plan* P, const F& f) {
     cudaStream_t s = P->stream;
     long long& launches = P->launches;
     const int T = 256;
@@ -324,6 +349,48 @@ static int run_plain(Plan* P, const F& f) {
     }
     GB_CUDA(cudaEventRecord(P->ev[1], s));
 
+    const uint32_t* final_rows = P->D;
+    int64_t rows_ld = P->ld;
+    BlockedOutput bo{};
+    if (P->blocked) {
+        BlockedInput bi{};
+        bi.p = (uint32_t)P->p;
+        bi.ncl = P->ncl;
+        bi.ncr = P->ncr;
+        bi.n_work = P->n_work;
+        bi.work = P->work;
+        bi.row_ptr = P->row_ptr;
+        bi.cols = P->cols;
+        bi.vals = P->vals;
+        bi.piv_row = P->piv_row;
+        bi.stream = s;
+        bi.form = P->form;
+        bi.err = P->counters + 6;
+        bo.piv_of_col = P->piv_of_col;
+        bo.ms_event_schur = P->ev[2];
+        bo.ms_event_echelon = P->ev[3];
+        const int rc = blocked_reduce(bi, &bo, &launches);
+        if (rc) {
+            blocked_release(&bo, s);
+            return rc;
+        }
+        final_rows = bo.rows;
+        rows_ld = bo.ld;
+        P->np = (int32_t)bo.rank;
+        P->stats.dense_rows = bo.dense_rows;
+        P->stats.echelon_rounds = bo.echelon_rounds;
+        GB_CUDA(cudaEventRecord(P->ev[4], s));
+        if (P->np > 0) {
+            GB_LAUNCH(k_pivot_flags<<<grid_for(P->ncr, T), T, 0, s>>>(P->ncr, P->piv_of_col, 1,
+                                                                       P->pflag));
+            size_t bytes = P->cub_bytes;
+            GB_CUDA(cub::DeviceScan::ExclusiveSum(P->cub_tmp, bytes, P->pflag, P->ppos, P->ncr, s));
+            ++launches;
+            GB_LAUNCH(k_pivot_list<<<grid_for(P->ncr, T), T, 0, s>>>(P->ncr, P->pflag, P->ppos, 1,
+                                                                      P->pivcol));
+        }
+    } else {
+
     // ---- known-pivot reduction ----------------------------------------
     SparseReduceArgs sa{};
     sa.row_ptr = P->row_ptr;
@@ -348,7 +415,6 @@ static int run_plain(Plan* P, const F& f) {
         GB_CALL(launch_reduce_sparse(sa, f, P->grid_sparse, P->smem_sparse, P->nc * 4, s));
     GB_CUDA(cudaEventRecord(P->ev[2], s));
 
-    const uint32_t* final_rows = P->D;
     if (P->mode == 0) {
         // ---- echelon rounds on the dense right block ------------------------
         GB_LAUNCH(k_fill_i32<<<grid_for(P->ncr, T), T, 0, s>>>(P->piv_of_col, P->ncr, -1));
@@ -449,13 +515,14 @@ static int run_plain(Plan* P, const F& f) {
         GB_CUDA(cudaEventRecord(P->ev[3], s));
         GB_CUDA(cudaEventRecord(P->ev[4], s));
     }
+    }  // sparse-row form
 
     // ---- compaction -----------------------------------------------------------
     const int32_t shift = P->mode == 0 ? P->ncl : 0;
     P->onnz = 0;
     if (P->np > 0) {
         GB_LAUNCH(k_row_nnz<<<grid_for((int64_t)P->np * 32, T), T, 0, s>>>(
-            P->np, P->pivcol, P->piv_of_col, final_rows, P->ld, width, P->counts));
+            P->np, P->pivcol, P->piv_of_col, final_rows, rows_ld, width, P->counts));
         GB_CUDA(cudaMemsetAsync(P->counts + P->np, 0, sizeof(int64_t), s));
         size_t bytes = P->cub_bytes;
         GB_CUDA(cub::DeviceScan::ExclusiveSum(P->cub_tmp, bytes, P->counts, P->offs, P->np + 1, s));
@@ -469,10 +536,20 @@ static int run_plain(Plan* P, const F& f) {
             P->out_cap = P->onnz;
         }
         GB_LAUNCH(k_row_write<<<grid_for((int64_t)P->np * 32, T), T, 0, s>>>(
-            P->np, P->pivcol, P->piv_of_col, final_rows, P->ld, width, P->offs, shift,
+            P->np, P->pivcol, P->piv_of_col, final_rows, rows_ld, width, P->offs, shift,
             P->out_cols, P->out_vals));
     }
     GB_CUDA(cudaEventRecord(P->ev[5], s));
+    if (P->blocked) {
+        blocked_release(&bo, s);
+        int32_t tc_status = 0;
+        GB_CUDA(cudaMemcpyAsync(&tc_status, P->counters + 6, 4, cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+        if (tc_status) {
+            set_error("tensor-core kernel: a bounded wait expired");
+            return tc_status;
+        }
+    }
     return GBGPU_OK;
 }
 
@@ -480,9 +557,9 @@ int plan_run(Plan* P) {
     P->launches = 0;
     int rc;
     if ((uint32_t)P->p < 65536u)
-        rc = run_plain(P, FieldSmall::make((uint32_t)P->p));
+        rc = run_form(P, FieldSmall::make((uint32_t)P->p));
     else
-        rc = run_plain(P, FieldMont::make((uint32_t)P->p));
+        rc = run_form(P, FieldMont::make((uint32_t)P->p));
     count_launch(P->launches);
     if (rc) return rc;
     GB_CUDA(cudaEventSynchronize(P->ev[5]));

@@ -134,6 +134,7 @@ typedef struct gbgpu_rows {
 #define GBGPU_FORM_AUTO 0
 #define GBGPU_FORM_PLAIN 1  /* sparse rows on CUDA cores                */
 #define GBGPU_FORM_TENSOR 2 /* blocked, int8 tensor-core modular GEMMs  */
+#define GBGPU_FORM_BLOCKED_PLAIN 3 /* blocked, CUDA-core modular GEMMs    */
 
 typedef struct gbgpu_options {
     int32_t form;       /* GBGPU_FORM_*                                  */

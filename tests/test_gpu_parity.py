@@ -14,7 +14,7 @@ from tests.helpers import all_captures, as_rows, f4_cases
 pytestmark = pytest.mark.gpu
 
 CAPTURES = all_captures()
-FORMS = [_lib.FORM_PLAIN]
+FORMS = [_lib.FORM_PLAIN, _lib.FORM_TENSOR, _lib.FORM_BLOCKED_PLAIN]
 
 
 def check_same(got: ReducedRows, want: ReducedRows):
@@ -56,34 +56,45 @@ def test_gpu_wide_matrix_global_accumulators():
     # nc and ncr beyond the shared-memory accumulator: global scratch path
     m = synth.random_macaulay(400, 40, 60000, 65521, density=0.0015, seed=11, dup_rows=3)
     want, _ = oracle.oracle_la(m)
-    check_same(la.linear_algebra(m), want)
+    for form in FORMS:
+        check_same(la.linear_algebra(m, form=form), want)
     m = synth.random_macaulay(300, 30, 70000, 2147483647, density=0.001, seed=12)
     want, _ = oracle.oracle_la(m)
-    check_same(la.linear_algebra(m), want)
+    for form in FORMS:
+        check_same(la.linear_algebra(m, form=form), want)
+
+
+@pytest.mark.parametrize("p", [251, 65521, 1000003, 2147483647])
+def test_gpu_blocked_many_rounds(p):
+    # many C|D rows on few leads with a rank-deficient right block: several
+    # claiming rounds and pivot blocks that span more than one 128-block
+    m = synth.random_macaulay(300, 700, 400, p, density=0.05, seed=21, dup_rows=40)
+    want, _ = oracle.oracle_la(m)
+    for form in FORMS:
+        check_same(la.linear_algebra(m, form=form), want)
 
 
 def test_gpu_edge_cases():
-    # no rows to reduce
-    m = synth.random_macaulay(20, 0, 10, 101, seed=1)
-    want, _ = oracle.oracle_la(m)
-    assert want.np == 0
-    check_same(la.linear_algebra(m), want)
-    # every lower row is a copy of a known pivot: everything reduces to zero
-    m = synth.random_macaulay(20, 12, 10, 32003, seed=2, dup_rows=12)
-    got = la.linear_algebra(m)
-    assert got.np == 0
-    # empty right block
-    m = synth.random_macaulay(15, 10, 0, 65521, seed=3, density=0.3)
-    got = la.linear_algebra(m)
-    assert got.np == 0
-    # one right column
-    m = synth.random_macaulay(15, 10, 1, 65521, seed=4, density=0.3)
-    want, _ = oracle.oracle_la(m)
-    check_same(la.linear_algebra(m), want)
-    # many rows colliding on few leads, rank-deficient right block
-    m = synth.random_macaulay(3, 80, 20, 7, seed=5, density=0.5)
-    want, _ = oracle.oracle_la(m)
-    check_same(la.linear_algebra(m), want)
+    for form in FORMS:
+        # no rows to reduce
+        m = synth.random_macaulay(20, 0, 10, 101, seed=1)
+        want, _ = oracle.oracle_la(m)
+        assert want.np == 0
+        check_same(la.linear_algebra(m, form=form), want)
+        # every lower row is a copy of a known pivot: everything reduces to zero
+        m = synth.random_macaulay(20, 12, 10, 32003, seed=2, dup_rows=12)
+        assert la.linear_algebra(m, form=form).np == 0
+        # empty right block
+        m = synth.random_macaulay(15, 10, 0, 65521, seed=3, density=0.3)
+        assert la.linear_algebra(m, form=form).np == 0
+        # one right column
+        m = synth.random_macaulay(15, 10, 1, 65521, seed=4, density=0.3)
+        want, _ = oracle.oracle_la(m)
+        check_same(la.linear_algebra(m, form=form), want)
+        # many rows colliding on few leads, rank-deficient right block
+        m = synth.random_macaulay(3, 80, 20, 7, seed=5, density=0.5)
+        want, _ = oracle.oracle_la(m)
+        check_same(la.linear_algebra(m, form=form), want)
 
 
 def _expect_einval(m):
