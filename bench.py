@@ -191,9 +191,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
+    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense"],
+                    help="staircase: the metric's workload; dense: exact modular GEMM "
+                         "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form)")
+    ap.add_argument("--n", type=int, default=16384, help="dense workload size")
+    ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload == "dense":
+        run_dense(args)
         return
 
     import torch
@@ -302,6 +310,56 @@ def _e2e(lib, mat, args, device):
     e2e_s = (time.perf_counter() - t0) / steps
     h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
     return e2e_s, h2d, d2h
+
+
+def run_dense(args):
+    """Exact modular GEMM D <- (D - A B) mod p on n x n blocks with uniform
+    residues (the dense block workload): int8 tensor-core form and, for n <=
+    8192, the CUDA-core form.  Device-resident operands, CUDA events on the
+    default stream, median of the timed steps."""
+    import torch
+    from gb_b200 import _lib
+    lib = _lib.load()
+    n, p = args.n, args.p
+    L = 1 if p < 1 << 8 else 2 if p < 1 << 16 else 3 if p < 1 << 24 else 4
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    mk = lambda: torch.randint(0, p, (n, n), device="cuda", dtype=torch.int64,
+                               generator=g).to(torch.int32)
+    A, B, D = mk(), mk(), mk()
+
+    def timed(form, steps):
+        opt = _lib.Options(form, 0, 1, 0, None)
+        for _ in range(max(args.warmup, 1)):
+            _lib.check(lib.gbgpu_dense_submul(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n,
+                                              D.data_ptr(), n, C.byref(opt)))
+        ts = []
+        for _ in range(steps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            _lib.check(lib.gbgpu_dense_submul(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n,
+                                              D.data_ptr(), n, C.byref(opt)))
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e))
+        return statistics.median(ts)
+
+    ms_t = timed(_lib.FORM_TENSOR, args.steps)
+    ops = 2.0 * n ** 3
+    int8_peak = 3040.7  # TOPS, torch._int_mm 8192^3 on this pool (DESIGN.md)
+    line = {"metric": "exact modular GEMM throughput (D - A B mod p)", "value": ops / ms_t / 1e9,
+            "unit": "modular TOPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"u32 residues, {L} u8 limbs", "data": "synthetic",
+            "config": {"workload": f"dense GEMM n={n} p={p}", "limbs": L},
+            "roofline": {"bound": "tensor", "achieved": L * L * ops / ms_t / 1e9,
+                         "peak": int8_peak, "unit": "TOPS",
+                         "frac": L * L * ops / ms_t / 1e9 / int8_peak}}
+    if n <= 8192:
+        ms_p = timed(_lib.FORM_PLAIN, 1)
+        line["plain_ms"] = ms_p
+        line["tensor_speedup_vs_plain"] = ms_p / ms_t
+    print(json.dumps(line), flush=True)
 
 
 def _work_counters(plan) -> int:
