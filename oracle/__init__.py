@@ -24,6 +24,8 @@ from gb_b200.matrix import MacaulayMatrix, ReducedRows
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgbref.so")
+# gb compiled with the integration recipe of INTEGRATION.md (linked to libgbgpu.so)
+GB_GPU_SO = os.path.join(HERE, "_ref", "libgb_gpu.so")
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
@@ -176,6 +178,53 @@ def ref_layout() -> np.ndarray:
     return out[:n]
 
 
+def _f4_binding(lib):
+    lib.f4_julia.restype = C.c_int64
+    lib.f4_julia.argtypes = [_PI32, C.POINTER(_PI32), C.POINTER(_PI32), C.POINTER(C.c_void_p),
+                             _i32p, _i32p, _i32p] + [C.c_int32] * 12
+    lib.free_julia_data.argtypes = [C.POINTER(_PI32), C.POINTER(_PI32),
+                                    C.POINTER(C.c_void_p), C.c_int64, C.c_int64]
+    return lib
+
+
+def _run_f4(lib, case: dict):
+    bld = C.c_int32()
+    blen, bexp = _PI32(), _PI32()
+    bcf = C.c_void_p()
+    lens = np.ascontiguousarray(case["lens"], dtype=np.int32)
+    exps = np.ascontiguousarray(case["exps"], dtype=np.int32)
+    cfs = np.ascontiguousarray(case["cfs"], dtype=np.int32)
+    lib.f4_julia(C.byref(bld), C.byref(blen), C.byref(bexp), C.byref(bcf), lens, exps, cfs,
+                 case["field_char"], case["mon_order"], case["nr_vars"], case["nr_gens"],
+                 case["ht_size"], case["nr_threads"], case["max_nr_pairs"],
+                 case["reset_hash_table"], case["la_option"], case["reduce_gb"], 0, 0)
+    n = bld.value
+    lens_out = np.ctypeslib.as_array(blen, shape=(n,)).copy()
+    nterms = int(lens_out.sum())
+    cf_ptr = C.cast(bcf, _PI32)
+    cfs_out = np.ctypeslib.as_array(cf_ptr, shape=(max(nterms, 1),))[:nterms].copy()
+    exps_out = np.ctypeslib.as_array(bexp, shape=(max(nterms * case["nr_vars"], 1),))[
+        : nterms * case["nr_vars"]].copy()
+    lib.free_julia_data(C.byref(blen), C.byref(bexp), C.byref(bcf), n, case["field_char"])
+    return lens_out, cfs_out, exps_out
+
+
+_gb_gpu = None
+
+
+def gb_gpu_available() -> bool:
+    return os.path.exists(GB_GPU_SO)
+
+
+def gb_gpu_f4(case: dict):
+    """F4 of gb compiled with the INTEGRATION.md recipe: every linear-algebra
+    call goes to libgbgpu.so.  Returns (lens, cfs, exps) of the basis."""
+    global _gb_gpu
+    if _gb_gpu is None:
+        _gb_gpu = _f4_binding(C.CDLL(GB_GPU_SO))
+    return _run_f4(_gb_gpu, case)
+
+
 def ref_f4(case: dict, la_fn=None, ir_fn=None, capture_dir: Optional[str] = None):
     """Run the reference's F4 (f4_julia, src/f4.c:190) on a golden case.
 
@@ -186,26 +235,8 @@ def ref_f4(case: dict, la_fn=None, ir_fn=None, capture_dir: Optional[str] = None
     lib = _load_ref()
     lib.gbref_set_la(la_fn, ir_fn)
     lib.gbref_set_capture(capture_dir.encode() if capture_dir else None)
-    bld = C.c_int32()
-    blen, bexp = _PI32(), _PI32()
-    bcf = C.c_void_p()
-    lens = np.ascontiguousarray(case["lens"], dtype=np.int32)
-    exps = np.ascontiguousarray(case["exps"], dtype=np.int32)
-    cfs = np.ascontiguousarray(case["cfs"], dtype=np.int32)
     try:
-        lib.f4_julia(C.byref(bld), C.byref(blen), C.byref(bexp), C.byref(bcf), lens, exps, cfs,
-                     case["field_char"], case["mon_order"], case["nr_vars"], case["nr_gens"],
-                     case["ht_size"], case["nr_threads"], case["max_nr_pairs"],
-                     case["reset_hash_table"], case["la_option"], case["reduce_gb"], 0, 0)
+        return _run_f4(lib, case)
     finally:
         lib.gbref_set_la(None, None)
         lib.gbref_set_capture(None)
-    n = bld.value
-    lens_out = np.ctypeslib.as_array(blen, shape=(n,)).copy()
-    nterms = int(lens_out.sum())
-    cf_ptr = C.cast(bcf, _PI32)
-    cfs_out = np.ctypeslib.as_array(cf_ptr, shape=(max(nterms, 1),))[:nterms].copy()
-    exps_out = np.ctypeslib.as_array(bexp, shape=(max(nterms * case["nr_vars"], 1),))[
-        : nterms * case["nr_vars"]].copy()
-    lib.free_julia_data(C.byref(blen), C.byref(bexp), C.byref(bcf), n, case["field_char"])
-    return lens_out, cfs_out, exps_out

@@ -101,3 +101,14 @@ def test_dense_lowrank_rank():
                 A[i] = (A[i] - A[i, c] * A[r]) % 101
         r += 1
     assert r == 5
+
+
+@pytest.mark.skipif(not oracle.gb_gpu_available(), reason="integration build absent")
+def test_integration_recipe_build_links_to_library():
+    """The INTEGRATION.md recipe reroutes only the two call sites: the gb build
+    exports f4_julia and imports exactly the two GPU entry points."""
+    out = subprocess.run(["nm", "-D", oracle.GB_GPU_SO], capture_output=True, text=True,
+                         check=True).stdout
+    undefined = set(re.findall(r" U (gbgpu_\w+)", out))
+    assert undefined == {"gbgpu_linear_algebra", "gbgpu_interreduce_matrix_rows"}
+    assert re.search(r" T f4_julia\b", out)
