@@ -65,6 +65,7 @@ EXPORTS = [
     "gbgpu_rows_free", "gbgpu_plan_create", "gbgpu_plan_run", "gbgpu_plan_result",
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
+    "gbgpu_dense_submul_noalloc",
 ]
 
 _lib = None
@@ -97,6 +98,9 @@ def load(path: str = LIB_PATH):
                                C.c_int64, C.POINTER(Options)]
     lib.gbgpu_dense_submul.argtypes = dense
     lib.gbgpu_dense_submul_host.argtypes = dense
+    lib.gbgpu_dense_submul_noalloc.argtypes = [C.c_int32] * 4 + [
+        C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
+        C.c_void_p]
     lib.gbgpu_last_error.restype = C.c_char_p
     lib.gbgpu_kernel_launches.restype = C.c_int64
     _lib = lib
