@@ -36,6 +36,7 @@ sys.path.insert(0, REPO)
 CONFIG = {"nru": 20000, "nrl": 5000, "ncr": 20000, "p": 65521, "dmin": 0.02, "dmax": 0.05,
           "seed": 1}
 METRIC = "GF(p) matrix reductions/s (20000x5000 A|B/C|D, 40000 cols, p=65521, bit-exact)"
+INT8_PEAK_TOPS = 3040.7  # torch._int_mm 8192^3 int8, best of 10, measured on this pool
 UNIT = "matrices/s"
 
 
@@ -196,6 +197,8 @@ def main():
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form)")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
+    ap.add_argument("--verify", type=int, default=1,
+                    help="1: check the timed form's answer against the sparse-row form")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -242,32 +245,60 @@ def main():
     answer = plan.result()
     work_sparse = _work_counters(plan)
     plan.close()
+    verified = None
+    if args.verify and stats["form_used"] != _lib.FORM_PLAIN:
+        # the answer of the timed form against the sparse-row form, full size
+        ref_plan = la.Plan(mat, form=_lib.FORM_PLAIN, device=local)
+        ref_plan.run()
+        verified = bool(ref_plan.result().equals(answer))
+        ref_plan.close()
 
     # ---- end to end through gbgpu_reduce with pinned host buffers ---------
     e2e_s, h2d, d2h = _e2e(lib, mat, args, local) if not args.no_e2e else (float("nan"), 0, 0)
 
     value = ws * 1000.0 / ms
     sch = float(np.mean(schur_ms))
-    alg = algorithmic_bytes_schur(mat, work_sparse, mat.ncr)
-    peaks = _peaks()
-    achieved = alg / (sch * 1e-3) / 1e9
+    form_used = stats["form_used"]
+    if form_used == _lib.FORM_PLAIN:
+        # dominant kernel: the sparse known-pivot reduction (HBM / L2 bound)
+        alg = algorithmic_bytes_schur(mat, work_sparse, mat.ncr)
+        peak, peak_src = _peaks()
+        achieved = alg / (sch * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_reduce_sparse", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": None, "alg_bytes_per_launch": alg, "launch_ms": sch}
+    else:
+        # dominant kernel: the tensor-core modular GEMM; one extra instrumented
+        # run times every launch with CUDA events on the library's stream
+        prof = la.Plan(mat, form=args.form, device=local, profile=True)
+        prof.run()
+        pst = prof.stats()
+        prof.close()
+        tops = pst["gemm_int8_ops"] / (pst["gemm_ms"] * 1e-3) / 1e12 if pst["gemm_ms"] else 0.0
+        roof = {"bound": "tensor", "kernel": "k_tc_submul", "achieved": tops,
+                "peak": INT8_PEAK_TOPS, "unit": "TOPS (int8)", "frac": tops / INT8_PEAK_TOPS,
+                "peak_source": "measured: torch._int_mm 8192^3 int8 on this pool (no int8 "
+                               "figure in MEASURED_PEAKS.json)",
+                "traffic": None, "launches": pst["gemm_launches"],
+                "ms_all_launches": pst["gemm_ms"], "int8_ops_all_launches": pst["gemm_int8_ops"],
+                "avg_launch_ms": pst["gemm_ms"] / max(pst["gemm_launches"], 1)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (mod p, exact)",
         "data": "synthetic (seeded, gb_b200.synth.staircase)",
-        "config": {"workload": workload_name(), "form": "plain" if args.form in (0, 1) else "tensor",
+        "config": {"workload": workload_name(),
+                   "form": {1: "plain", 2: "tensor", 3: "blocked-plain"}.get(form_used, "?"),
                    "l2": "inputs (CSR ~230 MB) larger than L2; no flush needed",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "e2e": {"value": ws / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "k_reduce_sparse", "achieved": achieved,
-                     "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
-                     "peak_source": peaks[1], "traffic": None,
-                     "alg_bytes_per_launch": alg, "launch_ms": sch},
+        "roofline": roof,
         "stages_ms": {k: stats[k] for k in ("ms_schur", "ms_echelon", "ms_rref", "ms_compact")},
+        "echelon_steps": stats["echelon_rounds"],
         "rank": answer.np, "out_nnz": answer.nnz, "wall_s_timed": wall,
+        "verified_against_plain_form": verified,
     }
     line["clocks"] = clk.summary()
     if args.scale != 1.0:
@@ -346,7 +377,7 @@ def run_dense(args):
 
     ms_t = timed(_lib.FORM_TENSOR, args.steps)
     ops = 2.0 * n ** 3
-    int8_peak = 3040.7  # TOPS, torch._int_mm 8192^3 on this pool
+    int8_peak = INT8_PEAK_TOPS
     line = {"metric": "exact modular GEMM throughput (D - A B mod p)", "value": ops / ms_t / 1e9,
             "unit": "modular TOPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_t, "higher_is_better": True, "scaling": "weak",

@@ -38,7 +38,7 @@ class Rows(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("form", C.c_int32), ("device", C.c_int32), ("check", C.c_int32),
-                ("reserved", C.c_int32), ("stream", C.c_void_p)]
+                ("profile", C.c_int32), ("stream", C.c_void_p)]
 
 
 class Stats(C.Structure):
@@ -46,7 +46,9 @@ class Stats(C.Structure):
                 ("ms_rref", C.c_double), ("ms_compact", C.c_double),
                 ("rows_reduced", C.c_int64), ("dense_rows", C.c_int64), ("rank", C.c_int64),
                 ("echelon_rounds", C.c_int64), ("kernel_launches", C.c_int64),
-                ("work_schur", C.c_int64), ("work_dense", C.c_int64)]
+                ("work_schur", C.c_int64), ("work_dense", C.c_int64),
+                ("gemm_launches", C.c_int64), ("gemm_ms", C.c_double),
+                ("gemm_int8_ops", C.c_double), ("form_used", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

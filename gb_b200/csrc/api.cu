@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "kernels.h"
+#include "tc_gemm.h"
 
 namespace gbgpu {
 
@@ -119,6 +120,8 @@ struct Plan {
     int mode = 0;  // 0: linear_algebra, 1: interreduction
     int form = GBGPU_FORM_PLAIN;
     int requested_form = GBGPU_FORM_AUTO;
+    int profile = 0;
+    unsigned long long* gemm_steps = nullptr;
     bool blocked = false;  // blocked (dense block) algorithm instead of sparse rows
     int check = 1;
     int32_t p = 0, nr = 0, ncl = 0, ncr = 0, nc = 0, n_work = 0;
@@ -212,6 +215,7 @@ static int plan_setup(Plan* P, const gbgpu_options* opt) {
     int rc = device_init(P->device, &P->dev);
     if (rc) return rc;
     P->requested_form = o.form;
+    P->profile = o.profile;
     P->check = 1;  // the contract check is cheap and guards every later index
     if (o.stream) {
         P->stream = (cudaStream_t)o.stream;
@@ -237,6 +241,7 @@ static int plan_alloc(Plan* P) {
     A(err, 1);
     A(counters, 8);
     A(work_count, 2);
+    A(gemm_steps, 1);
     const int32_t width = P->mode == 0 ? P->ncr : P->nc;
     P->ld = ((int64_t)width + 3) & ~(int64_t)3;
     // algorithm: the blocked form runs its dense steps as exact modular GEMMs
@@ -556,11 +561,35 @@ static int run_form(Plan* P, const F& f) {
 int plan_run(Plan* P) {
     P->launches = 0;
     int rc;
+    GemmProfile prof;
+    if (P->profile) {
+        prof.d_steps = P->gemm_steps;
+        GB_CUDA(cudaMemsetAsync(P->gemm_steps, 0, sizeof(unsigned long long), P->stream));
+        set_gemm_profile(&prof);
+    }
     if ((uint32_t)P->p < 65536u)
         rc = run_form(P, FieldSmall::make((uint32_t)P->p));
     else
         rc = run_form(P, FieldMont::make((uint32_t)P->p));
+    set_gemm_profile(nullptr);
     count_launch(P->launches);
+    P->stats.gemm_launches = (int64_t)prof.events.size();
+    P->stats.gemm_ms = 0;
+    P->stats.gemm_int8_ops = 0;
+    if (P->profile && !prof.events.empty()) {
+        unsigned long long steps = 0;
+        GB_CUDA(cudaMemcpyAsync(&steps, P->gemm_steps, sizeof(steps), cudaMemcpyDeviceToHost,
+                                P->stream));
+        GB_CUDA(cudaStreamSynchronize(P->stream));
+        for (auto& e : prof.events) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e.first, e.second);
+            P->stats.gemm_ms += ms;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        P->stats.gemm_int8_ops = 2.0 * (double)steps * prof.macs_per_step.front();
+    }
     if (rc) return rc;
     GB_CUDA(cudaEventSynchronize(P->ev[5]));
     int64_t wc[2] = {0, 0};
@@ -582,6 +611,9 @@ int plan_run(Plan* P) {
     P->stats.rows_reduced = P->n_work;
     P->stats.rank = P->np;
     P->stats.kernel_launches = P->launches;
+    P->stats.form_used = !P->blocked ? GBGPU_FORM_PLAIN
+                         : (P->form == GBGPU_FORM_TENSOR ? GBGPU_FORM_TENSOR
+                                                         : GBGPU_FORM_BLOCKED_PLAIN);
     return GBGPU_OK;
 }
 

@@ -8,17 +8,21 @@
 // a dense block operation on residue matrices, and every O(n^3) step is the
 // exact modular GEMM of tc_gemm.cu (int8 tensor cores):
 //
-//   1. Schur complement, right-looking over 128-column blocks k of A:
-//        X_k  = W[:, k] A_kk^-1                  (GEMM with a precomputed
-//                                                  block inverse)
-//        W[:, >k] -= X_k P_k[:, >k]              (GEMM)
-//      where W = [C | D] holds the C|D rows (sorted by lead, so only a prefix
-//      of rows is active for block k) and P = [A | B] the known pivots.
-//   2. Echelon of D' by claiming rounds: the first row of every lead column
-//      becomes a normalised pivot; the other rows are reduced by the round's
-//      new pivots with the same block elimination (gathered pivot columns),
-//      which leaves them zero at every pivot column, and the nonzero ones
-//      claim again.
+//   1. Schur complement.  W = [C | D] holds the C|D rows sorted by lead (so
+//      only a prefix of rows is active for a block of A), P = [A | B] the known
+//      pivots.  (a) X = C A^-1, right-looking over 128-column blocks k of A:
+//        X_k = W[:, k] A_kk^-1                   (GEMM, precomputed block inverse)
+//        W[:, k+1 .. e_k] -= X_k A[k, k+1 .. e_k] (GEMM; e_k = last left column the
+//                                                  pivots of block k touch)
+//      with X_k stored over W[:, k]; (b) D' = D - X B as one GEMM whose zero
+//      tiles (staircase X, banded B) are skipped.
+//   2. Echelon of D' over 128-column panels, left to right: the pending rows
+//      whose lead lies in the panel (128 at a time) are brought to echelon form
+//      inside the panel in shared memory (k_panel_factor), the recorded row
+//      transformation is applied to their trailing columns with one GEMM, the
+//      pivots found are registered, and the panel's other pending rows are
+//      eliminated against them (eliminate: gathered pivot columns, block
+//      inverses, GEMMs).
 //   3. Back substitution to reduced echelon form, blocks of 128 pivots from
 //      the last to the first: U_k -= U_k[:, piv(>k)] R_(>k) (GEMM against the
 //      already reduced later rows), then U_k = (U_k[:, piv(k)])^-1 U_k.
@@ -36,6 +40,7 @@
 
 #include "../../include/gbgpu.h"
 #include "blocked.h"
+#include "common.cuh"
 #include "field.cuh"
 #include "internal.h"
 #include "kernels.h"
@@ -79,6 +84,25 @@ __global__ void k_densify_pivots(int32_t ncl, const int32_t* __restrict__ piv_ro
         const int32_t r = piv_row[c];
         uint32_t* o = out + (size_t)c * ld;
         for (int64_t k = row_ptr[r] + lane; k < row_ptr[r + 1]; k += 32) o[cols[k]] = vals[k];
+    }
+}
+
+// span[b] = largest column < limit of the known pivots of rows [128 b, 128 b + 128)
+__global__ void k_block_span(int32_t ncl, const int32_t* __restrict__ piv_row,
+                             const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
+                             int32_t limit, int32_t* span) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = warp; c < ncl; c += nwarps) {
+        const int32_t r = piv_row[c];
+        int32_t mx = -1;
+        for (int64_t k = row_ptr[r] + lane; k < row_ptr[r + 1]; k += 32) {
+            const int32_t col = cols[k];
+            if (col < limit && col > mx) mx = col;
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0 && mx >= 0) atomicMax(&span[c / 128], mx);
     }
 }
 
@@ -212,65 +236,115 @@ __global__ void k_row_leads(int32_t rows, const int32_t* __restrict__ list, int3
     }
 }
 
-// scale each listed row by the inverse of its lead entry (warp per row)
-template <class F>
-__global__ void k_normalize_rows(int32_t n, const int32_t* __restrict__ list,
-                                 const int32_t* __restrict__ lead, int32_t ncols, uint32_t* M,
-                                 int64_t ld, F f) {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < n; i += nwarps) {
-        const int32_t r = list[i];
-        const int32_t c0 = lead[r];
-        uint32_t* row = M + (size_t)r * ld;
-        const uint32_t inv = inverse_mod(row[c0], f.p);
-        __syncwarp();
-        for (int c = c0 + 1 + lane; c < ncols; c += 32) {
-            const uint32_t v = row[c];
-            if (v) row[c] = f.mulmod(v, inv);
-        }
-        __syncwarp();
-        if (lane == 0) row[c0] = 1u;
-    }
-}
 
-// claim[lead[r]] = min r over candidate rows
-__global__ void k_claim_dense(int32_t n, const int32_t* __restrict__ cand,
-                              const int32_t* __restrict__ lead, int32_t* claim) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        atomicMin(&claim[lead[cand[i]]], cand[i]);
-}
 
-// winners -> piv_of_col and flags; losers -> list
-__global__ void k_split_claims(int32_t n, const int32_t* __restrict__ cand,
-                               const int32_t* __restrict__ lead, const int32_t* __restrict__ claim,
-                               int32_t* piv_of_col, int32_t* winner_flag, int32_t* losers,
-                               int32_t* n_losers) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int32_t r = cand[i];
-        const int32_t c = lead[r];
-        if (claim[c] == r) {
-            piv_of_col[c] = r;
-            winner_flag[c] = 1;
-        } else {
-            losers[atomicAdd(n_losers, 1)] = r;
-        }
-    }
-}
 
-// rows of `list` with lead >= 0 -> out
-__global__ void k_keep_nonzero(int32_t n, const int32_t* __restrict__ list,
-                               const int32_t* __restrict__ lead, int32_t* out, int32_t* n_out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        if (lead[list[i]] >= 0) out[atomicAdd(n_out, 1)] = list[i];
-}
 
 // columns with flag set, ascending, via a precomputed exclusive scan
 __global__ void k_compact_cols(int32_t n, const int32_t* __restrict__ flag,
                                const int32_t* __restrict__ pos, int32_t* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         if (flag[i]) out[pos[i]] = i;
+}
+
+
+// ---------------------------------------------------------------------------
+// panel echelon
+
+// pending rows (nonzero, not yet pivots) whose lead lies in [j, j + bw) -> act;
+// min lead over all pending rows -> *min_lead
+__global__ void k_collect_panel(int32_t t, const int32_t* __restrict__ lead,
+                                const uint8_t* __restrict__ is_piv, int32_t j, int32_t bw,
+                                int32_t* act, int32_t* n_act, int32_t* min_lead) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < t; r += gridDim.x * blockDim.x) {
+        const int32_t l = lead[r];
+        if (l < 0 || is_piv[r]) continue;
+        atomicMin(min_lead, l);
+        if (l >= j && l < j + bw) act[atomicAdd(n_act, 1)] = r;
+    }
+}
+
+// Row echelon of the panel (columns [0, bw) of the n <= KB rows of `old`,
+// leading dimension ldo) in shared memory, recording the transformation E
+// (E * old = rows whose panel part is in echelon form with unit pivots;
+// the rows that are not pivots become zero in the panel).  Writes -E
+// (n x n, ld KB), the panel-local index and column of every pivot, in
+// increasing column order, and their count.
+template <class F>
+__global__ void __launch_bounds__(KB)
+k_panel_factor(const uint32_t* __restrict__ old, int64_t ldo, int32_t n, int32_t bw,
+               int32_t col0, uint32_t* neg_e, int32_t* piv_pos, int32_t* piv_col,
+               int32_t* n_piv, F f) {
+    extern __shared__ uint32_t pf_smem[];
+    uint32_t(*P)[KB + 1] = (uint32_t(*)[KB + 1])pf_smem;
+    uint32_t(*E)[KB + 1] = (uint32_t(*)[KB + 1])(pf_smem + KB * (KB + 1));
+    __shared__ int s_scratch[KB / 32];
+    __shared__ uint8_t is_piv[KB];
+    __shared__ uint32_t s_inv;
+    const int r = threadIdx.x;
+    for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
+        const int i = t / KB, c = t % KB;
+        P[i][c] = (i < n && c < bw) ? old[(size_t)i * ldo + c] : 0u;
+        E[i][c] = i == c ? 1u : 0u;
+    }
+    is_piv[r] = 0;
+    __syncthreads();
+    int k = 0;
+    for (int c = 0; c < bw; ++c) {
+        const int cand = (r < n && !is_piv[r] && P[r][c] != 0u) ? r : INT_MAX;
+        const int i = block_min(cand, s_scratch);
+        if (i == INT_MAX) continue;
+        if (r == 0) {
+            s_inv = inverse_mod(P[i][c], f.p);
+            piv_pos[k] = i;
+            piv_col[k] = col0 + c;
+            is_piv[i] = 1;
+        }
+        __syncthreads();
+        const uint32_t inv = s_inv;
+        // scale the pivot row (panel part from c, transform part)
+        for (int cc = c + r; cc < bw; cc += blockDim.x) P[i][cc] = f.mulmod(P[i][cc], inv);
+        for (int cc = r; cc < n; cc += blockDim.x) E[i][cc] = f.mulmod(E[i][cc], inv);
+        __syncthreads();
+        // eliminate column c from every other non-pivot row
+        if (r < n && r != i && !is_piv[r]) {
+            const uint32_t m = P[r][c];
+            if (m != 0u) {
+                const uint32_t mp = f.prep(m);
+                for (int cc = c; cc < bw; ++cc) {
+                    const uint32_t v = P[i][cc];
+                    if (v) P[r][cc] = f.mulsub(P[r][cc], mp, v);
+                }
+                for (int cc = 0; cc < n; ++cc) {
+                    const uint32_t v = E[i][cc];
+                    if (v) E[r][cc] = f.mulsub(E[r][cc], mp, v);
+                }
+            }
+        }
+        __syncthreads();
+        ++k;
+    }
+    for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
+        const int i = t / KB, cc = t % KB;
+        const uint32_t v = (i < n && cc < n) ? E[i][cc] : 0u;
+        neg_e[t] = v ? f.p - v : 0u;
+    }
+    if (r == 0) *n_piv = k;
+}
+
+// register the chunk's pivots: pivot k is chunk row piv_pos[k] = act[...]
+__global__ void k_register_pivots(const int32_t* __restrict__ n_piv,
+                                  const int32_t* __restrict__ piv_pos,
+                                  const int32_t* __restrict__ piv_col,
+                                  const int32_t* __restrict__ act, int32_t* piv_of_col,
+                                  uint8_t* is_piv, int32_t* prow_out) {
+    const int n = *n_piv;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int32_t row = act[piv_pos[k]];
+        piv_of_col[piv_col[k]] = row;
+        is_piv[row] = 1;
+        prow_out[k] = row;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -438,105 +512,142 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         std::vector<int32_t> h_act(nbk);
         BL_CUDA(cudaMemcpyAsync(h_act.data(), act, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
+        // last left column touched by the known pivots of each 128-row block
+        int32_t* span = c.alloc<int32_t>(nbk);
+        if (!span) return GBGPU_ENOMEM;
+        BL_LAUNCH(k_fill_i32<<<grid_of(nbk), 256, 0, s>>>(span, nbk, -1));
+        BL_LAUNCH(k_block_span<<<grid_of((int64_t)ncl * 32), 256, 0, s>>>(
+            ncl, in.piv_row, in.row_ptr, in.cols, ncl, span));
+        std::vector<int32_t> h_span(nbk);
+        BL_CUDA(cudaMemcpyAsync(h_span.data(), span, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaStreamSynchronize(s));
+        // (a) X = C A^-1, in place in W[:, 0:ncl], block by block; the update of
+        //     the later left columns stops at the last column block k touches
         for (int k = 0; k < nbk; ++k) {
             const int32_t c0 = k * KB, kb = std::min(KB, ncl - c0), c1 = c0 + kb;
             const int32_t rows = h_act[k];
             if (rows <= 0) continue;
             BL_CUDA(cudaMemsetAsync(X, 0, sizeof(uint32_t) * (size_t)rows * KB, s));
-            // X = W[:, block] A_kk^-1
+            // X_k = W[:, block] A_kk^-1
             BL_CHECK(gemm(c, X, KB, W + c0, ld, Ninv + (size_t)k * KB * KB, KB, rows, kb, kb));
-            // W[:, c1:] -= X P[block rows, c1:]
-            BL_CHECK(gemm(c, W + c1, ld, X, KB, P + (size_t)c0 * ld + c1, ld, rows, nc - c1, kb));
+            BL_CUDA(cudaMemcpy2DAsync(W + c0, ld * 4, X, KB * 4, (size_t)kb * 4, rows,
+                                      cudaMemcpyDeviceToDevice, s));
+            // W[:, c1:e) -= X_k A[block rows, c1:e)
+            const int32_t e = std::min(ncl, h_span[k] + 1);
+            if (e > c1)
+                BL_CHECK(gemm(c, W + c1, ld, X, KB, P + (size_t)c0 * ld + c1, ld, rows, e - c1, kb));
         }
-        c.launches += 0;
+        // (b) D' = D - X B: one GEMM over the whole left block; the tile flags of
+        //     the GEMM skip the zero tiles of the staircase X and of B
+        BL_CHECK(gemm(c, W + ncl, ld, W, ld, P + ncl, ld, t, ncr, ncl));
     }
     if (out->ms_event_schur) BL_CUDA(cudaEventRecord(out->ms_event_schur, s));
 
-    // ---- 2. echelon of D' = W[:, ncl:] by claiming rounds ----------------------
+    // ---- 2. echelon of D' = W[:, ncl:], 128-column panels left to right ------------
+    // Pending rows whose lead falls in the panel (at most KB at a time) are
+    // brought to echelon form inside the panel by k_panel_factor; the recorded
+    // transformation is applied to their whole trailing part with one GEMM.
+    // The pivots found are registered, the other rows of the chunk are zero in
+    // the panel and move on; pending rows of the panel outside the chunk are
+    // eliminated against the new pivots (eliminate) and stay pending.
     uint32_t* Dp = W + ncl;  // t x ncr, leading dimension ld
     int32_t* lead = c.alloc<int32_t>(t);
-    int32_t* claim = c.alloc<int32_t>(ncr);
+    uint8_t* is_piv = c.alloc<uint8_t>(t);
     int32_t* piv_of_col = out->piv_of_col;  // [ncr], -1 if none
     int32_t* wflag = c.alloc<int32_t>(ncr);
     int32_t* wpos = c.alloc<int32_t>(ncr);
-    int32_t* cand = c.alloc<int32_t>(t);
-    int32_t* losers = c.alloc<int32_t>(t);
-    int32_t* counters = c.alloc<int32_t>(4);
-    int32_t* pc = c.alloc<int32_t>(ncr);      // pivot columns of the round
+    int32_t* act = c.alloc<int32_t>(t);
+    int32_t* counters = c.alloc<int32_t>(8);
+    int32_t* pc = c.alloc<int32_t>(ncr);      // pivot columns
     int32_t* prow = c.alloc<int32_t>(ncr);    // their rows
-    if (!lead || !claim || !wflag || !wpos || !cand || !losers || !counters || !pc || !prow)
+    int32_t* piv_pos = c.alloc<int32_t>(KB);
+    uint32_t* negE = c.alloc<uint32_t>((size_t)KB * KB);
+    uint32_t* Old = c.alloc<uint32_t>((size_t)KB * ld);
+    uint32_t* Out = c.alloc<uint32_t>((size_t)KB * ld);
+    if (!lead || !is_piv || !wflag || !wpos || !act || !counters || !pc || !prow || !piv_pos ||
+        !negE || !Old || !Out)
         return GBGPU_ENOMEM;
     size_t scan_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, wflag, wpos, ncr, s);
     void* scan_tmp = c.alloc<uint8_t>(scan_bytes);
     if (!scan_tmp) return GBGPU_ENOMEM;
     BL_LAUNCH(k_fill_i32<<<grid_of(ncr), 256, 0, s>>>(piv_of_col, ncr, -1));
-    int32_t n_cand = 0;
+    int32_t n_nonzero = 0;
     if (t > 0 && ncr > 0) {
+        BL_CUDA(cudaMemsetAsync(is_piv, 0, t, s));
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)t * 32), 256, 0, s>>>(t, nullptr, ncr, Dp, ld, lead));
-        BL_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int32_t), s));
-        BL_LAUNCH(k_collect_nonzero<<<grid_of(t), 256, 0, s>>>(t, lead, cand, counters));
-        BL_CUDA(cudaMemcpyAsync(&n_cand, counters, 4, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int32_t), s));
+        BL_LAUNCH(k_collect_nonzero<<<grid_of(t), 256, 0, s>>>(t, lead, act, counters));
+        BL_CUDA(cudaMemcpyAsync(&n_nonzero, counters, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
     }
-    out->dense_rows = n_cand;
-    int rounds = 0;
-    uint32_t* Ubuf = nullptr;
+    out->dense_rows = n_nonzero;
+    const int pf_bytes = 2 * KB * (KB + 1) * (int)sizeof(uint32_t);
+    BL_CUDA(cudaFuncSetAttribute(k_panel_factor<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 pf_bytes));
+    uint32_t* Ubuf = nullptr;   // gathered pivot rows / rest rows for eliminate
     size_t ubuf_rows = 0;
-    while (n_cand > 0) {
-        ++rounds;
-        BL_LAUNCH(k_fill_i32<<<grid_of(ncr), 256, 0, s>>>(claim, ncr, INT_MAX));
-        BL_CUDA(cudaMemsetAsync(wflag, 0, sizeof(int32_t) * ncr, s));
-        BL_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int32_t), s));
-        BL_LAUNCH(k_claim_dense<<<grid_of(n_cand), 256, 0, s>>>(n_cand, cand, lead, claim));
-        BL_LAUNCH(k_split_claims<<<grid_of(n_cand), 256, 0, s>>>(n_cand, cand, lead, claim,
-                                                                piv_of_col, wflag, losers,
-                                                                counters + 1));
-        // new pivots, ascending columns
-        BL_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wflag, wpos, ncr, s));
-        ++c.launches;
-        BL_LAUNCH(k_compact_cols<<<grid_of(ncr), 256, 0, s>>>(ncr, wflag, wpos, pc));
-        int32_t h[2] = {0, 0};
-        BL_CUDA(cudaMemcpyAsync(&h[1], counters + 1, 4, cudaMemcpyDeviceToHost, s));
-        int32_t last_pos = 0, last_flag = 0;
-        BL_CUDA(cudaMemcpyAsync(&last_pos, wpos + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaMemcpyAsync(&last_flag, wflag + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
+    int steps = 0;
+    int32_t j = 0;
+    while (n_nonzero > 0 && j < ncr) {
+        const int32_t bw = std::min(KB, ncr - j);
+        int32_t h[2] = {0, INT_MAX};  // n_act, min pending lead
+        BL_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(int32_t), s));
+        BL_LAUNCH(k_fill_i32<<<1, 1, 0, s>>>(counters + 2, 1, INT_MAX));
+        BL_LAUNCH(k_collect_panel<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, j, bw, act,
+                                                              counters + 1, counters + 2));
+        BL_CUDA(cudaMemcpyAsync(h, counters + 1, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
-        const int32_t n_new = last_pos + last_flag, n_lost = h[1];
-        // normalise the new pivots
-        BL_LAUNCH(k_gather_rows<<<grid_of(n_new), 256, 0, s>>>(n_new, pc, piv_of_col, prow,
-                                                               counters + 2));
-        BL_LAUNCH(k_normalize_rows<F><<<grid_of((int64_t)n_new * 32), 256, 0, s>>>(
-            n_new, prow, lead, ncr, Dp, ld, f));
-        if (n_lost == 0) break;
-        // losers -= (losers at pivot columns) (pivots at pivot columns)^-1 pivots
-        std::vector<int32_t> h_pc(n_new);
-        BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * n_new, cudaMemcpyDeviceToHost, s));
-        if ((size_t)n_new > ubuf_rows || (size_t)n_lost > ubuf_rows) {
-            ubuf_rows = std::max<size_t>(std::max(n_new, n_lost), ubuf_rows * 2);
-            Ubuf = c.alloc<uint32_t>(ubuf_rows * ld * 2);
-            if (!Ubuf) return GBGPU_ENOMEM;
+        if (h[1] == INT_MAX) break;  // nothing pending
+        if (h[0] == 0) {             // jump to the panel of the smallest pending lead
+            j = h[1] / KB * KB;
+            continue;
         }
-        uint32_t* Ucmp = Ubuf;                        // pivot rows, compact
-        uint32_t* Tcmp = Ubuf + ubuf_rows * ld;       // loser rows, compact
-        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_new * ncr), 256, 0, s>>>(
-            n_new, prow, ncr, Dp, ld, Ucmp, ld));
-        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_lost * ncr), 256, 0, s>>>(
-            n_lost, losers, ncr, Dp, ld, Tcmp, ld));
-        BL_CUDA(cudaStreamSynchronize(s));
-        BL_CHECK(eliminate(c, f, Tcmp, ld, n_lost, ncr, Ucmp, ld, n_new, pc, h_pc));
-        BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_lost * ncr), 256, 0, s>>>(
-            n_lost, losers, ncr, Tcmp, ld, Dp, ld));
-        // nonzero losers claim again
-        BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_lost * 32), 256, 0, s>>>(n_lost, losers, ncr,
-                                                                             Dp, ld, lead));
-        BL_CUDA(cudaMemsetAsync(counters + 3, 0, sizeof(int32_t), s));
-        BL_LAUNCH(k_keep_nonzero<<<grid_of(n_lost), 256, 0, s>>>(n_lost, losers, lead, cand,
-                                                                 counters + 3));
-        BL_CUDA(cudaMemcpyAsync(&n_cand, counters + 3, 4, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaStreamSynchronize(s));
+        ++steps;
+        const int32_t n_act = h[0], n_chunk = std::min(KB, n_act);
+        const int32_t width = ncr - j;
+        // E * (chunk rows from column j) with E from the panel factorization
+        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_chunk * width), 256, 0, s>>>(
+            n_chunk, act, width, Dp + j, ld, Old, ld));
+        BL_LAUNCH(k_panel_factor<F><<<1, KB, pf_bytes, s>>>(Old, ld, n_chunk, bw, j, negE, piv_pos,
+                                                             pc, counters + 3, f));
+        BL_CUDA(cudaMemsetAsync(Out, 0, sizeof(uint32_t) * (size_t)n_chunk * ld, s));
+        BL_CHECK(gemm(c, Out, ld, negE, KB, Old, ld, n_chunk, width, n_chunk));
+        BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_chunk * width), 256, 0, s>>>(
+            n_chunk, act, width, Out, ld, Dp + j, ld));
+        BL_LAUNCH(k_register_pivots<<<1, KB, 0, s>>>(counters + 3, piv_pos, pc, act, piv_of_col,
+                                                     is_piv, prow));
+        BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_chunk * 32), 256, 0, s>>>(n_chunk, act, ncr, Dp,
+                                                                              ld, lead));
+        if (n_act > n_chunk) {
+            // the rest of the panel's pending rows: eliminate against the new pivots
+            int32_t k = 0;
+            BL_CUDA(cudaMemcpyAsync(&k, counters + 3, 4, cudaMemcpyDeviceToHost, s));
+            BL_CUDA(cudaStreamSynchronize(s));
+            const int32_t n_rest = n_act - n_chunk;
+            std::vector<int32_t> h_pc(k);
+            BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s));
+            if ((size_t)std::max(k, n_rest) > ubuf_rows) {
+                ubuf_rows = std::max<size_t>(std::max(k, n_rest), ubuf_rows * 2);
+                Ubuf = c.alloc<uint32_t>(ubuf_rows * ld * 2);
+                if (!Ubuf) return GBGPU_ENOMEM;
+            }
+            uint32_t* Ucmp = Ubuf;
+            uint32_t* Tcmp = Ubuf + ubuf_rows * ld;
+            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)k * ncr), 256, 0, s>>>(
+                k, prow, ncr, Dp, ld, Ucmp, ld));
+            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
+                n_rest, act + n_chunk, ncr, Dp, ld, Tcmp, ld));
+            BL_CUDA(cudaStreamSynchronize(s));
+            BL_CHECK(eliminate(c, f, Tcmp, ld, n_rest, ncr, Ucmp, ld, k, pc, h_pc));
+            BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
+                n_rest, act + n_chunk, ncr, Tcmp, ld, Dp, ld));
+            BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_rest * 32), 256, 0, s>>>(
+                n_rest, act + n_chunk, ncr, Dp, ld, lead));
+        }
+        // stay on this panel until no pending lead is left in it
     }
-    out->echelon_rounds = rounds;
+    out->echelon_rounds = steps;
     if (out->ms_event_echelon) BL_CUDA(cudaEventRecord(out->ms_event_echelon, s));
 
     // ---- 3. back substitution --------------------------------------------------

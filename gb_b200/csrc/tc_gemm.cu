@@ -154,6 +154,12 @@ struct TcParams {
     uint32_t* D;
     int64_t ldd;
     int32_t M, N, Mp, Np, nkb;
+    // nonzero flags of the 128-row x 128-byte A tiles ([Mp/128][nkb]) and of the
+    // BN-row x 128-byte B tiles ([Np/BN][nkb]); a K step where either tile is
+    // zero contributes nothing and is skipped (NULL: no skipping)
+    const uint8_t* fa;
+    const uint8_t* fb;
+    unsigned long long* steps;  // optional: K steps executed, summed over tiles
     uint32_t p, pneg_inv;
     uint32_t cw[7];  // 2^(8w) R mod p
     int32_t* err;
@@ -183,7 +189,14 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
     const int nkb = prm.nkb;
-    const int npanels = (nkb + C::PANEL_KB - 1) / C::PANEL_KB;
+    const uint8_t* fa = prm.fa ? prm.fa + (size_t)blockIdx.y * nkb : nullptr;
+    const uint8_t* fb = prm.fb ? prm.fb + (size_t)blockIdx.x * nkb : nullptr;
+    auto live = [&](int kb) { return (!fa || fa[kb]) && (!fb || fb[kb]); };
+    int n_it = 0;  // K steps this tile really needs
+    for (int kb = 0; kb < nkb; ++kb) n_it += live(kb) ? 1 : 0;
+    if (n_it == 0) return;  // A B is zero on this tile: D stays as it is
+    if (prm.steps && threadIdx.x == 0) atomicAdd(prm.steps, (unsigned long long)n_it);
+    const int npanels = (n_it + C::PANEL_KB - 1) / C::PANEL_KB;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::STAGES; ++s) {
@@ -211,9 +224,10 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         if (lane == 0) {
             // ---- producer ----
             int issued = 0;
-            for (int kb = 0; kb < nkb; ++kb) {
-                const int s = kb % C::STAGES;
-                const uint32_t ph = (kb / C::STAGES) & 1;
+            for (int kb = 0, it = 0; kb < nkb; ++kb) {
+                if (!live(kb)) continue;
+                const int s = it % C::STAGES;
+                const uint32_t ph = (it / C::STAGES) & 1;
                 if (*abort_flag || !mbar_wait(empty_bar(s), ph ^ 1, prm.budget)) {
                     *abort_flag = 1;
                     break;
@@ -226,7 +240,7 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 for (int l = 0; l < L; ++l)
                     tma_load_2d(st + L * C::A_BYTES + l * C::B_BYTES, &mapB, kb * C::BK,
                                 l * prm.Np + n0, full_bar(s));
-                issued = kb + 1;
+                issued = ++it;
             }
             // on abort, let the copies already issued land before the CTA exits
             for (int kb = issued > C::STAGES ? issued - C::STAGES : 0; kb < issued; ++kb)
@@ -235,11 +249,12 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer ----
-            for (int kb = 0; kb < nkb; ++kb) {
-                const int s = kb % C::STAGES;
-                const uint32_t ph = (kb / C::STAGES) & 1;
-                const int pk = kb % C::PANEL_KB;
-                const int panel = kb / C::PANEL_KB;
+            for (int kb = 0, it = 0; kb < nkb; ++kb) {
+                if (!live(kb)) continue;
+                const int s = it % C::STAGES;
+                const uint32_t ph = (it / C::STAGES) & 1;
+                const int pk = it % C::PANEL_KB;
+                const int panel = it / C::PANEL_KB;
                 if (pk == 0 && panel > 0) {
                     // accumulators are free once the epilogue read the last panel
                     if (*abort_flag || !mbar_wait(tempty_bar, (panel - 1) & 1, prm.budget)) {
@@ -271,7 +286,8 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     }
                 }
                 tc_commit(empty_bar(s));
-                if (pk == C::PANEL_KB - 1 || kb == nkb - 1) tc_commit(tfull_bar);
+                if (pk == C::PANEL_KB - 1 || it == n_it - 1) tc_commit(tfull_bar);
+                ++it;
             }
         }
     } else {
@@ -339,7 +355,8 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 // ---------------------------------------------------------------------------
 // limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded
 __global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int32_t M, int32_t K,
-                             int32_t Mp, int32_t Kp, int32_t L, uint8_t* __restrict__ out) {
+                             int32_t Mp, int32_t Kp, int32_t L, uint8_t* __restrict__ out,
+                             uint8_t* flags) {
     const int64_t total = (int64_t)Mp * (Kp / 4);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
@@ -348,6 +365,7 @@ __global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int32_
         uint32_t v[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) v[i] = (m < M && k + i < K) ? A[(size_t)m * lda + k + i] : 0u;
+        if (flags && (v[0] | v[1] | v[2] | v[3])) flags[(size_t)(m / 128) * (Kp / 128) + k / 128] = 1;
         for (int l = 0; l < L; ++l) {
             const uint32_t packed = ((v[0] >> (8 * l)) & 255u) | (((v[1] >> (8 * l)) & 255u) << 8) |
                                     (((v[2] >> (8 * l)) & 255u) << 16) |
@@ -359,7 +377,8 @@ __global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int32_
 
 // transposing split: out[l][n][k] = byte l of B[k][n]
 __global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int32_t K, int32_t N,
-                             int32_t Np, int32_t Kp, int32_t L, uint8_t* __restrict__ out) {
+                             int32_t Np, int32_t Kp, int32_t L, uint8_t* __restrict__ out,
+                             uint8_t* flags, int32_t bn) {
     __shared__ uint32_t tile[32][33];
     const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
@@ -373,6 +392,7 @@ __global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int32_
         if (n < Np && k < Kp) {
             const uint32_t v = tile[tx][r];
             for (int l = 0; l < L; ++l) out[((size_t)l * Np + n) * Kp + k] = (uint8_t)(v >> (8 * l));
+            if (flags && v) flags[(size_t)(n / bn) * (Kp / 128) + k / 128] = 1;
         }
     }
 }
@@ -489,6 +509,10 @@ static int make_map(CUtensorMap* map, const void* base, int64_t inner, int64_t r
     return GBGPU_OK;
 }
 
+static thread_local GemmProfile* g_profile = nullptr;
+GemmProfile* gemm_profile() { return g_profile; }
+void set_gemm_profile(GemmProfile* p) { g_profile = p; }
+
 int limbs_for(uint32_t p) {
     if (p < (1u << 8)) return 1;
     if (p < (1u << 16)) return 2;
@@ -505,12 +529,20 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     const int32_t Kp = (g.K + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
     uint8_t* Ap = planes;
     uint8_t* Bp = planes + (size_t)L * Mp * Kp;
+    const int32_t nkb = Kp / Cfg::BK;
+    uint8_t* fa = Bp + (size_t)L * Np * Kp;                 // [Mp/128][nkb]
+    uint8_t* fb = fa + (size_t)(Mp / Cfg::BM) * nkb;         // [Np/BN][nkb]
+    const size_t flag_bytes = (size_t)(Mp / Cfg::BM + Np / Cfg::BN) * nkb;
+    if (cudaMemsetAsync(fa, 0, flag_bytes, s) != cudaSuccess) {
+        set_error("tile flag clear failed");
+        return GBGPU_ECUDA;
+    }
     {
         const int64_t total = (int64_t)Mp * (Kp / 4);
         const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
-        k_split_rows<<<grid, 256, 0, s>>>(g.A, g.lda, g.M, g.K, Mp, Kp, L, Ap);
+        k_split_rows<<<grid, 256, 0, s>>>(g.A, g.lda, g.M, g.K, Mp, Kp, L, Ap, fa);
         dim3 gb((Np + 31) / 32, (Kp + 31) / 32);
-        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.K, g.N, Np, Kp, L, Bp);
+        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.K, g.N, Np, Kp, L, Bp, fb, Cfg::BN);
         *launches += 2;
     }
     CUtensorMap ma, mb;
@@ -525,7 +557,9 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     prm.N = g.N;
     prm.Mp = Mp;
     prm.Np = Np;
-    prm.nkb = Kp / Cfg::BK;
+    prm.nkb = nkb;
+    prm.fa = fa;
+    prm.fb = fb;
     const FieldMont f = FieldMont::make(g.p);
     prm.p = g.p;
     prm.pneg_inv = f.pneg_inv;
@@ -544,8 +578,22 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         return GBGPU_ECUDA;
     }
     dim3 grid(Np / Cfg::BN, Mp / Cfg::BM);
+    GemmProfile* prof = gemm_profile();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        prm.steps = prof->d_steps;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s);
+    }
     k_tc_submul<L><<<grid, 192, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
     ++*launches;
+    if (prof) {
+        cudaEventRecord(e1, s);
+        prof->events.push_back({e0, e1});
+        // int8 MACs of one executed K step of one tile
+        prof->macs_per_step.push_back((double)Cfg::BM * Cfg::BN * Cfg::BK * L * L);
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("tc launch: ") + cudaGetErrorString(e));
@@ -559,7 +607,8 @@ size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K) {
     const int BN = L == 1 ? 256 : (L == 2 ? 128 : 64);
     const size_t Mp = (size_t)(M + 127) / 128 * 128, Np = (size_t)(N + BN - 1) / BN * BN;
     const size_t Kp = (size_t)(K + 127) / 128 * 128;
-    return (size_t)L * (Mp + Np) * Kp;
+    const size_t flags = (Mp / 128 + Np / BN) * (Kp / 128);
+    return (size_t)L * (Mp + Np) * Kp + ((flags + 255) & ~(size_t)255);
 }
 
 int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,

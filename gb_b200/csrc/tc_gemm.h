@@ -4,6 +4,9 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <utility>
+#include <vector>
+
 namespace gbgpu {
 
 struct TcGemmArgs {
@@ -16,6 +19,16 @@ struct TcGemmArgs {
     uint32_t* D;        // M x N, row-major, residues, updated in place
     int64_t ldd;
 };
+
+// Optional per-thread profiling of the tensor-core GEMM launches: CUDA events
+// around every k_tc_submul launch and a device counter of executed K steps.
+struct GemmProfile {
+    unsigned long long* d_steps = nullptr;  // device counter (all launches)
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<double> macs_per_step;      // per launch
+};
+GemmProfile* gemm_profile();
+void set_gemm_profile(GemmProfile* p);
 
 int limbs_for(uint32_t p);
 // bytes of device workspace the tensor-core path needs for the limb planes

@@ -19,8 +19,9 @@ from . import _lib
 from .matrix import MacaulayMatrix, ReducedRows
 
 
-def _options(form: int = _lib.FORM_AUTO, device: int = 0, stream: Optional[int] = None):
-    return _lib.Options(form, device, 1, 0, stream)
+def _options(form: int = _lib.FORM_AUTO, device: int = 0, stream: Optional[int] = None,
+             profile: bool = False):
+    return _lib.Options(form, device, 1, 1 if profile else 0, stream)
 
 
 def _csr(mat: MacaulayMatrix) -> _lib.Csr:
@@ -80,11 +81,12 @@ def reduce_batch(mats: Sequence[MacaulayMatrix], form: int = _lib.FORM_AUTO, dev
 class Plan:
     """Device-resident copy of one matrix for repeated runs (benchmarks)."""
 
-    def __init__(self, mat: MacaulayMatrix, form: int = _lib.FORM_AUTO, device: int = 0):
+    def __init__(self, mat: MacaulayMatrix, form: int = _lib.FORM_AUTO, device: int = 0,
+                 profile: bool = False):
         self._lib = _lib.load()
         self._mat = mat  # keep host arrays alive until the upload finished
         self._h = C.c_void_p()
-        opt = _options(form, device)
+        opt = _options(form, device, profile=profile)
         _lib.check(self._lib.gbgpu_plan_create(C.byref(_csr(mat)), C.byref(opt),
                                                C.byref(self._h)))
 

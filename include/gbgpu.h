@@ -140,7 +140,7 @@ typedef struct gbgpu_options {
     int32_t form;       /* GBGPU_FORM_*                                  */
     int32_t device;     /* CUDA device ordinal                           */
     int32_t check;      /* 1: validate the input contract on the device  */
-    int32_t reserved;
+    int32_t profile;    /* 1: time every tensor-core GEMM launch (events)  */
     void *stream;       /* cudaStream_t to run on; NULL = library stream */
 } gbgpu_options;
 
@@ -160,6 +160,11 @@ typedef struct gbgpu_stats {
                                lengths over every pivot application)        */
     int64_t work_dense;     /* dense-pivot entries applied in the echelon and
                                back substitution                            */
+    int64_t gemm_launches;  /* tensor-core GEMM kernels (k_tc_submul) run    */
+    double gemm_ms;         /* their summed device time (profile = 1 only)   */
+    double gemm_int8_ops;   /* int8 tensor ops they executed (2 per MAC, all
+                               limb products, zero tiles skipped)           */
+    int64_t form_used;      /* GBGPU_FORM_PLAIN / _TENSOR / _BLOCKED_PLAIN   */
 } gbgpu_stats;
 
 /* One-shot: host CSR in, host rows out (H2D, reduction, D2H). */
