@@ -237,11 +237,8 @@ def main():
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     launches = lib.gbgpu_kernel_launches() - launches0
-    ms = float(np.mean(step_ms))
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    from gb_b200 import dist
+    ms = dist.max_over_ranks(float(np.mean(step_ms)), device="cuda")
     answer = plan.result()
     work_sparse = _work_counters(plan)
     plan.close()
