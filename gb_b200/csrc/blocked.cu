@@ -16,8 +16,10 @@
 //                                                  pivots of block k touch)
 //      with X_k stored over W[:, k]; (b) D' = D - X B as one GEMM whose zero
 //      tiles (staircase X, banded B) are skipped.
-//   2. Echelon of D' over 128-column panels, left to right: the pending rows
-//      whose lead lies in the panel (128 at a time) are brought to echelon form
+//   2. Echelon of D': one claim round first (the first row of every distinct
+//      lead becomes a pivot, all other rows are eliminated against these at
+//      once), then 128-column panels, left to right, for the rows that remain:
+//      the pending rows whose lead lies in the panel (128 at a time) are brought to echelon form
 //      inside the panel in shared memory (k_panel_factor), the recorded row
 //      transformation is applied to their trailing columns with one GEMM, the
 //      pivots found are registered, and the panel's other pending rows are
@@ -87,10 +89,10 @@ __global__ void k_densify_pivots(int32_t ncl, const int32_t* __restrict__ piv_ro
     }
 }
 
-// span[b] = largest column < limit of the known pivots of rows [128 b, 128 b + 128)
+// span[b] = largest column < limit of the known pivots of rows [bs b, bs b + bs)
 __global__ void k_block_span(int32_t ncl, const int32_t* __restrict__ piv_row,
                              const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
-                             int32_t limit, int32_t* span) {
+                             int32_t limit, int32_t bs, int32_t* span) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -102,7 +104,7 @@ __global__ void k_block_span(int32_t ncl, const int32_t* __restrict__ piv_row,
             if (col < limit && col > mx) mx = col;
         }
         for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0 && mx >= 0) atomicMax(&span[c / 128], mx);
+        if (lane == 0 && mx >= 0) atomicMax(&span[c / bs], mx);
     }
 }
 
@@ -131,12 +133,12 @@ __global__ void k_count_below(int32_t n, const int32_t* __restrict__ v, int32_t 
 
 // -U^-1 mod p for unit upper triangular blocks.  Block b is read from
 // src + b * stride_b with leading dimension ld (kb x kb, kb <= KB); the result
-// goes to out + b * KB * KB (KB x KB, identity-padded).  One CTA per block,
-// thread j solves column j by back substitution.
+// (KB x KB, identity-padded) goes to out + b * ostride with leading dimension
+// old.  One CTA per block, thread j solves column j by back substitution.
 template <class F>
 __global__ void __launch_bounds__(KB)
 k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, int32_t n_blocks,
-              int32_t last_kb, uint32_t* out, F f) {
+              int32_t last_kb, uint32_t* out, int64_t ostride, int64_t old, F f) {
     extern __shared__ uint32_t inv_smem[];
     uint32_t(*U)[KB + 1] = (uint32_t(*)[KB + 1])inv_smem;
     uint32_t(*V)[KB + 1] = (uint32_t(*)[KB + 1])(inv_smem + KB * (KB + 1));
@@ -167,11 +169,11 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
         V[i][j] = acc ? f.p - acc : 0u;
     }
     __syncthreads();
-    uint32_t* o = out + (size_t)b * KB * KB;
+    uint32_t* o = out + (size_t)b * ostride;
     for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
         const int i = t / KB, jj = t % KB;
         const uint32_t v = V[i][jj];
-        o[t] = v ? f.p - v : 0u;  // -V
+        o[(size_t)i * old + jj] = v ? f.p - v : 0u;  // -V
     }
 }
 
@@ -332,6 +334,54 @@ k_panel_factor(const uint32_t* __restrict__ old, int64_t ldo, int32_t n, int32_t
     if (r == 0) *n_piv = k;
 }
 
+// claim round: claim[lead] = smallest candidate row with that lead
+__global__ void k_claim_rows(int32_t n, const int32_t* __restrict__ cand,
+                             const int32_t* __restrict__ lead, int32_t* claim) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicMin(&claim[lead[cand[i]]], cand[i]);
+}
+
+// winners become pivots (piv_of_col, is_piv, wflag), the others are listed
+__global__ void k_claim_split(int32_t n, const int32_t* __restrict__ cand,
+                              const int32_t* __restrict__ lead, const int32_t* __restrict__ claim,
+                              int32_t* piv_of_col, uint8_t* is_piv, int32_t* wflag,
+                              int32_t* losers, int32_t* n_losers) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t r = cand[i];
+        const int32_t c = lead[r];
+        if (claim[c] == r) {
+            piv_of_col[c] = r;
+            is_piv[r] = 1;
+            wflag[c] = 1;
+        } else {
+            losers[atomicAdd(n_losers, 1)] = r;
+        }
+    }
+}
+
+// scale each listed row by the inverse of its lead entry (warp per row)
+template <class F>
+__global__ void k_normalize_rows(int32_t n, const int32_t* __restrict__ list,
+                                 const int32_t* __restrict__ lead, int32_t ncols, uint32_t* M,
+                                 int64_t ld, F f) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < n; i += nwarps) {
+        const int32_t r = list[i];
+        const int32_t c0 = lead[r];
+        uint32_t* row = M + (size_t)r * ld;
+        const uint32_t inv = inverse_mod(row[c0], f.p);
+        __syncwarp();
+        for (int c = c0 + 1 + lane; c < ncols; c += 32) {
+            const uint32_t v = row[c];
+            if (v) row[c] = f.mulmod(v, inv);
+        }
+        __syncwarp();
+        if (lane == 0) row[c0] = 1u;
+    }
+}
+
 // register the chunk's pivots: pivot k is chunk row piv_pos[k] = act[...]
 __global__ void k_register_pivots(const int32_t* __restrict__ n_piv,
                                   const int32_t* __restrict__ piv_pos,
@@ -344,6 +394,25 @@ __global__ void k_register_pivots(const int32_t* __restrict__ n_piv,
         piv_of_col[piv_col[k]] = row;
         is_piv[row] = 1;
         prow_out[k] = row;
+    }
+}
+
+// dst block b (NB x NB, leading dimension NB, block stride NB (NB + 1)) =
+// src block b (nb_b x nb_b at src + b stride_src, leading dimension lds),
+// identity-padded; nb_b = NB except for the last block
+__global__ void k_copy_blocks(const uint32_t* __restrict__ src, int64_t lds, int64_t stride_src,
+                              int32_t n_blocks, int32_t last_nb, int32_t NB, uint32_t* dst) {
+    const int64_t per = (int64_t)NB * NB;
+    const int64_t total = per * n_blocks;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = (int32_t)(t / per);
+        const int32_t i = (int32_t)((t % per) / NB), j = (int32_t)(t % NB);
+        const int32_t nb = b == n_blocks - 1 ? last_nb : NB;
+        uint32_t v;
+        if (i < nb && j < nb) v = src[(size_t)b * stride_src + (size_t)i * lds + j];
+        else v = i == j ? 1u : 0u;
+        dst[(size_t)b * NB * (NB + 1) + (size_t)i * NB + j] = v;
     }
 }
 
@@ -422,47 +491,110 @@ static int gemm(Ctx& c, uint32_t* D, int64_t ldd, const uint32_t* A, int64_t lda
     return tc_submul(g, c.ws, c.s, c.err, &c.launches);
 }
 
+// batch of `batch` products D_z -= A_z B_z (element strides sA, sB, sD)
+static int gemm_batched(Ctx& c, uint32_t* D, int64_t ldd, int64_t sD, const uint32_t* A,
+                        int64_t lda, int64_t sA, const uint32_t* B, int64_t ldb, int64_t sB,
+                        int32_t M, int32_t N, int32_t K, int32_t batch) {
+    if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return GBGPU_OK;
+    TcGemmArgs g{c.p, M, N, K, A, lda, B, ldb, D, ldd};
+    g.batch = batch;
+    g.sA = sA;
+    g.sB = sB;
+    g.sD = sD;
+    if (c.form == GBGPU_FORM_PLAIN) return plain_submul(g, c.s, &c.launches);
+    const size_t need = tc_workspace_bytes(c.p, M, N, K, batch);
+    if (need > c.ws_bytes) {
+        if (c.ws) cudaFreeAsync(c.ws, c.s);
+        c.ws = nullptr;
+        const size_t bytes = std::max(need, c.ws_bytes * 2);
+        if (cudaMallocAsync(&c.ws, bytes, c.s) != cudaSuccess) {
+            set_error("GEMM workspace allocation failed");
+            return GBGPU_ENOMEM;
+        }
+        c.ws_bytes = bytes;
+    }
+    return tc_submul(g, c.ws, c.s, c.err, &c.launches);
+}
+
+// elimination block size: powers of two from 128 to 1024
+static int32_t nb_for(int64_t n) {
+    int32_t nb = KB;
+    while (nb < n && nb < 8 * KB) nb *= 2;
+    return nb;
+}
+
+// -U^-1 for n_blocks unit upper triangular blocks of size NB (block b at
+// src + b * stride_src, leading dimension lds; the last one last_nb x last_nb,
+// identity-padded).  Result: out + b NB (NB + 1), leading dimension NB.  The
+// 128 x 128 diagonal blocks are inverted by k_neg_inverse; blocks are then
+// merged by doubling,  -[[A, B], [0, C]]^-1 = [[-A^-1, A^-1 B C^-1], [0, -C^-1]],
+// with two batched GEMMs per level (the NB + 1 block stride makes the
+// diagonal blocks of one level equally spaced across all big blocks).
 template <class F>
-static int neg_inverse(Ctx& c, const F& f, const uint32_t* src, int64_t ld, int64_t stride_b,
-                       int32_t n_blocks, int32_t last_kb, uint32_t* out) {
+static int neg_inverse_big(Ctx& c, const F& f, const uint32_t* src, int64_t lds,
+                           int64_t stride_src, int32_t n_blocks, int32_t last_nb, int32_t NB,
+                           uint32_t* out) {
     if (n_blocks <= 0) return GBGPU_OK;
+    const int64_t bstride = (int64_t)NB * (NB + 1);
+    uint32_t* U = c.alloc<uint32_t>((size_t)n_blocks * bstride);
+    uint32_t* T = c.alloc<uint32_t>((size_t)n_blocks * NB * NB / 4 + 1);
+    if (!U || !T) return GBGPU_ENOMEM;
+    BL_LAUNCH(k_copy_blocks<<<grid_of((int64_t)n_blocks * NB * NB), 256, 0, c.s>>>(
+        src, lds, stride_src, n_blocks, last_nb, NB, U));
+    BL_CUDA(cudaMemsetAsync(out, 0, sizeof(uint32_t) * (size_t)n_blocks * bstride, c.s));
     const int bytes = 2 * KB * (KB + 1) * (int)sizeof(uint32_t);
     BL_CUDA(cudaFuncSetAttribute(k_neg_inverse<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    BL_LAUNCH(k_neg_inverse<F><<<n_blocks, KB, bytes, c.s>>>(src, ld, stride_b, n_blocks, last_kb, out, f));
+    const int32_t n_sub = n_blocks * (NB / KB);
+    const int64_t dstep = (int64_t)KB * (NB + 1);  // between 128-blocks on the diagonal
+    BL_LAUNCH(k_neg_inverse<F><<<n_sub, KB, bytes, c.s>>>(U, NB, dstep, n_sub, KB, out, dstep, NB, f));
+    for (int32_t sz = KB; sz < NB; sz *= 2) {
+        const int32_t items = n_blocks * (NB / (2 * sz));
+        const int64_t istep = (int64_t)2 * sz * (NB + 1);
+        const int64_t half = (int64_t)sz * (NB + 1);
+        BL_CUDA(cudaMemsetAsync(T, 0, sizeof(uint32_t) * (size_t)items * sz * sz, c.s));
+        // T = B C^-1 = 0 - B (-C^-1)
+        BL_CHECK(gemm_batched(c, T, sz, (int64_t)sz * sz, U + sz, NB, istep, out + half, NB, istep,
+                              sz, sz, sz, items));
+        // top right of -U^-1 = A^-1 B C^-1 = 0 - (-A^-1) T
+        BL_CHECK(gemm_batched(c, out + sz, NB, istep, out, NB, istep, T, sz, (int64_t)sz * sz, sz,
+                              sz, sz, items));
+    }
     return GBGPU_OK;
 }
 
 // T (rows x ncols, ld) <- T - T[:, pc] (U[:, pc])^-1 U for pivot rows U
 // (n_p x ncols, ld_u, sorted by lead, monic, zero left of their leads) with
 // pivot columns pc (ascending): afterwards T is zero at every pivot column.
-// Blocks of KB pivots, left to right.
+// Blocks of NB pivots, left to right.
 template <class F>
 static int eliminate(Ctx& c, const F& f, uint32_t* T, int64_t ldt, int32_t rows, int32_t ncols,
                      const uint32_t* U, int64_t ldu, int32_t n_p, const int32_t* d_pc,
                      const std::vector<int32_t>& pc) {
     if (rows <= 0 || n_p <= 0) return GBGPU_OK;
-    const int32_t nb = (n_p + KB - 1) / KB;
-    uint32_t* Ublk = c.alloc<uint32_t>((size_t)nb * KB * KB);   // U[:, pc] diagonal blocks
-    uint32_t* Ninv = c.alloc<uint32_t>((size_t)nb * KB * KB);
-    uint32_t* G = c.alloc<uint32_t>((size_t)rows * KB);         // T[:, pc_k]
-    uint32_t* X = c.alloc<uint32_t>((size_t)rows * KB);
+    const int32_t NB = nb_for(n_p);
+    const int32_t nb = (n_p + NB - 1) / NB;
+    const int64_t bstride = (int64_t)NB * (NB + 1);
+    uint32_t* Ublk = c.alloc<uint32_t>((size_t)nb * NB * NB);   // U[:, pc] diagonal blocks
+    uint32_t* Ninv = c.alloc<uint32_t>((size_t)nb * bstride);
+    uint32_t* G = c.alloc<uint32_t>((size_t)rows * NB);         // T[:, pc_k]
+    uint32_t* X = c.alloc<uint32_t>((size_t)rows * NB);
     if (!Ublk || !Ninv || !G || !X) return GBGPU_ENOMEM;
     for (int b = 0; b < nb; ++b) {
-        const int kb = std::min(KB, n_p - b * KB);
+        const int kb = std::min(NB, n_p - b * NB);
         BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)kb * kb), 256, 0, c.s>>>(
-            kb, kb, U + (size_t)b * KB * ldu, ldu, d_pc + b * KB, Ublk + (size_t)b * KB * KB, KB));
+            kb, kb, U + (size_t)b * NB * ldu, ldu, d_pc + b * NB, Ublk + (size_t)b * NB * NB, NB));
     }
-    BL_CHECK(neg_inverse(c, f, Ublk, KB, (int64_t)KB * KB, nb, n_p - (nb - 1) * KB, Ninv));
+    BL_CHECK(neg_inverse_big(c, f, Ublk, NB, (int64_t)NB * NB, nb, n_p - (nb - 1) * NB, NB, Ninv));
     for (int b = 0; b < nb; ++b) {
-        const int kb = std::min(KB, n_p - b * KB);
-        const int32_t first_col = pc[b * KB];
+        const int kb = std::min(NB, n_p - b * NB);
+        const int32_t first_col = pc[b * NB];
         BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)rows * kb), 256, 0, c.s>>>(
-            rows, kb, T, ldt, d_pc + b * KB, G, KB));
-        BL_CUDA(cudaMemsetAsync(X, 0, sizeof(uint32_t) * (size_t)rows * KB, c.s));
+            rows, kb, T, ldt, d_pc + b * NB, G, NB));
+        BL_CUDA(cudaMemsetAsync(X, 0, sizeof(uint32_t) * (size_t)rows * NB, c.s));
         // X = G * (U_kk)^-1 = 0 - G * (-(U_kk)^-1)
-        BL_CHECK(gemm(c, X, KB, G, KB, Ninv + (size_t)b * KB * KB, KB, rows, kb, kb));
+        BL_CHECK(gemm(c, X, NB, G, NB, Ninv + (size_t)b * bstride, NB, rows, kb, kb));
         // T[:, first_col:] -= X * U_k[:, first_col:]
-        BL_CHECK(gemm(c, T + first_col, ldt, X, KB, U + (size_t)b * KB * ldu + first_col, ldu, rows,
+        BL_CHECK(gemm(c, T + first_col, ldt, X, NB, U + (size_t)b * NB * ldu + first_col, ldu, rows,
                       ncols - first_col, kb));
     }
     return GBGPU_OK;
@@ -497,45 +629,46 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
             t, work_sorted, in.row_ptr, in.cols, in.vals, 0, nc, W, ld));
     }
     if (t > 0 && ncl > 0) {
+        const int32_t NB = nb_for(ncl);
+        const int64_t bstride = (int64_t)NB * (NB + 1);
         uint32_t* P = c.alloc<uint32_t>((size_t)ncl * ld);
-        const int32_t nbk = (ncl + KB - 1) / KB;
-        uint32_t* Ninv = c.alloc<uint32_t>((size_t)nbk * KB * KB);
-        uint32_t* X = c.alloc<uint32_t>((size_t)t * KB);
+        const int32_t nbk = (ncl + NB - 1) / NB;
+        uint32_t* Ninv = c.alloc<uint32_t>((size_t)nbk * bstride);
+        uint32_t* X = c.alloc<uint32_t>((size_t)t * NB);
         int32_t* act = c.alloc<int32_t>(nbk);
-        if (!P || !Ninv || !X || !act) return GBGPU_ENOMEM;
+        int32_t* span = c.alloc<int32_t>(nbk);
+        if (!P || !Ninv || !X || !act || !span) return GBGPU_ENOMEM;
         BL_CUDA(cudaMemsetAsync(P, 0, sizeof(uint32_t) * (size_t)ncl * ld, s));
         BL_LAUNCH(k_densify_pivots<<<grid_of((int64_t)ncl * 32), 256, 0, s>>>(
             ncl, in.piv_row, in.row_ptr, in.cols, in.vals, P, ld));
-        // -A_kk^-1 of every diagonal block of A (read in place from P)
-        BL_CHECK(neg_inverse(c, f, P, ld, (int64_t)KB * ld + KB, nbk, ncl - (nbk - 1) * KB, Ninv));
-        BL_LAUNCH(k_count_below<<<grid_of(nbk), 256, 0, s>>>(t, lead_sorted, nbk, KB, act));
-        std::vector<int32_t> h_act(nbk);
-        BL_CUDA(cudaMemcpyAsync(h_act.data(), act, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaStreamSynchronize(s));
-        // last left column touched by the known pivots of each 128-row block
-        int32_t* span = c.alloc<int32_t>(nbk);
-        if (!span) return GBGPU_ENOMEM;
+        // -A_kk^-1 of every NB x NB diagonal block of A (read in place from P)
+        BL_CHECK(neg_inverse_big(c, f, P, ld, (int64_t)NB * ld + NB, nbk, ncl - (nbk - 1) * NB, NB,
+                                 Ninv));
+        // active rows of each block (rows sorted by lead) and the last left
+        // column the known pivots of each block touch
+        BL_LAUNCH(k_count_below<<<grid_of(nbk), 256, 0, s>>>(t, lead_sorted, nbk, NB, act));
         BL_LAUNCH(k_fill_i32<<<grid_of(nbk), 256, 0, s>>>(span, nbk, -1));
         BL_LAUNCH(k_block_span<<<grid_of((int64_t)ncl * 32), 256, 0, s>>>(
-            ncl, in.piv_row, in.row_ptr, in.cols, ncl, span));
-        std::vector<int32_t> h_span(nbk);
+            ncl, in.piv_row, in.row_ptr, in.cols, ncl, NB, span));
+        std::vector<int32_t> h_act(nbk), h_span(nbk);
+        BL_CUDA(cudaMemcpyAsync(h_act.data(), act, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaMemcpyAsync(h_span.data(), span, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         // (a) X = C A^-1, in place in W[:, 0:ncl], block by block; the update of
         //     the later left columns stops at the last column block k touches
         for (int k = 0; k < nbk; ++k) {
-            const int32_t c0 = k * KB, kb = std::min(KB, ncl - c0), c1 = c0 + kb;
+            const int32_t c0 = k * NB, kb = std::min(NB, ncl - c0), c1 = c0 + kb;
             const int32_t rows = h_act[k];
             if (rows <= 0) continue;
-            BL_CUDA(cudaMemsetAsync(X, 0, sizeof(uint32_t) * (size_t)rows * KB, s));
+            BL_CUDA(cudaMemsetAsync(X, 0, sizeof(uint32_t) * (size_t)rows * NB, s));
             // X_k = W[:, block] A_kk^-1
-            BL_CHECK(gemm(c, X, KB, W + c0, ld, Ninv + (size_t)k * KB * KB, KB, rows, kb, kb));
-            BL_CUDA(cudaMemcpy2DAsync(W + c0, ld * 4, X, KB * 4, (size_t)kb * 4, rows,
+            BL_CHECK(gemm(c, X, NB, W + c0, ld, Ninv + (size_t)k * bstride, NB, rows, kb, kb));
+            BL_CUDA(cudaMemcpy2DAsync(W + c0, ld * 4, X, NB * 4, (size_t)kb * 4, rows,
                                       cudaMemcpyDeviceToDevice, s));
             // W[:, c1:e) -= X_k A[block rows, c1:e)
             const int32_t e = std::min(ncl, h_span[k] + 1);
             if (e > c1)
-                BL_CHECK(gemm(c, W + c1, ld, X, KB, P + (size_t)c0 * ld + c1, ld, rows, e - c1, kb));
+                BL_CHECK(gemm(c, W + c1, ld, X, NB, P + (size_t)c0 * ld + c1, ld, rows, e - c1, kb));
         }
         // (b) D' = D - X B: one GEMM over the whole left block; the tile flags of
         //     the GEMM skip the zero tiles of the staircase X and of B
@@ -588,6 +721,53 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
     uint32_t* Ubuf = nullptr;   // gathered pivot rows / rest rows for eliminate
     size_t ubuf_rows = 0;
     int steps = 0;
+    // claim round: the first row of every distinct lead becomes a pivot (a
+    // row with a lead of its own is already a pivot of the echelon form);
+    // the other rows are eliminated against all of them at once and go on
+    // to the panels
+    if (n_nonzero > 0) {
+        int32_t* claim = c.alloc<int32_t>(ncr);
+        int32_t* losers = c.alloc<int32_t>(t);
+        if (!claim || !losers) return GBGPU_ENOMEM;
+        BL_LAUNCH(k_fill_i32<<<grid_of(ncr), 256, 0, s>>>(claim, ncr, INT_MAX));
+        BL_CUDA(cudaMemsetAsync(wflag, 0, sizeof(int32_t) * ncr, s));
+        BL_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(int32_t), s));
+        BL_LAUNCH(k_claim_rows<<<grid_of(n_nonzero), 256, 0, s>>>(n_nonzero, act, lead, claim));
+        BL_LAUNCH(k_claim_split<<<grid_of(n_nonzero), 256, 0, s>>>(
+            n_nonzero, act, lead, claim, piv_of_col, is_piv, wflag, losers, counters + 4));
+        BL_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wflag, wpos, ncr, s));
+        ++c.launches;
+        BL_LAUNCH(k_compact_cols<<<grid_of(ncr), 256, 0, s>>>(ncr, wflag, wpos, pc));
+        int32_t n_lost = 0, last_pos = 0, last_flag = 0;
+        BL_CUDA(cudaMemcpyAsync(&n_lost, counters + 4, 4, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaMemcpyAsync(&last_pos, wpos + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaMemcpyAsync(&last_flag, wflag + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaStreamSynchronize(s));
+        const int32_t n_new = last_pos + last_flag;
+        BL_LAUNCH(k_gather_rows<<<grid_of(n_new), 256, 0, s>>>(n_new, pc, piv_of_col, prow,
+                                                               counters + 5));
+        BL_LAUNCH(k_normalize_rows<F><<<grid_of((int64_t)n_new * 32), 256, 0, s>>>(
+            n_new, prow, lead, ncr, Dp, ld, f));
+        if (n_lost > 0) {
+            std::vector<int32_t> h_pc(n_new);
+            BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * n_new, cudaMemcpyDeviceToHost,
+                                    s));
+            uint32_t* Ucmp = c.alloc<uint32_t>((size_t)n_new * ld);
+            uint32_t* Tcmp = c.alloc<uint32_t>((size_t)n_lost * ld);
+            if (!Ucmp || !Tcmp) return GBGPU_ENOMEM;
+            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_new * ncr), 256, 0, s>>>(
+                n_new, prow, ncr, Dp, ld, Ucmp, ld));
+            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_lost * ncr), 256, 0, s>>>(
+                n_lost, losers, ncr, Dp, ld, Tcmp, ld));
+            BL_CUDA(cudaStreamSynchronize(s));
+            BL_CHECK(eliminate(c, f, Tcmp, ld, n_lost, ncr, Ucmp, ld, n_new, pc, h_pc));
+            BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_lost * ncr), 256, 0, s>>>(
+                n_lost, losers, ncr, Tcmp, ld, Dp, ld));
+            BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_lost * 32), 256, 0, s>>>(n_lost, losers, ncr,
+                                                                                 Dp, ld, lead));
+        }
+        ++steps;
+    }
     int32_t j = 0;
     while (n_nonzero > 0 && j < ncr) {
         const int32_t bw = std::min(KB, ncr - j);
@@ -671,38 +851,39 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         BL_CUDA(cudaStreamSynchronize(s));
         BL_LAUNCH(k_gather_rows<<<grid_of(r), 256, 0, s>>>(r, pc, piv_of_col, prow, counters + 2));
         // compact echelon rows E (r x ncr), ascending lead
+        const int32_t NB = nb_for(r);
+        const int64_t bstride = (int64_t)NB * (NB + 1);
         uint32_t* E = c.alloc<uint32_t>((size_t)r * ld);
-        const int32_t nb = (r + KB - 1) / KB;
-        uint32_t* Ublk = c.alloc<uint32_t>((size_t)nb * KB * KB);
-        uint32_t* Ninv = c.alloc<uint32_t>((size_t)nb * KB * KB);
-        uint32_t* G = c.alloc<uint32_t>((size_t)KB * std::max(r, 1));
-        uint32_t* Y = c.alloc<uint32_t>((size_t)KB * ld);
+        const int32_t nb = (r + NB - 1) / NB;
+        uint32_t* Ublk = c.alloc<uint32_t>((size_t)nb * NB * NB);
+        uint32_t* Ninv = c.alloc<uint32_t>((size_t)nb * bstride);
+        uint32_t* G = c.alloc<uint32_t>((size_t)NB * std::max(r, 1));
+        uint32_t* Y = c.alloc<uint32_t>((size_t)NB * ld);
         if (!E || !Ublk || !Ninv || !G || !Y) return GBGPU_ENOMEM;
         BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)r * ncr), 256, 0, s>>>(r, prow, ncr, Dp,
                                                                                 ld, E, ld));
         for (int b = 0; b < nb; ++b) {
-            const int kb = std::min(KB, r - b * KB);
+            const int kb = std::min(NB, r - b * NB);
             BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)kb * kb), 256, 0, s>>>(
-                kb, kb, E + (size_t)b * KB * ld, ld, pc + b * KB, Ublk + (size_t)b * KB * KB, KB));
+                kb, kb, E + (size_t)b * NB * ld, ld, pc + b * NB, Ublk + (size_t)b * NB * NB, NB));
         }
-        BL_CHECK(neg_inverse(c, f, Ublk, KB, (int64_t)KB * KB, nb, r - (nb - 1) * KB, Ninv));
+        BL_CHECK(neg_inverse_big(c, f, Ublk, NB, (int64_t)NB * NB, nb, r - (nb - 1) * NB, NB, Ninv));
         for (int b = nb - 1; b >= 0; --b) {
-            const int kb = std::min(KB, r - b * KB);
-            const int32_t later = r - (b * KB + kb);
-            uint32_t* Ek = E + (size_t)b * KB * ld;
-            const int32_t c0 = h_pc[b * KB];
+            const int kb = std::min(NB, r - b * NB);
+            const int32_t later = r - (b * NB + kb);
+            uint32_t* Ek = E + (size_t)b * NB * ld;
+            const int32_t c0 = h_pc[b * NB];
             if (later > 0) {
                 // Ek -= Ek[:, pc(>k)] R(>k)
                 BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)kb * later), 256, 0, s>>>(
-                    kb, later, Ek, ld, pc + b * KB + kb, G, later));
-                const int32_t c_later = h_pc[b * KB + kb];
-                BL_CHECK(gemm(c, Ek + c_later, ld, G, later, E + (size_t)(b * KB + kb) * ld + c_later,
+                    kb, later, Ek, ld, pc + b * NB + kb, G, later));
+                const int32_t c_later = h_pc[b * NB + kb];
+                BL_CHECK(gemm(c, Ek + c_later, ld, G, later, E + (size_t)(b * NB + kb) * ld + c_later,
                               ld, kb, ncr - c_later, later));
             }
-            // Ek = (Ek[:, pc(k)])^-1 Ek = Ek - (-(U_kk)^-1 - I) ... computed as
-            // Y = 0 - (-(U_kk)^-1) Ek, then Ek = Y
-            BL_CUDA(cudaMemsetAsync(Y, 0, sizeof(uint32_t) * (size_t)KB * ld, s));
-            BL_CHECK(gemm(c, Y + c0, ld, Ninv + (size_t)b * KB * KB, KB, Ek + c0, ld, kb, ncr - c0, kb));
+            // Ek = (Ek[:, pc(k)])^-1 Ek, as Y = 0 - (-(U_kk)^-1) Ek, Ek = Y
+            BL_CUDA(cudaMemsetAsync(Y, 0, sizeof(uint32_t) * (size_t)NB * ld, s));
+            BL_CHECK(gemm(c, Y + c0, ld, Ninv + (size_t)b * bstride, NB, Ek + c0, ld, kb, ncr - c0, kb));
             BL_CUDA(cudaMemcpy2DAsync(Ek + c0, ld * 4, Y + c0, ld * 4, (size_t)(ncr - c0) * 4, kb,
                                       cudaMemcpyDeviceToDevice, s));
         }

@@ -152,7 +152,7 @@ struct TcCfg {
 
 struct TcParams {
     uint32_t* D;
-    int64_t ldd;
+    int64_t ldd, sD;
     int32_t M, N, Mp, Np, nkb;
     // nonzero flags of the 128-row x 128-byte A tiles ([Mp/128][nkb]) and of the
     // BN-row x 128-byte B tiles ([Np/BN][nkb]); a K step where either tile is
@@ -188,9 +188,12 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
+    const int z = blockIdx.z;  // batch item
     const int nkb = prm.nkb;
-    const uint8_t* fa = prm.fa ? prm.fa + (size_t)blockIdx.y * nkb : nullptr;
-    const uint8_t* fb = prm.fb ? prm.fb + (size_t)blockIdx.x * nkb : nullptr;
+    const uint8_t* fa =
+        prm.fa ? prm.fa + ((size_t)z * (prm.Mp / C::BM) + blockIdx.y) * nkb : nullptr;
+    const uint8_t* fb =
+        prm.fb ? prm.fb + ((size_t)z * (prm.Np / C::BN) + blockIdx.x) * nkb : nullptr;
     auto live = [&](int kb) { return (!fa || fa[kb]) && (!fb || fb[kb]); };
     int n_it = 0;  // K steps this tile really needs
     for (int kb = 0; kb < nkb; ++kb) n_it += live(kb) ? 1 : 0;
@@ -235,11 +238,11 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 mbar_expect_tx(full_bar(s), C::STAGE_BYTES);
                 const uint32_t st = base + s * C::STAGE_BYTES;
                 for (int l = 0; l < L; ++l)
-                    tma_load_2d(st + l * C::A_BYTES, &mapA, kb * C::BK, l * prm.Mp + m0,
-                                full_bar(s));
+                    tma_load_2d(st + l * C::A_BYTES, &mapA, kb * C::BK,
+                                (z * L + l) * prm.Mp + m0, full_bar(s));
                 for (int l = 0; l < L; ++l)
                     tma_load_2d(st + L * C::A_BYTES + l * C::B_BYTES, &mapB, kb * C::BK,
-                                l * prm.Np + n0, full_bar(s));
+                                (z * L + l) * prm.Np + n0, full_bar(s));
                 issued = ++it;
             }
             // on abort, let the copies already issued land before the CTA exits
@@ -325,7 +328,7 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     }
                 }
                 if (gm < prm.M) {
-                    uint32_t* drow = prm.D + (size_t)gm * prm.ldd;
+                    uint32_t* drow = prm.D + (size_t)z * prm.sD + (size_t)gm * prm.ldd;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const int gn = n0 + c0 + j;
@@ -354,13 +357,17 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
 // ---------------------------------------------------------------------------
 // limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded
-__global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int32_t M, int32_t K,
-                             int32_t Mp, int32_t Kp, int32_t L, uint8_t* __restrict__ out,
-                             uint8_t* flags) {
+__global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA, int32_t M,
+                             int32_t K, int32_t Mp, int32_t Kp, int32_t L,
+                             uint8_t* __restrict__ out, uint8_t* flags) {
+    // batch item blockIdx.y
+    A += (size_t)blockIdx.y * sA;
+    out += (size_t)blockIdx.y * L * Mp * Kp;
+    if (flags) flags += (size_t)blockIdx.y * (Mp / 128) * (Kp / 128);
     const int64_t total = (int64_t)Mp * (Kp / 4);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t m = (int32_t)(t / (Kp / 4));
+        const int32_t m = (int32_t)(t / (Kp / 4));  // row of this item
         const int32_t k = (int32_t)(t % (Kp / 4)) * 4;
         uint32_t v[4];
 #pragma unroll
@@ -376,10 +383,14 @@ __global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int32_
 }
 
 // transposing split: out[l][n][k] = byte l of B[k][n]
-__global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int32_t K, int32_t N,
-                             int32_t Np, int32_t Kp, int32_t L, uint8_t* __restrict__ out,
-                             uint8_t* flags, int32_t bn) {
+__global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB, int32_t K,
+                             int32_t N, int32_t Np, int32_t Kp, int32_t L,
+                             uint8_t* __restrict__ out, uint8_t* flags, int32_t bn) {
     __shared__ uint32_t tile[32][33];
+    // batch item blockIdx.z
+    B += (size_t)blockIdx.z * sB;
+    out += (size_t)blockIdx.z * L * Np * Kp;
+    if (flags) flags += (size_t)blockIdx.z * (Np / bn) * (Kp / 128);
     const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
     for (int r = ty; r < 32; r += 8) {
@@ -403,7 +414,10 @@ __global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int32_
 __global__ void __launch_bounds__(256)
 k_plain_submul(const uint32_t* __restrict__ A, int64_t lda, const uint32_t* __restrict__ B,
                int64_t ldb, uint32_t* D, int64_t ldd, int32_t M, int32_t N, int32_t K,
-               FieldMont f) {
+               int64_t strideA, int64_t strideB, int64_t strideD, FieldMont f) {
+    A += (size_t)blockIdx.z * strideA;
+    B += (size_t)blockIdx.z * strideB;
+    D += (size_t)blockIdx.z * strideD;
     __shared__ uint32_t sA[16][64 + 1];
     __shared__ uint32_t sB[16][64 + 1];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -527,32 +541,35 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     const int32_t Mp = (g.M + Cfg::BM - 1) / Cfg::BM * Cfg::BM;
     const int32_t Np = (g.N + Cfg::BN - 1) / Cfg::BN * Cfg::BN;
     const int32_t Kp = (g.K + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
-    uint8_t* Ap = planes;
-    uint8_t* Bp = planes + (size_t)L * Mp * Kp;
+    const int32_t nb = g.batch;
+    uint8_t* Ap = planes;                                    // [nb][L][Mp][Kp]
+    uint8_t* Bp = planes + (size_t)nb * L * Mp * Kp;         // [nb][L][Np][Kp]
     const int32_t nkb = Kp / Cfg::BK;
-    uint8_t* fa = Bp + (size_t)L * Np * Kp;                 // [Mp/128][nkb]
-    uint8_t* fb = fa + (size_t)(Mp / Cfg::BM) * nkb;         // [Np/BN][nkb]
-    const size_t flag_bytes = (size_t)(Mp / Cfg::BM + Np / Cfg::BN) * nkb;
+    uint8_t* fa = Bp + (size_t)nb * L * Np * Kp;             // [nb][Mp/128][nkb]
+    uint8_t* fb = fa + (size_t)nb * (Mp / Cfg::BM) * nkb;    // [nb][Np/BN][nkb]
+    const size_t flag_bytes = (size_t)nb * (Mp / Cfg::BM + Np / Cfg::BN) * nkb;
     if (cudaMemsetAsync(fa, 0, flag_bytes, s) != cudaSuccess) {
         set_error("tile flag clear failed");
         return GBGPU_ECUDA;
     }
     {
         const int64_t total = (int64_t)Mp * (Kp / 4);
-        const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
-        k_split_rows<<<grid, 256, 0, s>>>(g.A, g.lda, g.M, g.K, Mp, Kp, L, Ap, fa);
-        dim3 gb((Np + 31) / 32, (Kp + 31) / 32);
-        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.K, g.N, Np, Kp, L, Bp, fb, Cfg::BN);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256,
+                                                                       148 * 32 / nb + 1));
+        k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.M, g.K, Mp, Kp, L, Ap, fa);
+        dim3 gb((Np + 31) / 32, (Kp + 31) / 32, nb);
+        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.sB, g.K, g.N, Np, Kp, L, Bp, fb, Cfg::BN);
         *launches += 2;
     }
     CUtensorMap ma, mb;
-    int rc = make_map(&ma, Ap, Kp, (int64_t)L * Mp, Cfg::BK, Cfg::BM);
+    int rc = make_map(&ma, Ap, Kp, (int64_t)nb * L * Mp, Cfg::BK, Cfg::BM);
     if (rc) return rc;
-    rc = make_map(&mb, Bp, Kp, (int64_t)L * Np, Cfg::BK, Cfg::BN);
+    rc = make_map(&mb, Bp, Kp, (int64_t)nb * L * Np, Cfg::BK, Cfg::BN);
     if (rc) return rc;
     TcParams prm{};
     prm.D = g.D;
     prm.ldd = g.ldd;
+    prm.sD = g.sD;
     prm.M = g.M;
     prm.N = g.N;
     prm.Mp = Mp;
@@ -577,7 +594,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         set_error(std::string("tc smem attribute: ") + cudaGetErrorString(e));
         return GBGPU_ECUDA;
     }
-    dim3 grid(Np / Cfg::BN, Mp / Cfg::BM);
+    dim3 grid(Np / Cfg::BN, Mp / Cfg::BM, nb);
     GemmProfile* prof = gemm_profile();
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof) {
@@ -602,18 +619,23 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     return GBGPU_OK;
 }
 
-size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K) {
+size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K, int32_t batch) {
     const int L = limbs_for(p);
     const int BN = L == 1 ? 256 : (L == 2 ? 128 : 64);
     const size_t Mp = (size_t)(M + 127) / 128 * 128, Np = (size_t)(N + BN - 1) / BN * BN;
     const size_t Kp = (size_t)(K + 127) / 128 * 128;
-    const size_t flags = (Mp / 128 + Np / BN) * (Kp / 128);
-    return (size_t)L * (Mp + Np) * Kp + ((flags + 255) & ~(size_t)255);
+    const size_t nb = (size_t)(batch > 0 ? batch : 1);
+    const size_t flags = nb * (Mp / 128 + Np / BN) * (Kp / 128);
+    return nb * L * (Mp + Np) * Kp + ((flags + 255) & ~(size_t)255);
 }
 
 int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
               long long* launches) {
-    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return GBGPU_OK;
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.batch <= 0) return GBGPU_OK;
+    if (g.batch > 65535) {
+        set_error("tensor-core GEMM: batch too large");
+        return GBGPU_ERANGE;
+    }
     if ((g.p & 1u) == 0 || g.p < 3) {
         set_error("tensor-core path needs an odd prime");
         return GBGPU_EINVAL;
@@ -628,11 +650,12 @@ int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err
 }
 
 int plain_submul(const TcGemmArgs& g, cudaStream_t s, long long* launches) {
-    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return GBGPU_OK;
-    dim3 grid((g.N + 63) / 64, (g.M + 63) / 64);
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.batch <= 0) return GBGPU_OK;
+    dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);
     FieldMont f{};
     f.p = g.p;
-    k_plain_submul<<<grid, 256, 0, s>>>(g.A, g.lda, g.B, g.ldb, g.D, g.ldd, g.M, g.N, g.K, f);
+    k_plain_submul<<<grid, 256, 0, s>>>(g.A, g.lda, g.B, g.ldb, g.D, g.ldd, g.M, g.N, g.K, g.sA,
+                                        g.sB, g.sD, f);
     ++*launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -18,6 +18,10 @@ struct TcGemmArgs {
     int64_t ldb;
     uint32_t* D;        // M x N, row-major, residues, updated in place
     int64_t ldd;
+    // batched form: `batch` independent products, item z at A + z sA,
+    // B + z sB, D + z sD (element strides)
+    int32_t batch = 1;
+    int64_t sA = 0, sB = 0, sD = 0;
 };
 
 // Optional per-thread profiling of the tensor-core GEMM launches: CUDA events
@@ -32,7 +36,7 @@ void set_gemm_profile(GemmProfile* p);
 
 int limbs_for(uint32_t p);
 // bytes of device workspace the tensor-core path needs for the limb planes
-size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K);
+size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K, int32_t batch = 1);
 // tensor-core path (odd p); enqueues on s, *err receives GBGPU_ETIMEDOUT if a
 // bounded wait expired
 int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
