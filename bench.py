@@ -313,8 +313,11 @@ def main():
 
 
 def _e2e(lib, mat, args, device):
-    """Seconds per reduction through gbgpu_reduce (H2D from pinned host memory,
-    reduction, D2H of the answer), and the bytes moved each way per step."""
+    """Seconds per reduction through the public C ABI, host buffers in and out:
+    gbgpu_plan_create (H2D of the CSR from pinned host memory), gbgpu_plan_run,
+    gbgpu_plan_result_into (D2H of the answer into pinned host memory),
+    gbgpu_plan_destroy -- all inside the timed region, every step.  Returns
+    (seconds per step, H2D bytes per step, D2H bytes per step)."""
     import torch
     from gb_b200 import _lib
     ptr_h = torch.from_numpy(mat.row_ptr).pin_memory()
@@ -323,71 +326,38 @@ def _e2e(lib, mat, args, device):
     csr = _lib.Csr(mat.p, mat.laopt, mat.nr, mat.ncl, mat.ncr, ptr_h.data_ptr(),
                    cols_h.data_ptr(), vals_h.data_ptr())
     opt = _lib.Options(args.form, device, 1, 0, None)
-    steps = max(2, min(args.steps, 5))
-    out = _lib.Rows()
-    _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
-    lib.gbgpu_rows_free(C.byref(out))
+
+    def one(out_bufs):
+        h = C.c_void_p()
+        _lib.check(lib.gbgpu_plan_create(C.byref(csr), C.byref(opt), C.byref(h)))
+        try:
+            _lib.check(lib.gbgpu_plan_run(h))
+            npv, nnz = C.c_int32(), C.c_int64()
+            if out_bufs is None:
+                lib.gbgpu_plan_result_into(h, None, None, None, 0, 0, C.byref(npv), C.byref(nnz))
+                return int(npv.value), int(nnz.value)
+            rp, cc, vv = out_bufs
+            _lib.check(lib.gbgpu_plan_result_into(h, rp.data_ptr(), cc.data_ptr(), vv.data_ptr(),
+                                                  rp.numel(), cc.numel(), C.byref(npv),
+                                                  C.byref(nnz)))
+            return int(npv.value), int(nnz.value)
+        finally:
+            lib.gbgpu_plan_destroy(h)
+
+    npv, nnz = one(None)  # sizes of the answer
+    bufs = (torch.empty(npv + 1, dtype=torch.int64).pin_memory(),
+            torch.empty(max(nnz, 1), dtype=torch.int32).pin_memory(),
+            torch.empty(max(nnz, 1), dtype=torch.int32).pin_memory())
+    one(bufs)  # warm
     torch.cuda.synchronize()
+    steps = max(2, min(args.steps, 5))
     t0 = time.perf_counter()
-    d2h = 0
     for _ in range(steps):
-        out = _lib.Rows()
-        _lib.check(lib.gbgpu_reduce(C.byref(csr), C.byref(opt), C.byref(out)))
-        d2h = (out.np + 1) * 8 + out.nnz * 8
-        lib.gbgpu_rows_free(C.byref(out))
+        one(bufs)
     e2e_s = (time.perf_counter() - t0) / steps
     h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
+    d2h = (npv + 1) * 8 + nnz * 8
     return e2e_s, h2d, d2h
-
-
-def run_dense(args):
-    """Exact modular GEMM D <- (D - A B) mod p on n x n blocks with uniform
-    residues (the dense block workload): int8 tensor-core form and, for n <=
-    8192, the CUDA-core form.  Device-resident operands, CUDA events on the
-    default stream, median of the timed steps."""
-    import torch
-    from gb_b200 import _lib
-    lib = _lib.load()
-    n, p = args.n, args.p
-    L = 1 if p < 1 << 8 else 2 if p < 1 << 16 else 3 if p < 1 << 24 else 4
-    g = torch.Generator(device="cuda")
-    g.manual_seed(1)
-    mk = lambda: torch.randint(0, p, (n, n), device="cuda", dtype=torch.int64,
-                               generator=g).to(torch.int32)
-    A, B, D = mk(), mk(), mk()
-
-    def timed(form, steps):
-        opt = _lib.Options(form, 0, 1, 0, None)
-        for _ in range(max(args.warmup, 1)):
-            _lib.check(lib.gbgpu_dense_submul(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n,
-                                              D.data_ptr(), n, C.byref(opt)))
-        ts = []
-        for _ in range(steps):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            _lib.check(lib.gbgpu_dense_submul(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n,
-                                              D.data_ptr(), n, C.byref(opt)))
-            e.record()
-            torch.cuda.synchronize()
-            ts.append(s.elapsed_time(e))
-        return statistics.median(ts)
-
-    ms_t = timed(_lib.FORM_TENSOR, args.steps)
-    ops = 2.0 * n ** 3
-    int8_peak = INT8_PEAK_TOPS
-    line = {"metric": "exact modular GEMM throughput (D - A B mod p)", "value": ops / ms_t / 1e9,
-            "unit": "modular TOPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_t, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": f"u32 residues, {L} u8 limbs", "data": "synthetic",
-            "config": {"workload": f"dense GEMM n={n} p={p}", "limbs": L},
-            "roofline": {"bound": "tensor", "achieved": L * L * ops / ms_t / 1e9,
-                         "peak": int8_peak, "unit": "TOPS",
-                         "frac": L * L * ops / ms_t / 1e9 / int8_peak}}
-    if n <= 8192:
-        ms_p = timed(_lib.FORM_PLAIN, 1)
-        line["plain_ms"] = ms_p
-        line["tensor_speedup_vs_plain"] = ms_p / ms_t
-    print(json.dumps(line), flush=True)
 
 
 def _work_counters(plan) -> int:

@@ -67,7 +67,7 @@ EXPORTS = [
     "gbgpu_rows_free", "gbgpu_plan_create", "gbgpu_plan_run", "gbgpu_plan_result",
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
-    "gbgpu_dense_submul_noalloc",
+    "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into",
 ]
 
 _lib = None
@@ -91,6 +91,8 @@ def load(path: str = LIB_PATH):
     lib.gbgpu_plan_run.argtypes = [C.c_void_p]
     lib.gbgpu_plan_result.argtypes = [C.c_void_p, C.POINTER(Rows)]
     lib.gbgpu_plan_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    lib.gbgpu_plan_result_into.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_int64, C.c_int64, _PI32, _PI64]
     lib.gbgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.gbgpu_plan_destroy.restype = None
     lib.gbgpu_reduce_batch.argtypes = [C.c_int32, C.POINTER(Csr), C.POINTER(Options),

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -84,30 +85,39 @@ static int grid_for(int64_t n, int threads, int cap = 148 * 16) {
 }
 
 int device_init(int device, DeviceInfo* info) {
+    // properties are read once per device (cudaGetDeviceProperties is slow)
+    static std::mutex mu;
+    static DeviceInfo cache[64];
+    static bool known[64] = {};
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
         set_error("no CUDA device");
         return GBGPU_ENODEV;
     }
-    if (device < 0 || device >= n) {
+    if (device < 0 || device >= n || device >= 64) {
         set_error("device ordinal out of range");
         return GBGPU_ENODEV;
     }
     GB_CUDA(cudaSetDevice(device));
-    cudaDeviceProp prop;
-    GB_CUDA(cudaGetDeviceProperties(&prop, device));
-    if (prop.major != 10) {
-        set_error("libgbgpu is built for sm_100 (B200) only");
-        return GBGPU_ENODEV;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!known[device]) {
+        cudaDeviceProp prop;
+        GB_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major != 10) {
+            set_error("libgbgpu is built for sm_100 (B200) only");
+            return GBGPU_ENODEV;
+        }
+        cache[device].sms = prop.multiProcessorCount;
+        cache[device].smem_optin = (int)prop.sharedMemPerBlockOptin;
+        // keep freed blocks in the stream-ordered pool between reductions
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        known[device] = true;
     }
-    info->sms = prop.multiProcessorCount;
-    info->smem_optin = (int)prop.sharedMemPerBlockOptin;
-    // keep freed blocks in the stream-ordered pool between reductions
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
+    *info = cache[device];
     return GBGPU_OK;
 }
 
@@ -695,6 +705,31 @@ int plan_result(Plan* P, gbgpu_rows* out) {
     return GBGPU_OK;
 }
 
+// copy the answer into caller-provided host arrays (no allocation)
+int plan_result_into(Plan* P, int64_t* row_ptr, int32_t* cols, int32_t* vals, int64_t cap_rows,
+                     int64_t cap_nnz, int32_t* np, int64_t* nnz) {
+    GB_CUDA(cudaStreamSynchronize(P->stream));
+    *np = P->np;
+    *nnz = P->onnz;
+    if ((int64_t)P->np + 1 > cap_rows || P->onnz > cap_nnz) {
+        set_error("result buffers too small");
+        return GBGPU_ERANGE;
+    }
+    row_ptr[0] = 0;
+    if (P->np > 0) {
+        GB_CUDA(cudaMemcpyAsync(row_ptr, P->offs, sizeof(int64_t) * (P->np + 1),
+                                cudaMemcpyDeviceToHost, P->stream));
+        if (P->onnz > 0) {
+            GB_CUDA(cudaMemcpyAsync(cols, P->out_cols, sizeof(int32_t) * P->onnz,
+                                    cudaMemcpyDeviceToHost, P->stream));
+            GB_CUDA(cudaMemcpyAsync(vals, P->out_vals, sizeof(int32_t) * P->onnz,
+                                    cudaMemcpyDeviceToHost, P->stream));
+        }
+        GB_CUDA(cudaStreamSynchronize(P->stream));
+    }
+    return GBGPU_OK;
+}
+
 void plan_destroy(Plan* P) { delete P; }
 const gbgpu_stats& plan_stats(const Plan* P) { return P->stats; }
 
@@ -727,6 +762,14 @@ int gbgpu_plan_run(gbgpu_plan* plan) {
 int gbgpu_plan_result(gbgpu_plan* plan, gbgpu_rows* out) {
     if (!plan || !out) return GBGPU_EINVAL;
     return plan_result(plan->impl, out);
+}
+
+int gbgpu_plan_result_into(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, int32_t* vals,
+                           int64_t cap_rows, int64_t cap_nnz, int32_t* np, int64_t* nnz) {
+    if (!plan || !np || !nnz) return GBGPU_EINVAL;
+    if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
+    // NULL buffers with zero capacities query the sizes (GBGPU_ERANGE)
+    return plan_result_into(plan->impl, row_ptr, cols, vals, cap_rows, cap_nnz, np, nnz);
 }
 
 int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {

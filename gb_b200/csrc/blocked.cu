@@ -253,16 +253,130 @@ __global__ void k_compact_cols(int32_t n, const int32_t* __restrict__ flag,
 // ---------------------------------------------------------------------------
 // panel echelon
 
-// pending rows (nonzero, not yet pivots) whose lead lies in [j, j + bw) -> act;
-// min lead over all pending rows -> *min_lead
-__global__ void k_collect_panel(int32_t t, const int32_t* __restrict__ lead,
-                                const uint8_t* __restrict__ is_piv, int32_t j, int32_t bw,
-                                int32_t* act, int32_t* n_act, int32_t* min_lead) {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < t; r += gridDim.x * blockDim.x) {
-        const int32_t l = lead[r];
-        if (l < 0 || is_piv[r]) continue;
-        atomicMin(min_lead, l);
-        if (l >= j && l < j + bw) act[atomicAdd(n_act, 1)] = r;
+// pending rows: nonzero and not yet pivots
+__global__ void k_collect_pending(int32_t t, const int32_t* __restrict__ lead,
+                                  const uint8_t* __restrict__ is_piv, int32_t* pend,
+                                  int32_t* n_pend) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < t; r += gridDim.x * blockDim.x)
+        if (lead[r] >= 0 && !is_piv[r]) pend[atomicAdd(n_pend, 1)] = r;
+}
+
+// rows per lead column and per 128-column panel; a panel is "dirty" when
+// two pending rows share a lead in it
+__global__ void k_lead_hist(int32_t n, const int32_t* __restrict__ pend,
+                            const int32_t* __restrict__ lead, int32_t* hist, int32_t* pcnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t l = lead[pend[i]];
+        atomicAdd(&hist[l], 1);
+        atomicAdd(&pcnt[l / KB], 1);
+    }
+}
+__global__ void k_dirty_panels(int32_t n, const int32_t* __restrict__ pend,
+                               const int32_t* __restrict__ lead, const int32_t* __restrict__ hist,
+                               int32_t* pdirty) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t l = lead[pend[i]];
+        if (hist[l] > 1) pdirty[l / KB] = 1;
+    }
+}
+
+// rows of collision-free panels have leads of their own: they are pivots
+__global__ void k_claim_clean(int32_t n, const int32_t* __restrict__ pend,
+                              const int32_t* __restrict__ lead, const int32_t* __restrict__ pdirty,
+                              int32_t* piv_of_col, uint8_t* is_piv, int32_t* wflag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t r = pend[i], l = lead[r];
+        if (!pdirty[l / KB]) {
+            piv_of_col[l] = r;
+            is_piv[r] = 1;
+            wflag[l] = 1;
+        }
+    }
+}
+
+// pending rows of the selected dirty panels (dslot[p] >= 0) into their
+// panel's chunk (at most KB rows; the others stay pending)
+__global__ void k_bucket_dirty(int32_t n, const int32_t* __restrict__ pend,
+                               const int32_t* __restrict__ lead, const int32_t* __restrict__ dslot,
+                               int32_t* cursor, int32_t* chunk_rows) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t r = pend[i];
+        const int32_t d = dslot[lead[r] / KB];
+        if (d < 0) continue;
+        const int32_t slot = atomicAdd(&cursor[d], 1);
+        if (slot < KB) chunk_rows[d * KB + slot] = r;
+    }
+}
+
+// OldB[d][i][0, width) = Dp[chunk row i of d][j0, j0 + width), zero rows padded
+__global__ void k_gather_chunks(int32_t n_dirty, const int32_t* __restrict__ cursor,
+                                const int32_t* __restrict__ chunk_rows,
+                                const uint32_t* __restrict__ Dp, int64_t ld, int32_t j0,
+                                int32_t width, uint32_t* OldB, int64_t ldo) {
+    const int64_t per = (int64_t)KB * width;
+    const int64_t total = per * n_dirty;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = (int32_t)(t / per);
+        const int32_t i = (int32_t)((t % per) / width), col = (int32_t)(t % width);
+        const int32_t nd = min(cursor[d], KB);
+        OldB[((int64_t)d * KB + i) * ldo + col] =
+            i < nd ? Dp[(int64_t)chunk_rows[d * KB + i] * ld + j0 + col] : 0u;
+    }
+}
+
+__global__ void k_scatter_chunks(int32_t n_dirty, const int32_t* __restrict__ cursor,
+                                 const int32_t* __restrict__ chunk_rows,
+                                 const uint32_t* __restrict__ OutB, int64_t ldo, int32_t j0,
+                                 int32_t width, uint32_t* Dp, int64_t ld) {
+    const int64_t per = (int64_t)KB * width;
+    const int64_t total = per * n_dirty;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = (int32_t)(t / per);
+        const int32_t i = (int32_t)((t % per) / width), col = (int32_t)(t % width);
+        if (i < min(cursor[d], KB))
+            Dp[(int64_t)chunk_rows[d * KB + i] * ld + j0 + col] = OutB[((int64_t)d * KB + i) * ldo + col];
+    }
+}
+
+// the factorized pivots of every chunk
+__global__ void k_register_chunks(const int32_t* __restrict__ n_piv,
+                                  const int32_t* __restrict__ piv_pos,
+                                  const int32_t* __restrict__ piv_col,
+                                  const int32_t* __restrict__ chunk_rows, int32_t* piv_of_col,
+                                  uint8_t* is_piv, int32_t* wflag) {
+    const int d = blockIdx.x;
+    for (int k = threadIdx.x; k < n_piv[d]; k += blockDim.x) {
+        const int32_t row = chunk_rows[d * KB + piv_pos[d * KB + k]];
+        const int32_t col = piv_col[d * KB + k];
+        piv_of_col[col] = row;
+        is_piv[row] = 1;
+        wflag[col] = 1;
+    }
+}
+
+// scale row rows[i] by the inverse of its entry at column cols[i] (warp per row)
+template <class F>
+__global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
+                               const int32_t* __restrict__ cols, int32_t ncols, uint32_t* M,
+                               int64_t ld, F f) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < n; i += nwarps) {
+        uint32_t* row = M + (size_t)rows[i] * ld;
+        const int32_t c0 = cols[i];
+        const uint32_t lv = row[c0];
+        if (lv == 1u) continue;
+        const uint32_t inv = inverse_mod(lv, f.p);
+        __syncwarp();
+        for (int c = c0 + 1 + lane; c < ncols; c += 32) {
+            const uint32_t v = row[c];
+            if (v) row[c] = f.mulmod(v, inv);
+        }
+        __syncwarp();
+        if (lane == 0) row[c0] = 1u;
     }
 }
 
@@ -274,9 +388,18 @@ __global__ void k_collect_panel(int32_t t, const int32_t* __restrict__ lead,
 // increasing column order, and their count.
 template <class F>
 __global__ void __launch_bounds__(KB)
-k_panel_factor(const uint32_t* __restrict__ old, int64_t ldo, int32_t n, int32_t bw,
-               int32_t col0, uint32_t* neg_e, int32_t* piv_pos, int32_t* piv_col,
-               int32_t* n_piv, F f) {
+k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __restrict__ dpanel,
+               const int32_t* __restrict__ cursor, int32_t j0, int32_t ncr,
+               uint32_t* neg_e_b, int32_t* piv_pos_b, int32_t* piv_col_b, int32_t* n_piv_b, F f) {
+    // chunk blockIdx.x: panel dpanel[d], its rows start at column j0 of oldb
+    const int d = blockIdx.x;
+    const int32_t pj = dpanel[d] * KB;
+    const int32_t n = min(cursor[d], KB), bw = min(KB, ncr - pj), col0 = pj;
+    const uint32_t* old = oldb + (size_t)d * KB * ldo + (pj - j0);
+    uint32_t* neg_e = neg_e_b + (size_t)d * KB * KB;
+    int32_t* piv_pos = piv_pos_b + d * KB;
+    int32_t* piv_col = piv_col_b + d * KB;
+    int32_t* n_piv = n_piv_b + d;
     extern __shared__ uint32_t pf_smem[];
     uint32_t(*P)[KB + 1] = (uint32_t(*)[KB + 1])pf_smem;
     uint32_t(*E)[KB + 1] = (uint32_t(*)[KB + 1])(pf_smem + KB * (KB + 1));
@@ -334,68 +457,8 @@ k_panel_factor(const uint32_t* __restrict__ old, int64_t ldo, int32_t n, int32_t
     if (r == 0) *n_piv = k;
 }
 
-// claim round: claim[lead] = smallest candidate row with that lead
-__global__ void k_claim_rows(int32_t n, const int32_t* __restrict__ cand,
-                             const int32_t* __restrict__ lead, int32_t* claim) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        atomicMin(&claim[lead[cand[i]]], cand[i]);
-}
 
-// winners become pivots (piv_of_col, is_piv, wflag), the others are listed
-__global__ void k_claim_split(int32_t n, const int32_t* __restrict__ cand,
-                              const int32_t* __restrict__ lead, const int32_t* __restrict__ claim,
-                              int32_t* piv_of_col, uint8_t* is_piv, int32_t* wflag,
-                              int32_t* losers, int32_t* n_losers) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int32_t r = cand[i];
-        const int32_t c = lead[r];
-        if (claim[c] == r) {
-            piv_of_col[c] = r;
-            is_piv[r] = 1;
-            wflag[c] = 1;
-        } else {
-            losers[atomicAdd(n_losers, 1)] = r;
-        }
-    }
-}
 
-// scale each listed row by the inverse of its lead entry (warp per row)
-template <class F>
-__global__ void k_normalize_rows(int32_t n, const int32_t* __restrict__ list,
-                                 const int32_t* __restrict__ lead, int32_t ncols, uint32_t* M,
-                                 int64_t ld, F f) {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < n; i += nwarps) {
-        const int32_t r = list[i];
-        const int32_t c0 = lead[r];
-        uint32_t* row = M + (size_t)r * ld;
-        const uint32_t inv = inverse_mod(row[c0], f.p);
-        __syncwarp();
-        for (int c = c0 + 1 + lane; c < ncols; c += 32) {
-            const uint32_t v = row[c];
-            if (v) row[c] = f.mulmod(v, inv);
-        }
-        __syncwarp();
-        if (lane == 0) row[c0] = 1u;
-    }
-}
-
-// register the chunk's pivots: pivot k is chunk row piv_pos[k] = act[...]
-__global__ void k_register_pivots(const int32_t* __restrict__ n_piv,
-                                  const int32_t* __restrict__ piv_pos,
-                                  const int32_t* __restrict__ piv_col,
-                                  const int32_t* __restrict__ act, int32_t* piv_of_col,
-                                  uint8_t* is_piv, int32_t* prow_out) {
-    const int n = *n_piv;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int32_t row = act[piv_pos[k]];
-        piv_of_col[piv_col[k]] = row;
-        is_piv[row] = 1;
-        prow_out[k] = row;
-    }
-}
 
 // dst block b (NB x NB, leading dimension NB, block stride NB (NB + 1)) =
 // src block b (nb_b x nb_b at src + b stride_src, leading dimension lds),
@@ -676,157 +739,160 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
     }
     if (out->ms_event_schur) BL_CUDA(cudaEventRecord(out->ms_event_schur, s));
 
-    // ---- 2. echelon of D' = W[:, ncl:], 128-column panels left to right ------------
-    // Pending rows whose lead falls in the panel (at most KB at a time) are
-    // brought to echelon form inside the panel by k_panel_factor; the recorded
-    // transformation is applied to their whole trailing part with one GEMM.
-    // The pivots found are registered, the other rows of the chunk are zero in
-    // the panel and move on; pending rows of the panel outside the chunk are
-    // eliminated against the new pivots (eliminate) and stay pending.
+    // ---- 2. echelon of D' = W[:, ncl:] by rounds ----------------------------------
+    // Every round looks at all pending rows (nonzero, not yet pivots) at once:
+    //  * a 128-column panel in which no two pending rows share a lead is
+    //    "clean": each of its rows has a lead of its own and becomes a pivot;
+    //  * every other ("dirty") panel gets up to KB of its pending rows
+    //    factorized in shared memory (k_panel_factor, one CTA per panel); the
+    //    recorded row transformation E is applied to their trailing columns
+    //    by one batched GEMM over all dirty panels;
+    //  * the pending rows that did not become pivots are eliminated against
+    //    all pivots of the round (eliminate), which leaves them zero at every
+    //    pivot column, and the next round starts from their new leads.
     uint32_t* Dp = W + ncl;  // t x ncr, leading dimension ld
+    const int32_t npan = (ncr + KB - 1) / KB;
     int32_t* lead = c.alloc<int32_t>(t);
     uint8_t* is_piv = c.alloc<uint8_t>(t);
     int32_t* piv_of_col = out->piv_of_col;  // [ncr], -1 if none
     int32_t* wflag = c.alloc<int32_t>(ncr);
     int32_t* wpos = c.alloc<int32_t>(ncr);
-    int32_t* act = c.alloc<int32_t>(t);
+    int32_t* pend = c.alloc<int32_t>(t);
     int32_t* counters = c.alloc<int32_t>(8);
     int32_t* pc = c.alloc<int32_t>(ncr);      // pivot columns
     int32_t* prow = c.alloc<int32_t>(ncr);    // their rows
-    int32_t* piv_pos = c.alloc<int32_t>(KB);
-    uint32_t* negE = c.alloc<uint32_t>((size_t)KB * KB);
-    uint32_t* Old = c.alloc<uint32_t>((size_t)KB * ld);
-    uint32_t* Out = c.alloc<uint32_t>((size_t)KB * ld);
-    if (!lead || !is_piv || !wflag || !wpos || !act || !counters || !pc || !prow || !piv_pos ||
-        !negE || !Old || !Out)
+    int32_t* hist = c.alloc<int32_t>(ncr);
+    int32_t* pcnt = c.alloc<int32_t>(npan);
+    int32_t* pdirty = c.alloc<int32_t>(npan);
+    int32_t* dslot = c.alloc<int32_t>(npan);
+    int32_t* dpanel = c.alloc<int32_t>(npan);
+    if (!lead || !is_piv || !wflag || !wpos || !pend || !counters || !pc || !prow || !hist ||
+        !pcnt || !pdirty || !dslot || !dpanel)
         return GBGPU_ENOMEM;
     size_t scan_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, wflag, wpos, ncr, s);
     void* scan_tmp = c.alloc<uint8_t>(scan_bytes);
     if (!scan_tmp) return GBGPU_ENOMEM;
     BL_LAUNCH(k_fill_i32<<<grid_of(ncr), 256, 0, s>>>(piv_of_col, ncr, -1));
-    int32_t n_nonzero = 0;
     if (t > 0 && ncr > 0) {
         BL_CUDA(cudaMemsetAsync(is_piv, 0, t, s));
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)t * 32), 256, 0, s>>>(t, nullptr, ncr, Dp, ld, lead));
-        BL_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int32_t), s));
-        BL_LAUNCH(k_collect_nonzero<<<grid_of(t), 256, 0, s>>>(t, lead, act, counters));
-        BL_CUDA(cudaMemcpyAsync(&n_nonzero, counters, 4, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaStreamSynchronize(s));
     }
-    out->dense_rows = n_nonzero;
     const int pf_bytes = 2 * KB * (KB + 1) * (int)sizeof(uint32_t);
     BL_CUDA(cudaFuncSetAttribute(k_panel_factor<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  pf_bytes));
-    uint32_t* Ubuf = nullptr;   // gathered pivot rows / rest rows for eliminate
-    size_t ubuf_rows = 0;
-    int steps = 0;
-    // claim round: the first row of every distinct lead becomes a pivot (a
-    // row with a lead of its own is already a pivot of the echelon form);
-    // the other rows are eliminated against all of them at once and go on
-    // to the panels
-    if (n_nonzero > 0) {
-        int32_t* claim = c.alloc<int32_t>(ncr);
-        int32_t* losers = c.alloc<int32_t>(t);
-        if (!claim || !losers) return GBGPU_ENOMEM;
-        BL_LAUNCH(k_fill_i32<<<grid_of(ncr), 256, 0, s>>>(claim, ncr, INT_MAX));
+    const int32_t max_dirty = 64;  // dirty panels factorized per round (memory bound)
+    int32_t* chunk_rows = c.alloc<int32_t>((size_t)max_dirty * KB);
+    int32_t* cursor = c.alloc<int32_t>(max_dirty);
+    uint32_t* negEB = c.alloc<uint32_t>((size_t)max_dirty * KB * KB);
+    int32_t* piv_pos = c.alloc<int32_t>((size_t)max_dirty * KB);
+    int32_t* piv_colb = c.alloc<int32_t>((size_t)max_dirty * KB);
+    int32_t* n_piv = c.alloc<int32_t>(max_dirty);
+    if (!chunk_rows || !cursor || !negEB || !piv_pos || !piv_colb || !n_piv) return GBGPU_ENOMEM;
+    uint32_t* OldB = nullptr;
+    uint32_t* OutB = nullptr;
+    size_t chunk_cap = 0;  // elements of OldB / OutB
+    int rounds = 0;
+    bool first = true;
+    while (t > 0 && ncr > 0) {
+        int32_t n_pend = 0;
+        BL_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int32_t), s));
+        BL_LAUNCH(k_collect_pending<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, pend, counters));
+        BL_CUDA(cudaMemcpyAsync(&n_pend, counters, 4, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaStreamSynchronize(s));
+        if (first) out->dense_rows = n_pend;
+        first = false;
+        if (n_pend == 0) break;
+        ++rounds;
+        BL_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * ncr, s));
+        BL_CUDA(cudaMemsetAsync(pcnt, 0, sizeof(int32_t) * npan, s));
+        BL_CUDA(cudaMemsetAsync(pdirty, 0, sizeof(int32_t) * npan, s));
         BL_CUDA(cudaMemsetAsync(wflag, 0, sizeof(int32_t) * ncr, s));
-        BL_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(int32_t), s));
-        BL_LAUNCH(k_claim_rows<<<grid_of(n_nonzero), 256, 0, s>>>(n_nonzero, act, lead, claim));
-        BL_LAUNCH(k_claim_split<<<grid_of(n_nonzero), 256, 0, s>>>(
-            n_nonzero, act, lead, claim, piv_of_col, is_piv, wflag, losers, counters + 4));
+        BL_LAUNCH(k_lead_hist<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, hist, pcnt));
+        BL_LAUNCH(k_dirty_panels<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, hist, pdirty));
+        BL_LAUNCH(k_claim_clean<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, pdirty,
+                                                                 piv_of_col, is_piv, wflag));
+        // dirty panels, leftmost first, at most max_dirty of them this round
+        std::vector<int32_t> h_dirty(npan);
+        BL_CUDA(cudaMemcpyAsync(h_dirty.data(), pdirty, sizeof(int32_t) * npan,
+                                cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> h_dpanel, h_dslot(npan, -1);
+        for (int32_t p = 0; p < npan && (int32_t)h_dpanel.size() < max_dirty; ++p) {
+            if (h_dirty[p]) {
+                h_dslot[p] = (int32_t)h_dpanel.size();
+                h_dpanel.push_back(p);
+            }
+        }
+        const int32_t n_dirty = (int32_t)h_dpanel.size();
+        if (n_dirty > 0) {
+            const int32_t j0 = h_dpanel[0] * KB, width = ncr - j0;
+            const int64_t ldo = ((int64_t)width + 3) & ~(int64_t)3;
+            const size_t need = (size_t)n_dirty * KB * ldo;
+            if (need > chunk_cap) {
+                OldB = c.alloc<uint32_t>(need);
+                OutB = c.alloc<uint32_t>(need);
+                if (!OldB || !OutB) return GBGPU_ENOMEM;
+                chunk_cap = need;
+            }
+            BL_CUDA(cudaMemcpyAsync(dslot, h_dslot.data(), sizeof(int32_t) * npan,
+                                    cudaMemcpyHostToDevice, s));
+            BL_CUDA(cudaMemcpyAsync(dpanel, h_dpanel.data(), sizeof(int32_t) * n_dirty,
+                                    cudaMemcpyHostToDevice, s));
+            BL_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int32_t) * n_dirty, s));
+            BL_LAUNCH(k_bucket_dirty<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, dslot,
+                                                                      cursor, chunk_rows));
+            BL_LAUNCH(k_gather_chunks<<<grid_of((int64_t)n_dirty * KB * width), 256, 0, s>>>(
+                n_dirty, cursor, chunk_rows, Dp, ld, j0, width, OldB, ldo));
+            BL_LAUNCH(k_panel_factor<F><<<n_dirty, KB, pf_bytes, s>>>(
+                OldB, ldo, dpanel, cursor, j0, ncr, negEB, piv_pos, piv_colb, n_piv, f));
+            BL_CUDA(cudaMemsetAsync(OutB, 0, sizeof(uint32_t) * need, s));
+            // OutB[d] = E_d OldB[d] = 0 - (-E_d) OldB[d]
+            BL_CHECK(gemm_batched(c, OutB, ldo, (int64_t)KB * ldo, negEB, KB, (int64_t)KB * KB, OldB,
+                                  ldo, (int64_t)KB * ldo, KB, width, KB, n_dirty));
+            BL_LAUNCH(k_scatter_chunks<<<grid_of((int64_t)n_dirty * KB * width), 256, 0, s>>>(
+                n_dirty, cursor, chunk_rows, OutB, ldo, j0, width, Dp, ld));
+            BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
+                                                                piv_of_col, is_piv, wflag));
+        }
+        // all pivots of the round, ascending columns; normalise
         BL_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wflag, wpos, ncr, s));
         ++c.launches;
         BL_LAUNCH(k_compact_cols<<<grid_of(ncr), 256, 0, s>>>(ncr, wflag, wpos, pc));
-        int32_t n_lost = 0, last_pos = 0, last_flag = 0;
-        BL_CUDA(cudaMemcpyAsync(&n_lost, counters + 4, 4, cudaMemcpyDeviceToHost, s));
+        int32_t last_pos = 0, last_flag = 0;
         BL_CUDA(cudaMemcpyAsync(&last_pos, wpos + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaMemcpyAsync(&last_flag, wflag + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         const int32_t n_new = last_pos + last_flag;
         BL_LAUNCH(k_gather_rows<<<grid_of(n_new), 256, 0, s>>>(n_new, pc, piv_of_col, prow,
-                                                               counters + 5));
-        BL_LAUNCH(k_normalize_rows<F><<<grid_of((int64_t)n_new * 32), 256, 0, s>>>(
-            n_new, prow, lead, ncr, Dp, ld, f));
-        if (n_lost > 0) {
-            std::vector<int32_t> h_pc(n_new);
-            BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * n_new, cudaMemcpyDeviceToHost,
-                                    s));
-            uint32_t* Ucmp = c.alloc<uint32_t>((size_t)n_new * ld);
-            uint32_t* Tcmp = c.alloc<uint32_t>((size_t)n_lost * ld);
-            if (!Ucmp || !Tcmp) return GBGPU_ENOMEM;
-            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_new * ncr), 256, 0, s>>>(
-                n_new, prow, ncr, Dp, ld, Ucmp, ld));
-            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_lost * ncr), 256, 0, s>>>(
-                n_lost, losers, ncr, Dp, ld, Tcmp, ld));
-            BL_CUDA(cudaStreamSynchronize(s));
-            BL_CHECK(eliminate(c, f, Tcmp, ld, n_lost, ncr, Ucmp, ld, n_new, pc, h_pc));
-            BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_lost * ncr), 256, 0, s>>>(
-                n_lost, losers, ncr, Tcmp, ld, Dp, ld));
-            BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_lost * 32), 256, 0, s>>>(n_lost, losers, ncr,
-                                                                                 Dp, ld, lead));
-        }
-        ++steps;
-    }
-    int32_t j = 0;
-    while (n_nonzero > 0 && j < ncr) {
-        const int32_t bw = std::min(KB, ncr - j);
-        int32_t h[2] = {0, INT_MAX};  // n_act, min pending lead
-        BL_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(int32_t), s));
-        BL_LAUNCH(k_fill_i32<<<1, 1, 0, s>>>(counters + 2, 1, INT_MAX));
-        BL_LAUNCH(k_collect_panel<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, j, bw, act,
-                                                              counters + 1, counters + 2));
-        BL_CUDA(cudaMemcpyAsync(h, counters + 1, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+                                                               counters + 2));
+        BL_LAUNCH(k_normalize_at<F><<<grid_of((int64_t)n_new * 32), 256, 0, s>>>(
+            n_new, prow, pc, ncr, Dp, ld, f));
+        // the rest: eliminated against every pivot of the round
+        int32_t n_rest = 0;
+        BL_LAUNCH(k_collect_pending<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, pend,
+                                                                counters + 3));
+        BL_CUDA(cudaMemcpyAsync(&n_rest, counters + 3, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
-        if (h[1] == INT_MAX) break;  // nothing pending
-        if (h[0] == 0) {             // jump to the panel of the smallest pending lead
-            j = h[1] / KB * KB;
-            continue;
-        }
-        ++steps;
-        const int32_t n_act = h[0], n_chunk = std::min(KB, n_act);
-        const int32_t width = ncr - j;
-        // E * (chunk rows from column j) with E from the panel factorization
-        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_chunk * width), 256, 0, s>>>(
-            n_chunk, act, width, Dp + j, ld, Old, ld));
-        BL_LAUNCH(k_panel_factor<F><<<1, KB, pf_bytes, s>>>(Old, ld, n_chunk, bw, j, negE, piv_pos,
-                                                             pc, counters + 3, f));
-        BL_CUDA(cudaMemsetAsync(Out, 0, sizeof(uint32_t) * (size_t)n_chunk * ld, s));
-        BL_CHECK(gemm(c, Out, ld, negE, KB, Old, ld, n_chunk, width, n_chunk));
-        BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_chunk * width), 256, 0, s>>>(
-            n_chunk, act, width, Out, ld, Dp + j, ld));
-        BL_LAUNCH(k_register_pivots<<<1, KB, 0, s>>>(counters + 3, piv_pos, pc, act, piv_of_col,
-                                                     is_piv, prow));
-        BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_chunk * 32), 256, 0, s>>>(n_chunk, act, ncr, Dp,
-                                                                              ld, lead));
-        if (n_act > n_chunk) {
-            // the rest of the panel's pending rows: eliminate against the new pivots
-            int32_t k = 0;
-            BL_CUDA(cudaMemcpyAsync(&k, counters + 3, 4, cudaMemcpyDeviceToHost, s));
-            BL_CUDA(cudaStreamSynchronize(s));
-            const int32_t n_rest = n_act - n_chunk;
-            std::vector<int32_t> h_pc(k);
-            BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s));
-            if ((size_t)std::max(k, n_rest) > ubuf_rows) {
-                ubuf_rows = std::max<size_t>(std::max(k, n_rest), ubuf_rows * 2);
-                Ubuf = c.alloc<uint32_t>(ubuf_rows * ld * 2);
-                if (!Ubuf) return GBGPU_ENOMEM;
-            }
-            uint32_t* Ucmp = Ubuf;
-            uint32_t* Tcmp = Ubuf + ubuf_rows * ld;
-            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)k * ncr), 256, 0, s>>>(
-                k, prow, ncr, Dp, ld, Ucmp, ld));
-            BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
-                n_rest, act + n_chunk, ncr, Dp, ld, Tcmp, ld));
-            BL_CUDA(cudaStreamSynchronize(s));
-            BL_CHECK(eliminate(c, f, Tcmp, ld, n_rest, ncr, Ucmp, ld, k, pc, h_pc));
-            BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
-                n_rest, act + n_chunk, ncr, Tcmp, ld, Dp, ld));
-            BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_rest * 32), 256, 0, s>>>(
-                n_rest, act + n_chunk, ncr, Dp, ld, lead));
-        }
-        // stay on this panel until no pending lead is left in it
+        if (n_rest == 0) break;
+        std::vector<int32_t> h_pc(n_new);
+        BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * n_new, cudaMemcpyDeviceToHost, s));
+        uint32_t* Ucmp = c.alloc<uint32_t>((size_t)n_new * ld);
+        uint32_t* Tcmp = c.alloc<uint32_t>((size_t)n_rest * ld);
+        if (!Ucmp || !Tcmp) return GBGPU_ENOMEM;
+        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_new * ncr), 256, 0, s>>>(
+            n_new, prow, ncr, Dp, ld, Ucmp, ld));
+        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
+            n_rest, pend, ncr, Dp, ld, Tcmp, ld));
+        BL_CUDA(cudaStreamSynchronize(s));
+        BL_CHECK(eliminate(c, f, Tcmp, ld, n_rest, ncr, Ucmp, ld, n_new, pc, h_pc));
+        BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
+            n_rest, pend, ncr, Tcmp, ld, Dp, ld));
+        BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_rest * 32), 256, 0, s>>>(n_rest, pend, ncr, Dp,
+                                                                             ld, lead));
+        // Ucmp / Tcmp stay allocated until the reduction ends (stream-ordered)
     }
+    const int steps = rounds;
     out->echelon_rounds = steps;
     if (out->ms_event_echelon) BL_CUDA(cudaEventRecord(out->ms_event_echelon, s));
 

@@ -23,6 +23,8 @@ int device_init(int device, DeviceInfo* info);
 int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** out);
 int plan_run(Plan* P);
 int plan_result(Plan* P, gbgpu_rows* out);
+int plan_result_into(Plan* P, int64_t* row_ptr, int32_t* cols, int32_t* vals, int64_t cap_rows,
+                     int64_t cap_nnz, int32_t* np, int64_t* nnz);
 void plan_destroy(Plan* P);
 const gbgpu_stats& plan_stats(const Plan* P);
 

@@ -191,6 +191,13 @@ int gbgpu_plan_create(const gbgpu_csr *m, const gbgpu_options *opt,
 int gbgpu_plan_run(gbgpu_plan *plan);
 /* Block until the last run finished and copy its answer to host memory. */
 int gbgpu_plan_result(gbgpu_plan *plan, gbgpu_rows *out);
+/* Same into caller-provided host arrays (pinned memory makes the copy run at
+ * full PCIe speed): cap_rows >= np + 1 and cap_nnz >= nnz entries, else
+ * GBGPU_ERANGE with *np / *nnz set to the sizes needed (NULL arrays with zero
+ * capacities just query the sizes). */
+int gbgpu_plan_result_into(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
+                           int32_t *vals, int64_t cap_rows, int64_t cap_nnz,
+                           int32_t *np, int64_t *nnz);
 int gbgpu_plan_stats(const gbgpu_plan *plan, gbgpu_stats *stats);
 void gbgpu_plan_destroy(gbgpu_plan *plan);
 

@@ -195,3 +195,22 @@ def test_integration_recipe_build_matches_golden(case):
     assert lens.tolist() == exp["tlen"]
     assert cfs.tolist() == exp["tcf"]
     assert exps.tolist() == exp["texp"]
+
+
+def test_plan_result_into_caller_buffers():
+    m = synth.staircase(600, 150, 600, 32003, seed=4)
+    want, _ = oracle.oracle_la(m)
+    lib = _lib.load()
+    plan = la.Plan(m)
+    plan.run()
+    npv, nnz = C.c_int32(), C.c_int64()
+    rc = lib.gbgpu_plan_result_into(plan._h, None, None, None, 0, 0, C.byref(npv), C.byref(nnz))
+    assert rc == _lib.GBGPU_ERANGE and npv.value == want.np and nnz.value == want.nnz
+    rp = np.zeros(npv.value + 1, dtype=np.int64)
+    cols = np.zeros(nnz.value, dtype=np.int32)
+    vals = np.zeros(nnz.value, dtype=np.int32)
+    _lib.check(lib.gbgpu_plan_result_into(plan._h, rp.ctypes.data, cols.ctypes.data,
+                                          vals.ctypes.data, rp.shape[0], cols.shape[0],
+                                          C.byref(npv), C.byref(nnz)))
+    check_same(ReducedRows(rp, cols, vals), want)
+    plan.close()
