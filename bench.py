@@ -292,7 +292,8 @@ def main():
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": roof,
-        "stages_ms": {k: stats[k] for k in ("ms_schur", "ms_echelon", "ms_rref", "ms_compact")},
+        "stages_ms": {k: stats[k] for k in ("ms_classify", "ms_check", "ms_schur", "ms_echelon",
+                                             "ms_rref", "ms_compact")},
         "echelon_steps": stats["echelon_rounds"],
         "rank": answer.np, "out_nnz": answer.nnz, "wall_s_timed": wall,
         "verified_against_plain_form": verified,

@@ -48,7 +48,8 @@ class Stats(C.Structure):
                 ("echelon_rounds", C.c_int64), ("kernel_launches", C.c_int64),
                 ("work_schur", C.c_int64), ("work_dense", C.c_int64),
                 ("gemm_launches", C.c_int64), ("gemm_ms", C.c_double),
-                ("gemm_int8_ops", C.c_double), ("form_used", C.c_int64)]
+                ("gemm_int8_ops", C.c_double), ("form_used", C.c_int64),
+                ("ms_classify", C.c_double), ("ms_check", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -67,7 +68,7 @@ EXPORTS = [
     "gbgpu_rows_free", "gbgpu_plan_create", "gbgpu_plan_run", "gbgpu_plan_result",
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
-    "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into",
+    "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into", "gbgpu_dense_rref",
 ]
 
 _lib = None
@@ -105,6 +106,8 @@ def load(path: str = LIB_PATH):
     lib.gbgpu_dense_submul_noalloc.argtypes = [C.c_int32] * 4 + [
         C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
         C.c_void_p]
+    lib.gbgpu_dense_rref.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
+                                     _PI32, C.c_void_p, C.POINTER(Options)]
     lib.gbgpu_last_error.restype = C.c_char_p
     lib.gbgpu_kernel_launches.restype = C.c_int64
     _lib = lib

@@ -179,7 +179,7 @@ struct Plan {
     int64_t onnz = 0;
     uint32_t errbits = 0;
     gbgpu_stats stats{};
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[8] = {};
     long long launches = 0;
 
     template <class T>
@@ -341,8 +341,10 @@ static int run_form(Plan* P, const F& f) {
                                                             P->mode == 1));
     if (P->mode == 0)
         GB_LAUNCH(k_check_pivots<<<grid_for(P->ncl, T), T, 0, s>>>(P->ncl, P->piv_row, P->err));
+    GB_CUDA(cudaEventRecord(P->ev[6], s));
     GB_CUDA(cudaMemcpyAsync(&P->errbits, P->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
+    GB_CUDA(cudaEventRecord(P->ev[7], s));
     if (P->errbits) {
         std::string msg;
         int rc = err_to_status(P->errbits, &msg);
@@ -618,6 +620,11 @@ int plan_run(Plan* P) {
     P->stats.ms_echelon = ms[2];
     P->stats.ms_rref = ms[3];
     P->stats.ms_compact = ms[4];
+    float mc = 0, mv = 0;
+    cudaEventElapsedTime(&mc, P->ev[0], P->ev[1]);
+    cudaEventElapsedTime(&mv, P->ev[0], P->ev[6]);
+    P->stats.ms_classify = mc;
+    P->stats.ms_check = mv;
     P->stats.rows_reduced = P->n_work;
     P->stats.rank = P->np;
     P->stats.kernel_launches = P->launches;

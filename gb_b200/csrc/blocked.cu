@@ -154,19 +154,23 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
     }
     __syncthreads();
     const int j = threadIdx.x;
-    // V[., j] solves U x = e_j; V[i][j] = -sum_{i<k<=j} U[i][k] V[k][j]
+    // V[., j] solves U x = e_j; V[i][j] = -sum_{i<k<=j} U[i][k] V[k][j].
+    // The sum is accumulated without reduction: V is split into 16-bit
+    // halves, so each of the at most 128 products is < 2^47 and both partial
+    // sums stay below 2^54; one reduction per entry.
     V[j][j] = 1u;
     for (int i = KB - 1; i > j; --i) V[i][j] = 0u;
+    const uint64_t p = f.p;
     for (int i = j - 1; i >= 0; --i) {
-        uint32_t acc = 0;
+        uint64_t lo = 0, hi = 0;
         for (int k = i + 1; k <= j; ++k) {
-            const uint32_t u = U[i][k];
-            if (u) {
-                const uint32_t t = f.mulmod(u, V[k][j]);
-                acc = acc + t >= f.p ? acc + t - f.p : acc + t;
-            }
+            const uint64_t u = U[i][k];
+            const uint32_t v = V[k][j];
+            lo += u * (v & 0xFFFFu);
+            hi += u * (v >> 16);
         }
-        V[i][j] = acc ? f.p - acc : 0u;
+        const uint64_t acc = (lo % p + ((hi % p) << 16) % p) % p;
+        V[i][j] = acc ? (uint32_t)(p - acc) : 0u;
     }
     __syncthreads();
     uint32_t* o = out + (size_t)b * ostride;
@@ -216,9 +220,12 @@ __global__ void k_scatter_rows_dense(int32_t nrows, const int32_t* __restrict__ 
     }
 }
 
-// first nonzero column of every row (-1 for zero rows), one warp per row
+// first nonzero column of every row (-1 for zero rows), one warp per row;
+// with from_prev the scan starts at the row's current lead (leads only move
+// right under elimination)
 __global__ void k_row_leads(int32_t rows, const int32_t* __restrict__ list, int32_t ncols,
-                            const uint32_t* __restrict__ M, int64_t ld, int32_t* lead) {
+                            const uint32_t* __restrict__ M, int64_t ld, int32_t* lead,
+                            int32_t from_prev = 0) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -226,7 +233,8 @@ __global__ void k_row_leads(int32_t rows, const int32_t* __restrict__ list, int3
         const int32_t r = list ? list[i] : i;
         const uint32_t* row = M + (size_t)r * ld;
         int found = -1;
-        for (int base = 0; base < ncols; base += 32) {
+        const int start = from_prev && lead[r] > 0 ? lead[r] : 0;
+        for (int base = start; base < ncols; base += 32) {
             const int c = base + lane;
             const unsigned bal = __ballot_sync(0xffffffffu, c < ncols && row[c] != 0u);
             if (bal) {
@@ -386,8 +394,10 @@ __global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
 // the rows that are not pivots become zero in the panel).  Writes -E
 // (n x n, ld KB), the panel-local index and column of every pivot, in
 // increasing column order, and their count.
+constexpr int PF_GROUPS = 4;  // threads per row in k_panel_factor
+
 template <class F>
-__global__ void __launch_bounds__(KB)
+__global__ void __launch_bounds__(KB * PF_GROUPS)
 k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __restrict__ dpanel,
                const int32_t* __restrict__ cursor, int32_t j0, int32_t ncr,
                uint32_t* neg_e_b, int32_t* piv_pos_b, int32_t* piv_col_b, int32_t* n_piv_b, F f) {
@@ -403,23 +413,24 @@ k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __
     extern __shared__ uint32_t pf_smem[];
     uint32_t(*P)[KB + 1] = (uint32_t(*)[KB + 1])pf_smem;
     uint32_t(*E)[KB + 1] = (uint32_t(*)[KB + 1])(pf_smem + KB * (KB + 1));
-    __shared__ int s_scratch[KB / 32];
+    __shared__ int s_scratch[KB * PF_GROUPS / 32];
     __shared__ uint8_t is_piv[KB];
     __shared__ uint32_t s_inv;
-    const int r = threadIdx.x;
-    for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int r = tid % KB, g = tid / KB;  // row and column group of this thread
+    for (int t = tid; t < KB * KB; t += nt) {
         const int i = t / KB, c = t % KB;
         P[i][c] = (i < n && c < bw) ? old[(size_t)i * ldo + c] : 0u;
         E[i][c] = i == c ? 1u : 0u;
     }
-    is_piv[r] = 0;
+    if (tid < KB) is_piv[tid] = 0;
     __syncthreads();
     int k = 0;
     for (int c = 0; c < bw; ++c) {
-        const int cand = (r < n && !is_piv[r] && P[r][c] != 0u) ? r : INT_MAX;
+        const int cand = (g == 0 && r < n && !is_piv[r] && P[r][c] != 0u) ? r : INT_MAX;
         const int i = block_min(cand, s_scratch);
         if (i == INT_MAX) continue;
-        if (r == 0) {
+        if (tid == 0) {
             s_inv = inverse_mod(P[i][c], f.p);
             piv_pos[k] = i;
             piv_col[k] = col0 + c;
@@ -428,33 +439,34 @@ k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __
         __syncthreads();
         const uint32_t inv = s_inv;
         // scale the pivot row (panel part from c, transform part)
-        for (int cc = c + r; cc < bw; cc += blockDim.x) P[i][cc] = f.mulmod(P[i][cc], inv);
-        for (int cc = r; cc < n; cc += blockDim.x) E[i][cc] = f.mulmod(E[i][cc], inv);
+        for (int cc = c + tid; cc < bw; cc += nt) P[i][cc] = f.mulmod(P[i][cc], inv);
+        for (int cc = tid; cc < n; cc += nt) E[i][cc] = f.mulmod(E[i][cc], inv);
         __syncthreads();
-        // eliminate column c from every other non-pivot row
-        if (r < n && r != i && !is_piv[r]) {
-            const uint32_t m = P[r][c];
-            if (m != 0u) {
-                const uint32_t mp = f.prep(m);
-                for (int cc = c; cc < bw; ++cc) {
-                    const uint32_t v = P[i][cc];
-                    if (v) P[r][cc] = f.mulsub(P[r][cc], mp, v);
-                }
-                for (int cc = 0; cc < n; ++cc) {
-                    const uint32_t v = E[i][cc];
-                    if (v) E[r][cc] = f.mulsub(E[r][cc], mp, v);
-                }
+        // eliminate column c from every other non-pivot row: the four threads
+        // of a row read its multiplier before any of them writes the row
+        const bool active = r < n && r != i && !is_piv[r];
+        const uint32_t m = active ? P[r][c] : 0u;
+        __syncthreads();
+        if (m != 0u) {
+            const uint32_t mp = f.prep(m);
+            for (int cc = c + g; cc < bw; cc += PF_GROUPS) {
+                const uint32_t v = P[i][cc];
+                if (v) P[r][cc] = f.mulsub(P[r][cc], mp, v);
+            }
+            for (int cc = g; cc < n; cc += PF_GROUPS) {
+                const uint32_t v = E[i][cc];
+                if (v) E[r][cc] = f.mulsub(E[r][cc], mp, v);
             }
         }
         __syncthreads();
         ++k;
     }
-    for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
-        const int i = t / KB, cc = t % KB;
-        const uint32_t v = (i < n && cc < n) ? E[i][cc] : 0u;
+    for (int t = tid; t < KB * KB; t += nt) {
+        const int ii = t / KB, cc = t % KB;
+        const uint32_t v = (ii < n && cc < n) ? E[ii][cc] : 0u;
         neg_e[t] = v ? f.p - v : 0u;
     }
-    if (r == 0) *n_piv = k;
+    if (tid == 0) *n_piv = k;
 }
 
 
@@ -665,6 +677,10 @@ static int eliminate(Ctx& c, const F& f, uint32_t* T, int64_t ldt, int32_t rows,
 
 // ---------------------------------------------------------------------------
 template <class F>
+static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t, int32_t ncr,
+                        BlockedOutput* out);
+
+template <class F>
 static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const F& f) {
     const int32_t ncl = in.ncl, ncr = in.ncr, nc = ncl + ncr, t = in.n_work;
     const int64_t ld = ((int64_t)nc + 3) & ~(int64_t)3;
@@ -738,7 +754,20 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         BL_CHECK(gemm(c, W + ncl, ld, W, ld, P + ncl, ld, t, ncr, ncl));
     }
     if (out->ms_event_schur) BL_CUDA(cudaEventRecord(out->ms_event_schur, s));
+    BL_CHECK(echelon_rref(c, f, W + ncl, ld, t, ncr, out));
+    out->rows = W + ncl;
+    out->ld = ld;
+    return GBGPU_OK;
+}
 
+// Steps 2 and 3 on the dense t x ncr residue matrix Dp (leading dimension
+// ld), in place: afterwards out->piv_of_col[c] is the row of Dp holding the
+// reduced pivot row of column c (-1 for non-pivot columns), out->rank is the
+// rank, and every other row's content is unspecified.
+template <class F>
+static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t, int32_t ncr,
+                        BlockedOutput* out) {
+    cudaStream_t s = c.s;
     // ---- 2. echelon of D' = W[:, ncl:] by rounds ----------------------------------
     // Every round looks at all pending rows (nonzero, not yet pivots) at once:
     //  * a 128-column panel in which no two pending rows share a lead is
@@ -750,7 +779,6 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
     //  * the pending rows that did not become pivots are eliminated against
     //    all pivots of the round (eliminate), which leaves them zero at every
     //    pivot column, and the next round starts from their new leads.
-    uint32_t* Dp = W + ncl;  // t x ncr, leading dimension ld
     const int32_t npan = (ncr + KB - 1) / KB;
     int32_t* lead = c.alloc<int32_t>(t);
     uint8_t* is_piv = c.alloc<uint8_t>(t);
@@ -844,7 +872,7 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
                                                                       cursor, chunk_rows));
             BL_LAUNCH(k_gather_chunks<<<grid_of((int64_t)n_dirty * KB * width), 256, 0, s>>>(
                 n_dirty, cursor, chunk_rows, Dp, ld, j0, width, OldB, ldo));
-            BL_LAUNCH(k_panel_factor<F><<<n_dirty, KB, pf_bytes, s>>>(
+            BL_LAUNCH(k_panel_factor<F><<<n_dirty, KB * PF_GROUPS, pf_bytes, s>>>(
                 OldB, ldo, dpanel, cursor, j0, ncr, negEB, piv_pos, piv_colb, n_piv, f));
             BL_CUDA(cudaMemsetAsync(OutB, 0, sizeof(uint32_t) * need, s));
             // OutB[d] = E_d OldB[d] = 0 - (-E_d) OldB[d]
@@ -889,7 +917,7 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
             n_rest, pend, ncr, Tcmp, ld, Dp, ld));
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_rest * 32), 256, 0, s>>>(n_rest, pend, ncr, Dp,
-                                                                             ld, lead));
+                                                                             ld, lead, 1));
         // Ucmp / Tcmp stay allocated until the reduction ends (stream-ordered)
     }
     const int steps = rounds;
@@ -957,8 +985,6 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)r * ncr), 256, 0, s>>>(r, prow, ncr, E,
                                                                                  ld, Dp, ld));
     }
-    out->rows = Dp;
-    out->ld = ld;
     return GBGPU_OK;
 }
 
@@ -976,6 +1002,67 @@ int blocked_reduce(const BlockedInput& in, BlockedOutput* out, long long* launch
     *launches += c.launches;
     out->keep = new std::vector<void*>(c.tmp);
     if (c.ws) out->keep->push_back(c.ws);
+    return rc;
+}
+
+// dst row i = src row order[i] (all ncols), rows >= n zeroed up to `rows`
+__global__ void k_order_rows(int32_t n, int32_t rows, const int32_t* __restrict__ order,
+                             int32_t ncols, const uint32_t* __restrict__ src, int64_t lds,
+                             uint32_t* dst, int64_t ldd) {
+    const int64_t total = (int64_t)rows * ncols;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / ncols;
+        const int j = (int)(t % ncols);
+        dst[i * ldd + j] = i < n ? src[(int64_t)order[i] * lds + j] : 0u;
+    }
+}
+
+template <class F>
+static int dense_rref_run(const DenseRrefInput& in, int32_t* rank, Ctx& c, const F& f) {
+    BlockedOutput out{};
+    int32_t* piv_of_col = c.alloc<int32_t>(in.cols);
+    if (!piv_of_col) return GBGPU_ENOMEM;
+    out.piv_of_col = piv_of_col;
+    BL_CHECK(echelon_rref(c, f, in.D, in.ld, in.rows, in.cols, &out));
+    const int32_t r = (int32_t)out.rank;
+    *rank = r;
+    // pivot rows in ascending pivot order into the first r rows, zeros after
+    int32_t* flag = c.alloc<int32_t>(in.cols);
+    int32_t* pos = c.alloc<int32_t>(in.cols);
+    int32_t* order = c.alloc<int32_t>(std::max(r, 1));
+    int32_t* cnt = c.alloc<int32_t>(1);
+    uint32_t* tmp = c.alloc<uint32_t>((size_t)in.rows * in.ld);
+    if (!flag || !pos || !order || !cnt || !tmp) return GBGPU_ENOMEM;
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag, pos, in.cols, c.s);
+    void* scan_tmp = c.alloc<uint8_t>(bytes);
+    if (!scan_tmp) return GBGPU_ENOMEM;
+    BL_LAUNCH(k_pivot_flags<<<grid_of(in.cols), 256, 0, c.s>>>(in.cols, piv_of_col, 0, flag));
+    BL_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, flag, pos, in.cols, c.s));
+    BL_LAUNCH(k_compact_cols<<<grid_of(in.cols), 256, 0, c.s>>>(in.cols, flag, pos, in.piv_cols));
+    if (r > 0)
+        BL_LAUNCH(k_gather_rows<<<grid_of(r), 256, 0, c.s>>>(r, in.piv_cols, piv_of_col, order, cnt));
+    BL_LAUNCH(k_order_rows<<<grid_of((int64_t)in.rows * in.cols), 256, 0, c.s>>>(
+        r, in.rows, order, in.cols, in.D, in.ld, tmp, in.ld));
+    BL_CUDA(cudaMemcpy2DAsync(in.D, in.ld * 4, tmp, in.ld * 4, (size_t)in.cols * 4, in.rows,
+                              cudaMemcpyDeviceToDevice, c.s));
+    return GBGPU_OK;
+}
+
+int dense_rref(const DenseRrefInput& in, int32_t* rank, long long* launches) {
+    Ctx c;
+    c.s = in.stream;
+    c.p = in.p;
+    c.form = in.form;
+    c.err = in.err;
+    int rc;
+    if (in.p < 65536u)
+        rc = dense_rref_run(in, rank, c, FieldSmall::make(in.p));
+    else
+        rc = dense_rref_run(in, rank, c, FieldMont::make(in.p));
+    *launches += c.launches;
+    c.release();
     return rc;
 }
 

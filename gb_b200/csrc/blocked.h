@@ -31,6 +31,19 @@ struct BlockedOutput {
 };
 
 int blocked_reduce(const BlockedInput& in, BlockedOutput* out, long long* launches);
+
+// reduced row echelon form of a dense residue matrix, in place (device memory)
+struct DenseRrefInput {
+    uint32_t p;
+    int32_t rows, cols;
+    uint32_t* D;        // rows x cols, leading dimension ld
+    int64_t ld;
+    int32_t* piv_cols;  // device, >= min(rows, cols) entries: the pivot columns
+    cudaStream_t stream;
+    int form;
+    int32_t* err;
+};
+int dense_rref(const DenseRrefInput& in, int32_t* rank, long long* launches);
 void blocked_release(BlockedOutput* out, cudaStream_t s);
 
 }  // namespace gbgpu

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "../../include/gbgpu.h"
+#include "blocked.h"
 #include "internal.h"
 #include "tc_gemm.h"
 
@@ -124,6 +125,45 @@ int gbgpu_dense_submul_host(int32_t p, int32_t M, int32_t N, int32_t K, const ui
     if (!rc && e != cudaSuccess) {
         set_error(std::string("dense GEMM copy: ") + cudaGetErrorString(e));
         rc = GBGPU_ECUDA;
+    }
+    return rc;
+}
+
+int gbgpu_dense_rref(int32_t p, int32_t rows, int32_t cols, uint32_t* D, int64_t ld,
+                     int32_t* rank, int32_t* piv_cols, const gbgpu_options* opt) {
+    if (p < 2 || rows < 0 || cols < 0 || ld < cols || !rank || (rows > 0 && cols > 0 && (!D || !piv_cols))) {
+        set_error("bad dense RREF arguments");
+        return GBGPU_EINVAL;
+    }
+    *rank = 0;
+    DeviceInfo dev;
+    int rc = device_init(opt ? opt->device : 0, &dev);
+    if (rc) return rc;
+    if (rows == 0 || cols == 0) return GBGPU_OK;
+    cudaStream_t s = opt ? (cudaStream_t)opt->stream : nullptr;
+    int32_t* err = nullptr;
+    if (cudaMallocAsync((void**)&err, sizeof(int32_t), s) != cudaSuccess) return GBGPU_ENOMEM;
+    cudaMemsetAsync(err, 0, sizeof(int32_t), s);
+    const int form = opt ? opt->form : GBGPU_FORM_AUTO;
+    DenseRrefInput in{(uint32_t)p, rows, cols, D, ld, piv_cols, s,
+                      (form == GBGPU_FORM_PLAIN || form == GBGPU_FORM_BLOCKED_PLAIN || !(p & 1) || p < 3)
+                          ? GBGPU_FORM_PLAIN
+                          : GBGPU_FORM_TENSOR,
+                      err};
+    long long launches = 0;
+    rc = dense_rref(in, rank, &launches);
+    count_launch(launches);
+    int32_t herr = 0;
+    cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(err, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) {
+        set_error(std::string("dense RREF: ") + cudaGetErrorString(e));
+        rc = GBGPU_ECUDA;
+    }
+    if (!rc && herr) {
+        set_error("dense RREF: a bounded wait expired");
+        rc = herr;
     }
     return rc;
 }

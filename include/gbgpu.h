@@ -165,6 +165,8 @@ typedef struct gbgpu_stats {
     double gemm_int8_ops;   /* int8 tensor ops they executed (2 per MAC, all
                                limb products, zero tiles skipped)           */
     int64_t form_used;      /* GBGPU_FORM_PLAIN / _TENSOR / _BLOCKED_PLAIN   */
+    double ms_classify;     /* input checks, known pivots, C|D row list      */
+    double ms_check;        /* the device-side input checks alone            */
 } gbgpu_stats;
 
 /* One-shot: host CSR in, host rows out (H2D, reduction, D2H). */
@@ -227,6 +229,19 @@ int gbgpu_dense_submul_host(int32_t p, int32_t M, int32_t N, int32_t K,
                             const uint32_t *A, int64_t lda, const uint32_t *B,
                             int64_t ldb, uint32_t *D, int64_t ldd,
                             const gbgpu_options *opt);
+
+/* Reduced row echelon form of a dense residue matrix (rows x cols, row-major,
+ * device memory, leading dimension ld >= cols), in place: on return the
+ * first *rank rows are the reduced rows in ascending pivot-column order
+ * (lead 1, zero at every other pivot column), the remaining rows are zero,
+ * and piv_cols[0 .. *rank) (device memory, min(rows, cols) entries) holds the
+ * pivot columns.  This is the dense echelon + interreduction of the D block
+ * (src/la_ff_16.c:873-989 and :837-871) run blockwise: claiming rounds,
+ * shared-memory panel factorizations and tensor-core GEMMs for the updates
+ * (GBGPU_FORM_PLAIN: CUDA-core GEMMs). */
+int gbgpu_dense_rref(int32_t p, int32_t rows, int32_t cols, uint32_t *D,
+                     int64_t ld, int32_t *rank, int32_t *piv_cols,
+                     const gbgpu_options *opt);
 
 /* Allocation-free variant of gbgpu_dense_submul (tensor-core form, odd p):
  * for callers that may not call cudaMalloc / cudaFree once they run (inside

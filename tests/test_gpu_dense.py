@@ -85,3 +85,51 @@ def test_dense_submul_rejects_bad_arguments():
     rc = lib.gbgpu_dense_submul_host(101, 2, 2, 4, buf.ctypes.data, 2, buf.ctypes.data, 2,
                                      buf.ctypes.data, 2, C.byref(opt))
     assert rc == _lib.GBGPU_EINVAL  # lda < K
+
+
+def cpu_rref(D, p):
+    """Reduced row echelon form over GF(p) (numpy int64, exact)."""
+    A = np.array(D, dtype=np.int64) % p
+    rows, cols = A.shape
+    r = 0
+    piv = []
+    for c in range(cols):
+        nz = np.nonzero(A[r:, c])[0]
+        if nz.size == 0:
+            continue
+        i = r + nz[0]
+        A[[r, i]] = A[[i, r]]
+        inv = pow(int(A[r, c]), p - 2, p)
+        A[r] = (A[r] * inv) % p
+        others = np.nonzero(A[:, c])[0]
+        for o in others:
+            if o != r:
+                A[o] = (A[o] - A[o, c] * A[r]) % p
+        piv.append(c)
+        r += 1
+        if r == rows:
+            break
+    return A[:r].astype(np.uint32), piv
+
+
+@pytest.mark.parametrize("p,rows,cols,rank", [
+    (251, 200, 260, 120), (65521, 300, 300, 300), (65521, 520, 300, 170),
+    (2147483647, 260, 400, 200), (3, 150, 200, 60), (1000003, 129, 1030, 100)])
+@pytest.mark.parametrize("form", [_lib.FORM_TENSOR, _lib.FORM_PLAIN])
+def test_dense_rref_exact(form, p, rows, cols, rank):
+    torch = pytest.importorskip("torch")
+    from gb_b200 import synth
+    D = synth.dense_lowrank(rows, cols, rank, p, seed=rows + cols)
+    want, piv = cpu_rref(D, p)
+    lib = _lib.load()
+    dev = torch.from_numpy(D.astype(np.uint32).view(np.int32)).cuda()
+    pc = torch.zeros(min(rows, cols), dtype=torch.int32, device="cuda")
+    rk = C.c_int32()
+    opt = _lib.Options(form, 0, 1, 0, None)
+    _lib.check(lib.gbgpu_dense_rref(p, rows, cols, dev.data_ptr(), cols, C.byref(rk),
+                                    pc.data_ptr(), C.byref(opt)))
+    got = dev.cpu().numpy().view(np.uint32)
+    assert rk.value == len(piv)
+    assert pc.cpu().numpy()[: rk.value].tolist() == piv
+    assert np.array_equal(got[: rk.value], want)
+    assert not got[rk.value:].any()
