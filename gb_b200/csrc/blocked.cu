@@ -181,16 +181,17 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
     }
 }
 
-// dst[i][j] = src[i][cols[j]]
+// dst[i][j] = src[r_i][cols[j]], r_i = rlist[i] (i without a list)
 __global__ void k_gather_cols(int32_t rows, int32_t n, const uint32_t* __restrict__ src,
                               int64_t lds, const int32_t* __restrict__ cols, uint32_t* dst,
-                              int64_t ldd) {
+                              int64_t ldd, const int32_t* __restrict__ rlist = nullptr) {
     const int64_t total = (int64_t)rows * n;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = t / n;
         const int j = (int)(t % n);
-        dst[i * ldd + j] = src[i * lds + cols[j]];
+        const int64_t r = rlist ? (int64_t)rlist[i] : i;
+        dst[i * ldd + j] = src[r * lds + cols[j]];
     }
 }
 
@@ -316,38 +317,6 @@ __global__ void k_bucket_dirty(int32_t n, const int32_t* __restrict__ pend,
     }
 }
 
-// OldB[d][i][0, width) = Dp[chunk row i of d][j0, j0 + width), zero rows padded
-__global__ void k_gather_chunks(int32_t n_dirty, const int32_t* __restrict__ cursor,
-                                const int32_t* __restrict__ chunk_rows,
-                                const uint32_t* __restrict__ Dp, int64_t ld, int32_t j0,
-                                int32_t width, uint32_t* OldB, int64_t ldo) {
-    const int64_t per = (int64_t)KB * width;
-    const int64_t total = per * n_dirty;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t d = (int32_t)(t / per);
-        const int32_t i = (int32_t)((t % per) / width), col = (int32_t)(t % width);
-        const int32_t nd = min(cursor[d], KB);
-        OldB[((int64_t)d * KB + i) * ldo + col] =
-            i < nd ? Dp[(int64_t)chunk_rows[d * KB + i] * ld + j0 + col] : 0u;
-    }
-}
-
-__global__ void k_scatter_chunks(int32_t n_dirty, const int32_t* __restrict__ cursor,
-                                 const int32_t* __restrict__ chunk_rows,
-                                 const uint32_t* __restrict__ OutB, int64_t ldo, int32_t j0,
-                                 int32_t width, uint32_t* Dp, int64_t ld) {
-    const int64_t per = (int64_t)KB * width;
-    const int64_t total = per * n_dirty;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t d = (int32_t)(t / per);
-        const int32_t i = (int32_t)((t % per) / width), col = (int32_t)(t % width);
-        if (i < min(cursor[d], KB))
-            Dp[(int64_t)chunk_rows[d * KB + i] * ld + j0 + col] = OutB[((int64_t)d * KB + i) * ldo + col];
-    }
-}
-
 // the factorized pivots of every chunk
 __global__ void k_register_chunks(const int32_t* __restrict__ n_piv,
                                   const int32_t* __restrict__ piv_pos,
@@ -388,25 +357,27 @@ __global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
     }
 }
 
-// Row echelon of the panel (columns [0, bw) of the n <= KB rows of `old`,
-// leading dimension ldo) in shared memory, recording the transformation E
-// (E * old = rows whose panel part is in echelon form with unit pivots;
-// the rows that are not pivots become zero in the panel).  Writes -E
-// (n x n, ld KB), the panel-local index and column of every pivot, in
-// increasing column order, and their count.
+// Row echelon of one panel (the 128 columns of panel dpanel[d], on the n <= KB
+// rows chunk_rows[d KB + i] of Dp) in shared memory, recording the
+// transformation E (E * old = rows whose panel part is in echelon form with
+// unit pivots; the rows that are not pivots become zero in the panel).
+// Writes I - E (KB x KB, zero outside the leading n x n block), so that
+// old - (I - E) old = E old is one in-place GEMM update of the chunk rows,
+// and the panel-local index and column of every pivot, in increasing column
+// order, and their count.
 constexpr int PF_GROUPS = 4;  // threads per row in k_panel_factor
 
 template <class F>
 __global__ void __launch_bounds__(KB * PF_GROUPS)
-k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __restrict__ dpanel,
-               const int32_t* __restrict__ cursor, int32_t j0, int32_t ncr,
-               uint32_t* neg_e_b, int32_t* piv_pos_b, int32_t* piv_col_b, int32_t* n_piv_b, F f) {
-    // chunk blockIdx.x: panel dpanel[d], its rows start at column j0 of oldb
+k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __restrict__ chunk_rows,
+               const int32_t* __restrict__ dpanel, const int32_t* __restrict__ cursor, int32_t ncr,
+               uint32_t* ime_b, int32_t* piv_pos_b, int32_t* piv_col_b, int32_t* n_piv_b, F f) {
+    // chunk blockIdx.x: panel dpanel[d]
     const int d = blockIdx.x;
     const int32_t pj = dpanel[d] * KB;
     const int32_t n = min(cursor[d], KB), bw = min(KB, ncr - pj), col0 = pj;
-    const uint32_t* old = oldb + (size_t)d * KB * ldo + (pj - j0);
-    uint32_t* neg_e = neg_e_b + (size_t)d * KB * KB;
+    const int32_t* rows = chunk_rows + (size_t)d * KB;
+    uint32_t* ime = ime_b + (size_t)d * KB * KB;
     int32_t* piv_pos = piv_pos_b + d * KB;
     int32_t* piv_col = piv_col_b + d * KB;
     int32_t* n_piv = n_piv_b + d;
@@ -420,7 +391,7 @@ k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __
     const int r = tid % KB, g = tid / KB;  // row and column group of this thread
     for (int t = tid; t < KB * KB; t += nt) {
         const int i = t / KB, c = t % KB;
-        P[i][c] = (i < n && c < bw) ? old[(size_t)i * ldo + c] : 0u;
+        P[i][c] = (i < n && c < bw) ? Dp[(size_t)rows[i] * ld + pj + c] : 0u;
         E[i][c] = i == c ? 1u : 0u;
     }
     if (tid < KB) is_piv[tid] = 0;
@@ -463,8 +434,13 @@ k_panel_factor(const uint32_t* __restrict__ oldb, int64_t ldo, const int32_t* __
     }
     for (int t = tid; t < KB * KB; t += nt) {
         const int ii = t / KB, cc = t % KB;
-        const uint32_t v = (ii < n && cc < n) ? E[ii][cc] : 0u;
-        neg_e[t] = v ? f.p - v : 0u;
+        uint32_t v = 0u;
+        if (ii < n && cc < n) {
+            const uint32_t e = E[ii][cc];
+            const uint32_t one = ii == cc ? 1u : 0u;
+            v = one >= e ? one - e : one + (f.p - e);
+        }
+        ime[t] = v;
     }
     if (tid == 0) *n_piv = k;
 }
@@ -546,13 +522,13 @@ static int grid_of(int64_t n, int t = 256) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
 }
 
-// D (M x N) -= A (M x K) B (K x N), exact mod p
-static int gemm(Ctx& c, uint32_t* D, int64_t ldd, const uint32_t* A, int64_t lda,
-                const uint32_t* B, int64_t ldb, int32_t M, int32_t N, int32_t K) {
-    if (M <= 0 || N <= 0 || K <= 0) return GBGPU_OK;
-    TcGemmArgs g{c.p, M, N, K, A, lda, B, ldb, D, ldd};
+// D (M x N) -= A (M x K) B (K x N), exact mod p, for any TcGemmArgs (batch,
+// row lists); the tensor-core workspace grows on demand
+static int gemm_args(Ctx& c, TcGemmArgs g) {
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.batch <= 0) return GBGPU_OK;
+    g.p = c.p;
     if (c.form == GBGPU_FORM_PLAIN) return plain_submul(g, c.s, &c.launches);
-    const size_t need = tc_workspace_bytes(c.p, M, N, K);
+    const size_t need = tc_workspace_bytes(c.p, g.M, g.N, g.K, g.batch);
     if (need > c.ws_bytes) {
         if (c.ws) cudaFreeAsync(c.ws, c.s);
         c.ws = nullptr;
@@ -566,29 +542,22 @@ static int gemm(Ctx& c, uint32_t* D, int64_t ldd, const uint32_t* A, int64_t lda
     return tc_submul(g, c.ws, c.s, c.err, &c.launches);
 }
 
+static int gemm(Ctx& c, uint32_t* D, int64_t ldd, const uint32_t* A, int64_t lda,
+                const uint32_t* B, int64_t ldb, int32_t M, int32_t N, int32_t K) {
+    TcGemmArgs g{c.p, M, N, K, A, lda, B, ldb, D, ldd};
+    return gemm_args(c, g);
+}
+
 // batch of `batch` products D_z -= A_z B_z (element strides sA, sB, sD)
 static int gemm_batched(Ctx& c, uint32_t* D, int64_t ldd, int64_t sD, const uint32_t* A,
                         int64_t lda, int64_t sA, const uint32_t* B, int64_t ldb, int64_t sB,
                         int32_t M, int32_t N, int32_t K, int32_t batch) {
-    if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return GBGPU_OK;
     TcGemmArgs g{c.p, M, N, K, A, lda, B, ldb, D, ldd};
     g.batch = batch;
     g.sA = sA;
     g.sB = sB;
     g.sD = sD;
-    if (c.form == GBGPU_FORM_PLAIN) return plain_submul(g, c.s, &c.launches);
-    const size_t need = tc_workspace_bytes(c.p, M, N, K, batch);
-    if (need > c.ws_bytes) {
-        if (c.ws) cudaFreeAsync(c.ws, c.s);
-        c.ws = nullptr;
-        const size_t bytes = std::max(need, c.ws_bytes * 2);
-        if (cudaMallocAsync(&c.ws, bytes, c.s) != cudaSuccess) {
-            set_error("GEMM workspace allocation failed");
-            return GBGPU_ENOMEM;
-        }
-        c.ws_bytes = bytes;
-    }
-    return tc_submul(g, c.ws, c.s, c.err, &c.launches);
+    return gemm_args(c, g);
 }
 
 // elimination block size: powers of two from 128 to 1024
@@ -637,14 +606,17 @@ static int neg_inverse_big(Ctx& c, const F& f, const uint32_t* src, int64_t lds,
     return GBGPU_OK;
 }
 
-// T (rows x ncols, ld) <- T - T[:, pc] (U[:, pc])^-1 U for pivot rows U
-// (n_p x ncols, ld_u, sorted by lead, monic, zero left of their leads) with
-// pivot columns pc (ascending): afterwards T is zero at every pivot column.
-// Blocks of NB pivots, left to right.
+// Rows t_rows[0 .. rows) of M (leading dimension ld, ncols columns) are
+// reduced by the pivot rows u_rows[0 .. n_p) of M (sorted by lead, monic,
+// zero left of their leads, pivot columns pc ascending):
+//   T <- T - T[:, pc] (U[:, pc])^-1 U,
+// after which every T row is zero at every pivot column.  Blocks of NB
+// pivots, left to right; the rows are read and written in place through the
+// row lists (T and U rows are distinct).
 template <class F>
-static int eliminate(Ctx& c, const F& f, uint32_t* T, int64_t ldt, int32_t rows, int32_t ncols,
-                     const uint32_t* U, int64_t ldu, int32_t n_p, const int32_t* d_pc,
-                     const std::vector<int32_t>& pc) {
+static int eliminate(Ctx& c, const F& f, uint32_t* M, int64_t ld, const int32_t* t_rows,
+                     int32_t rows, int32_t ncols, const int32_t* u_rows, int32_t n_p,
+                     const int32_t* d_pc, const std::vector<int32_t>& pc) {
     if (rows <= 0 || n_p <= 0) return GBGPU_OK;
     const int32_t NB = nb_for(n_p);
     const int32_t nb = (n_p + NB - 1) / NB;
@@ -657,20 +629,22 @@ static int eliminate(Ctx& c, const F& f, uint32_t* T, int64_t ldt, int32_t rows,
     for (int b = 0; b < nb; ++b) {
         const int kb = std::min(NB, n_p - b * NB);
         BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)kb * kb), 256, 0, c.s>>>(
-            kb, kb, U + (size_t)b * NB * ldu, ldu, d_pc + b * NB, Ublk + (size_t)b * NB * NB, NB));
+            kb, kb, M, ld, d_pc + b * NB, Ublk + (size_t)b * NB * NB, NB, u_rows + b * NB));
     }
     BL_CHECK(neg_inverse_big(c, f, Ublk, NB, (int64_t)NB * NB, nb, n_p - (nb - 1) * NB, NB, Ninv));
     for (int b = 0; b < nb; ++b) {
         const int kb = std::min(NB, n_p - b * NB);
         const int32_t first_col = pc[b * NB];
         BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)rows * kb), 256, 0, c.s>>>(
-            rows, kb, T, ldt, d_pc + b * NB, G, NB));
+            rows, kb, M, ld, d_pc + b * NB, G, NB, t_rows));
         BL_CUDA(cudaMemsetAsync(X, 0, sizeof(uint32_t) * (size_t)rows * NB, c.s));
         // X = G * (U_kk)^-1 = 0 - G * (-(U_kk)^-1)
         BL_CHECK(gemm(c, X, NB, G, NB, Ninv + (size_t)b * bstride, NB, rows, kb, kb));
         // T[:, first_col:] -= X * U_k[:, first_col:]
-        BL_CHECK(gemm(c, T + first_col, ldt, X, NB, U + (size_t)b * NB * ldu + first_col, ldu, rows,
-                      ncols - first_col, kb));
+        TcGemmArgs g{c.p, rows, ncols - first_col, kb, X, NB, M + first_col, ld, M + first_col, ld};
+        g.b_rows = u_rows + b * NB;
+        g.d_rows = t_rows;
+        BL_CHECK(gemm_args(c, g));
     }
     return GBGPU_OK;
 }
@@ -812,14 +786,11 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     const int32_t max_dirty = 64;  // dirty panels factorized per round (memory bound)
     int32_t* chunk_rows = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* cursor = c.alloc<int32_t>(max_dirty);
-    uint32_t* negEB = c.alloc<uint32_t>((size_t)max_dirty * KB * KB);
+    uint32_t* imeB = c.alloc<uint32_t>((size_t)max_dirty * KB * KB);
     int32_t* piv_pos = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* piv_colb = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* n_piv = c.alloc<int32_t>(max_dirty);
-    if (!chunk_rows || !cursor || !negEB || !piv_pos || !piv_colb || !n_piv) return GBGPU_ENOMEM;
-    uint32_t* OldB = nullptr;
-    uint32_t* OutB = nullptr;
-    size_t chunk_cap = 0;  // elements of OldB / OutB
+    if (!chunk_rows || !cursor || !imeB || !piv_pos || !piv_colb || !n_piv) return GBGPU_ENOMEM;
     int rounds = 0;
     bool first = true;
     while (t > 0 && ncr > 0) {
@@ -855,31 +826,27 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         const int32_t n_dirty = (int32_t)h_dpanel.size();
         if (n_dirty > 0) {
             const int32_t j0 = h_dpanel[0] * KB, width = ncr - j0;
-            const int64_t ldo = ((int64_t)width + 3) & ~(int64_t)3;
-            const size_t need = (size_t)n_dirty * KB * ldo;
-            if (need > chunk_cap) {
-                OldB = c.alloc<uint32_t>(need);
-                OutB = c.alloc<uint32_t>(need);
-                if (!OldB || !OutB) return GBGPU_ENOMEM;
-                chunk_cap = need;
-            }
             BL_CUDA(cudaMemcpyAsync(dslot, h_dslot.data(), sizeof(int32_t) * npan,
                                     cudaMemcpyHostToDevice, s));
             BL_CUDA(cudaMemcpyAsync(dpanel, h_dpanel.data(), sizeof(int32_t) * n_dirty,
                                     cudaMemcpyHostToDevice, s));
             BL_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int32_t) * n_dirty, s));
+            BL_LAUNCH(k_fill_i32<<<grid_of((int64_t)n_dirty * KB), 256, 0, s>>>(
+                chunk_rows, n_dirty * KB, -1));
             BL_LAUNCH(k_bucket_dirty<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, dslot,
                                                                       cursor, chunk_rows));
-            BL_LAUNCH(k_gather_chunks<<<grid_of((int64_t)n_dirty * KB * width), 256, 0, s>>>(
-                n_dirty, cursor, chunk_rows, Dp, ld, j0, width, OldB, ldo));
             BL_LAUNCH(k_panel_factor<F><<<n_dirty, KB * PF_GROUPS, pf_bytes, s>>>(
-                OldB, ldo, dpanel, cursor, j0, ncr, negEB, piv_pos, piv_colb, n_piv, f));
-            BL_CUDA(cudaMemsetAsync(OutB, 0, sizeof(uint32_t) * need, s));
-            // OutB[d] = E_d OldB[d] = 0 - (-E_d) OldB[d]
-            BL_CHECK(gemm_batched(c, OutB, ldo, (int64_t)KB * ldo, negEB, KB, (int64_t)KB * KB, OldB,
-                                  ldo, (int64_t)KB * ldo, KB, width, KB, n_dirty));
-            BL_LAUNCH(k_scatter_chunks<<<grid_of((int64_t)n_dirty * KB * width), 256, 0, s>>>(
-                n_dirty, cursor, chunk_rows, OutB, ldo, j0, width, Dp, ld));
+                Dp, ld, chunk_rows, dpanel, cursor, ncr, imeB, piv_pos, piv_colb, n_piv, f));
+            // chunk rows (columns j0..) <- old - (I - E_d) old = E_d old, in place:
+            // the limb planes of `old` are cut before the product writes the rows
+            TcGemmArgs g{c.p, KB, width, KB, imeB, KB, Dp + j0, ld, Dp + j0, ld};
+            g.batch = n_dirty;
+            g.sA = (int64_t)KB * KB;
+            g.b_rows = chunk_rows;
+            g.sBr = KB;
+            g.d_rows = chunk_rows;
+            g.sDr = KB;
+            BL_CHECK(gemm_args(c, g));
             BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
                                                                 piv_of_col, is_piv, wflag));
         }
@@ -905,20 +872,10 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         if (n_rest == 0) break;
         std::vector<int32_t> h_pc(n_new);
         BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * n_new, cudaMemcpyDeviceToHost, s));
-        uint32_t* Ucmp = c.alloc<uint32_t>((size_t)n_new * ld);
-        uint32_t* Tcmp = c.alloc<uint32_t>((size_t)n_rest * ld);
-        if (!Ucmp || !Tcmp) return GBGPU_ENOMEM;
-        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_new * ncr), 256, 0, s>>>(
-            n_new, prow, ncr, Dp, ld, Ucmp, ld));
-        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
-            n_rest, pend, ncr, Dp, ld, Tcmp, ld));
         BL_CUDA(cudaStreamSynchronize(s));
-        BL_CHECK(eliminate(c, f, Tcmp, ld, n_rest, ncr, Ucmp, ld, n_new, pc, h_pc));
-        BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)n_rest * ncr), 256, 0, s>>>(
-            n_rest, pend, ncr, Tcmp, ld, Dp, ld));
+        BL_CHECK(eliminate(c, f, Dp, ld, pend, n_rest, ncr, prow, n_new, pc, h_pc));
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_rest * 32), 256, 0, s>>>(n_rest, pend, ncr, Dp,
                                                                              ld, lead, 1));
-        // Ucmp / Tcmp stay allocated until the reduction ends (stream-ordered)
     }
     const int steps = rounds;
     out->echelon_rounds = steps;
@@ -944,46 +901,46 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * r, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         BL_LAUNCH(k_gather_rows<<<grid_of(r), 256, 0, s>>>(r, pc, piv_of_col, prow, counters + 2));
-        // compact echelon rows E (r x ncr), ascending lead
+        // echelon rows prow[0 .. r), ascending lead, reduced in place
         const int32_t NB = nb_for(r);
         const int64_t bstride = (int64_t)NB * (NB + 1);
-        uint32_t* E = c.alloc<uint32_t>((size_t)r * ld);
         const int32_t nb = (r + NB - 1) / NB;
         uint32_t* Ublk = c.alloc<uint32_t>((size_t)nb * NB * NB);
         uint32_t* Ninv = c.alloc<uint32_t>((size_t)nb * bstride);
         uint32_t* G = c.alloc<uint32_t>((size_t)NB * std::max(r, 1));
         uint32_t* Y = c.alloc<uint32_t>((size_t)NB * ld);
-        if (!E || !Ublk || !Ninv || !G || !Y) return GBGPU_ENOMEM;
-        BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)r * ncr), 256, 0, s>>>(r, prow, ncr, Dp,
-                                                                                ld, E, ld));
+        if (!Ublk || !Ninv || !G || !Y) return GBGPU_ENOMEM;
         for (int b = 0; b < nb; ++b) {
             const int kb = std::min(NB, r - b * NB);
             BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)kb * kb), 256, 0, s>>>(
-                kb, kb, E + (size_t)b * NB * ld, ld, pc + b * NB, Ublk + (size_t)b * NB * NB, NB));
+                kb, kb, Dp, ld, pc + b * NB, Ublk + (size_t)b * NB * NB, NB, prow + b * NB));
         }
         BL_CHECK(neg_inverse_big(c, f, Ublk, NB, (int64_t)NB * NB, nb, r - (nb - 1) * NB, NB, Ninv));
         for (int b = nb - 1; b >= 0; --b) {
             const int kb = std::min(NB, r - b * NB);
             const int32_t later = r - (b * NB + kb);
-            uint32_t* Ek = E + (size_t)b * NB * ld;
+            const int32_t* rows_k = prow + b * NB;
             const int32_t c0 = h_pc[b * NB];
             if (later > 0) {
-                // Ek -= Ek[:, pc(>k)] R(>k)
+                // E_k -= E_k[:, pc(>k)] R(>k)
                 BL_LAUNCH(k_gather_cols<<<grid_of((int64_t)kb * later), 256, 0, s>>>(
-                    kb, later, Ek, ld, pc + b * NB + kb, G, later));
+                    kb, later, Dp, ld, pc + b * NB + kb, G, later, rows_k));
                 const int32_t c_later = h_pc[b * NB + kb];
-                BL_CHECK(gemm(c, Ek + c_later, ld, G, later, E + (size_t)(b * NB + kb) * ld + c_later,
-                              ld, kb, ncr - c_later, later));
+                TcGemmArgs g{c.p, kb, ncr - c_later, later, G, later, Dp + c_later, ld,
+                             Dp + c_later, ld};
+                g.b_rows = rows_k + kb;
+                g.d_rows = rows_k;
+                BL_CHECK(gemm_args(c, g));
             }
-            // Ek = (Ek[:, pc(k)])^-1 Ek, as Y = 0 - (-(U_kk)^-1) Ek, Ek = Y
-            BL_CUDA(cudaMemsetAsync(Y, 0, sizeof(uint32_t) * (size_t)NB * ld, s));
-            BL_CHECK(gemm(c, Y + c0, ld, Ninv + (size_t)b * bstride, NB, Ek + c0, ld, kb, ncr - c0, kb));
-            BL_CUDA(cudaMemcpy2DAsync(Ek + c0, ld * 4, Y + c0, ld * 4, (size_t)(ncr - c0) * 4, kb,
-                                      cudaMemcpyDeviceToDevice, s));
+            // E_k = (E_k[:, pc(k)])^-1 E_k, as Y = 0 - (-(U_kk)^-1) E_k, E_k = Y
+            BL_CUDA(cudaMemset2DAsync(Y + c0, ld * 4, 0, (size_t)(ncr - c0) * 4, kb, s));
+            TcGemmArgs g{c.p, kb, ncr - c0, kb, Ninv + (size_t)b * bstride, NB, Dp + c0, ld, Y + c0,
+                         ld};
+            g.b_rows = rows_k;
+            BL_CHECK(gemm_args(c, g));
+            BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)kb * (ncr - c0)), 256, 0, s>>>(
+                kb, rows_k, ncr - c0, Y + c0, ld, Dp + c0, ld));
         }
-        // reduced rows back to their D' slots for the compaction
-        BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)r * ncr), 256, 0, s>>>(r, prow, ncr, E,
-                                                                                 ld, Dp, ld));
     }
     return GBGPU_OK;
 }

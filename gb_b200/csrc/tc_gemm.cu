@@ -139,9 +139,14 @@ struct TcCfg {
     static constexpr int A_BYTES = BM * BK;
     static constexpr int B_BYTES = BN * BK;
     static constexpr int STAGE_BYTES = L * (A_BYTES + B_BYTES);
-    static constexpr int STAGES = L == 1 ? 4 : (L == 2 ? 3 : (L == 3 ? 3 : 2));
+    static constexpr int STAGES = L == 1 ? 4 : (L == 2 ? 3 : 2);
     static constexpr int TMEM_COLS = NW * BN <= 256 ? 256 : 512;
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    // epilogue staging: a 32 x 32 block per epilogue warp (padded rows) and the
+    // D row pointers of its 32 rows
+    static constexpr int STG_BYTES = 4 * 32 * 33 * 4;
+    static constexpr int ROWP_BYTES = 4 * 32 * 8;
+    static constexpr int SMEM_BYTES =
+        STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + STG_BYTES + ROWP_BYTES;
     // K bytes per panel: L * 255^2 * K < 2^31
     static constexpr int PANEL_KB = L == 1 ? 256 : (L == 2 ? 128 : (L == 3 ? 85 : 64));
     static constexpr uint32_t IDESC = (2u << 4)                      // D = s32
@@ -153,6 +158,8 @@ struct TcCfg {
 struct TcParams {
     uint32_t* D;
     int64_t ldd, sD;
+    const int32_t* d_rows;  // optional: row m of D is D + d_rows[m] ldd (< 0: not written)
+    int64_t sDr;
     int32_t M, N, Mp, Np, nkb;
     // nonzero flags of the 128-row x 128-byte A tiles ([Mp/128][nkb]) and of the
     // BN-row x 128-byte B tiles ([Np/BN][nkb]); a K step where either tile is
@@ -295,10 +302,27 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         }
     } else {
         // ---- epilogue: warps 2..5, TMEM lane quarter (warp % 4) ----
+        // Thread `lane` folds row q*32+lane of the tile; the 32 x 32 result
+        // block goes through shared memory so that the read-modify-write of D
+        // runs along rows (one 128-byte row segment per warp instruction).
         const int q = warp & 3;
         const int row = q * 32 + lane;
         const int gm = m0 + row;
         const uint32_t p = prm.p;
+        uint32_t(*stg)[33] = (uint32_t(*)[33])(gbase + C::STAGES * C::STAGE_BYTES + 256 +
+                                               (size_t)(warp - 2) * 32 * 33 * 4);
+        uint32_t** rowp = (uint32_t**)(gbase + C::STAGES * C::STAGE_BYTES + 256 + C::STG_BYTES +
+                                       (size_t)(warp - 2) * 32 * 8);
+        {
+            uint32_t* mine = nullptr;
+            if (gm < prm.M) {
+                int64_t ri = gm;
+                if (prm.d_rows) ri = prm.d_rows[(size_t)z * prm.sDr + gm];
+                if (ri >= 0) mine = prm.D + (size_t)z * prm.sD + (size_t)ri * prm.ldd;
+            }
+            rowp[lane] = mine;
+        }
+        __syncwarp();
         for (int panel = 0; panel < npanels; ++panel) {
             bool ok = true;
             if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar, panel & 1, prm.budget);
@@ -309,6 +333,15 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             }
             tc_fence_after();
             for (int c0 = 0; c0 < C::BN; c0 += 32) {
+                const int gn = n0 + c0 + lane;
+                const bool col_ok = gn < prm.N;
+                // D values of the block (row r, column gn), issued before the fold
+                uint32_t dv[32];
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    const uint32_t* rp = rowp[r];
+                    dv[r] = (rp && col_ok) ? rp[gn] : 0u;
+                }
                 uint32_t v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[j] = 0;
@@ -327,17 +360,19 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                         v[j] = sum >= p ? sum - p : sum;
                     }
                 }
-                if (gm < prm.M) {
-                    uint32_t* drow = prm.D + (size_t)z * prm.sD + (size_t)gm * prm.ldd;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int gn = n0 + c0 + j;
-                        if (gn < prm.N) {
-                            const uint32_t d = drow[gn];
-                            drow[gn] = d >= v[j] ? d - v[j] : d + (p - v[j]);
-                        }
+                for (int j = 0; j < 32; ++j) stg[lane][j] = v[j];
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    uint32_t* rp = rowp[r];
+                    if (rp && col_ok) {
+                        const uint32_t vv = stg[r][lane];
+                        const uint32_t d = dv[r];
+                        rp[gn] = d >= vv ? d - vv : d + (p - vv);
                     }
                 }
+                __syncwarp();
             }
             tc_fence_before();
             __syncwarp();
@@ -356,12 +391,15 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 }
 
 // ---------------------------------------------------------------------------
-// limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded
-__global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA, int32_t M,
+// limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded; row m
+// of A is A + a_rows[m] lda when a_rows is given (negative: a zero row)
+__global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
+                             const int32_t* __restrict__ a_rows, int64_t sAr, int32_t M,
                              int32_t K, int32_t Mp, int32_t Kp, int32_t L,
                              uint8_t* __restrict__ out, uint8_t* flags) {
     // batch item blockIdx.y
     A += (size_t)blockIdx.y * sA;
+    if (a_rows) a_rows += (size_t)blockIdx.y * sAr;
     out += (size_t)blockIdx.y * L * Mp * Kp;
     if (flags) flags += (size_t)blockIdx.y * (Mp / 128) * (Kp / 128);
     const int64_t total = (int64_t)Mp * (Kp / 4);
@@ -369,9 +407,12 @@ __global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_
          t += (int64_t)gridDim.x * blockDim.x) {
         const int32_t m = (int32_t)(t / (Kp / 4));  // row of this item
         const int32_t k = (int32_t)(t % (Kp / 4)) * 4;
+        int64_t src = -1;
+        if (m < M) src = a_rows ? (int64_t)a_rows[m] : (int64_t)m;
+        const uint32_t* row = src >= 0 ? A + (size_t)src * lda : nullptr;
         uint32_t v[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) v[i] = (m < M && k + i < K) ? A[(size_t)m * lda + k + i] : 0u;
+        for (int i = 0; i < 4; ++i) v[i] = (row && k + i < K) ? row[k + i] : 0u;
         if (flags && (v[0] | v[1] | v[2] | v[3])) flags[(size_t)(m / 128) * (Kp / 128) + k / 128] = 1;
         for (int l = 0; l < L; ++l) {
             const uint32_t packed = ((v[0] >> (8 * l)) & 255u) | (((v[1] >> (8 * l)) & 255u) << 8) |
@@ -382,31 +423,66 @@ __global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_
     }
 }
 
-// transposing split: out[l][n][k] = byte l of B[k][n]
-__global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB, int32_t K,
-                             int32_t N, int32_t Np, int32_t Kp, int32_t L,
-                             uint8_t* __restrict__ out, uint8_t* flags, int32_t bn) {
-    __shared__ uint32_t tile[32][33];
+// transposing split: out[l][n][k] = byte l of B[k][n]; row k of B is
+// B + b_rows[k] ldb when b_rows is given (negative: a zero row).
+// One 64 (k) x 64 (n) tile per 256 threads: rows are read 128 bytes per warp
+// instruction, and every thread writes 16 consecutive k bytes of one n per limb.
+__global__ void __launch_bounds__(256)
+k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
+             const int32_t* __restrict__ b_rows, int64_t sBr, int32_t K, int32_t N, int32_t Np,
+             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t bn) {
+    __shared__ uint32_t tile[64][65];
+    __shared__ const uint32_t* rowp[64];
     // batch item blockIdx.z
     B += (size_t)blockIdx.z * sB;
+    if (b_rows) b_rows += (size_t)blockIdx.z * sBr;
     out += (size_t)blockIdx.z * L * Np * Kp;
     if (flags) flags += (size_t)blockIdx.z * (Np / bn) * (Kp / 128);
-    const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
-    for (int r = ty; r < 32; r += 8) {
-        const int k = k0 + r, n = n0 + tx;
-        tile[r][tx] = (k < K && n < N) ? B[(size_t)k * ldb + n] : 0u;
+    const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    if (threadIdx.x < 64) {
+        const int k = k0 + threadIdx.x;
+        int64_t src = -1;
+        if (k < K) src = b_rows ? (int64_t)b_rows[k] : (int64_t)k;
+        rowp[threadIdx.x] = src >= 0 ? B + (size_t)src * ldb : nullptr;
     }
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const int n = n0 + r, k = k0 + tx;
-        if (n < Np && k < Kp) {
-            const uint32_t v = tile[tx][r];
-            for (int l = 0; l < L; ++l) out[((size_t)l * Np + n) * Kp + k] = (uint8_t)(v >> (8 * l));
-            if (flags && v) flags[(size_t)(n / bn) * (Kp / 128) + k / 128] = 1;
+    {
+        const int c = threadIdx.x & 63, r0 = threadIdx.x >> 6;  // 4 rows per pass
+        const int n = n0 + c;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int r = r0 + 4 * i;
+            const uint32_t* rp = rowp[r];
+            tile[r][c] = (rp && n < N) ? rp[n] : 0u;
         }
     }
+    __syncthreads();
+    const int nn = threadIdx.x & 63, kq = (threadIdx.x >> 6) * 16;
+    uint32_t v[16];
+    uint32_t any = 0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        v[i] = tile[kq + i][nn];
+        any |= v[i];
+    }
+    const int n = n0 + nn, k = k0 + kq;  // n < Np and k + 16 <= Kp by the grid
+    for (int l = 0; l < L; ++l) {
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            w[j] = ((v[4 * j] >> (8 * l)) & 255u) | (((v[4 * j + 1] >> (8 * l)) & 255u) << 8) |
+                   (((v[4 * j + 2] >> (8 * l)) & 255u) << 16) |
+                   (((v[4 * j + 3] >> (8 * l)) & 255u) << 24);
+        *(uint4*)(out + ((size_t)l * Np + n) * Kp + k) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    if (flags && any) flags[(size_t)(n / bn) * (Kp / 128) + k / 128] = 1;
 }
+
+// row index lists of the plain GEMM (see TcGemmArgs)
+struct RowLists {
+    const int32_t *a, *b, *d;
+    int64_t sa, sb, sd;
+};
 
 // ---------------------------------------------------------------------------
 // plain CUDA-core modular GEMM: 64 x 64 tile per 256 threads, 4 x 4 per thread;
@@ -414,14 +490,20 @@ __global__ void k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_
 __global__ void __launch_bounds__(256)
 k_plain_submul(const uint32_t* __restrict__ A, int64_t lda, const uint32_t* __restrict__ B,
                int64_t ldb, uint32_t* D, int64_t ldd, int32_t M, int32_t N, int32_t K,
-               int64_t strideA, int64_t strideB, int64_t strideD, FieldMont f) {
+               int64_t strideA, int64_t strideB, int64_t strideD, RowLists rl, FieldMont f) {
     A += (size_t)blockIdx.z * strideA;
     B += (size_t)blockIdx.z * strideB;
     D += (size_t)blockIdx.z * strideD;
+    const int32_t* a_rows = rl.a ? rl.a + (size_t)blockIdx.z * rl.sa : nullptr;
+    const int32_t* b_rows = rl.b ? rl.b + (size_t)blockIdx.z * rl.sb : nullptr;
+    const int32_t* d_rows = rl.d ? rl.d + (size_t)blockIdx.z * rl.sd : nullptr;
     __shared__ uint32_t sA[16][64 + 1];
     __shared__ uint32_t sB[16][64 + 1];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    // row index of A row m / B row k (negative: zero row)
+    auto arow = [&](int m) -> int64_t { return a_rows ? (int64_t)a_rows[m] : (int64_t)m; };
+    auto brow = [&](int k) -> int64_t { return b_rows ? (int64_t)b_rows[k] : (int64_t)k; };
     uint64_t lo[4][4], hi[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -432,10 +514,12 @@ k_plain_submul(const uint32_t* __restrict__ A, int64_t lda, const uint32_t* __re
         for (int t = threadIdx.x; t < 16 * 64; t += 256) {
             const int kk = t & 15, mm = t >> 4;
             const int m = m0 + mm, k = k0 + kk;
-            sA[kk][mm] = (m < M && k < K) ? A[(size_t)m * lda + k] : 0u;
+            const int64_t ra = (m < M && k < K) ? arow(m) : -1;
+            sA[kk][mm] = ra >= 0 ? A[(size_t)ra * lda + k] : 0u;
             const int nn = t & 63, kr = t >> 6;
             const int n = n0 + nn, k2 = k0 + kr;
-            sB[kr][nn] = (n < N && k2 < K) ? B[(size_t)k2 * ldb + n] : 0u;
+            const int64_t rb = (n < N && k2 < K) ? brow(k2) : -1;
+            sB[kr][nn] = rb >= 0 ? B[(size_t)rb * ldb + n] : 0u;
         }
         __syncthreads();
 #pragma unroll 4
@@ -470,14 +554,16 @@ k_plain_submul(const uint32_t* __restrict__ A, int64_t lda, const uint32_t* __re
     for (int i = 0; i < 4; ++i) {
         const int m = m0 + ty * 4 + i;
         if (m >= M) continue;
+        const int64_t rd = d_rows ? (int64_t)d_rows[m] : (int64_t)m;
+        if (rd < 0) continue;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int n = n0 + tx * 4 + j;
             if (n >= N) continue;
             const uint64_t h = (hi[i][j] % f.p) << 16;
             const uint32_t v = (uint32_t)((lo[i][j] % f.p + h % f.p) % f.p);
-            const uint32_t d = D[(size_t)m * ldd + n];
-            D[(size_t)m * ldd + n] = d >= v ? d - v : d + (f.p - v);
+            const uint32_t d = D[(size_t)rd * ldd + n];
+            D[(size_t)rd * ldd + n] = d >= v ? d - v : d + (f.p - v);
         }
     }
 }
@@ -556,9 +642,11 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         const int64_t total = (int64_t)Mp * (Kp / 4);
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256,
                                                                        148 * 32 / nb + 1));
-        k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.M, g.K, Mp, Kp, L, Ap, fa);
-        dim3 gb((Np + 31) / 32, (Kp + 31) / 32, nb);
-        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.sB, g.K, g.N, Np, Kp, L, Bp, fb, Cfg::BN);
+        k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.a_rows, g.sAr, g.M, g.K,
+                                                    Mp, Kp, L, Ap, fa);
+        dim3 gb(Np / 64, Kp / 64, nb);
+        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K, g.N, Np, Kp, L,
+                                        Bp, fb, Cfg::BN);
         *launches += 2;
     }
     CUtensorMap ma, mb;
@@ -570,6 +658,8 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     prm.D = g.D;
     prm.ldd = g.ldd;
     prm.sD = g.sD;
+    prm.d_rows = g.d_rows;
+    prm.sDr = g.sDr;
     prm.M = g.M;
     prm.N = g.N;
     prm.Mp = Mp;
@@ -654,8 +744,9 @@ int plain_submul(const TcGemmArgs& g, cudaStream_t s, long long* launches) {
     dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);
     FieldMont f{};
     f.p = g.p;
+    const RowLists rl{g.a_rows, g.b_rows, g.d_rows, g.sAr, g.sBr, g.sDr};
     k_plain_submul<<<grid, 256, 0, s>>>(g.A, g.lda, g.B, g.ldb, g.D, g.ldd, g.M, g.N, g.K, g.sA,
-                                        g.sB, g.sD, f);
+                                        g.sB, g.sD, rl, f);
     ++*launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

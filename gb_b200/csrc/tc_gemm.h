@@ -22,6 +22,14 @@ struct TcGemmArgs {
     // B + z sB, D + z sD (element strides)
     int32_t batch = 1;
     int64_t sA = 0, sB = 0, sD = 0;
+    // optional row indirection: row m of A is A + a_rows[m] lda (row k of B
+    // is B + b_rows[k] ldb, row m of D is D + d_rows[m] ldd); a negative index
+    // is a zero row of A or B and a row of D that is left untouched.  Batch
+    // item z reads its indices at a_rows + z sAr (b_rows + z sBr, d_rows + z sDr).
+    const int32_t* a_rows = nullptr;
+    const int32_t* b_rows = nullptr;
+    const int32_t* d_rows = nullptr;
+    int64_t sAr = 0, sBr = 0, sDr = 0;
 };
 
 // Optional per-thread profiling of the tensor-core GEMM launches: CUDA events
