@@ -131,12 +131,30 @@ __global__ void k_count_below(int32_t n, const int32_t* __restrict__ v, int32_t 
     }
 }
 
+// x mod p for any 64-bit x (p < 2^31) by Barrett reduction with
+// m = floor((2^64 - 1) / p): the estimated quotient is at most 2 short.
+__device__ __forceinline__ uint32_t mod64(uint64_t x, uint32_t p, uint64_t m) {
+    const uint64_t q = __umul64hi(x, m);
+    uint64_t r = x - q * p;
+    r = r >= p ? r - p : r;
+    r = r >= p ? r - p : r;
+    return (uint32_t)r;
+}
+
+constexpr int INV_LANES = 4;  // threads per column in k_neg_inverse
+
 // -U^-1 mod p for unit upper triangular blocks.  Block b is read from
 // src + b * stride_b with leading dimension ld (kb x kb, kb <= KB); the result
 // (KB x KB, identity-padded) goes to out + b * ostride with leading dimension
-// old.  One CTA per block, thread j solves column j by back substitution.
+// old.  One CTA per block; column j of V = U^-1 is solved by back
+// substitution by the INV_LANES threads j*INV_LANES.. of one warp, each
+// summing a quarter of the terms,
+//   V[i][j] = -sum_{i<k<=j} U[i][k] V[k][j],
+// so the recurrence needs only warp-level synchronisation.  V is split into
+// 16-bit halves: each product is below 2^47 and the sums stay below 2^54, one
+// Barrett reduction per entry.
 template <class F>
-__global__ void __launch_bounds__(KB)
+__global__ void __launch_bounds__(KB * INV_LANES)
 k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, int32_t n_blocks,
               int32_t last_kb, uint32_t* out, int64_t ostride, int64_t old, F f) {
     extern __shared__ uint32_t inv_smem[];
@@ -151,27 +169,38 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
         if (i < kb && j < kb) v = s[(size_t)i * ld + j];
         else v = i == j ? 1u : 0u;
         U[i][j] = v;
+        V[i][j] = i == j ? 1u : 0u;
     }
     __syncthreads();
-    const int j = threadIdx.x;
-    // V[., j] solves U x = e_j; V[i][j] = -sum_{i<k<=j} U[i][k] V[k][j].
-    // The sum is accumulated without reduction: V is split into 16-bit
-    // halves, so each of the at most 128 products is < 2^47 and both partial
-    // sums stay below 2^54; one reduction per entry.
-    V[j][j] = 1u;
-    for (int i = KB - 1; i > j; --i) V[i][j] = 0u;
-    const uint64_t p = f.p;
-    for (int i = j - 1; i >= 0; --i) {
+    const uint32_t p = f.p;
+    const uint64_t m = ~0ull / p;
+    const int lane = threadIdx.x & 31;
+    const int j = threadIdx.x / INV_LANES, sub = threadIdx.x % INV_LANES;
+    // largest column of this warp: the loop runs uniformly over the warp
+    const int jmax = (threadIdx.x | 31) / INV_LANES;
+    for (int i = jmax - 1; i >= 0; --i) {
         uint64_t lo = 0, hi = 0;
-        for (int k = i + 1; k <= j; ++k) {
-            const uint64_t u = U[i][k];
-            const uint32_t v = V[k][j];
-            lo += u * (v & 0xFFFFu);
-            hi += u * (v >> 16);
+        if (i < j) {
+            for (int k = i + 1 + sub; k <= j; k += INV_LANES) {
+                const uint64_t u = U[i][k];
+                const uint32_t v = V[k][j];
+                lo += u * (v & 0xFFFFu);
+                hi += u * (v >> 16);
+            }
         }
-        const uint64_t acc = (lo % p + ((hi % p) << 16) % p) % p;
-        V[i][j] = acc ? (uint32_t)(p - acc) : 0u;
+#pragma unroll
+        for (int o = 1; o < INV_LANES; o <<= 1) {
+            lo += __shfl_xor_sync(0xffffffffu, lo, o);
+            hi += __shfl_xor_sync(0xffffffffu, hi, o);
+        }
+        if (i < j && sub == 0) {
+            const uint32_t hr = mod64(hi, p, m);
+            const uint32_t acc = mod64((uint64_t)mod64(lo, p, m) + ((uint64_t)hr << 16), p, m);
+            V[i][j] = acc ? p - acc : 0u;
+        }
+        __syncwarp();
     }
+    (void)lane;
     __syncthreads();
     uint32_t* o = out + (size_t)b * ostride;
     for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
@@ -333,27 +362,27 @@ __global__ void k_register_chunks(const int32_t* __restrict__ n_piv,
     }
 }
 
-// scale row rows[i] by the inverse of its entry at column cols[i] (warp per row)
+// scale row rows[i] by the inverse of its entry at column cols[i] (one CTA
+// per row)
 template <class F>
 __global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
                                const int32_t* __restrict__ cols, int32_t ncols, uint32_t* M,
                                int64_t ld, F f) {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < n; i += nwarps) {
+    __shared__ uint32_t s_inv;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
         uint32_t* row = M + (size_t)rows[i] * ld;
         const int32_t c0 = cols[i];
         const uint32_t lv = row[c0];
-        if (lv == 1u) continue;
-        const uint32_t inv = inverse_mod(lv, f.p);
-        __syncwarp();
-        for (int c = c0 + 1 + lane; c < ncols; c += 32) {
+        if (lv == 1u) continue;  // uniform over the CTA
+        if (threadIdx.x == 0) s_inv = inverse_mod(lv, f.p);
+        __syncthreads();
+        const uint32_t inv = s_inv;
+        for (int c = c0 + 1 + threadIdx.x; c < ncols; c += blockDim.x) {
             const uint32_t v = row[c];
             if (v) row[c] = f.mulmod(v, inv);
         }
-        __syncwarp();
-        if (lane == 0) row[c0] = 1u;
+        __syncthreads();
+        if (threadIdx.x == 0) row[c0] = 1u;
     }
 }
 
@@ -590,7 +619,8 @@ static int neg_inverse_big(Ctx& c, const F& f, const uint32_t* src, int64_t lds,
     BL_CUDA(cudaFuncSetAttribute(k_neg_inverse<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     const int32_t n_sub = n_blocks * (NB / KB);
     const int64_t dstep = (int64_t)KB * (NB + 1);  // between 128-blocks on the diagonal
-    BL_LAUNCH(k_neg_inverse<F><<<n_sub, KB, bytes, c.s>>>(U, NB, dstep, n_sub, KB, out, dstep, NB, f));
+    BL_LAUNCH(k_neg_inverse<F><<<n_sub, KB * INV_LANES, bytes, c.s>>>(U, NB, dstep, n_sub, KB, out,
+                                                                   dstep, NB, f));
     for (int32_t sz = KB; sz < NB; sz *= 2) {
         const int32_t items = n_blocks * (NB / (2 * sz));
         const int64_t istep = (int64_t)2 * sz * (NB + 1);
@@ -861,7 +891,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         const int32_t n_new = last_pos + last_flag;
         BL_LAUNCH(k_gather_rows<<<grid_of(n_new), 256, 0, s>>>(n_new, pc, piv_of_col, prow,
                                                                counters + 2));
-        BL_LAUNCH(k_normalize_at<F><<<grid_of((int64_t)n_new * 32), 256, 0, s>>>(
+        BL_LAUNCH(k_normalize_at<F><<<std::max(1, std::min(n_new, 148 * 8)), 256, 0, s>>>(
             n_new, prow, pc, ncr, Dp, ld, f));
         // the rest: eliminated against every pivot of the round
         int32_t n_rest = 0;

@@ -83,13 +83,16 @@ struct FieldMont {
 // Inverse of a (0 < a < p) by the extended Euclidean algorithm, as the
 // reference's mod_p_inverse_32 (src/tools.c:83-110).
 __host__ __device__ inline uint32_t inverse_mod(uint32_t a, uint32_t p) {
-    int64_t r0 = p, r1 = a % p, s0 = 0, s1 = 1;
+    // extended Euclid; remainders stay below p < 2^31 (32-bit division),
+    // Bezout coefficients stay within (-p, p)
+    uint32_t r0 = p, r1 = a % p;
+    int64_t s0 = 0, s1 = 1;
     while (r1 != 0) {
-        const int64_t q = r0 / r1;
-        const int64_t r2 = r0 - q * r1;
+        const uint32_t q = r0 / r1;
+        const uint32_t r2 = r0 - q * r1;
         r0 = r1;
         r1 = r2;
-        const int64_t s2 = s0 - q * s1;
+        const int64_t s2 = s0 - (int64_t)q * s1;
         s0 = s1;
         s1 = s2;
     }

@@ -130,29 +130,41 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
 }
 
 // ---------------------------------------------------------------------------
-template <int L>
+// Two tile shapes per limb count.  The large one (one CTA per SM) serves long
+// K; the small one (K <= 256, two CTAs per SM, TMEM <= 256 columns each) lets
+// one CTA's loads and MMAs overlap the other's D read-modify-write when the
+// epilogue dominates.  The small shape stages its epilogue blocks in the
+// (then idle) operand ring.
+template <int L, bool SMALL = false>
 struct TcCfg {
     static constexpr int BM = 128;
     static constexpr int BK = 128;  // bytes of K per stage (one swizzle row)
-    static constexpr int BN = L == 1 ? 256 : (L == 2 ? 128 : 64);
+    static constexpr int BN = SMALL ? (L == 1 ? 128 : 64) : (L == 1 ? 256 : (L == 2 ? 128 : 64));
     static constexpr int NW = 2 * L - 1;
     static constexpr int A_BYTES = BM * BK;
     static constexpr int B_BYTES = BN * BK;
     static constexpr int STAGE_BYTES = L * (A_BYTES + B_BYTES);
-    static constexpr int STAGES = L == 1 ? 4 : (L == 2 ? 3 : 2);
-    static constexpr int TMEM_COLS = NW * BN <= 256 ? 256 : 512;
+    static constexpr int STAGES = SMALL ? 2 : (L == 1 ? 4 : (L == 2 ? 3 : 2));
+    static constexpr int TMEM_COLS =
+        NW * BN <= 64 ? 64 : (NW * BN <= 128 ? 128 : (NW * BN <= 256 ? 256 : 512));
     // epilogue staging: a 32 x 32 block per epilogue warp (padded rows) and the
     // D row pointers of its 32 rows
-    static constexpr int STG_BYTES = 4 * 32 * 33 * 4;
+    static constexpr int STG_BYTES = SMALL ? 0 : 4 * 32 * 33 * 4;
     static constexpr int ROWP_BYTES = 4 * 32 * 8;
-    static constexpr int SMEM_BYTES =
-        STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + STG_BYTES + ROWP_BYTES;
+    static constexpr int BAR_OFF = STAGES * STAGE_BYTES;
+    static constexpr int STG_OFF = SMALL ? 0 : BAR_OFF + 256;
+    static constexpr int ROWP_OFF = BAR_OFF + 256 + STG_BYTES;
+    static constexpr int SMEM_BYTES = ROWP_OFF + ROWP_BYTES + 1024 /*align*/;
+    static constexpr int MIN_CTAS = SMALL ? 2 : 1;
     // K bytes per panel: L * 255^2 * K < 2^31
     static constexpr int PANEL_KB = L == 1 ? 256 : (L == 2 ? 128 : (L == 3 ? 85 : 64));
     static constexpr uint32_t IDESC = (2u << 4)                      // D = s32
                                       | (0u << 7) | (0u << 10)       // A, B = u8
                                       | ((uint32_t)(BN >> 3) << 17)  // N
                                       | ((uint32_t)(BM >> 4) << 24); // M
+    static_assert(!SMALL || L <= 2, "small tiles for one or two limbs only");
+    static_assert(!SMALL || STAGES * STAGE_BYTES >= 4 * 32 * 33 * 4, "staging fits the ring");
+    static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 };
 
 struct TcParams {
@@ -173,17 +185,17 @@ struct TcParams {
     long long budget;
 };
 
-template <int L>
-__global__ void __launch_bounds__(192, 1)
+template <int L, bool SMALL>
+__global__ void __launch_bounds__(192, TcCfg<L, SMALL>::MIN_CTAS)
 k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const TcParams prm) {
-    using C = TcCfg<L>;
+    using C = TcCfg<L, SMALL>;
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte aligned tile region (shared-window address)
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* gbase = smem_raw + (base - raw);
-    uint64_t* bars = (uint64_t*)(gbase + C::STAGES * C::STAGE_BYTES);
+    uint64_t* bars = (uint64_t*)(gbase + C::BAR_OFF);
     // bars: full[STAGES], empty[STAGES], tmem_full, tmem_empty; then tmem slot, abort flag
     const uint32_t bar0 = smem_u32(bars);
     auto full_bar = [&](int s) { return bar0 + 8u * s; };
@@ -309,10 +321,10 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         const int row = q * 32 + lane;
         const int gm = m0 + row;
         const uint32_t p = prm.p;
-        uint32_t(*stg)[33] = (uint32_t(*)[33])(gbase + C::STAGES * C::STAGE_BYTES + 256 +
-                                               (size_t)(warp - 2) * 32 * 33 * 4);
-        uint32_t** rowp = (uint32_t**)(gbase + C::STAGES * C::STAGE_BYTES + 256 + C::STG_BYTES +
-                                       (size_t)(warp - 2) * 32 * 8);
+        // (small tiles: one K panel, so the ring is idle once the accumulators are full)
+        uint32_t(*stg)[33] =
+            (uint32_t(*)[33])(gbase + C::STG_OFF + (size_t)(warp - 2) * 32 * 33 * 4);
+        uint32_t** rowp = (uint32_t**)(gbase + C::ROWP_OFF + (size_t)(warp - 2) * 32 * 8);
         {
             uint32_t* mine = nullptr;
             if (gm < prm.M) {
@@ -392,90 +404,109 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
 // ---------------------------------------------------------------------------
 // limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded; row m
-// of A is A + a_rows[m] lda when a_rows is given (negative: a zero row)
-__global__ void k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
-                             const int32_t* __restrict__ a_rows, int64_t sAr, int32_t M,
-                             int32_t K, int32_t Mp, int32_t Kp, int32_t L,
-                             uint8_t* __restrict__ out, uint8_t* flags) {
+// of A is A + a_rows[m] lda when a_rows is given (negative: a zero row).
+// Every thread splits 16 consecutive k of one row (one 16-byte store per limb).
+__global__ void __launch_bounds__(256)
+k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
+             const int32_t* __restrict__ a_rows, int64_t sAr, int32_t M, int32_t K, int32_t Mp,
+             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags) {
     // batch item blockIdx.y
     A += (size_t)blockIdx.y * sA;
     if (a_rows) a_rows += (size_t)blockIdx.y * sAr;
     out += (size_t)blockIdx.y * L * Mp * Kp;
     if (flags) flags += (size_t)blockIdx.y * (Mp / 128) * (Kp / 128);
-    const int64_t total = (int64_t)Mp * (Kp / 4);
+    const int32_t kq = Kp / 16;  // 16-column groups per row
+    const int64_t total = (int64_t)Mp * kq;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t m = (int32_t)(t / (Kp / 4));  // row of this item
-        const int32_t k = (int32_t)(t % (Kp / 4)) * 4;
+        const int32_t m = (int32_t)(t / kq);
+        const int32_t k = (int32_t)(t % kq) * 16;
         int64_t src = -1;
         if (m < M) src = a_rows ? (int64_t)a_rows[m] : (int64_t)m;
         const uint32_t* row = src >= 0 ? A + (size_t)src * lda : nullptr;
-        uint32_t v[4];
+        uint32_t v[16];
+        uint32_t any = 0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) v[i] = (row && k + i < K) ? row[k + i] : 0u;
-        if (flags && (v[0] | v[1] | v[2] | v[3])) flags[(size_t)(m / 128) * (Kp / 128) + k / 128] = 1;
+        for (int i = 0; i < 16; ++i) {
+            v[i] = (row && k + i < K) ? row[k + i] : 0u;
+            any |= v[i];
+        }
+        if (flags && any) flags[(size_t)(m / 128) * (Kp / 128) + k / 128] = 1;
         for (int l = 0; l < L; ++l) {
-            const uint32_t packed = ((v[0] >> (8 * l)) & 255u) | (((v[1] >> (8 * l)) & 255u) << 8) |
-                                    (((v[2] >> (8 * l)) & 255u) << 16) |
-                                    (((v[3] >> (8 * l)) & 255u) << 24);
-            *(uint32_t*)(out + ((size_t)l * Mp + m) * Kp + k) = packed;
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                w[j] = ((v[4 * j] >> (8 * l)) & 255u) | (((v[4 * j + 1] >> (8 * l)) & 255u) << 8) |
+                       (((v[4 * j + 2] >> (8 * l)) & 255u) << 16) |
+                       (((v[4 * j + 3] >> (8 * l)) & 255u) << 24);
+            *(uint4*)(out + ((size_t)l * Mp + m) * Kp + k) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
 
 // transposing split: out[l][n][k] = byte l of B[k][n]; row k of B is
 // B + b_rows[k] ldb when b_rows is given (negative: a zero row).
-// One 64 (k) x 64 (n) tile per 256 threads: rows are read 128 bytes per warp
-// instruction, and every thread writes 16 consecutive k bytes of one n per limb.
+// One 128 (k) x 64 (n) tile per 256 threads.  Rows of B are read 256 bytes
+// per pair of warps; the bytes go to shared memory as [l][n][k] (rows padded
+// to 132 bytes: conflict-free in both phases) and leave as whole 128-byte
+// k-rows of every n, four threads per row.
+constexpr int SPLIT_ROW = 132;
 __global__ void __launch_bounds__(256)
 k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
              const int32_t* __restrict__ b_rows, int64_t sBr, int32_t K, int32_t N, int32_t Np,
              int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t bn) {
-    __shared__ uint32_t tile[64][65];
-    __shared__ const uint32_t* rowp[64];
+    extern __shared__ uint8_t split_smem[];  // [L][64][SPLIT_ROW] bytes
+    __shared__ const uint32_t* rowp[128];
     // batch item blockIdx.z
     B += (size_t)blockIdx.z * sB;
     if (b_rows) b_rows += (size_t)blockIdx.z * sBr;
     out += (size_t)blockIdx.z * L * Np * Kp;
     if (flags) flags += (size_t)blockIdx.z * (Np / bn) * (Kp / 128);
-    const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    if (threadIdx.x < 64) {
+    const int k0 = blockIdx.y * 128, n0 = blockIdx.x * 64;
+    if (threadIdx.x < 128) {
         const int k = k0 + threadIdx.x;
         int64_t src = -1;
         if (k < K) src = b_rows ? (int64_t)b_rows[k] : (int64_t)k;
         rowp[threadIdx.x] = src >= 0 ? B + (size_t)src * ldb : nullptr;
     }
     __syncthreads();
-    {
-        const int c = threadIdx.x & 63, r0 = threadIdx.x >> 6;  // 4 rows per pass
-        const int n = n0 + c;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int r = r0 + 4 * i;
-            const uint32_t* rp = rowp[r];
-            tile[r][c] = (rp && n < N) ? rp[n] : 0u;
-        }
-    }
-    __syncthreads();
-    const int nn = threadIdx.x & 63, kq = (threadIdx.x >> 6) * 16;
-    uint32_t v[16];
     uint32_t any = 0;
+    {
+        const int c = threadIdx.x & 63, r0 = threadIdx.x >> 6;  // 4 k rows per pass
+        const int n = n0 + c;
+        // all 32 loads first (no shared-memory store between them)
+        uint32_t v[32];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        v[i] = tile[kq + i][nn];
-        any |= v[i];
+        for (int i = 0; i < 32; ++i) {
+            const uint32_t* rp = rowp[r0 + 4 * i];
+            v[i] = (rp && n < N) ? rp[n] : 0u;
+        }
+        for (int l = 0; l < L; ++l) {
+            uint8_t* dst = split_smem + ((size_t)l * 64 + c) * SPLIT_ROW + r0;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) dst[4 * i] = (uint8_t)(v[i] >> (8 * l));
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) any |= v[i];
     }
-    const int n = n0 + nn, k = k0 + kq;  // n < Np and k + 16 <= Kp by the grid
+    any = __syncthreads_or(any != 0);
+    // thread: n = tid / 4, bytes [32 part, 32 part + 32) of the 128-byte k row
+    const int nn = threadIdx.x >> 2, part = threadIdx.x & 3;
+    const int n = n0 + nn;  // n < Np and k0 + 128 <= Kp by the grid
     for (int l = 0; l < L; ++l) {
-        uint32_t w[4];
+        const uint32_t* src =
+            (const uint32_t*)(split_smem + ((size_t)l * 64 + nn) * SPLIT_ROW + 32 * part);
+        uint32_t w[8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            w[j] = ((v[4 * j] >> (8 * l)) & 255u) | (((v[4 * j + 1] >> (8 * l)) & 255u) << 8) |
-                   (((v[4 * j + 2] >> (8 * l)) & 255u) << 16) |
-                   (((v[4 * j + 3] >> (8 * l)) & 255u) << 24);
-        *(uint4*)(out + ((size_t)l * Np + n) * Kp + k) = make_uint4(w[0], w[1], w[2], w[3]);
+        for (int j = 0; j < 8; ++j) w[j] = src[j];
+        uint4* dst = (uint4*)(out + ((size_t)l * Np + n) * Kp + k0 + 32 * part);
+        dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
     }
-    if (flags && any) flags[(size_t)(n / bn) * (Kp / 128) + k / 128] = 1;
+    if (flags && any && threadIdx.x == 0) {
+        // the 64 columns lie inside one bn-wide tile (bn is a multiple of 64)
+        flags[(size_t)(n0 / bn) * (Kp / 128) + k0 / 128] = 1;
+    }
 }
 
 // row index lists of the plain GEMM (see TcGemmArgs)
@@ -620,10 +651,10 @@ int limbs_for(uint32_t p) {
     return 4;
 }
 
-template <int L>
+template <int L, bool SMALL>
 static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t* err,
                   long long* launches) {
-    using Cfg = TcCfg<L>;
+    using Cfg = TcCfg<L, SMALL>;
     const int32_t Mp = (g.M + Cfg::BM - 1) / Cfg::BM * Cfg::BM;
     const int32_t Np = (g.N + Cfg::BN - 1) / Cfg::BN * Cfg::BN;
     const int32_t Kp = (g.K + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
@@ -639,14 +670,14 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         return GBGPU_ECUDA;
     }
     {
-        const int64_t total = (int64_t)Mp * (Kp / 4);
+        const int64_t total = (int64_t)Mp * (Kp / 16);
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256,
                                                                        148 * 32 / nb + 1));
         k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.a_rows, g.sAr, g.M, g.K,
                                                     Mp, Kp, L, Ap, fa);
-        dim3 gb(Np / 64, Kp / 64, nb);
-        k_split_cols<<<gb, 256, 0, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K, g.N, Np, Kp, L,
-                                        Bp, fb, Cfg::BN);
+        dim3 gb(Np / 64, Kp / 128, nb);
+        k_split_cols<<<gb, 256, L * 64 * SPLIT_ROW, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K,
+                                                          g.N, Np, Kp, L, Bp, fb, Cfg::BN);
         *launches += 2;
     }
     CUtensorMap ma, mb;
@@ -678,7 +709,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     }
     prm.err = err;
     prm.budget = 4000000000LL;  // about 2 s at 2 GHz per wait
-    cudaError_t e = cudaFuncSetAttribute(k_tc_submul<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_tc_submul<L, SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          Cfg::SMEM_BYTES);
     if (e != cudaSuccess) {
         set_error(std::string("tc smem attribute: ") + cudaGetErrorString(e));
@@ -693,7 +724,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
     }
-    k_tc_submul<L><<<grid, 192, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
+    k_tc_submul<L, SMALL><<<grid, 192, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
     ++*launches;
     if (prof) {
         cudaEventRecord(e1, s);
@@ -711,11 +742,12 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
 
 size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K, int32_t batch) {
     const int L = limbs_for(p);
-    const int BN = L == 1 ? 256 : (L == 2 ? 128 : 64);
-    const size_t Mp = (size_t)(M + 127) / 128 * 128, Np = (size_t)(N + BN - 1) / BN * BN;
+    // planes padded for the widest tile (256 columns), flags counted for the
+    // narrowest (64): enough for either tile shape
+    const size_t Mp = (size_t)(M + 127) / 128 * 128, Np = (size_t)(N + 255) / 256 * 256;
     const size_t Kp = (size_t)(K + 127) / 128 * 128;
     const size_t nb = (size_t)(batch > 0 ? batch : 1);
-    const size_t flags = nb * (Mp / 128 + Np / BN) * (Kp / 128);
+    const size_t flags = nb * (Mp / 128 + (size_t)(N + 63) / 64) * (Kp / 128);
     return nb * L * (Mp + Np) * Kp + ((flags + 255) & ~(size_t)255);
 }
 
@@ -731,11 +763,16 @@ int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err
         return GBGPU_EINVAL;
     }
     uint8_t* planes = (uint8_t*)workspace;
+    const bool small = g.K <= 256;  // at most two K steps: the small tile shape
     switch (limbs_for(g.p)) {
-        case 1: return tc_run<1>(g, planes, s, err, launches);
-        case 2: return tc_run<2>(g, planes, s, err, launches);
-        case 3: return tc_run<3>(g, planes, s, err, launches);
-        default: return tc_run<4>(g, planes, s, err, launches);
+        case 1:
+            return small ? tc_run<1, true>(g, planes, s, err, launches)
+                         : tc_run<1, false>(g, planes, s, err, launches);
+        case 2:
+            return small ? tc_run<2, true>(g, planes, s, err, launches)
+                         : tc_run<2, false>(g, planes, s, err, launches);
+        case 3: return tc_run<3, false>(g, planes, s, err, launches);
+        default: return tc_run<4, false>(g, planes, s, err, launches);
     }
 }
 
