@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -51,6 +52,12 @@
 namespace gbgpu {
 
 constexpr int KB = 128;  // pivots per elimination block
+
+// per-round statistics of the echelon on stderr when GBGPU_DEBUG is set
+static bool trace_rounds() {
+    static const bool on = getenv("GBGPU_DEBUG") != nullptr;
+    return on;
+}
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -70,6 +77,41 @@ __global__ void k_densify(int32_t n, const int32_t* __restrict__ rows,
         for (int64_t k = row_ptr[r] + lane; k < row_ptr[r + 1]; k += 32) {
             const int32_t c = cols[k] - col0;
             if (c >= 0 && c < width) o[c] = vals[k];
+        }
+    }
+}
+
+// Dense rows from CSR without a separate clear: row i of out (i < n) receives
+// CSR row rows[i], columns [from_i, nc), from_i = (i / stride) stride (0 when
+// stride is 0); columns left of from_i are not written.  Each CTA assembles
+// DS_COLS-column segments of a row in shared memory and writes them whole
+// with 16-byte stores (ld a multiple of 4, out 16-byte aligned).
+constexpr int DS_COLS = 16384;
+__global__ void __launch_bounds__(512)
+k_densify_seg(int32_t n, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_ptr,
+              const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals, int32_t nc,
+              int32_t stride, uint32_t* out, int64_t ld) {
+    extern __shared__ uint4 ds_smem[];
+    uint32_t* seg = (uint32_t*)ds_smem;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int32_t r = rows ? rows[i] : i;
+        const int64_t b = row_ptr[r], e = row_ptr[r + 1];
+        const int32_t from = stride ? (i / stride) * stride : 0;
+        uint32_t* o = out + (size_t)i * ld;
+        for (int32_t s0 = from; s0 < nc; s0 += DS_COLS) {
+            const int32_t w = min(DS_COLS, nc - s0);
+            for (int j = threadIdx.x; j < (w + 3) / 4; j += blockDim.x)
+                ds_smem[j] = make_uint4(0u, 0u, 0u, 0u);
+            __syncthreads();
+            for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
+                const int32_t c = cols[k] - s0;
+                if (c >= 0 && c < w) seg[c] = vals[k];
+            }
+            __syncthreads();
+            uint4* o4 = (uint4*)(o + s0);
+            for (int j = threadIdx.x; j < w / 4; j += blockDim.x) o4[j] = ds_smem[j];
+            for (int j = (w / 4) * 4 + threadIdx.x; j < w; j += blockDim.x) o[s0 + j] = seg[j];
+            __syncthreads();
         }
     }
 }
@@ -141,29 +183,57 @@ __device__ __forceinline__ uint32_t mod64(uint64_t x, uint32_t p, uint64_t m) {
     return (uint32_t)r;
 }
 
-constexpr int INV_LANES = 4;  // threads per column in k_neg_inverse
+constexpr int INV_THREADS = 512;  // threads of k_neg_inverse
+
+// sum of u_k v_k mod p for u_k, v_k < p < 2^31, from 16-bit halves of v
+// accumulated without reduction (each product < 2^47, at most 128 terms)
+__device__ __forceinline__ uint32_t fold_lohi(uint64_t lo, uint64_t hi, uint32_t p, uint64_t m) {
+    const uint32_t hr = mod64(hi, p, m);
+    return mod64((uint64_t)mod64(lo, p, m) + ((uint64_t)hr << 16), p, m);
+}
+
+// sum_{k in [k0, k1)} a[k sa] b[k sb] mod p (residues < p < 2^31), two
+// independent 16-bit-split accumulator pairs
+__device__ __forceinline__ uint32_t dot_lohi(const uint32_t* a, int sa, const uint32_t* b, int sb,
+                                             int k0, int k1, uint32_t p, uint64_t m) {
+    uint64_t lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0;
+    int k = k0;
+    for (; k + 1 < k1; k += 2) {
+        const uint32_t u0 = a[k * sa], v0 = b[k * sb];
+        const uint32_t u1 = a[(k + 1) * sa], v1 = b[(k + 1) * sb];
+        lo0 += (uint64_t)u0 * (v0 & 0xFFFFu);
+        hi0 += (uint64_t)u0 * (v0 >> 16);
+        lo1 += (uint64_t)u1 * (v1 & 0xFFFFu);
+        hi1 += (uint64_t)u1 * (v1 >> 16);
+    }
+    if (k < k1) {
+        const uint32_t u0 = a[k * sa], v0 = b[k * sb];
+        lo0 += (uint64_t)u0 * (v0 & 0xFFFFu);
+        hi0 += (uint64_t)u0 * (v0 >> 16);
+    }
+    return fold_lohi(lo0 + lo1, hi0 + hi1, p, m);
+}
 
 // -U^-1 mod p for unit upper triangular blocks.  Block b is read from
 // src + b * stride_b with leading dimension ld (kb x kb, kb <= KB); the result
 // (KB x KB, identity-padded) goes to out + b * ostride with leading dimension
-// old.  One CTA per block; column j of V = U^-1 is solved by back
-// substitution by the INV_LANES threads j*INV_LANES.. of one warp, each
-// summing a quarter of the terms,
-//   V[i][j] = -sum_{i<k<=j} U[i][k] V[k][j],
-// so the recurrence needs only warp-level synchronisation.  V is split into
-// 16-bit halves: each product is below 2^47 and the sums stay below 2^54, one
-// Barrett reduction per entry.
+// old.  One CTA per block, V = U^-1 built by doubling in shared memory: the
+// 8 x 8 diagonal blocks by back substitution, then for sz = 8, 16, 32, 64
+// every 2sz x 2sz diagonal block [[A, B], [0, C]] gets its top-right part
+// -A^-1 B C^-1 as two small products (T = B C^-1, then -A^-1 T).
 template <class F>
-__global__ void __launch_bounds__(KB * INV_LANES)
+__global__ void __launch_bounds__(INV_THREADS)
 k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, int32_t n_blocks,
               int32_t last_kb, uint32_t* out, int64_t ostride, int64_t old, F f) {
     extern __shared__ uint32_t inv_smem[];
     uint32_t(*U)[KB + 1] = (uint32_t(*)[KB + 1])inv_smem;
     uint32_t(*V)[KB + 1] = (uint32_t(*)[KB + 1])(inv_smem + KB * (KB + 1));
+    uint32_t* T = inv_smem + 2 * KB * (KB + 1);  // KB * KB / 4 entries
     const int b = blockIdx.x;
     const int kb = b == n_blocks - 1 ? last_kb : KB;
     const uint32_t* s = src + (size_t)b * stride_b;
-    for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
+    const int tid = threadIdx.x;
+    for (int t = tid; t < KB * KB; t += blockDim.x) {
         const int i = t / KB, j = t % KB;
         uint32_t v;
         if (i < kb && j < kb) v = s[(size_t)i * ld + j];
@@ -174,36 +244,44 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
     __syncthreads();
     const uint32_t p = f.p;
     const uint64_t m = ~0ull / p;
-    const int lane = threadIdx.x & 31;
-    const int j = threadIdx.x / INV_LANES, sub = threadIdx.x % INV_LANES;
-    // largest column of this warp: the loop runs uniformly over the warp
-    const int jmax = (threadIdx.x | 31) / INV_LANES;
-    for (int i = jmax - 1; i >= 0; --i) {
-        uint64_t lo = 0, hi = 0;
-        if (i < j) {
-            for (int k = i + 1 + sub; k <= j; k += INV_LANES) {
-                const uint64_t u = U[i][k];
+    if (tid < KB) {
+        // 8 x 8 diagonal blocks: V[i][j] = -sum_{i<k<=j} U[i][k] V[k][j]
+        const int b0 = tid & ~7, j = b0 + (tid & 7);
+        for (int i = j - 1; i >= b0; --i) {
+            uint64_t lo = 0, hi = 0;
+            for (int k = i + 1; k <= j; ++k) {
+                const uint32_t u = U[i][k];
                 const uint32_t v = V[k][j];
-                lo += u * (v & 0xFFFFu);
-                hi += u * (v >> 16);
+                lo += (uint64_t)u * (v & 0xFFFFu);
+                hi += (uint64_t)u * (v >> 16);
             }
-        }
-#pragma unroll
-        for (int o = 1; o < INV_LANES; o <<= 1) {
-            lo += __shfl_xor_sync(0xffffffffu, lo, o);
-            hi += __shfl_xor_sync(0xffffffffu, hi, o);
-        }
-        if (i < j && sub == 0) {
-            const uint32_t hr = mod64(hi, p, m);
-            const uint32_t acc = mod64((uint64_t)mod64(lo, p, m) + ((uint64_t)hr << 16), p, m);
+            const uint32_t acc = fold_lohi(lo, hi, p, m);
             V[i][j] = acc ? p - acc : 0u;
         }
-        __syncwarp();
     }
-    (void)lane;
     __syncthreads();
+    for (int sz = 8; sz < KB; sz *= 2) {
+        const int per = sz * sz, total = (KB / (2 * sz)) * per;
+        // T = B C^-1 (C^-1 upper triangular: k <= j)
+        for (int e = tid; e < total; e += blockDim.x) {
+            const int b0 = (e / per) * 2 * sz, i = (e % per) / sz, j = e % sz;
+            const uint32_t* urow = &U[b0 + i][b0 + sz];
+            const uint32_t* vcol = &V[b0 + sz][b0 + sz + j];
+            T[e] = dot_lohi(urow, 1, vcol, KB + 1, 0, j + 1, p, m);
+        }
+        __syncthreads();
+        // top-right of V = -A^-1 T (A^-1 upper triangular: k >= i)
+        for (int e = tid; e < total; e += blockDim.x) {
+            const int pr = e / per, b0 = pr * 2 * sz, i = (e % per) / sz, j = e % sz;
+            const uint32_t* Tp = T + pr * per;
+            const uint32_t acc =
+                dot_lohi(&V[b0 + i][b0], 1, Tp + j, sz, i, sz, p, m);
+            V[b0 + i][b0 + sz + j] = acc ? p - acc : 0u;
+        }
+        __syncthreads();
+    }
     uint32_t* o = out + (size_t)b * ostride;
-    for (int t = threadIdx.x; t < KB * KB; t += blockDim.x) {
+    for (int t = tid; t < KB * KB; t += blockDim.x) {
         const int i = t / KB, jj = t % KB;
         const uint32_t v = V[i][jj];
         o[(size_t)i * old + jj] = v ? f.p - v : 0u;  // -V
@@ -413,10 +491,10 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     extern __shared__ uint32_t pf_smem[];
     uint32_t(*P)[KB + 1] = (uint32_t(*)[KB + 1])pf_smem;
     uint32_t(*E)[KB + 1] = (uint32_t(*)[KB + 1])(pf_smem + KB * (KB + 1));
-    __shared__ int s_scratch[KB * PF_GROUPS / 32];
+    __shared__ int s_min[2][KB * PF_GROUPS / 32];  // double-buffered block minimum
     __shared__ uint8_t is_piv[KB];
-    __shared__ uint32_t s_inv;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
     const int r = tid % KB, g = tid / KB;  // row and column group of this thread
     for (int t = tid; t < KB * KB; t += nt) {
         const int i = t / KB, c = t % KB;
@@ -425,38 +503,53 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     }
     if (tid < KB) is_piv[tid] = 0;
     __syncthreads();
+    // Fraction-free: pivot rows are not scaled (they are normalised after the
+    // round) and a row r is updated as row_r <- a row_r - m row_i with
+    // a = P[i][c], m = P[r][c] (a nonzero multiple of the usual update, so the
+    // row space is the same) on the columns after c and on E; no inverse lies
+    // on the sequential path.  Column c itself is never read again, so no
+    // thread writes it and the multipliers need no barrier.  Two barriers per
+    // column: the minimum's and the end of the update.
     int k = 0;
     for (int c = 0; c < bw; ++c) {
-        const int cand = (g == 0 && r < n && !is_piv[r] && P[r][c] != 0u) ? r : INT_MAX;
-        const int i = block_min(cand, s_scratch);
-        if (i == INT_MAX) continue;
+        int cand = (g == 0 && r < n && !is_piv[r] && P[r][c] != 0u) ? r : INT_MAX;
+        for (int o = 16; o > 0; o >>= 1) cand = min(cand, __shfl_xor_sync(0xffffffffu, cand, o));
+        int* sm = s_min[c & 1];
+        if (lane == 0) sm[warp] = cand;
+        __syncthreads();
+        int i = sm[0];
+#pragma unroll
+        for (int w = 1; w < KB * PF_GROUPS / 32; ++w) i = min(i, sm[w]);
+        if (i == INT_MAX) continue;  // uniform: no barrier skipped by some threads only
         if (tid == 0) {
-            s_inv = inverse_mod(P[i][c], f.p);
             piv_pos[k] = i;
             piv_col[k] = col0 + c;
             is_piv[i] = 1;
         }
-        __syncthreads();
-        const uint32_t inv = s_inv;
-        // scale the pivot row (panel part from c, transform part)
-        for (int cc = c + tid; cc < bw; cc += nt) P[i][cc] = f.mulmod(P[i][cc], inv);
-        for (int cc = tid; cc < n; cc += nt) E[i][cc] = f.mulmod(E[i][cc], inv);
-        __syncthreads();
-        // eliminate column c from every other non-pivot row: the four threads
-        // of a row read its multiplier before any of them writes the row
         const bool active = r < n && r != i && !is_piv[r];
         const uint32_t m = active ? P[r][c] : 0u;
-        __syncthreads();
         if (m != 0u) {
+            const uint32_t ap = f.prep(P[i][c]);
             const uint32_t mp = f.prep(m);
-            for (int cc = c + g; cc < bw; cc += PF_GROUPS) {
-                const uint32_t v = P[i][cc];
-                if (v) P[r][cc] = f.mulsub(P[r][cc], mp, v);
-            }
-            for (int cc = g; cc < n; cc += PF_GROUPS) {
-                const uint32_t v = E[i][cc];
-                if (v) E[r][cc] = f.mulsub(E[r][cc], mp, v);
-            }
+            // four independent columns per pass (loads first, then stores)
+            auto update = [&](uint32_t* dst, const uint32_t* piv, int from, int to) {
+                for (int cc = from; cc < to; cc += 4 * PF_GROUPS) {
+                    uint32_t x[4], v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int col = cc + u * PF_GROUPS;
+                        v[u] = col < to ? piv[col] : 0u;
+                        x[u] = col < to ? dst[col] : 0u;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int col = cc + u * PF_GROUPS;
+                        if (col < to) dst[col] = f.mulsub(f.mulp(x[u], ap), mp, v[u]);
+                    }
+                }
+            };
+            update(P[r], P[i], c + 1 + g, bw);
+            update(E[r], E[i], g, n);
         }
         __syncthreads();
         ++k;
@@ -615,11 +708,11 @@ static int neg_inverse_big(Ctx& c, const F& f, const uint32_t* src, int64_t lds,
     BL_LAUNCH(k_copy_blocks<<<grid_of((int64_t)n_blocks * NB * NB), 256, 0, c.s>>>(
         src, lds, stride_src, n_blocks, last_nb, NB, U));
     BL_CUDA(cudaMemsetAsync(out, 0, sizeof(uint32_t) * (size_t)n_blocks * bstride, c.s));
-    const int bytes = 2 * KB * (KB + 1) * (int)sizeof(uint32_t);
+    const int bytes = (2 * KB * (KB + 1) + KB * KB / 4) * (int)sizeof(uint32_t);
     BL_CUDA(cudaFuncSetAttribute(k_neg_inverse<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     const int32_t n_sub = n_blocks * (NB / KB);
     const int64_t dstep = (int64_t)KB * (NB + 1);  // between 128-blocks on the diagonal
-    BL_LAUNCH(k_neg_inverse<F><<<n_sub, KB * INV_LANES, bytes, c.s>>>(U, NB, dstep, n_sub, KB, out,
+    BL_LAUNCH(k_neg_inverse<F><<<n_sub, INV_THREADS, bytes, c.s>>>(U, NB, dstep, n_sub, KB, out,
                                                                    dstep, NB, f));
     for (int32_t sz = KB; sz < NB; sz *= 2) {
         const int32_t items = n_blocks * (NB / (2 * sz));
@@ -707,9 +800,10 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         BL_CUDA(cub::DeviceRadixSort::SortPairs(tmp, bytes, lead_in, lead_sorted, in.work,
                                                 work_sorted, t, 0, 32, s));
         ++c.launches;
-        BL_CUDA(cudaMemsetAsync(W, 0, sizeof(uint32_t) * (size_t)t * ld, s));
-        BL_LAUNCH(k_densify<<<grid_of((int64_t)t * 32), 256, 0, s>>>(
-            t, work_sorted, in.row_ptr, in.cols, in.vals, 0, nc, W, ld));
+        BL_CUDA(cudaFuncSetAttribute(k_densify_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     DS_COLS * 4));
+        BL_LAUNCH(k_densify_seg<<<std::min(t, 148 * 3), 512, DS_COLS * 4, s>>>(
+            t, work_sorted, in.row_ptr, in.cols, in.vals, nc, 0, W, ld));
     }
     if (t > 0 && ncl > 0) {
         const int32_t NB = nb_for(ncl);
@@ -721,9 +815,10 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         int32_t* act = c.alloc<int32_t>(nbk);
         int32_t* span = c.alloc<int32_t>(nbk);
         if (!P || !Ninv || !X || !act || !span) return GBGPU_ENOMEM;
-        BL_CUDA(cudaMemsetAsync(P, 0, sizeof(uint32_t) * (size_t)ncl * ld, s));
-        BL_LAUNCH(k_densify_pivots<<<grid_of((int64_t)ncl * 32), 256, 0, s>>>(
-            ncl, in.piv_row, in.row_ptr, in.cols, in.vals, P, ld));
+        // pivot row of lead c into row c of P, from its diagonal block on (the
+        // only part any later step reads)
+        BL_LAUNCH(k_densify_seg<<<std::min(ncl, 148 * 3), 512, DS_COLS * 4, s>>>(
+            ncl, in.piv_row, in.row_ptr, in.cols, in.vals, nc, NB, P, ld));
         // -A_kk^-1 of every NB x NB diagonal block of A (read in place from P)
         BL_CHECK(neg_inverse_big(c, f, P, ld, (int64_t)NB * ld + NB, nbk, ncl - (nbk - 1) * NB, NB,
                                  Ninv));
@@ -813,7 +908,8 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     const int pf_bytes = 2 * KB * (KB + 1) * (int)sizeof(uint32_t);
     BL_CUDA(cudaFuncSetAttribute(k_panel_factor<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  pf_bytes));
-    const int32_t max_dirty = 64;  // dirty panels factorized per round (memory bound)
+    // every dirty panel is factorized in the round that finds it (batch <= 4096)
+    const int32_t max_dirty = std::max<int32_t>(1, std::min<int32_t>(npan, 4096));
     int32_t* chunk_rows = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* cursor = c.alloc<int32_t>(max_dirty);
     uint32_t* imeB = c.alloc<uint32_t>((size_t)max_dirty * KB * KB);
@@ -879,6 +975,23 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             BL_CHECK(gemm_args(c, g));
             BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
                                                                 piv_of_col, is_piv, wflag));
+            if (trace_rounds()) {
+                std::vector<int32_t> h_cur(n_dirty), h_np(n_dirty);
+                BL_CUDA(cudaMemcpyAsync(h_cur.data(), cursor, 4 * n_dirty, cudaMemcpyDeviceToHost, s));
+                BL_CUDA(cudaMemcpyAsync(h_np.data(), n_piv, 4 * n_dirty, cudaMemcpyDeviceToHost, s));
+                BL_CUDA(cudaStreamSynchronize(s));
+                long long rows_in = 0, piv = 0;
+                int mx = 0;
+                for (int q = 0; q < n_dirty; ++q) {
+                    rows_in += std::min(h_cur[q], KB);
+                    piv += h_np[q];
+                    mx = std::max(mx, h_cur[q]);
+                }
+                fprintf(stderr,
+                        "gbgpu echelon round %d: pending %d, dirty panels %d (first %d), chunk rows "
+                        "%lld (max %d), chunk pivots %lld\n",
+                        rounds, n_pend, n_dirty, j0 / KB, rows_in, mx, piv);
+            }
         }
         // all pivots of the round, ascending columns; normalise
         BL_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wflag, wpos, ncr, s));
@@ -889,6 +1002,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         BL_CUDA(cudaMemcpyAsync(&last_flag, wflag + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         const int32_t n_new = last_pos + last_flag;
+        if (trace_rounds()) fprintf(stderr, "gbgpu echelon round %d: new pivots %d\n", rounds, n_new);
         BL_LAUNCH(k_gather_rows<<<grid_of(n_new), 256, 0, s>>>(n_new, pc, piv_of_col, prow,
                                                                counters + 2));
         BL_LAUNCH(k_normalize_at<F><<<std::max(1, std::min(n_new, 148 * 8)), 256, 0, s>>>(

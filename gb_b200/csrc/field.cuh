@@ -44,6 +44,17 @@ struct FieldSmall {
     }
     // a * b mod p for arbitrary a, b < p (normalisation)
     __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) const { return mul(a, b); }
+    // x * a mod p with ap = prep(a)
+    __device__ __forceinline__ uint32_t mulp(uint32_t x, uint32_t ap) const { return mul(ap, x); }
+    // a^-1 = a^(p-2) mod p (0 < a < p), square and multiply
+    __device__ __forceinline__ uint32_t inv(uint32_t a) const {
+        uint32_t r = 1u, b = a;
+        for (uint32_t e = p - 2u; e; e >>= 1) {
+            if (e & 1u) r = mul(r, b);
+            b = mul(b, b);
+        }
+        return r;
+    }
 };
 
 struct FieldMont {
@@ -77,6 +88,19 @@ struct FieldMont {
     }
     __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) const {
         return redc((uint64_t)prep(a) * b);
+    }
+    // x * a mod p with ap = prep(a)
+    __device__ __forceinline__ uint32_t mulp(uint32_t x, uint32_t ap) const {
+        return redc((uint64_t)ap * x);
+    }
+    // a^-1 = a^(p-2) mod p (0 < a < p), square and multiply in Montgomery form
+    __device__ __forceinline__ uint32_t inv(uint32_t a) const {
+        uint32_t r = prep(1u), b = prep(a);
+        for (uint32_t e = p - 2u; e; e >>= 1) {
+            if (e & 1u) r = redc((uint64_t)r * b);
+            b = redc((uint64_t)b * b);
+        }
+        return redc(r);
     }
 };
 
