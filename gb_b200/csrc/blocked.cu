@@ -466,13 +466,23 @@ __global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
 
 // Row echelon of one panel (the 128 columns of panel dpanel[d], on the n <= KB
 // rows chunk_rows[d KB + i] of Dp) in shared memory, recording the
-// transformation E (E * old = rows whose panel part is in echelon form with
-// unit pivots; the rows that are not pivots become zero in the panel).
-// Writes I - E (KB x KB, zero outside the leading n x n block), so that
-// old - (I - E) old = E old is one in-place GEMM update of the chunk rows,
-// and the panel-local index and column of every pivot, in increasing column
-// order, and their count.
-constexpr int PF_GROUPS = 4;  // threads per row in k_panel_factor
+// transformation E (E * old = rows whose panel part is in echelon form; the
+// rows that are not pivots become zero in the panel).  Writes I - E (KB x KB,
+// zero outside the leading n x n block), so that old - (I - E) old = E old is
+// one in-place GEMM update of the chunk rows, and the panel-local index and
+// column of every pivot, in increasing column order, and their count.
+//
+// Every row keeps its lead (first nonzero panel column).  A step takes the
+// non-pivot row with the smallest (lead, index) as the next pivot -- the same
+// pivot the column-by-column search finds -- and updates exactly the other
+// non-pivot rows with that lead, fraction-free: row_r <- a row_r - m row_i
+// (a = P[i][c], m = P[r][c]), which keeps the row space and needs no inverse
+// (pivot rows are normalised after the round).  Column c is never read
+// again, so it is not written.  The eight threads of a row are adjacent lanes;
+// they recompute the row's lead from the values they just wrote.  One step
+// per pivot, two barriers per step.
+constexpr int PF_GROUPS = 8;     // threads (adjacent lanes) per row in k_panel_factor
+constexpr int PF_LD = KB + 8;    // row stride of P and E: conflict-free for 8 lanes per row
 
 template <class F>
 __global__ void __launch_bounds__(KB * PF_GROUPS)
@@ -489,67 +499,99 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     int32_t* piv_col = piv_col_b + d * KB;
     int32_t* n_piv = n_piv_b + d;
     extern __shared__ uint32_t pf_smem[];
-    uint32_t(*P)[KB + 1] = (uint32_t(*)[KB + 1])pf_smem;
-    uint32_t(*E)[KB + 1] = (uint32_t(*)[KB + 1])(pf_smem + KB * (KB + 1));
+    uint32_t(*P)[PF_LD] = (uint32_t(*)[PF_LD])pf_smem;
+    uint32_t(*E)[PF_LD] = (uint32_t(*)[PF_LD])(pf_smem + KB * PF_LD);
     __shared__ int s_min[2][KB * PF_GROUPS / 32];  // double-buffered block minimum
+    __shared__ int lead[KB];
     __shared__ uint8_t is_piv[KB];
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int r = tid % KB, g = tid / KB;  // row and column group of this thread
+    const int r = tid / PF_GROUPS, g = tid % PF_GROUPS;  // row and column group of this thread
+    const unsigned grp = 0xFFu << (lane & ~7);           // the row's eight lanes
     for (int t = tid; t < KB * KB; t += nt) {
         const int i = t / KB, c = t % KB;
         P[i][c] = (i < n && c < bw) ? Dp[(size_t)rows[i] * ld + pj + c] : 0u;
         E[i][c] = i == c ? 1u : 0u;
     }
-    if (tid < KB) is_piv[tid] = 0;
     __syncthreads();
-    // Fraction-free: pivot rows are not scaled (they are normalised after the
-    // round) and a row r is updated as row_r <- a row_r - m row_i with
-    // a = P[i][c], m = P[r][c] (a nonzero multiple of the usual update, so the
-    // row space is the same) on the columns after c and on E; no inverse lies
-    // on the sequential path.  Column c itself is never read again, so no
-    // thread writes it and the multipliers need no barrier.  Two barriers per
-    // column: the minimum's and the end of the update.
+    {
+        int l = INT_MAX;
+        if (r < n)
+            for (int cc = g; cc < bw; cc += PF_GROUPS)
+                if (P[r][cc] != 0u) {
+                    l = cc;
+                    break;
+                }
+        l = min(l, __shfl_xor_sync(0xffffffffu, l, 1));
+        l = min(l, __shfl_xor_sync(0xffffffffu, l, 2));
+        l = min(l, __shfl_xor_sync(0xffffffffu, l, 4));
+        if (g == 0) {
+            lead[r] = l;
+            is_piv[r] = 0;
+        }
+    }
+    __syncthreads();
     int k = 0;
-    for (int c = 0; c < bw; ++c) {
-        int cand = (g == 0 && r < n && !is_piv[r] && P[r][c] != 0u) ? r : INT_MAX;
-        for (int o = 16; o > 0; o >>= 1) cand = min(cand, __shfl_xor_sync(0xffffffffu, cand, o));
-        int* sm = s_min[c & 1];
-        if (lane == 0) sm[warp] = cand;
+    for (int step = 0; step < KB; ++step) {
+        int key = INT_MAX;
+        if (g == 0 && r < n && !is_piv[r] && lead[r] != INT_MAX) key = lead[r] * KB + r;
+        for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+        int* sm = s_min[step & 1];
+        if (lane == 0) sm[warp] = key;
         __syncthreads();
-        int i = sm[0];
+        int best = sm[0];
 #pragma unroll
-        for (int w = 1; w < KB * PF_GROUPS / 32; ++w) i = min(i, sm[w]);
-        if (i == INT_MAX) continue;  // uniform: no barrier skipped by some threads only
+        for (int w = 1; w < KB * PF_GROUPS / 32; ++w) best = min(best, sm[w]);
+        if (best == INT_MAX) break;  // uniform: no pivot left in the panel
+        const int c = best / KB, i = best % KB;
         if (tid == 0) {
             piv_pos[k] = i;
             piv_col[k] = col0 + c;
             is_piv[i] = 1;
         }
-        const bool active = r < n && r != i && !is_piv[r];
-        const uint32_t m = active ? P[r][c] : 0u;
-        if (m != 0u) {
+        const bool active = r < n && r != i && !is_piv[r] && lead[r] == c;
+        __syncwarp();  // every lane has read lead[] before a lane of its row writes it
+        if (active) {
             const uint32_t ap = f.prep(P[i][c]);
-            const uint32_t mp = f.prep(m);
+            const uint32_t mp = f.prep(P[r][c]);
+            int nl = INT_MAX;
             // four independent columns per pass (loads first, then stores)
-            auto update = [&](uint32_t* dst, const uint32_t* piv, int from, int to) {
-                for (int cc = from; cc < to; cc += 4 * PF_GROUPS) {
-                    uint32_t x[4], v[4];
+            for (int cc = c + 1 + g; cc < bw; cc += 4 * PF_GROUPS) {
+                uint32_t x[4], v[4];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int col = cc + u * PF_GROUPS;
-                        v[u] = col < to ? piv[col] : 0u;
-                        x[u] = col < to ? dst[col] : 0u;
-                    }
+                for (int u = 0; u < 4; ++u) {
+                    const int col = cc + u * PF_GROUPS;
+                    v[u] = col < bw ? P[i][col] : 0u;
+                    x[u] = col < bw ? P[r][col] : 0u;
+                }
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int col = cc + u * PF_GROUPS;
-                        if (col < to) dst[col] = f.mulsub(f.mulp(x[u], ap), mp, v[u]);
+                for (int u = 0; u < 4; ++u) {
+                    const int col = cc + u * PF_GROUPS;
+                    if (col < bw) {
+                        const uint32_t y = f.mulsub(f.mulp(x[u], ap), mp, v[u]);
+                        P[r][col] = y;
+                        if (y != 0u && col < nl) nl = col;
                     }
                 }
-            };
-            update(P[r], P[i], c + 1 + g, bw);
-            update(E[r], E[i], g, n);
+            }
+            for (int cc = g; cc < n; cc += 4 * PF_GROUPS) {
+                uint32_t x[4], v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int col = cc + u * PF_GROUPS;
+                    v[u] = col < n ? E[i][col] : 0u;
+                    x[u] = col < n ? E[r][col] : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int col = cc + u * PF_GROUPS;
+                    if (col < n) E[r][col] = f.mulsub(f.mulp(x[u], ap), mp, v[u]);
+                }
+            }
+            nl = min(nl, __shfl_xor_sync(grp, nl, 1));
+            nl = min(nl, __shfl_xor_sync(grp, nl, 2));
+            nl = min(nl, __shfl_xor_sync(grp, nl, 4));
+            if (g == 0) lead[r] = nl;
         }
         __syncthreads();
         ++k;
@@ -905,7 +947,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         BL_CUDA(cudaMemsetAsync(is_piv, 0, t, s));
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)t * 32), 256, 0, s>>>(t, nullptr, ncr, Dp, ld, lead));
     }
-    const int pf_bytes = 2 * KB * (KB + 1) * (int)sizeof(uint32_t);
+    const int pf_bytes = 2 * KB * PF_LD * (int)sizeof(uint32_t);
     BL_CUDA(cudaFuncSetAttribute(k_panel_factor<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  pf_bytes));
     // every dirty panel is factorized in the round that finds it (batch <= 4096)
