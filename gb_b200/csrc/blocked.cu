@@ -424,6 +424,18 @@ __global__ void k_bucket_dirty(int32_t n, const int32_t* __restrict__ pend,
     }
 }
 
+// row list of the pivot rows of every chunk (the others -1): only the pivot
+// rows take the panel transformation; the rest are cleared later by the
+// round's elimination against all new pivots
+__global__ void k_pivot_rowlist(const int32_t* __restrict__ n_piv, const int32_t* __restrict__ piv_pos,
+                                const int32_t* __restrict__ chunk_rows, int32_t* drows) {
+    const int d = blockIdx.x;
+    for (int k = threadIdx.x; k < n_piv[d]; k += blockDim.x) {
+        const int32_t pos = piv_pos[d * KB + k];
+        drows[d * KB + pos] = chunk_rows[d * KB + pos];
+    }
+}
+
 // the factorized pivots of every chunk
 __global__ void k_register_chunks(const int32_t* __restrict__ n_piv,
                                   const int32_t* __restrict__ piv_pos,
@@ -724,10 +736,10 @@ static int gemm_batched(Ctx& c, uint32_t* D, int64_t ldd, int64_t sD, const uint
     return gemm_args(c, g);
 }
 
-// elimination block size: powers of two from 128 to 1024
-static int32_t nb_for(int64_t n) {
+// elimination block size: powers of two from 128 to `cap` (1024 by default)
+static int32_t nb_for(int64_t n, int32_t cap = 8 * KB) {
     int32_t nb = KB;
-    while (nb < n && nb < 8 * KB) nb *= 2;
+    while (nb < n && nb < cap) nb *= 2;
     return nb;
 }
 
@@ -848,7 +860,7 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
             t, work_sorted, in.row_ptr, in.cols, in.vals, nc, 0, W, ld));
     }
     if (t > 0 && ncl > 0) {
-        const int32_t NB = nb_for(ncl);
+        const int32_t NB = nb_for(ncl, 16 * KB);
         const int64_t bstride = (int64_t)NB * (NB + 1);
         uint32_t* P = c.alloc<uint32_t>((size_t)ncl * ld);
         const int32_t nbk = (ncl + NB - 1) / NB;
@@ -958,7 +970,9 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     int32_t* piv_pos = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* piv_colb = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* n_piv = c.alloc<int32_t>(max_dirty);
-    if (!chunk_rows || !cursor || !imeB || !piv_pos || !piv_colb || !n_piv) return GBGPU_ENOMEM;
+    int32_t* piv_rows = c.alloc<int32_t>((size_t)max_dirty * KB);
+    if (!chunk_rows || !cursor || !imeB || !piv_pos || !piv_colb || !n_piv || !piv_rows)
+        return GBGPU_ENOMEM;
     int rounds = 0;
     bool first = true;
     while (t > 0 && ncr > 0) {
@@ -1005,14 +1019,20 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
                                                                       cursor, chunk_rows));
             BL_LAUNCH(k_panel_factor<F><<<n_dirty, KB * PF_GROUPS, pf_bytes, s>>>(
                 Dp, ld, chunk_rows, dpanel, cursor, ncr, imeB, piv_pos, piv_colb, n_piv, f));
-            // chunk rows (columns j0..) <- old - (I - E_d) old = E_d old, in place:
-            // the limb planes of `old` are cut before the product writes the rows
+            // pivot rows of every chunk (columns j0..) <- old - (I - E_d) old =
+            // E_d old, in place: the limb planes of `old` are cut before the
+            // product writes the rows.  The non-pivot chunk rows keep their
+            // values: their panel parts lie in the span of the pivot rows', so
+            // the elimination against the round's pivots below clears them.
+            BL_LAUNCH(k_fill_i32<<<grid_of((int64_t)n_dirty * KB), 256, 0, s>>>(
+                piv_rows, n_dirty * KB, -1));
+            BL_LAUNCH(k_pivot_rowlist<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, chunk_rows, piv_rows));
             TcGemmArgs g{c.p, KB, width, KB, imeB, KB, Dp + j0, ld, Dp + j0, ld};
             g.batch = n_dirty;
             g.sA = (int64_t)KB * KB;
             g.b_rows = chunk_rows;
             g.sBr = KB;
-            g.d_rows = chunk_rows;
+            g.d_rows = piv_rows;
             g.sDr = KB;
             BL_CHECK(gemm_args(c, g));
             BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
