@@ -133,8 +133,7 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
 // Two tile shapes per limb count.  The large one (one CTA per SM) serves long
 // K; the small one (K <= 256, two CTAs per SM, TMEM <= 256 columns each) lets
 // one CTA's loads and MMAs overlap the other's D read-modify-write when the
-// epilogue dominates.  The small shape stages its epilogue blocks in the
-// (then idle) operand ring.
+// epilogue dominates.
 template <int L, bool SMALL = false>
 struct TcCfg {
     static constexpr int BM = 128;
@@ -144,17 +143,20 @@ struct TcCfg {
     static constexpr int A_BYTES = BM * BK;
     static constexpr int B_BYTES = BN * BK;
     static constexpr int STAGE_BYTES = L * (A_BYTES + B_BYTES);
-    static constexpr int STAGES = SMALL ? 2 : (L == 1 ? 4 : (L == 2 ? 3 : 2));
+    static constexpr int STAGES = SMALL ? 1 : (L == 1 ? 4 : (L == 2 ? 3 : 2));
     static constexpr int TMEM_COLS =
         NW * BN <= 64 ? 64 : (NW * BN <= 128 ? 128 : (NW * BN <= 256 ? 256 : 512));
     // epilogue staging: a 32 x 32 block per epilogue warp (padded rows) and the
     // D row pointers of its 32 rows
-    static constexpr int STG_BYTES = SMALL ? 0 : 4 * 32 * 33 * 4;
+    static constexpr int STG_BYTES = 4 * 32 * 33 * 4;
     static constexpr int ROWP_BYTES = 4 * 32 * 8;
     static constexpr int BAR_OFF = STAGES * STAGE_BYTES;
-    static constexpr int STG_OFF = SMALL ? 0 : BAR_OFF + 256;
-    static constexpr int ROWP_OFF = BAR_OFF + 256 + STG_BYTES;
-    static constexpr int SMEM_BYTES = ROWP_OFF + ROWP_BYTES + 1024 /*align*/;
+    static constexpr int STG_OFF = BAR_OFF + 256;
+    static constexpr int ROWP_OFF = STG_OFF + STG_BYTES;
+    static constexpr int USED_BYTES = ROWP_OFF + ROWP_BYTES + 1024 /*align*/;
+    // the small shape asks for enough shared memory that at most two CTAs
+    // share an SM (their TMEM allocations, 2 x 256 columns, then always fit)
+    static constexpr int SMEM_BYTES = SMALL && USED_BYTES < 100 * 1024 ? 100 * 1024 : USED_BYTES;
     static constexpr int MIN_CTAS = SMALL ? 2 : 1;
     // K bytes per panel: L * 255^2 * K < 2^31
     static constexpr int PANEL_KB = L == 1 ? 256 : (L == 2 ? 128 : (L == 3 ? 85 : 64));
@@ -163,16 +165,21 @@ struct TcCfg {
                                       | ((uint32_t)(BN >> 3) << 17)  // N
                                       | ((uint32_t)(BM >> 4) << 24); // M
     static_assert(!SMALL || L <= 2, "small tiles for one or two limbs only");
-    static_assert(!SMALL || STAGES * STAGE_BYTES >= 4 * 32 * 33 * 4, "staging fits the ring");
+    static_assert(!SMALL || 2 * TMEM_COLS <= 512, "two small CTAs share the TMEM");
     static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 };
+
+// tiles of one batch item are visited in groups of TC_GROUP_M row tiles, all
+// column tiles of a group before the next, so that the B tiles of a column are
+// reused from L2 by the row tiles of the group
+constexpr int TC_GROUP_M = 8;
 
 struct TcParams {
     uint32_t* D;
     int64_t ldd, sD;
     const int32_t* d_rows;  // optional: row m of D is D + d_rows[m] ldd (< 0: not written)
     int64_t sDr;
-    int32_t M, N, Mp, Np, nkb;
+    int32_t M, N, Mp, Np, nkb, batch;
     // nonzero flags of the 128-row x 128-byte A tiles ([Mp/128][nkb]) and of the
     // BN-row x 128-byte B tiles ([Np/BN][nkb]); a K step where either tile is
     // zero contributes nothing and is skipped (NULL: no skipping)
@@ -206,19 +213,34 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
-    const int z = blockIdx.z;  // batch item
     const int nkb = prm.nkb;
-    const uint8_t* fa =
-        prm.fa ? prm.fa + ((size_t)z * (prm.Mp / C::BM) + blockIdx.y) * nkb : nullptr;
-    const uint8_t* fb =
-        prm.fb ? prm.fb + ((size_t)z * (prm.Np / C::BN) + blockIdx.x) * nkb : nullptr;
-    auto live = [&](int kb) { return (!fa || fa[kb]) && (!fb || fb[kb]); };
-    int n_it = 0;  // K steps this tile really needs
-    for (int kb = 0; kb < nkb; ++kb) n_it += live(kb) ? 1 : 0;
-    if (n_it == 0) return;  // A B is zero on this tile: D stays as it is
-    if (prm.steps && threadIdx.x == 0) atomicAdd(prm.steps, (unsigned long long)n_it);
-    const int npanels = (n_it + C::PANEL_KB - 1) / C::PANEL_KB;
+    const int tiles_m = prm.Mp / C::BM, tiles_n = prm.Np / C::BN;
+    const int per_z = tiles_m * tiles_n;
+    const int total = per_z * prm.batch;
+    // tile t -> batch item z, row tile mt, column tile nt (grouped raster)
+    auto coords = [&](int t, int& z, int& mt, int& nt) {
+        z = t / per_z;
+        const int r = t - z * per_z;
+        const int span = TC_GROUP_M * tiles_n;
+        const int first_m = (r / span) * TC_GROUP_M;
+        const int gm = min(TC_GROUP_M, tiles_m - first_m);
+        const int rr = r - (r / span) * span;
+        mt = first_m + rr % gm;
+        nt = rr / gm;
+    };
+    // flags of the tile's A row block and B column block (NULL: all live)
+    auto flag_ptrs = [&](int z, int mt, int nt, const uint8_t*& fa, const uint8_t*& fb) {
+        fa = prm.fa ? prm.fa + ((size_t)z * tiles_m + mt) * nkb : nullptr;
+        fb = prm.fb ? prm.fb + ((size_t)z * tiles_n + nt) * nkb : nullptr;
+    };
+    auto live = [&](const uint8_t* fa, const uint8_t* fb, int kb) {
+        return (!fa || fa[kb]) && (!fb || fb[kb]);
+    };
+    auto live_steps = [&](const uint8_t* fa, const uint8_t* fb) {
+        int n_it = 0;
+        for (int kb = 0; kb < nkb; ++kb) n_it += live(fa, fb, kb) ? 1 : 0;
+        return n_it;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::STAGES; ++s) {
@@ -242,74 +264,103 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
+    // Every role walks the same tile sequence and skips the tiles whose
+    // product is zero.  The operand ring and the accumulator phases continue
+    // across tiles, so the producer fetches the next tile while the epilogue
+    // drains the current one.
     if (warp == 0) {
         if (lane == 0) {
             // ---- producer ----
-            int issued = 0;
-            for (int kb = 0, it = 0; kb < nkb; ++kb) {
-                if (!live(kb)) continue;
-                const int s = it % C::STAGES;
-                const uint32_t ph = (it / C::STAGES) & 1;
-                if (*abort_flag || !mbar_wait(empty_bar(s), ph ^ 1, prm.budget)) {
-                    *abort_flag = 1;
-                    break;
+            int it = 0;
+            bool stop = false;
+            for (int t = blockIdx.x; t < total && !stop; t += gridDim.x) {
+                int z, mt, nt;
+                coords(t, z, mt, nt);
+                const uint8_t *fa, *fb;
+                flag_ptrs(z, mt, nt, fa, fb);
+                const int m0 = mt * C::BM, n0 = nt * C::BN;
+                int n_tile = 0;
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!live(fa, fb, kb)) continue;
+                    const int s = it % C::STAGES;
+                    const uint32_t ph = (it / C::STAGES) & 1;
+                    if (*abort_flag || !mbar_wait(empty_bar(s), ph ^ 1, prm.budget)) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    mbar_expect_tx(full_bar(s), C::STAGE_BYTES);
+                    const uint32_t st = base + s * C::STAGE_BYTES;
+                    for (int l = 0; l < L; ++l)
+                        tma_load_2d(st + l * C::A_BYTES, &mapA, kb * C::BK,
+                                    (z * L + l) * prm.Mp + m0, full_bar(s));
+                    for (int l = 0; l < L; ++l)
+                        tma_load_2d(st + L * C::A_BYTES + l * C::B_BYTES, &mapB, kb * C::BK,
+                                    (z * L + l) * prm.Np + n0, full_bar(s));
+                    ++it;
+                    ++n_tile;
                 }
-                mbar_expect_tx(full_bar(s), C::STAGE_BYTES);
-                const uint32_t st = base + s * C::STAGE_BYTES;
-                for (int l = 0; l < L; ++l)
-                    tma_load_2d(st + l * C::A_BYTES, &mapA, kb * C::BK,
-                                (z * L + l) * prm.Mp + m0, full_bar(s));
-                for (int l = 0; l < L; ++l)
-                    tma_load_2d(st + L * C::A_BYTES + l * C::B_BYTES, &mapB, kb * C::BK,
-                                (z * L + l) * prm.Np + n0, full_bar(s));
-                issued = ++it;
+                if (prm.steps && n_tile) atomicAdd(prm.steps, (unsigned long long)n_tile);
             }
             // on abort, let the copies already issued land before the CTA exits
-            for (int kb = issued > C::STAGES ? issued - C::STAGES : 0; kb < issued; ++kb)
-                mbar_wait(full_bar(kb % C::STAGES), (kb / C::STAGES) & 1, prm.budget);
+            for (int q = it > C::STAGES ? it - C::STAGES : 0; q < it; ++q)
+                mbar_wait(full_bar(q % C::STAGES), (q / C::STAGES) & 1, prm.budget);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer ----
-            for (int kb = 0, it = 0; kb < nkb; ++kb) {
-                if (!live(kb)) continue;
-                const int s = it % C::STAGES;
-                const uint32_t ph = (it / C::STAGES) & 1;
-                const int pk = it % C::PANEL_KB;
-                const int panel = it / C::PANEL_KB;
-                if (pk == 0 && panel > 0) {
-                    // accumulators are free once the epilogue read the last panel
-                    if (*abort_flag || !mbar_wait(tempty_bar, (panel - 1) & 1, prm.budget)) {
-                        *abort_flag = 1;
-                        break;
-                    }
-                }
-                if (*abort_flag || !mbar_wait(full_bar(s), ph, prm.budget)) {
-                    *abort_flag = 1;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t st = base + s * C::STAGE_BYTES;
-#pragma unroll
-                for (int i = 0; i < L; ++i) {
-#pragma unroll
-                    for (int j = 0; j < L; ++j) {
-                        const int w = i + j;
-                        const bool first_pair = (i == (w > L - 1 ? w - (L - 1) : 0));
-#pragma unroll
-                        for (int kk = 0; kk < C::BK / 32; ++kk) {
-                            const uint64_t ad =
-                                umma_desc_sw128(st + i * C::A_BYTES + kk * 32);
-                            const uint64_t bd = umma_desc_sw128(
-                                st + L * C::A_BYTES + j * C::B_BYTES + kk * 32);
-                            const uint32_t acc = (pk == 0 && kk == 0 && first_pair) ? 0u : 1u;
-                            tc_mma_i8(tmem + (uint32_t)(w * C::BN), ad, bd, C::IDESC, acc);
+            int it = 0, pc = 0;  // k steps and accumulator panels so far
+            bool stop = false;
+            for (int t = blockIdx.x; t < total && !stop; t += gridDim.x) {
+                int z, mt, nt;
+                coords(t, z, mt, nt);
+                const uint8_t *fa, *fb;
+                flag_ptrs(z, mt, nt, fa, fb);
+                const int n_it = live_steps(fa, fb);
+                for (int kb = 0, j = 0; kb < nkb && j < n_it; ++kb) {
+                    if (!live(fa, fb, kb)) continue;
+                    const int s = it % C::STAGES;
+                    const uint32_t ph = (it / C::STAGES) & 1;
+                    const int pk = j % C::PANEL_KB;
+                    if (pk == 0 && pc > 0) {
+                        // accumulators are free once the epilogue read the last panel
+                        if (*abort_flag || !mbar_wait(tempty_bar, (pc - 1) & 1, prm.budget)) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
                         }
                     }
+                    if (*abort_flag || !mbar_wait(full_bar(s), ph, prm.budget)) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = base + s * C::STAGE_BYTES;
+#pragma unroll
+                    for (int i = 0; i < L; ++i) {
+#pragma unroll
+                        for (int jj = 0; jj < L; ++jj) {
+                            const int w = i + jj;
+                            const bool first_pair = (i == (w > L - 1 ? w - (L - 1) : 0));
+#pragma unroll
+                            for (int kk = 0; kk < C::BK / 32; ++kk) {
+                                const uint64_t ad = umma_desc_sw128(st + i * C::A_BYTES + kk * 32);
+                                const uint64_t bd = umma_desc_sw128(
+                                    st + L * C::A_BYTES + jj * C::B_BYTES + kk * 32);
+                                const uint32_t acc = (pk == 0 && kk == 0 && first_pair) ? 0u : 1u;
+                                tc_mma_i8(tmem + (uint32_t)(w * C::BN), ad, bd, C::IDESC, acc);
+                            }
+                        }
+                    }
+                    tc_commit(empty_bar(s));
+                    if (pk == C::PANEL_KB - 1 || j == n_it - 1) {
+                        tc_commit(tfull_bar);
+                        ++pc;
+                    }
+                    ++it;
+                    ++j;
                 }
-                tc_commit(empty_bar(s));
-                if (pk == C::PANEL_KB - 1 || it == n_it - 1) tc_commit(tfull_bar);
-                ++it;
             }
         }
     } else {
@@ -319,76 +370,89 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         // runs along rows (one 128-byte row segment per warp instruction).
         const int q = warp & 3;
         const int row = q * 32 + lane;
-        const int gm = m0 + row;
         const uint32_t p = prm.p;
-        // (small tiles: one K panel, so the ring is idle once the accumulators are full)
         uint32_t(*stg)[33] =
             (uint32_t(*)[33])(gbase + C::STG_OFF + (size_t)(warp - 2) * 32 * 33 * 4);
         uint32_t** rowp = (uint32_t**)(gbase + C::ROWP_OFF + (size_t)(warp - 2) * 32 * 8);
-        {
-            uint32_t* mine = nullptr;
-            if (gm < prm.M) {
-                int64_t ri = gm;
-                if (prm.d_rows) ri = prm.d_rows[(size_t)z * prm.sDr + gm];
-                if (ri >= 0) mine = prm.D + (size_t)z * prm.sD + (size_t)ri * prm.ldd;
-            }
-            rowp[lane] = mine;
-        }
-        __syncwarp();
-        for (int panel = 0; panel < npanels; ++panel) {
-            bool ok = true;
-            if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar, panel & 1, prm.budget);
-            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-            if (!ok) {
-                if (lane == 0) *abort_flag = 1;
-                break;
-            }
-            tc_fence_after();
-            for (int c0 = 0; c0 < C::BN; c0 += 32) {
-                const int gn = n0 + c0 + lane;
-                const bool col_ok = gn < prm.N;
-                // D values of the block (row r, column gn), issued before the fold
-                uint32_t dv[32];
-#pragma unroll
-                for (int r = 0; r < 32; ++r) {
-                    const uint32_t* rp = rowp[r];
-                    dv[r] = (rp && col_ok) ? rp[gn] : 0u;
+        int pc = 0;
+        bool stop = false;
+        for (int t = blockIdx.x; t < total && !stop; t += gridDim.x) {
+            int z, mt, nt;
+            coords(t, z, mt, nt);
+            const uint8_t *fa, *fb;
+            flag_ptrs(z, mt, nt, fa, fb);
+            const int n_it = live_steps(fa, fb);
+            if (n_it == 0) continue;  // A B is zero on this tile: D stays as it is
+            const int npanels = (n_it + C::PANEL_KB - 1) / C::PANEL_KB;
+            const int m0 = mt * C::BM, n0 = nt * C::BN;
+            const int gm = m0 + row;
+            {
+                uint32_t* mine = nullptr;
+                if (gm < prm.M) {
+                    int64_t ri = gm;
+                    if (prm.d_rows) ri = prm.d_rows[(size_t)z * prm.sDr + gm];
+                    if (ri >= 0) mine = prm.D + (size_t)z * prm.sD + (size_t)ri * prm.ldd;
                 }
-                uint32_t v[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j) v[j] = 0;
-#pragma unroll
-                for (int w = 0; w < C::NW; ++w) {
-                    uint32_t a[32];
-                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * C::BN + c0), a);
-                    const uint32_t cw = prm.cw[w];
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const uint64_t T = (uint64_t)a[j] * cw;
-                        const uint32_t qq = (uint32_t)T * prm.pneg_inv;
-                        uint32_t r = (uint32_t)((T + (uint64_t)qq * p) >> 32);
-                        r = r >= p ? r - p : r;
-                        const uint32_t sum = v[j] + r;
-                        v[j] = sum >= p ? sum - p : sum;
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < 32; ++j) stg[lane][j] = v[j];
-                __syncwarp();
-#pragma unroll
-                for (int r = 0; r < 32; ++r) {
-                    uint32_t* rp = rowp[r];
-                    if (rp && col_ok) {
-                        const uint32_t vv = stg[r][lane];
-                        const uint32_t d = dv[r];
-                        rp[gn] = d >= vv ? d - vv : d + (p - vv);
-                    }
-                }
+                __syncwarp();  // the previous tile's readers are done with rowp
+                rowp[lane] = mine;
                 __syncwarp();
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(tempty_bar);
+            for (int panel = 0; panel < npanels; ++panel, ++pc) {
+                bool ok = true;
+                if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar, pc & 1, prm.budget);
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                if (!ok) {
+                    if (lane == 0) *abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                for (int c0 = 0; c0 < C::BN; c0 += 32) {
+                    const int gn = n0 + c0 + lane;
+                    const bool col_ok = gn < prm.N;
+                    // D values of the block (row r, column gn), issued before the fold
+                    uint32_t dv[32];
+#pragma unroll
+                    for (int r = 0; r < 32; ++r) {
+                        const uint32_t* rp = rowp[r];
+                        dv[r] = (rp && col_ok) ? rp[gn] : 0u;
+                    }
+                    uint32_t v[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = 0;
+#pragma unroll
+                    for (int w = 0; w < C::NW; ++w) {
+                        uint32_t a[32];
+                        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * C::BN + c0), a);
+                        const uint32_t cw = prm.cw[w];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const uint64_t T = (uint64_t)a[j] * cw;
+                            const uint32_t qq = (uint32_t)T * prm.pneg_inv;
+                            uint32_t r = (uint32_t)((T + (uint64_t)qq * p) >> 32);
+                            r = r >= p ? r - p : r;
+                            const uint32_t sum = v[j] + r;
+                            v[j] = sum >= p ? sum - p : sum;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[lane][j] = v[j];
+                    __syncwarp();
+#pragma unroll
+                    for (int r = 0; r < 32; ++r) {
+                        uint32_t* rp = rowp[r];
+                        if (rp && col_ok) {
+                            const uint32_t vv = stg[r][lane];
+                            const uint32_t d = dv[r];
+                            rp[gn] = d >= vv ? d - vv : d + (p - vv);
+                        }
+                    }
+                    __syncwarp();
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(tempty_bar);
+            }
         }
     }
     tc_fence_before();
@@ -651,6 +715,15 @@ int limbs_for(uint32_t p) {
     return 4;
 }
 
+// SMs of the current device (persistent GEMM grid)
+static int num_sms() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+        return 148;
+    return n;
+}
+
 template <int L, bool SMALL>
 static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t* err,
                   long long* launches) {
@@ -715,7 +788,10 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         set_error(std::string("tc smem attribute: ") + cudaGetErrorString(e));
         return GBGPU_ECUDA;
     }
-    dim3 grid(Np / Cfg::BN, Mp / Cfg::BM, nb);
+    prm.batch = nb;
+    const int64_t tiles = (int64_t)(Np / Cfg::BN) * (Mp / Cfg::BM) * nb;
+    const dim3 grid((unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(tiles, (int64_t)num_sms() * Cfg::MIN_CTAS)));
     GemmProfile* prof = gemm_profile();
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof) {
