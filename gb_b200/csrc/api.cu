@@ -72,6 +72,9 @@ void count_launch(long long n) { g_launches += n; }
         ++launches;                                                                \
     } while (0)
 
+// per-launch executed-K-step counters of a profiled run
+constexpr int kGemmProfileSlots = 4096;
+
 static bool debug_trace() {
     static const bool on = getenv("GBGPU_DEBUG") != nullptr;
     return on;
@@ -251,7 +254,7 @@ static int plan_alloc(Plan* P) {
     A(err, 1);
     A(counters, 8);
     A(work_count, 2);
-    A(gemm_steps, 1);
+    A(gemm_steps, kGemmProfileSlots);
     const int32_t width = P->mode == 0 ? P->ncr : P->nc;
     P->ld = ((int64_t)width + 3) & ~(int64_t)3;
     // algorithm: the blocked form runs its dense steps as exact modular GEMMs
@@ -576,7 +579,9 @@ int plan_run(Plan* P) {
     GemmProfile prof;
     if (P->profile) {
         prof.d_steps = P->gemm_steps;
-        GB_CUDA(cudaMemsetAsync(P->gemm_steps, 0, sizeof(unsigned long long), P->stream));
+        prof.capacity = kGemmProfileSlots;
+        GB_CUDA(cudaMemsetAsync(P->gemm_steps, 0, sizeof(unsigned long long) * kGemmProfileSlots,
+                                P->stream));
         set_gemm_profile(&prof);
     }
     if ((uint32_t)P->p < 65536u)
@@ -589,18 +594,24 @@ int plan_run(Plan* P) {
     P->stats.gemm_ms = 0;
     P->stats.gemm_int8_ops = 0;
     if (P->profile && !prof.events.empty()) {
-        unsigned long long steps = 0;
-        GB_CUDA(cudaMemcpyAsync(&steps, P->gemm_steps, sizeof(steps), cudaMemcpyDeviceToHost,
-                                P->stream));
+        std::vector<unsigned long long> steps(kGemmProfileSlots, 0);
+        GB_CUDA(cudaMemcpyAsync(steps.data(), P->gemm_steps, sizeof(unsigned long long) * steps.size(),
+                                cudaMemcpyDeviceToHost, P->stream));
         GB_CUDA(cudaStreamSynchronize(P->stream));
-        for (auto& e : prof.events) {
+        for (size_t i = 0; i < prof.events.size(); ++i) {
             float ms = 0;
-            cudaEventElapsedTime(&ms, e.first, e.second);
+            cudaEventElapsedTime(&ms, prof.events[i].first, prof.events[i].second);
+            cudaEventDestroy(prof.events[i].first);
+            cudaEventDestroy(prof.events[i].second);
+            const double ops =
+                i < steps.size() ? 2.0 * (double)steps[i] * prof.macs_per_step[i] : 0.0;
             P->stats.gemm_ms += ms;
-            cudaEventDestroy(e.first);
-            cudaEventDestroy(e.second);
+            P->stats.gemm_int8_ops += ops;
+            if (debug_trace())
+                fprintf(stderr, "gbgpu gemm %3zu: M %6d N %6d K %6d batch %5d  %8.3f ms  %8.1f TOPS\n",
+                        i, prof.shape[4 * i], prof.shape[4 * i + 1], prof.shape[4 * i + 2],
+                        prof.shape[4 * i + 3], ms, ms > 0 ? ops / (ms * 1e-3) / 1e12 : 0.0);
         }
-        P->stats.gemm_int8_ops = 2.0 * (double)steps * prof.macs_per_step.front();
     }
     if (rc) return rc;
     GB_CUDA(cudaEventSynchronize(P->ev[5]));

@@ -795,7 +795,9 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     GemmProfile* prof = gemm_profile();
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof) {
-        prm.steps = prof->d_steps;
+        const int slot = (int)prof->events.size();
+        prm.steps = slot < prof->capacity ? prof->d_steps + slot : nullptr;
+        prof->shape.insert(prof->shape.end(), {g.M, g.N, g.K, nb});
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);

@@ -35,9 +35,11 @@ struct TcGemmArgs {
 // Optional per-thread profiling of the tensor-core GEMM launches: CUDA events
 // around every k_tc_submul launch and a device counter of executed K steps.
 struct GemmProfile {
-    unsigned long long* d_steps = nullptr;  // device counter (all launches)
+    unsigned long long* d_steps = nullptr;  // device counters, one per launch
+    int capacity = 0;                       // counters in d_steps
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     std::vector<double> macs_per_step;      // per launch
+    std::vector<int> shape;                 // per launch: M, N, K, batch
 };
 GemmProfile* gemm_profile();
 void set_gemm_profile(GemmProfile* p);
