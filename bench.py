@@ -192,9 +192,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
-    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense"],
+    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense", "rref"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
-                         "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form)")
+                         "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
+                         "rref: RREF of a rank-3n/4 n x n block")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
@@ -203,7 +204,7 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args)
         return
-    if args.workload == "dense":
+    if args.workload in ("dense", "rref"):
         run_dense(args)
         return
 
@@ -359,6 +360,97 @@ def _e2e(lib, mat, args, device):
     h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
     d2h = (npv + 1) * 8 + nnz * 8
     return e2e_s, h2d, d2h
+
+
+def run_dense(args):
+    """Dense D-block workloads with uniform residues, device-resident operands,
+    CUDA events on the default stream, median of the timed steps:
+      dense -- exact modular GEMM D <- (D - A B) mod p on n x n blocks (int8
+               tensor-core form; for n <= 8192 also the CUDA-core form);
+      rref  -- reduced row echelon form of a rank-deficient D = L R (L n x 3n/4,
+               R 3n/4 x n) through gbgpu_dense_rref, D restored before each step."""
+    import torch
+    from gb_b200 import _lib
+    lib = _lib.load()
+    n, p = args.n, args.p
+    L = 1 if p < 1 << 8 else 2 if p < 1 << 16 else 3 if p < 1 << 24 else 4
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    mk = lambda r, c: torch.randint(0, p, (r, c), device="cuda", dtype=torch.int64,
+                                    generator=g).to(torch.int32)
+    opt_t = _lib.Options(_lib.FORM_TENSOR, 0, 1, 0, None)
+
+    def submul(A, B, D, m, nn, k, opt):
+        _lib.check(lib.gbgpu_dense_submul(p, m, nn, k, A.data_ptr(), k, B.data_ptr(), nn,
+                                          D.data_ptr(), nn, C.byref(opt)))
+
+    def events(fn, steps, before=None):
+        ts = []
+        for _ in range(steps):
+            if before:
+                before()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e))
+        return statistics.median(ts)
+
+    if args.workload == "rref":
+        r = 3 * n // 4
+        Lm, R = mk(n, r), mk(r, n)
+        Rn = torch.remainder(p - R.to(torch.int64), p).to(torch.int32)
+        D0 = torch.zeros(n, n, device="cuda", dtype=torch.int32)
+        submul(Lm, Rn, D0, n, n, r, opt_t)  # D0 = 0 - L (-R) = L R
+        D = torch.empty_like(D0)
+        piv = torch.empty(n, device="cuda", dtype=torch.int32)
+        rank = C.c_int32()
+
+        def restore():
+            D.copy_(D0)
+
+        def one():
+            _lib.check(lib.gbgpu_dense_rref(p, n, n, D.data_ptr(), n, C.byref(rank),
+                                            piv.data_ptr(), C.byref(opt_t)))
+
+        for _ in range(max(args.warmup, 1)):
+            restore()
+            one()
+        ms = events(one, args.steps, restore)
+        line = {"metric": "dense RREF throughput (rank-deficient n x n block)",
+                "value": 1000.0 / ms, "unit": "RREFs/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": f"u32 residues, {L} u8 limbs",
+                "data": "synthetic (seeded uniform L, R)",
+                "config": {"workload": f"dense RREF n={n} rank={r} p={p}", "limbs": L},
+                "rank": rank.value}
+        print(json.dumps(line), flush=True)
+        return
+
+    A, B, D = mk(n, n), mk(n, n), mk(n, n)
+
+    def timed(form, steps):
+        opt = _lib.Options(form, 0, 1, 0, None)
+        for _ in range(max(args.warmup, 1)):
+            submul(A, B, D, n, n, n, opt)
+        return events(lambda: submul(A, B, D, n, n, n, opt), steps)
+
+    ms_t = timed(_lib.FORM_TENSOR, args.steps)
+    ops = 2.0 * n ** 3
+    line = {"metric": "exact modular GEMM throughput (D - A B mod p)", "value": ops / ms_t / 1e9,
+            "unit": "modular TOPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"u32 residues, {L} u8 limbs", "data": "synthetic",
+            "config": {"workload": f"dense GEMM n={n} p={p}", "limbs": L},
+            "roofline": {"bound": "tensor", "achieved": L * L * ops / ms_t / 1e9,
+                         "peak": INT8_PEAK_TOPS, "unit": "TOPS",
+                         "frac": L * L * ops / ms_t / 1e9 / INT8_PEAK_TOPS}}
+    if n <= 8192:
+        ms_p = timed(_lib.FORM_PLAIN, 1)
+        line["plain_ms"] = ms_p
+        line["tensor_speedup_vs_plain"] = ms_p / ms_t
+    print(json.dumps(line), flush=True)
 
 
 def _work_counters(plan) -> int:
