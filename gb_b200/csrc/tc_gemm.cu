@@ -146,10 +146,16 @@ struct TcCfg {
     static constexpr int STAGES = SMALL ? 1 : (L == 1 ? 4 : (L == 2 ? 3 : 2));
     static constexpr int TMEM_COLS =
         NW * BN <= 64 ? 64 : (NW * BN <= 128 ? 128 : (NW * BN <= 256 ? 256 : 512));
-    // epilogue staging: a 32 x 32 block per epilogue warp (padded rows) and the
-    // D row pointers of its 32 rows
-    static constexpr int STG_BYTES = 4 * 32 * 33 * 4;
-    static constexpr int ROWP_BYTES = 4 * 32 * 8;
+    // epilogue warps: two per TMEM lane quarter (each half of the columns) for
+    // the one-CTA-per-SM shapes with one or two limbs, one otherwise
+    static constexpr int EPI_WARPS = (!SMALL && L <= 2) ? 8 : 4;
+    static constexpr int THREADS = 64 + 32 * EPI_WARPS;
+    // epilogue staging: a 32 x 32 block per epilogue warp (XOR-swizzled
+    // columns) and the D row indices of its 32 rows
+    static constexpr int STG_BYTES = EPI_WARPS * 32 * 32 * 4;
+    // (64-bit pointers when there is room, 32-bit row indices otherwise)
+    static constexpr bool ROW_PTRS = EPI_WARPS == 4;
+    static constexpr int ROWP_BYTES = EPI_WARPS * 32 * (ROW_PTRS ? 8 : 4);
     static constexpr int BAR_OFF = STAGES * STAGE_BYTES;
     static constexpr int STG_OFF = BAR_OFF + 256;
     static constexpr int ROWP_OFF = STG_OFF + STG_BYTES;
@@ -179,9 +185,10 @@ struct TcParams {
     int64_t ldd, sD;
     const int32_t* d_rows;  // optional: row m of D is D + d_rows[m] ldd (< 0: not written)
     int64_t sDr;
-    int32_t M, N, Mp, Np, nkb, batch;
-    // nonzero flags of the 128-row x 128-byte A tiles ([Mp/128][nkb]) and of the
-    // BN-row x 128-byte B tiles ([Np/BN][nkb]); a K step where either tile is
+    int32_t M, N, Mp, Np, nkb, nkbp, batch;
+    // nonzero flags of the 128-row x 128-byte A tiles ([Mp/128][nkbp]) and of the
+    // BN-row x 128-byte B tiles ([Np/BN][nkbp], nkbp = nkb rounded up to 64, the
+    // padding zero); a K step where either tile is
     // zero contributes nothing and is skipped (NULL: no skipping)
     const uint8_t* fa;
     const uint8_t* fb;
@@ -193,7 +200,7 @@ struct TcParams {
 };
 
 template <int L, bool SMALL>
-__global__ void __launch_bounds__(192, TcCfg<L, SMALL>::MIN_CTAS)
+__global__ void __launch_bounds__(TcCfg<L, SMALL>::THREADS, TcCfg<L, SMALL>::MIN_CTAS)
 k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const TcParams prm) {
     using C = TcCfg<L, SMALL>;
@@ -229,16 +236,45 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         nt = rr / gm;
     };
     // flags of the tile's A row block and B column block (NULL: all live)
+    const int nkbp = prm.nkbp;
     auto flag_ptrs = [&](int z, int mt, int nt, const uint8_t*& fa, const uint8_t*& fb) {
-        fa = prm.fa ? prm.fa + ((size_t)z * tiles_m + mt) * nkb : nullptr;
-        fb = prm.fb ? prm.fb + ((size_t)z * tiles_n + nt) * nkb : nullptr;
+        fa = prm.fa ? prm.fa + ((size_t)z * tiles_m + mt) * nkbp : nullptr;
+        fb = prm.fb ? prm.fb + ((size_t)z * tiles_n + nt) * nkbp : nullptr;
     };
-    auto live = [&](const uint8_t* fa, const uint8_t* fb, int kb) {
-        return (!fa || fa[kb]) && (!fb || fb[kb]);
+    // live K steps [64 ch, 64 ch + 64) of a tile as a bit mask, from 16-byte
+    // loads of both flag rows (flags are 0 or 1 bytes)
+    auto live_mask = [&](const uint8_t* fa, const uint8_t* fb, int ch) -> uint64_t {
+        uint64_t msk = 0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int kb0 = ch * 64 + v * 16;
+            if (kb0 >= nkb) break;  // padding only
+            uint4 a = make_uint4(0x01010101u, 0x01010101u, 0x01010101u, 0x01010101u);
+            uint4 b = a;
+            if (fa) a = *(const uint4*)(fa + kb0);
+            if (fb) b = *(const uint4*)(fb + kb0);
+            const uint32_t w[4] = {a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t x = w[j];
+                const uint32_t bits = (x & 1u) | ((x >> 7) & 2u) | ((x >> 14) & 4u) | ((x >> 21) & 8u);
+                msk |= (uint64_t)bits << (v * 16 + j * 4);
+            }
+        }
+        if (!fa && !fb) {
+            // no flags at all: every real K step is live
+            const int rem = nkb - ch * 64;
+            msk = rem >= 64 ? ~0ull : (rem > 0 ? ((1ull << rem) - 1ull) : 0ull);
+        } else if (nkb - ch * 64 < 64) {
+            const int rem = nkb - ch * 64;
+            msk &= rem > 0 ? ((1ull << rem) - 1ull) : 0ull;
+        }
+        return msk;
     };
+    const int nch = (nkb + 63) / 64;
     auto live_steps = [&](const uint8_t* fa, const uint8_t* fb) {
         int n_it = 0;
-        for (int kb = 0; kb < nkb; ++kb) n_it += live(fa, fb, kb) ? 1 : 0;
+        for (int ch = 0; ch < nch; ++ch) n_it += __popcll(live_mask(fa, fb, ch));
         return n_it;
     };
 
@@ -248,7 +284,7 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             mbar_init(empty_bar(s), 1);
         }
         mbar_init(tfull_bar, 1);
-        mbar_init(tempty_bar, 4);
+        mbar_init(tempty_bar, C::EPI_WARPS);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -280,8 +316,11 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 flag_ptrs(z, mt, nt, fa, fb);
                 const int m0 = mt * C::BM, n0 = nt * C::BN;
                 int n_tile = 0;
-                for (int kb = 0; kb < nkb; ++kb) {
-                    if (!live(fa, fb, kb)) continue;
+                for (int ch = 0; ch < nch && !stop; ++ch) {
+                  uint64_t msk = live_mask(fa, fb, ch);
+                  while (msk) {
+                    const int kb = ch * 64 + __ffsll((long long)msk) - 1;
+                    msk &= msk - 1;
                     const int s = it % C::STAGES;
                     const uint32_t ph = (it / C::STAGES) & 1;
                     if (*abort_flag || !mbar_wait(empty_bar(s), ph ^ 1, prm.budget)) {
@@ -299,6 +338,7 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                                     (z * L + l) * prm.Np + n0, full_bar(s));
                     ++it;
                     ++n_tile;
+                  }
                 }
                 if (prm.steps && n_tile) atomicAdd(prm.steps, (unsigned long long)n_tile);
             }
@@ -317,8 +357,11 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 const uint8_t *fa, *fb;
                 flag_ptrs(z, mt, nt, fa, fb);
                 const int n_it = live_steps(fa, fb);
-                for (int kb = 0, j = 0; kb < nkb && j < n_it; ++kb) {
-                    if (!live(fa, fb, kb)) continue;
+                int j = 0;
+                for (int ch = 0; ch < nch && !stop; ++ch) {
+                  uint64_t msk = live_mask(fa, fb, ch);
+                  while (msk) {
+                    msk &= msk - 1;
                     const int s = it % C::STAGES;
                     const uint32_t ph = (it / C::STAGES) & 1;
                     const int pk = j % C::PANEL_KB;
@@ -360,20 +403,26 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     }
                     ++it;
                     ++j;
+                  }
                 }
             }
         }
     } else {
-        // ---- epilogue: warps 2..5, TMEM lane quarter (warp % 4) ----
+        // ---- epilogue: warps 2.., TMEM lane quarter warp % 4, column half ----
         // Thread `lane` folds row q*32+lane of the tile; the 32 x 32 result
         // block goes through shared memory so that the read-modify-write of D
         // runs along rows (one 128-byte row segment per warp instruction).
+        const int e = warp - 2;
         const int q = warp & 3;
+        constexpr int HALVES = C::EPI_WARPS / 4;
+        constexpr int COLS = C::BN / HALVES;  // columns of this warp
+        const int cbeg = (e / 4) * COLS;
         const int row = q * 32 + lane;
         const uint32_t p = prm.p;
-        uint32_t(*stg)[33] =
-            (uint32_t(*)[33])(gbase + C::STG_OFF + (size_t)(warp - 2) * 32 * 33 * 4);
-        uint32_t** rowp = (uint32_t**)(gbase + C::ROWP_OFF + (size_t)(warp - 2) * 32 * 8);
+        uint32_t* stg = (uint32_t*)(gbase + C::STG_OFF + (size_t)e * 32 * 32 * 4);
+        uint8_t* rowb = gbase + C::ROWP_OFF + (size_t)e * 32 * (C::ROW_PTRS ? 8 : 4);
+        int32_t* rowi = (int32_t*)rowb;
+        uint32_t** rowp = (uint32_t**)rowb;
         int pc = 0;
         bool stop = false;
         for (int t = blockIdx.x; t < total && !stop; t += gridDim.x) {
@@ -386,17 +435,26 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             const int npanels = (n_it + C::PANEL_KB - 1) / C::PANEL_KB;
             const int m0 = mt * C::BM, n0 = nt * C::BN;
             const int gm = m0 + row;
+            uint32_t* Dz = prm.D + (size_t)z * prm.sD;
             {
-                uint32_t* mine = nullptr;
-                if (gm < prm.M) {
-                    int64_t ri = gm;
-                    if (prm.d_rows) ri = prm.d_rows[(size_t)z * prm.sDr + gm];
-                    if (ri >= 0) mine = prm.D + (size_t)z * prm.sD + (size_t)ri * prm.ldd;
-                }
-                __syncwarp();  // the previous tile's readers are done with rowp
-                rowp[lane] = mine;
+                int32_t ri = -1;
+                if (gm < prm.M) ri = prm.d_rows ? prm.d_rows[(size_t)z * prm.sDr + gm] : gm;
+                __syncwarp();  // the previous tile's readers are done with the rows
+                if constexpr (C::ROW_PTRS)
+                    rowp[lane] = ri >= 0 ? Dz + (size_t)ri * prm.ldd : nullptr;
+                else
+                    rowi[lane] = ri;
                 __syncwarp();
             }
+            // row r of the tile in D (nullptr: not written)
+            auto drow = [&](int r) -> uint32_t* {
+                if constexpr (C::ROW_PTRS) {
+                    return rowp[r];
+                } else {
+                    const int32_t ri = rowi[r];
+                    return ri >= 0 ? Dz + (size_t)ri * prm.ldd : nullptr;
+                }
+            };
             for (int panel = 0; panel < npanels; ++panel, ++pc) {
                 bool ok = true;
                 if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar, pc & 1, prm.budget);
@@ -407,14 +465,14 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     break;
                 }
                 tc_fence_after();
-                for (int c0 = 0; c0 < C::BN; c0 += 32) {
+                for (int c0 = cbeg; c0 < cbeg + COLS; c0 += 32) {
                     const int gn = n0 + c0 + lane;
                     const bool col_ok = gn < prm.N;
                     // D values of the block (row r, column gn), issued before the fold
                     uint32_t dv[32];
 #pragma unroll
                     for (int r = 0; r < 32; ++r) {
-                        const uint32_t* rp = rowp[r];
+                        const uint32_t* rp = drow(r);
                         dv[r] = (rp && col_ok) ? rp[gn] : 0u;
                     }
                     uint32_t v[32];
@@ -435,14 +493,15 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                             v[j] = sum >= p ? sum - p : sum;
                         }
                     }
+                    // stage (row lane, column j) at [lane][j ^ lane]
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) stg[lane][j] = v[j];
+                    for (int j = 0; j < 32; ++j) stg[lane * 32 + (j ^ lane)] = v[j];
                     __syncwarp();
 #pragma unroll
                     for (int r = 0; r < 32; ++r) {
-                        uint32_t* rp = rowp[r];
+                        uint32_t* rp = drow(r);
                         if (rp && col_ok) {
-                            const uint32_t vv = stg[r][lane];
+                            const uint32_t vv = stg[r * 32 + (lane ^ r)];
                             const uint32_t d = dv[r];
                             rp[gn] = d >= vv ? d - vv : d + (p - vv);
                         }
@@ -473,12 +532,12 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 __global__ void __launch_bounds__(256)
 k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
              const int32_t* __restrict__ a_rows, int64_t sAr, int32_t M, int32_t K, int32_t Mp,
-             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags) {
+             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t fstride) {
     // batch item blockIdx.y
     A += (size_t)blockIdx.y * sA;
     if (a_rows) a_rows += (size_t)blockIdx.y * sAr;
     out += (size_t)blockIdx.y * L * Mp * Kp;
-    if (flags) flags += (size_t)blockIdx.y * (Mp / 128) * (Kp / 128);
+    if (flags) flags += (size_t)blockIdx.y * (Mp / 128) * fstride;
     const int32_t kq = Kp / 16;  // 16-column groups per row
     const int64_t total = (int64_t)Mp * kq;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
@@ -495,7 +554,7 @@ k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
             v[i] = (row && k + i < K) ? row[k + i] : 0u;
             any |= v[i];
         }
-        if (flags && any) flags[(size_t)(m / 128) * (Kp / 128) + k / 128] = 1;
+        if (flags && any) flags[(size_t)(m / 128) * fstride + k / 128] = 1;
         for (int l = 0; l < L; ++l) {
             uint32_t w[4];
 #pragma unroll
@@ -518,14 +577,15 @@ constexpr int SPLIT_ROW = 132;
 __global__ void __launch_bounds__(256)
 k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
              const int32_t* __restrict__ b_rows, int64_t sBr, int32_t K, int32_t N, int32_t Np,
-             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t bn) {
+             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t bn,
+             int32_t fstride) {
     extern __shared__ uint8_t split_smem[];  // [L][64][SPLIT_ROW] bytes
     __shared__ const uint32_t* rowp[128];
     // batch item blockIdx.z
     B += (size_t)blockIdx.z * sB;
     if (b_rows) b_rows += (size_t)blockIdx.z * sBr;
     out += (size_t)blockIdx.z * L * Np * Kp;
-    if (flags) flags += (size_t)blockIdx.z * (Np / bn) * (Kp / 128);
+    if (flags) flags += (size_t)blockIdx.z * (Np / bn) * fstride;
     const int k0 = blockIdx.y * 128, n0 = blockIdx.x * 64;
     if (threadIdx.x < 128) {
         const int k = k0 + threadIdx.x;
@@ -569,7 +629,7 @@ k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
     }
     if (flags && any && threadIdx.x == 0) {
         // the 64 columns lie inside one bn-wide tile (bn is a multiple of 64)
-        flags[(size_t)(n0 / bn) * (Kp / 128) + k0 / 128] = 1;
+        flags[(size_t)(n0 / bn) * fstride + k0 / 128] = 1;
     }
 }
 
@@ -735,9 +795,10 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     uint8_t* Ap = planes;                                    // [nb][L][Mp][Kp]
     uint8_t* Bp = planes + (size_t)nb * L * Mp * Kp;         // [nb][L][Np][Kp]
     const int32_t nkb = Kp / Cfg::BK;
-    uint8_t* fa = Bp + (size_t)nb * L * Np * Kp;             // [nb][Mp/128][nkb]
-    uint8_t* fb = fa + (size_t)nb * (Mp / Cfg::BM) * nkb;    // [nb][Np/BN][nkb]
-    const size_t flag_bytes = (size_t)nb * (Mp / Cfg::BM + Np / Cfg::BN) * nkb;
+    const int32_t nkbp = (nkb + 63) / 64 * 64;
+    uint8_t* fa = Bp + (size_t)nb * L * Np * Kp;             // [nb][Mp/128][nkbp]
+    uint8_t* fb = fa + (size_t)nb * (Mp / Cfg::BM) * nkbp;   // [nb][Np/BN][nkbp]
+    const size_t flag_bytes = (size_t)nb * (Mp / Cfg::BM + Np / Cfg::BN) * nkbp;
     if (cudaMemsetAsync(fa, 0, flag_bytes, s) != cudaSuccess) {
         set_error("tile flag clear failed");
         return GBGPU_ECUDA;
@@ -747,10 +808,10 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256,
                                                                        148 * 32 / nb + 1));
         k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.a_rows, g.sAr, g.M, g.K,
-                                                    Mp, Kp, L, Ap, fa);
+                                                    Mp, Kp, L, Ap, fa, nkbp);
         dim3 gb(Np / 64, Kp / 128, nb);
         k_split_cols<<<gb, 256, L * 64 * SPLIT_ROW, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K,
-                                                          g.N, Np, Kp, L, Bp, fb, Cfg::BN);
+                                                          g.N, Np, Kp, L, Bp, fb, Cfg::BN, nkbp);
         *launches += 2;
     }
     CUtensorMap ma, mb;
@@ -769,6 +830,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     prm.Mp = Mp;
     prm.Np = Np;
     prm.nkb = nkb;
+    prm.nkbp = nkbp;
     prm.fa = fa;
     prm.fb = fb;
     const FieldMont f = FieldMont::make(g.p);
@@ -802,7 +864,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
     }
-    k_tc_submul<L, SMALL><<<grid, 192, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
+    k_tc_submul<L, SMALL><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
     ++*launches;
     if (prof) {
         cudaEventRecord(e1, s);
@@ -821,11 +883,13 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
 size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K, int32_t batch) {
     const int L = limbs_for(p);
     // planes padded for the widest tile (256 columns), flags counted for the
-    // narrowest (64): enough for either tile shape
+    // narrowest (64) with flag rows padded to 64 K steps: enough for either
+    // tile shape
     const size_t Mp = (size_t)(M + 127) / 128 * 128, Np = (size_t)(N + 255) / 256 * 256;
     const size_t Kp = (size_t)(K + 127) / 128 * 128;
+    const size_t nkbp = (Kp / 128 + 63) / 64 * 64;
     const size_t nb = (size_t)(batch > 0 ? batch : 1);
-    const size_t flags = nb * (Mp / 128 + (size_t)(N + 63) / 64) * (Kp / 128);
+    const size_t flags = nb * (Mp / 128 + (size_t)(N + 63) / 64) * nkbp;
     return nb * L * (Mp + Np) * Kp + ((flags + 255) & ~(size_t)255);
 }
 
