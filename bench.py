@@ -252,7 +252,16 @@ def main():
         ref_plan.close()
 
     # ---- end to end through gbgpu_reduce with pinned host buffers ---------
-    e2e_s, h2d, d2h = _e2e(lib, mat, args, local) if not args.no_e2e else (float("nan"), 0, 0)
+    e2e_s, h2d, d2h, e2e_out = (_e2e(lib, mat, args, local) if not args.no_e2e
+                                else (float("nan"), 0, 0, None))
+    e2e_ok = None
+    if e2e_out is not None:
+        (rp, cc, vv), npv, nnz, vb = e2e_out
+        e2e_ok = (npv == answer.np and nnz == answer.nnz
+                  and np.array_equal(rp.numpy(), answer.row_ptr)
+                  and np.array_equal(cc.numpy()[:nnz], answer.cols)
+                  and np.array_equal(vv.numpy()[:nnz].astype(np.int64) & ((1 << (8 * vb)) - 1),
+                                     answer.vals.astype(np.int64)))
 
     value = ws * 1000.0 / ms
     sch = float(np.mean(schur_ms))
@@ -290,7 +299,7 @@ def main():
                    "l2": "inputs (CSR ~230 MB) larger than L2; no flush needed",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "e2e": {"value": ws / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "answer_equals_device_answer": e2e_ok},
         "gpu_launches": int(launches),
         "roofline": roof,
         "stages_ms": {k: stats[k] for k in ("ms_classify", "ms_check", "ms_schur", "ms_echelon",
@@ -317,16 +326,20 @@ def main():
 def _e2e(lib, mat, args, device):
     """Seconds per reduction through the public C ABI, host buffers in and out:
     gbgpu_plan_create (H2D of the CSR from pinned host memory), gbgpu_plan_run,
-    gbgpu_plan_result_into (D2H of the answer into pinned host memory),
-    gbgpu_plan_destroy -- all inside the timed region, every step.  Returns
-    (seconds per step, H2D bytes per step, D2H bytes per step)."""
+    gbgpu_plan_result_into_v (D2H of the answer into pinned host memory),
+    gbgpu_plan_destroy -- all inside the timed region, every step.  Values
+    travel at the reference's own coefficient width (cf_8 / cf_16 / cf_32:
+    1, 2 or 4 bytes).  Returns (seconds per step, H2D bytes, D2H bytes)."""
     import torch
     from gb_b200 import _lib
+    vb = 1 if mat.p < 1 << 8 else 2 if mat.p < 1 << 16 else 4
+    vdt = {1: np.uint8, 2: np.uint16, 4: np.int32}[vb]
+    tdt = {1: torch.uint8, 2: torch.int16, 4: torch.int32}[vb]
     ptr_h = torch.from_numpy(mat.row_ptr).pin_memory()
     cols_h = torch.from_numpy(mat.cols).pin_memory()
-    vals_h = torch.from_numpy(mat.vals).pin_memory()
+    vals_h = torch.from_numpy(mat.vals.astype(vdt).view({1: np.uint8, 2: np.int16, 4: np.int32}[vb])).pin_memory()
     csr = _lib.Csr(mat.p, mat.laopt, mat.nr, mat.ncl, mat.ncr, ptr_h.data_ptr(),
-                   cols_h.data_ptr(), vals_h.data_ptr())
+                   cols_h.data_ptr(), vals_h.data_ptr(), vb)
     opt = _lib.Options(args.form, device, 1, 0, None)
 
     def one(out_bufs):
@@ -336,12 +349,13 @@ def _e2e(lib, mat, args, device):
             _lib.check(lib.gbgpu_plan_run(h))
             npv, nnz = C.c_int32(), C.c_int64()
             if out_bufs is None:
-                lib.gbgpu_plan_result_into(h, None, None, None, 0, 0, C.byref(npv), C.byref(nnz))
+                lib.gbgpu_plan_result_into_v(h, None, None, None, vb, 0, 0, C.byref(npv),
+                                             C.byref(nnz))
                 return int(npv.value), int(nnz.value)
             rp, cc, vv = out_bufs
-            _lib.check(lib.gbgpu_plan_result_into(h, rp.data_ptr(), cc.data_ptr(), vv.data_ptr(),
-                                                  rp.numel(), cc.numel(), C.byref(npv),
-                                                  C.byref(nnz)))
+            _lib.check(lib.gbgpu_plan_result_into_v(h, rp.data_ptr(), cc.data_ptr(),
+                                                    vv.data_ptr(), vb, rp.numel(), cc.numel(),
+                                                    C.byref(npv), C.byref(nnz)))
             return int(npv.value), int(nnz.value)
         finally:
             lib.gbgpu_plan_destroy(h)
@@ -349,7 +363,7 @@ def _e2e(lib, mat, args, device):
     npv, nnz = one(None)  # sizes of the answer
     bufs = (torch.empty(npv + 1, dtype=torch.int64).pin_memory(),
             torch.empty(max(nnz, 1), dtype=torch.int32).pin_memory(),
-            torch.empty(max(nnz, 1), dtype=torch.int32).pin_memory())
+            torch.empty(max(nnz, 1), dtype=tdt).pin_memory())
     one(bufs)  # warm
     torch.cuda.synchronize()
     steps = max(2, min(args.steps, 5))
@@ -357,9 +371,10 @@ def _e2e(lib, mat, args, device):
     for _ in range(steps):
         one(bufs)
     e2e_s = (time.perf_counter() - t0) / steps
-    h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.vals.nbytes
-    d2h = (npv + 1) * 8 + nnz * 8
-    return e2e_s, h2d, d2h
+    h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.nnz * vb
+    d2h = (npv + 1) * 8 + nnz * (4 + vb)
+    # the answer that crossed the bus is the device answer
+    return e2e_s, h2d, d2h, (bufs, npv, nnz, vb)
 
 
 def run_dense(args):

@@ -28,7 +28,7 @@ _PI32 = C.POINTER(C.c_int32)
 class Csr(C.Structure):
     _fields_ = [("p", C.c_int32), ("laopt", C.c_int32), ("nr", C.c_int32), ("ncl", C.c_int32),
                 ("ncr", C.c_int32), ("row_ptr", C.c_void_p), ("cols", C.c_void_p),
-                ("vals", C.c_void_p)]
+                ("vals", C.c_void_p), ("val_bytes", C.c_int32)]
 
 
 class Rows(C.Structure):
@@ -69,6 +69,7 @@ EXPORTS = [
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
     "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into", "gbgpu_dense_rref",
+    "gbgpu_plan_result_into_v",
 ]
 
 _lib = None
@@ -94,6 +95,8 @@ def load(path: str = LIB_PATH):
     lib.gbgpu_plan_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
     lib.gbgpu_plan_result_into.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_int64, C.c_int64, _PI32, _PI64]
+    lib.gbgpu_plan_result_into_v.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_int32, C.c_int64, C.c_int64, _PI32, _PI64]
     lib.gbgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.gbgpu_plan_destroy.restype = None
     lib.gbgpu_reduce_batch.argtypes = [C.c_int32, C.POINTER(Csr), C.POINTER(Options),

@@ -176,6 +176,8 @@ struct Plan {
     size_t cub_bytes = 0;
     int32_t* out_cols = nullptr;
     int32_t* out_vals = nullptr;
+    uint8_t* wire = nullptr;  // narrow values in transit (val_bytes 1 or 2)
+    size_t wire_cap = 0;
     int64_t out_cap = 0;
     // answer
     int32_t np = 0;
@@ -645,6 +647,22 @@ int plan_run(Plan* P) {
     return GBGPU_OK;
 }
 
+// residues of vb bytes (1 or 2) <-> uint32
+__global__ void k_widen(const uint8_t* __restrict__ in, int32_t vb, int64_t n, uint32_t* out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = vb == 1 ? (uint32_t)in[i] : (uint32_t)((const uint16_t*)in)[i];
+}
+__global__ void k_narrow(const uint32_t* __restrict__ in, int32_t vb, int64_t n, uint8_t* out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (vb == 1) out[i] = (uint8_t)in[i];
+        else ((uint16_t*)out)[i] = (uint16_t)in[i];
+    }
+}
+
+static int val_bytes_of(const gbgpu_csr* m) { return m->val_bytes ? m->val_bytes : 4; }
+
 int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** out) {
     *out = nullptr;
     if (!m || m->p < 2 || m->nr < 0 || m->ncl < 0 || m->ncr < 0 ||
@@ -654,6 +672,11 @@ int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** o
     }
     if (m->nr > 0 && (!m->row_ptr || !m->cols || !m->vals)) {
         set_error("null CSR array");
+        return GBGPU_EINVAL;
+    }
+    const int vb = val_bytes_of(m);
+    if (!(vb == 1 || vb == 2 || vb == 4) || (vb < 4 && (int64_t)m->p >= ((int64_t)1 << (8 * vb)))) {
+        set_error("val_bytes must be 4, 2 (p < 2^16) or 1 (p < 2^8)");
         return GBGPU_EINVAL;
     }
     Plan* P = new (std::nothrow) Plan();
@@ -685,8 +708,25 @@ int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** o
                                      cudaMemcpyHostToDevice, P->stream);
     cudaError_t e2 = cudaMemcpyAsync(P->cols, m->cols, sizeof(int32_t) * P->nnz,
                                      cudaMemcpyHostToDevice, P->stream);
-    cudaError_t e3 = cudaMemcpyAsync(P->vals, m->vals, sizeof(int32_t) * P->nnz,
-                                     cudaMemcpyHostToDevice, P->stream);
+    cudaError_t e3 = cudaSuccess;
+    if (vb == 4) {
+        e3 = cudaMemcpyAsync(P->vals, m->vals, sizeof(int32_t) * P->nnz, cudaMemcpyHostToDevice,
+                             P->stream);
+    } else if (P->nnz > 0) {
+        // narrow values on the wire, widened on the device
+        if ((rc = P->alloc(&P->wire, (size_t)P->nnz * vb))) {
+            delete P;
+            return rc;
+        }
+        P->wire_cap = (size_t)P->nnz * vb;
+        e3 = cudaMemcpyAsync(P->wire, m->vals, (size_t)P->nnz * vb, cudaMemcpyHostToDevice,
+                             P->stream);
+        if (e3 == cudaSuccess) {
+            k_widen<<<grid_for(P->nnz, 256), 256, 0, P->stream>>>(P->wire, vb, P->nnz, P->vals);
+            e3 = cudaGetLastError();
+            count_launch(1);
+        }
+    }
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
         set_error("host to device copy failed");
         delete P;
@@ -748,6 +788,46 @@ int plan_result_into(Plan* P, int64_t* row_ptr, int32_t* cols, int32_t* vals, in
     return GBGPU_OK;
 }
 
+// the same with values of vb bytes (1, 2: narrowed on the device first)
+int plan_result_into_v(Plan* P, int64_t* row_ptr, int32_t* cols, void* vals, int32_t vb,
+                       int64_t cap_rows, int64_t cap_nnz, int32_t* np, int64_t* nnz) {
+    if (vb == 4)
+        return plan_result_into(P, row_ptr, cols, (int32_t*)vals, cap_rows, cap_nnz, np, nnz);
+    if (!(vb == 1 || vb == 2) || (int64_t)P->p >= ((int64_t)1 << (8 * vb))) {
+        set_error("val_bytes must be 4, 2 (p < 2^16) or 1 (p < 2^8)");
+        return GBGPU_EINVAL;
+    }
+    GB_CUDA(cudaStreamSynchronize(P->stream));
+    *np = P->np;
+    *nnz = P->onnz;
+    if ((int64_t)P->np + 1 > cap_rows || P->onnz > cap_nnz) {
+        set_error("result buffers too small");
+        return GBGPU_ERANGE;
+    }
+    row_ptr[0] = 0;
+    if (P->np > 0) {
+        GB_CUDA(cudaMemcpyAsync(row_ptr, P->offs, sizeof(int64_t) * (P->np + 1),
+                                cudaMemcpyDeviceToHost, P->stream));
+        if (P->onnz > 0) {
+            const size_t need = (size_t)P->onnz * vb;
+            if (need > P->wire_cap) {
+                int rc = P->alloc(&P->wire, need);
+                if (rc) return rc;
+                P->wire_cap = need;
+            }
+            GB_CUDA(cudaMemcpyAsync(cols, P->out_cols, sizeof(int32_t) * P->onnz,
+                                    cudaMemcpyDeviceToHost, P->stream));
+            k_narrow<<<grid_for(P->onnz, 256), 256, 0, P->stream>>>((const uint32_t*)P->out_vals,
+                                                                     vb, P->onnz, P->wire);
+            GB_CUDA(cudaGetLastError());
+            count_launch(1);
+            GB_CUDA(cudaMemcpyAsync(vals, P->wire, need, cudaMemcpyDeviceToHost, P->stream));
+        }
+        GB_CUDA(cudaStreamSynchronize(P->stream));
+    }
+    return GBGPU_OK;
+}
+
 void plan_destroy(Plan* P) { delete P; }
 const gbgpu_stats& plan_stats(const Plan* P) { return P->stats; }
 
@@ -788,6 +868,15 @@ int gbgpu_plan_result_into(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, in
     if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
     // NULL buffers with zero capacities query the sizes (GBGPU_ERANGE)
     return plan_result_into(plan->impl, row_ptr, cols, vals, cap_rows, cap_nnz, np, nnz);
+}
+
+int gbgpu_plan_result_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, void* vals,
+                             int32_t val_bytes, int64_t cap_rows, int64_t cap_nnz, int32_t* np,
+                             int64_t* nnz) {
+    if (!plan || !np || !nnz) return GBGPU_EINVAL;
+    if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
+    return plan_result_into_v(plan->impl, row_ptr, cols, vals, val_bytes, cap_rows, cap_nnz, np,
+                              nnz);
 }
 
 int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {

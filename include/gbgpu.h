@@ -119,6 +119,11 @@ typedef struct gbgpu_csr {
     const int64_t *row_ptr; /* [nr + 1], host or device (see flags)      */
     const int32_t *cols;    /* [nnz]; first entry of a row = its lead     */
     const int32_t *vals;    /* [nnz]; residues in [1, p), lead = 1        */
+    /* Width of one entry of vals in bytes: 4 (int32, also when 0), 2 (uint16,
+     * p < 2^16) or 1 (uint8, p < 2^8) -- the coefficient widths of the
+     * reference's cf_32 / cf_16 / cf_8 arrays (src/data.h), which halve or
+     * quarter the host-to-device traffic of the values. */
+    int32_t val_bytes;
 } gbgpu_csr;
 
 /* Reduced rows in host memory allocated by the library with malloc. */
@@ -200,6 +205,12 @@ int gbgpu_plan_result(gbgpu_plan *plan, gbgpu_rows *out);
 int gbgpu_plan_result_into(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
                            int32_t *vals, int64_t cap_rows, int64_t cap_nnz,
                            int32_t *np, int64_t *nnz);
+/* gbgpu_plan_result_into with values of val_bytes bytes each (4: int32,
+ * 2: uint16 for p < 2^16, 1: uint8 for p < 2^8), the widths the reference
+ * keeps in mat->cf_32 / cf_16 / cf_8; narrower values shorten the copy. */
+int gbgpu_plan_result_into_v(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
+                             void *vals, int32_t val_bytes, int64_t cap_rows,
+                             int64_t cap_nnz, int32_t *np, int64_t *nnz);
 int gbgpu_plan_stats(const gbgpu_plan *plan, gbgpu_stats *stats);
 void gbgpu_plan_destroy(gbgpu_plan *plan);
 

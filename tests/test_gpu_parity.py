@@ -214,3 +214,45 @@ def test_plan_result_into_caller_buffers():
                                           C.byref(npv), C.byref(nnz)))
     check_same(ReducedRows(rp, cols, vals), want)
     plan.close()
+
+
+@pytest.mark.parametrize("p,vb", [(251, 1), (32003, 2), (65521, 2)])
+@pytest.mark.parametrize("form", [_lib.FORM_PLAIN, _lib.FORM_TENSOR])
+def test_narrow_values_in_and_out(form, p, vb):
+    """Values at the reference's coefficient width (cf_8 / cf_16) on the way in
+    (gbgpu_csr.val_bytes) and out (gbgpu_plan_result_into_v): same answer as
+    the oracle."""
+    m = synth.staircase(700, 180, 650, p, seed=9)
+    want, _ = oracle.oracle_la(m)
+    lib = _lib.load()
+    vdt = np.uint8 if vb == 1 else np.uint16
+    vals_in = np.ascontiguousarray(m.vals.astype(vdt))
+    csr = _lib.Csr(m.p, m.laopt, m.nr, m.ncl, m.ncr, m.row_ptr.ctypes.data, m.cols.ctypes.data,
+                   vals_in.ctypes.data, vb)
+    opt = _lib.Options(form, 0, 1, 0, None)
+    h = C.c_void_p()
+    _lib.check(lib.gbgpu_plan_create(C.byref(csr), C.byref(opt), C.byref(h)))
+    try:
+        _lib.check(lib.gbgpu_plan_run(h))
+        npv, nnz = C.c_int32(), C.c_int64()
+        rc = lib.gbgpu_plan_result_into_v(h, None, None, None, vb, 0, 0, C.byref(npv),
+                                          C.byref(nnz))
+        assert rc == _lib.GBGPU_ERANGE and npv.value == want.np and nnz.value == want.nnz
+        rp = np.zeros(npv.value + 1, dtype=np.int64)
+        cols = np.zeros(max(nnz.value, 1), dtype=np.int32)
+        vals = np.zeros(max(nnz.value, 1), dtype=vdt)
+        _lib.check(lib.gbgpu_plan_result_into_v(h, rp.ctypes.data, cols.ctypes.data,
+                                                vals.ctypes.data, vb, rp.shape[0], cols.shape[0],
+                                                C.byref(npv), C.byref(nnz)))
+        check_same(ReducedRows(rp, cols[:nnz.value], vals[:nnz.value].astype(np.int32)), want)
+        # a width too narrow for the prime is rejected
+        if p > 255:
+            rc = lib.gbgpu_plan_result_into_v(h, rp.ctypes.data, cols.ctypes.data,
+                                              vals.ctypes.data, 1, rp.shape[0], cols.shape[0],
+                                              C.byref(npv), C.byref(nnz))
+            assert rc == _lib.GBGPU_EINVAL
+    finally:
+        lib.gbgpu_plan_destroy(h)
+    bad = _lib.Csr(m.p, m.laopt, m.nr, m.ncl, m.ncr, m.row_ptr.ctypes.data, m.cols.ctypes.data,
+                   vals_in.ctypes.data, 3)
+    assert lib.gbgpu_plan_create(C.byref(bad), C.byref(opt), C.byref(h)) == _lib.GBGPU_EINVAL
