@@ -484,15 +484,16 @@ __global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
 // one in-place GEMM update of the chunk rows, and the panel-local index and
 // column of every pivot, in increasing column order, and their count.
 //
-// Every row keeps its lead (first nonzero panel column).  A step takes the
-// non-pivot row with the smallest (lead, index) as the next pivot -- the same
-// pivot the column-by-column search finds -- and updates exactly the other
-// non-pivot rows with that lead, fraction-free: row_r <- a row_r - m row_i
-// (a = P[i][c], m = P[r][c]), which keeps the row space and needs no inverse
-// (pivot rows are normalised after the round).  Column c is never read
-// again, so it is not written.  The eight threads of a row are adjacent lanes;
-// they recompute the row's lead from the values they just wrote.  One step
-// per pivot, two barriers per step.
+// Every row keeps its lead (first nonzero panel column) in registers of its
+// eight threads (adjacent lanes).  A step takes the non-pivot row with the
+// smallest (lead, index) as the next pivot -- the same pivot the column-by-
+// column search finds -- and updates exactly the other non-pivot rows with that
+// lead: row_r -= (P[r][c] / P[i][c]) row_i on the columns after c and on E.
+// Pivot rows are not scaled (they are normalised after the round).  Column c
+// is never read again, so it is not written, and the multipliers need no
+// barrier; the updated rows recompute their leads from the values they wrote
+// and publish their keys for the next step.  Two barriers per pivot: the
+// minimum's and the pivot inverse's (one thread, Fermat).
 constexpr int PF_GROUPS = 8;     // threads (adjacent lanes) per row in k_panel_factor
 constexpr int PF_LD = KB + 8;    // row stride of P and E: conflict-free for 8 lanes per row
 
@@ -514,8 +515,7 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     uint32_t(*P)[PF_LD] = (uint32_t(*)[PF_LD])pf_smem;
     uint32_t(*E)[PF_LD] = (uint32_t(*)[PF_LD])(pf_smem + KB * PF_LD);
     __shared__ int s_min[2][KB * PF_GROUPS / 32];  // double-buffered block minimum
-    __shared__ int lead[KB];
-    __shared__ uint8_t is_piv[KB];
+    __shared__ uint32_t s_inv;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int r = tid / PF_GROUPS, g = tid % PF_GROUPS;  // row and column group of this thread
@@ -526,31 +526,24 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
         E[i][c] = i == c ? 1u : 0u;
     }
     __syncthreads();
-    {
-        int l = INT_MAX;
-        if (r < n)
-            for (int cc = g; cc < bw; cc += PF_GROUPS)
-                if (P[r][cc] != 0u) {
-                    l = cc;
-                    break;
-                }
-        l = min(l, __shfl_xor_sync(0xffffffffu, l, 1));
-        l = min(l, __shfl_xor_sync(0xffffffffu, l, 2));
-        l = min(l, __shfl_xor_sync(0xffffffffu, l, 4));
-        if (g == 0) {
-            lead[r] = l;
-            is_piv[r] = 0;
-        }
-    }
-    __syncthreads();
+    int my_lead = INT_MAX;  // this row's lead (INT_MAX: zero in the panel or not a row)
+    bool my_piv = false;
+    if (r < n)
+        for (int cc = g; cc < bw; cc += PF_GROUPS)
+            if (P[r][cc] != 0u) {
+                my_lead = cc;
+                break;
+            }
+    my_lead = min(my_lead, __shfl_xor_sync(0xffffffffu, my_lead, 1));
+    my_lead = min(my_lead, __shfl_xor_sync(0xffffffffu, my_lead, 2));
+    my_lead = min(my_lead, __shfl_xor_sync(0xffffffffu, my_lead, 4));
     int k = 0;
     for (int step = 0; step < KB; ++step) {
-        int key = INT_MAX;
-        if (g == 0 && r < n && !is_piv[r] && lead[r] != INT_MAX) key = lead[r] * KB + r;
+        int key = (g == 0 && !my_piv && my_lead != INT_MAX) ? my_lead * KB + r : INT_MAX;
         for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
         int* sm = s_min[step & 1];
         if (lane == 0) sm[warp] = key;
-        __syncthreads();
+        __syncthreads();  // also: the previous step's updates are visible
         int best = sm[0];
 #pragma unroll
         for (int w = 1; w < KB * PF_GROUPS / 32; ++w) best = min(best, sm[w]);
@@ -559,13 +552,12 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
         if (tid == 0) {
             piv_pos[k] = i;
             piv_col[k] = col0 + c;
-            is_piv[i] = 1;
+            s_inv = f.inv(P[i][c]);
         }
-        const bool active = r < n && r != i && !is_piv[r] && lead[r] == c;
-        __syncwarp();  // every lane has read lead[] before a lane of its row writes it
-        if (active) {
-            const uint32_t ap = f.prep(P[i][c]);
-            const uint32_t mp = f.prep(P[r][c]);
+        __syncthreads();
+        if (r == i) my_piv = true;
+        if (!my_piv && my_lead == c) {
+            const uint32_t mp = f.prep(f.mulmod(P[r][c], s_inv));
             int nl = INT_MAX;
             // four independent columns per pass (loads first, then stores)
             for (int cc = c + 1 + g; cc < bw; cc += 4 * PF_GROUPS) {
@@ -580,8 +572,8 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
                 for (int u = 0; u < 4; ++u) {
                     const int col = cc + u * PF_GROUPS;
                     if (col < bw) {
-                        const uint32_t y = f.mulsub(f.mulp(x[u], ap), mp, v[u]);
-                        P[r][col] = y;
+                        const uint32_t y = v[u] ? f.mulsub(x[u], mp, v[u]) : x[u];
+                        if (v[u]) P[r][col] = y;
                         if (y != 0u && col < nl) nl = col;
                     }
                 }
@@ -592,20 +584,19 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
                 for (int u = 0; u < 4; ++u) {
                     const int col = cc + u * PF_GROUPS;
                     v[u] = col < n ? E[i][col] : 0u;
-                    x[u] = col < n ? E[r][col] : 0u;
+                    x[u] = col < n && v[u] ? E[r][col] : 0u;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int col = cc + u * PF_GROUPS;
-                    if (col < n) E[r][col] = f.mulsub(f.mulp(x[u], ap), mp, v[u]);
+                    if (col < n && v[u]) E[r][col] = f.mulsub(x[u], mp, v[u]);
                 }
             }
             nl = min(nl, __shfl_xor_sync(grp, nl, 1));
             nl = min(nl, __shfl_xor_sync(grp, nl, 2));
             nl = min(nl, __shfl_xor_sync(grp, nl, 4));
-            if (g == 0) lead[r] = nl;
+            my_lead = nl;
         }
-        __syncthreads();
         ++k;
     }
     for (int t = tid; t < KB * KB; t += nt) {
