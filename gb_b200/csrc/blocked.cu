@@ -32,6 +32,8 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 
 #include <algorithm>
 #include <climits>
@@ -375,6 +377,44 @@ __global__ void k_collect_pending(int32_t t, const int32_t* __restrict__ lead,
                                   int32_t* n_pend) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < t; r += gridDim.x * blockDim.x)
         if (lead[r] >= 0 && !is_piv[r]) pend[atomicAdd(n_pend, 1)] = r;
+}
+
+// pending flags for an ordered compaction (rows in ascending order)
+__global__ void k_pending_flags(int32_t t, const int32_t* __restrict__ lead,
+                                const uint8_t* __restrict__ is_piv, uint8_t* flag) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < t; r += gridDim.x * blockDim.x)
+        flag[r] = (lead[r] >= 0 && !is_piv[r]) ? 1 : 0;
+}
+
+// chunk slot key of every pending row: its panel's slot, n_dirty for rows of
+// panels not factorized this round
+__global__ void k_panel_keys(int32_t n, const int32_t* __restrict__ pend,
+                             const int32_t* __restrict__ lead, const int32_t* __restrict__ dslot,
+                             int32_t n_dirty, int32_t* key) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t d = dslot[lead[pend[i]] / KB];
+        key[i] = d >= 0 ? d : n_dirty;
+    }
+}
+
+// rows sorted by (chunk slot, row): the first KB rows of every selected panel
+// fill its chunk in ascending row order; cursor = the panel's pending rows
+__global__ void k_bucket_sorted(int32_t n, const int32_t* __restrict__ key,
+                                const int32_t* __restrict__ rows, int32_t n_dirty,
+                                int32_t* chunk_rows, int32_t* cursor) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int32_t d = key[q];
+        if (d >= n_dirty) continue;
+        int lo = 0, hi = q;  // first position of this run
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (key[mid] < d) lo = mid + 1;
+            else hi = mid;
+        }
+        const int slot = q - lo;
+        if (slot < KB) chunk_rows[d * KB + slot] = rows[q];
+        if (q == n - 1 || key[q + 1] != d) cursor[d] = q - lo + 1;
+    }
 }
 
 // rows per lead column and per 128-column panel; a panel is "dirty" when
@@ -962,14 +1002,36 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     int32_t* piv_colb = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* n_piv = c.alloc<int32_t>(max_dirty);
     int32_t* piv_rows = c.alloc<int32_t>((size_t)max_dirty * KB);
-    if (!chunk_rows || !cursor || !imeB || !piv_pos || !piv_colb || !n_piv || !piv_rows)
+    // ordered compaction of the pending rows and the stable (panel, row) sort
+    // that fills the chunks: the same rows, in the same order, on every run
+    uint8_t* pflag = c.alloc<uint8_t>(t);
+    int32_t* pkey = c.alloc<int32_t>(t);
+    int32_t* pkey_sorted = c.alloc<int32_t>(t);
+    int32_t* prow_sorted = c.alloc<int32_t>(t);
+    size_t sel_bytes = 0, sort_bytes = 0;
+    cub::CountingInputIterator<int32_t> row_ids(0);
+    cub::DeviceSelect::Flagged(nullptr, sel_bytes, row_ids, pflag, pend, counters, t, s);
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, pkey, pkey_sorted, pend, prow_sorted, t,
+                                    0, 32, s);
+    void* sel_tmp = c.alloc<uint8_t>(sel_bytes);
+    void* sort_tmp = c.alloc<uint8_t>(sort_bytes);
+    if (!chunk_rows || !cursor || !imeB || !piv_pos || !piv_colb || !n_piv || !piv_rows ||
+        !pflag || !pkey || !pkey_sorted || !prow_sorted || !sel_tmp || !sort_tmp)
         return GBGPU_ENOMEM;
+    // pending rows (nonzero, not pivots) into pend[0 .. *count), ascending
+    auto collect_pending = [&](int32_t* count) -> int {
+        BL_LAUNCH(k_pending_flags<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, pflag));
+        size_t bytes = sel_bytes;
+        BL_CUDA(cub::DeviceSelect::Flagged(sel_tmp, bytes, row_ids, pflag, pend, count, t, s));
+        ++c.launches;
+        return GBGPU_OK;
+    };
     int rounds = 0;
     bool first = true;
     while (t > 0 && ncr > 0) {
         int32_t n_pend = 0;
         BL_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int32_t), s));
-        BL_LAUNCH(k_collect_pending<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, pend, counters));
+        BL_CHECK(collect_pending(counters));
         BL_CUDA(cudaMemcpyAsync(&n_pend, counters, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         if (first) out->dense_rows = n_pend;
@@ -1006,8 +1068,18 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             BL_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int32_t) * n_dirty, s));
             BL_LAUNCH(k_fill_i32<<<grid_of((int64_t)n_dirty * KB), 256, 0, s>>>(
                 chunk_rows, n_dirty * KB, -1));
-            BL_LAUNCH(k_bucket_dirty<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, dslot,
-                                                                      cursor, chunk_rows));
+            BL_LAUNCH(k_panel_keys<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, dslot,
+                                                                    n_dirty, pkey));
+            {
+                int bits = 1;
+                while ((1 << bits) <= n_dirty) ++bits;
+                size_t bytes = sort_bytes;
+                BL_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, pkey, pkey_sorted, pend,
+                                                        prow_sorted, n_pend, 0, bits, s));
+                ++c.launches;
+            }
+            BL_LAUNCH(k_bucket_sorted<<<grid_of(n_pend), 256, 0, s>>>(
+                n_pend, pkey_sorted, prow_sorted, n_dirty, chunk_rows, cursor));
             BL_LAUNCH(k_panel_factor<F><<<n_dirty, KB * PF_GROUPS, pf_bytes, s>>>(
                 Dp, ld, chunk_rows, dpanel, cursor, ncr, imeB, piv_pos, piv_colb, n_piv, f));
             // pivot rows of every chunk (columns j0..) <- old - (I - E_d) old =
@@ -1062,8 +1134,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             n_new, prow, pc, ncr, Dp, ld, f));
         // the rest: eliminated against every pivot of the round
         int32_t n_rest = 0;
-        BL_LAUNCH(k_collect_pending<<<grid_of(t), 256, 0, s>>>(t, lead, is_piv, pend,
-                                                                counters + 3));
+        BL_CHECK(collect_pending(counters + 3));
         BL_CUDA(cudaMemcpyAsync(&n_rest, counters + 3, 4, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         if (n_rest == 0) break;
