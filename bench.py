@@ -192,10 +192,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
-    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense", "rref"],
+    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense", "rref", "batch"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
-                         "rref: RREF of a rank-3n/4 n x n block")
+                         "rref: RREF of a rank-3n/4 n x n block; batch: 2 x 128 independent "
+                         "matrices through the batch entry point")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
@@ -206,6 +207,9 @@ def main():
         return
     if args.workload in ("dense", "rref"):
         run_dense(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
 
     import torch
@@ -465,6 +469,76 @@ def run_dense(args):
         ms_p = timed(_lib.FORM_PLAIN, 1)
         line["plain_ms"] = ms_p
         line["tensor_speedup_vs_plain"] = ms_p / ms_t
+    print(json.dumps(line), flush=True)
+
+
+def batch_matrices(n_images: int = 128, n_mixed: int = 128, seed: int = 5):
+    """The two batches of the batched workload:
+    (a) one integer system (staircase structure, 2400 x 600, 3600 columns,
+        coefficients in [-2^20, 2^20]) reduced modulo the n_images largest
+        primes below 2^31 -- same structure, different coefficients;
+    (b) n_mixed staircase matrices over p = 32003 with total rows log-uniform
+        in [500, 5000] (a fifth of them C|D rows), columns 1.5-3 x rows,
+        density U[1%, 10%]."""
+    from gb_b200 import synth
+    base = synth.integer_staircase(2400, 600, 2400, seed=seed)
+    imgs = [synth.image_mod(base, q) for q in synth.largest_primes_below(1 << 31, n_images)]
+    rng = np.random.default_rng(seed)
+    mixed = []
+    for i in range(n_mixed):
+        rows = int(np.exp(rng.uniform(np.log(500), np.log(5000))))
+        nrl = max(1, rows // 5)
+        nru = rows - nrl
+        ncr = max(16, int(rows * rng.uniform(1.5, 3.0)) - nru)
+        mixed.append(synth.staircase(nru, nrl, ncr, 32003, 0.01, 0.10, seed=seed * 1000 + i))
+    return imgs, mixed
+
+
+def run_batch(args):
+    """Batched workload: 2 x 128 independent matrices through gbgpu_reduce_batch
+    (host CSR in, host rows out), timed end to end on the host clock around the
+    call (the call returns when every answer is in host memory)."""
+    import torch
+    from gb_b200 import _lib, la
+    _lib.load()
+    imgs, mixed = batch_matrices()
+    out = {}
+    for name, mats in (("prime images", imgs), ("mixed sizes p=32003", mixed)):
+        la.reduce_batch(mats[:4])  # warm
+        ts = []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res, st = la.reduce_batch(mats)
+            ts.append(time.perf_counter() - t0)
+            assert all(x == 0 for x in st), st
+        sec = statistics.median(ts)
+        # spot check: the batched answers equal single-matrix reductions
+        for i in (0, len(mats) // 2, len(mats) - 1):
+            assert res[i].equals(la.linear_algebra(mats[i])), (name, i)
+        entry = {"matrices": len(mats), "seconds": sec, "matrices_per_s": len(mats) / sec,
+                 "rows_total": int(sum(m.nr for m in mats)),
+                 "nnz_total": int(sum(m.nnz for m in mats))}
+        if not args.no_cpu:
+            # the reference's la (oracle/_ref, option 1, all host threads) on
+            # every 16th matrix of the batch, scaled to the whole batch
+            import oracle
+            threads = os.cpu_count() or 1
+            sample = mats[::16]
+            cpu = sum(oracle.ref_la(m, 1, nthreads=threads)[1] for m in sample)
+            entry["cpu_reference_matrices_per_s"] = len(sample) / cpu
+            entry["cpu_sample"] = f"{len(sample)} of {len(mats)} matrices, {threads} threads"
+        out[name] = entry
+    n = sum(v["matrices"] for v in out.values())
+    sec = sum(v["seconds"] for v in out.values())
+    line = {"metric": "batched GF(p) matrix reductions/s (end to end, host CSR in/out)",
+            "value": n / sec, "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (mod p, exact)",
+            "data": "synthetic (seeded staircase batches)",
+            "config": {"workload": "batch: 128 images of one integer system mod the largest "
+                                   "primes < 2^31 + 128 mixed-size matrices over 32003",
+                       "batches": out}}
     print(json.dumps(line), flush=True)
 
 

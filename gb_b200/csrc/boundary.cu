@@ -17,6 +17,8 @@
 #include <cstring>
 #include <ctime>
 #include <sys/time.h>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "../../include/gbgpu.h"
@@ -203,21 +205,40 @@ void gbgpu_interreduce_matrix_rows(gbgpu_mat_t* mat, gbgpu_bs_t* bs, const gbgpu
 int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
                        gbgpu_rows* outs, int32_t* status) {
     if (n < 0 || (n > 0 && (!ms || !outs || !status))) return GBGPU_EINVAL;
-    std::vector<Plan*> plans((size_t)n, nullptr);
-    // every matrix gets its own stream so independent reductions overlap
     for (int32_t i = 0; i < n; ++i) {
         memset(&outs[i], 0, sizeof(gbgpu_rows));
-        gbgpu_options o{};
-        if (opt) o = *opt;
-        o.stream = nullptr;
-        status[i] = plan_create(&ms[i], &o, 0, &plans[i]);
+        status[i] = GBGPU_OK;
     }
-    for (int32_t i = 0; i < n; ++i)
-        if (!status[i]) status[i] = plan_run(plans[i]);
-    for (int32_t i = 0; i < n; ++i) {
-        if (!status[i]) status[i] = plan_result(plans[i], &outs[i]);
-        if (plans[i]) plan_destroy(plans[i]);
-    }
+    // A few host workers, each reducing one matrix at a time on a stream of
+    // its own: the reductions of different matrices overlap on the device
+    // (their host round trips and small launches interleave), and at most
+    // `workers` matrices hold device memory at once.
+    int workers = 4;
+    if (const char* w = getenv("GBGPU_BATCH_WORKERS")) workers = std::max(1, atoi(w));
+    workers = std::min<int>(workers, std::max<int32_t>(n, 1));
+    const int device = opt ? opt->device : 0;
+    std::atomic<int32_t> next{0};
+    auto work = [&]() {
+        if (cudaSetDevice(device) != cudaSuccess) {
+            for (int32_t i; (i = next.fetch_add(1)) < n;) status[i] = GBGPU_ECUDA;
+            return;
+        }
+        for (int32_t i; (i = next.fetch_add(1)) < n;) {
+            gbgpu_options o{};
+            if (opt) o = *opt;
+            o.stream = nullptr;  // the plan creates its own stream
+            Plan* P = nullptr;
+            int rc = plan_create(&ms[i], &o, 0, &P);
+            if (!rc) rc = plan_run(P);
+            if (!rc) rc = plan_result(P, &outs[i]);
+            if (P) plan_destroy(P);
+            status[i] = rc;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int k = 1; k < workers; ++k) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
     return GBGPU_OK;
 }
 

@@ -76,6 +76,57 @@ def staircase(nru: int = 20000, nrl: int = 5000, ncr: int = 20000, p: int = 6552
     return MacaulayMatrix(p, ncl, ncr, ptr, cols, vals, laopt)
 
 
+def integer_staircase(nru: int, nrl: int, ncr: int, bound: int = 1 << 20,
+                      dmin: float = 0.02, dmax: float = 0.05, seed: int = 1) -> MacaulayMatrix:
+    """The staircase structure with integer coefficients in [-bound, bound]
+    without 0 (leads 1): one "system" whose images modulo many primes
+    (``image_mod``) share their sparsity structure.  The returned matrix holds
+    the integers in ``vals`` (int64) and ``p`` = 2 bound + 1."""
+    m = staircase(nru, nrl, ncr, 2 * bound + 1, dmin, dmax, seed=seed)
+    v = m.vals.astype(np.int64)
+    ints = np.where(v > bound, v - (2 * bound + 1), v)  # [1, bound] U [-bound, -1]
+    return MacaulayMatrix(m.p, m.ncl, m.ncr, m.row_ptr, m.cols, ints, m.laopt)
+
+
+def image_mod(m: MacaulayMatrix, p: int) -> MacaulayMatrix:
+    """The image of an integer matrix (``integer_staircase``) modulo a prime
+    p > bound: every coefficient stays nonzero, leads stay 1."""
+    vals = np.mod(np.asarray(m.vals, dtype=np.int64), p).astype(np.int32)
+    return MacaulayMatrix(p, m.ncl, m.ncr, m.row_ptr, m.cols, vals, m.laopt)
+
+
+def largest_primes_below(bound: int, count: int) -> list:
+    """The `count` largest primes below `bound` (deterministic Miller-Rabin
+    for 64-bit integers)."""
+    def is_prime(n: int) -> bool:
+        if n < 2:
+            return False
+        for q in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+            if n % q == 0:
+                return n == q
+        d, r = n - 1, 0
+        while d % 2 == 0:
+            d //= 2
+            r += 1
+        for a in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+            x = pow(a, d, n)
+            if x in (1, n - 1):
+                continue
+            for _ in range(r - 1):
+                x = x * x % n
+                if x == n - 1:
+                    break
+            else:
+                return False
+        return True
+    out, n = [], bound - 1
+    while len(out) < count and n > 1:
+        if is_prime(n):
+            out.append(n)
+        n -= 1
+    return out
+
+
 def random_macaulay(nru: int, nrl: int, ncr: int, p: int, density: float = 0.1,
                     seed: int = 0, laopt: int = 1, dup_rows: int = 0,
                     right_only_frac: float = 0.0) -> MacaulayMatrix:
