@@ -192,11 +192,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
-    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense", "rref", "batch"],
+    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense", "rref", "batch", "f4"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
                          "rref: RREF of a rank-3n/4 n x n block; batch: 2 x 128 independent "
-                         "matrices through the batch entry point")
+                         "matrices through the batch entry point; f4: the captured la calls "
+                         "of the dense F4 systems")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
@@ -210,6 +211,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args)
+        return
+    if args.workload == "f4":
+        run_f4_captures(args)
         return
 
     import torch
@@ -539,6 +543,51 @@ def run_batch(args):
             "config": {"workload": "batch: 128 images of one integer system mod the largest "
                                    "primes < 2^31 + 128 mixed-size matrices over 32003",
                        "batches": out}}
+    print(json.dumps(line), flush=True)
+
+
+def run_f4_captures(args):
+    """The linear-algebra calls of F4 on the dense systems (reference-captured
+    matrices under tests/golden/mats): dense_quadratic_7 (7 quadratics in 7
+    variables, p = 32003, la option 2) and dense_cubic_5_p31 (5 cubics in 5
+    variables, p = 2^31 - 1, la option 1).  Each step reduces every captured
+    matrix of a system once through gbgpu_reduce (host CSR in, host rows out,
+    the call the drop-in makes); every answer is compared with the reference's
+    captured answer.  The CPU column is the reference's la on the same calls."""
+    from gb_b200 import _lib, la
+    from gb_b200.matrix import load_captures
+    _lib.load()
+    systems = {}
+    for name in ("dense_quadratic_7", "dense_cubic_5_p31"):
+        caps = load_captures(os.path.join(REPO, "tests", "golden", "mats", name + ".npz"))
+        caps = [c for c in caps if c.kind == 0]
+        for c in caps:  # warm
+            la.linear_algebra(c.mat)
+        ts = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            for c in caps:
+                ans = la.linear_algebra(c.mat)
+                assert ans.equals(c.answer), name
+            ts.append(time.perf_counter() - t0)
+        entry = {"matrices": len(caps), "largest": max([c.mat.nr, c.mat.nc] for c in caps),
+                 "gpu_ms_per_system": statistics.median(ts) * 1e3}
+        if not args.no_cpu:
+            import oracle
+            threads = os.cpu_count() or 1
+            cpu = sum(oracle.ref_la(c.mat, c.mat.laopt, nthreads=threads)[1] for c in caps)
+            entry["cpu_reference_ms_per_system"] = cpu * 1e3
+            entry["cpu_threads"] = threads
+        systems[name] = entry
+    ms = sum(v["gpu_ms_per_system"] for v in systems.values())
+    n = sum(v["matrices"] for v in systems.values())
+    line = {"metric": "F4 linear-algebra calls/s (reference-captured dense systems, end to end)",
+            "value": n / (ms * 1e-3), "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (mod p, exact)",
+            "data": "reference-captured F4 matrices (tests/golden/mats)",
+            "config": {"workload": "f4 captures: dense_quadratic_7 (p=32003) + "
+                                   "dense_cubic_5_p31 (p=2^31-1)", "systems": systems}}
     print(json.dumps(line), flush=True)
 
 

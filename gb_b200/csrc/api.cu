@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <climits>
 #include <cstdio>
@@ -37,6 +38,20 @@ static std::atomic<long long> g_launches{0};
 
 void set_error(const std::string& s) { g_last_error = s; }
 void count_launch(long long n) { g_launches += n; }
+
+cudaError_t ensure_smem_limit(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> limits;  // (kernel, device) -> bytes
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int& cur = limits[{kernel, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 
 #define GB_CUDA(call)                                                              \
     do {                                                                           \

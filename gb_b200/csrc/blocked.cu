@@ -794,7 +794,7 @@ static int neg_inverse_big(Ctx& c, const F& f, const uint32_t* src, int64_t lds,
         src, lds, stride_src, n_blocks, last_nb, NB, U));
     BL_CUDA(cudaMemsetAsync(out, 0, sizeof(uint32_t) * (size_t)n_blocks * bstride, c.s));
     const int bytes = (2 * KB * (KB + 1) + KB * KB / 4) * (int)sizeof(uint32_t);
-    BL_CUDA(cudaFuncSetAttribute(k_neg_inverse<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    BL_CUDA(ensure_smem_limit((const void*)k_neg_inverse<F>, bytes));
     const int32_t n_sub = n_blocks * (NB / KB);
     const int64_t dstep = (int64_t)KB * (NB + 1);  // between 128-blocks on the diagonal
     BL_LAUNCH(k_neg_inverse<F><<<n_sub, INV_THREADS, bytes, c.s>>>(U, NB, dstep, n_sub, KB, out,
@@ -885,8 +885,7 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         BL_CUDA(cub::DeviceRadixSort::SortPairs(tmp, bytes, lead_in, lead_sorted, in.work,
                                                 work_sorted, t, 0, 32, s));
         ++c.launches;
-        BL_CUDA(cudaFuncSetAttribute(k_densify_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     DS_COLS * 4));
+        BL_CUDA(ensure_smem_limit((const void*)k_densify_seg, DS_COLS * 4));
         BL_LAUNCH(k_densify_seg<<<std::min(t, 148 * 3), 512, DS_COLS * 4, s>>>(
             t, work_sorted, in.row_ptr, in.cols, in.vals, nc, 0, W, ld));
     }
@@ -991,8 +990,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)t * 32), 256, 0, s>>>(t, nullptr, ncr, Dp, ld, lead));
     }
     const int pf_bytes = 2 * KB * PF_LD * (int)sizeof(uint32_t);
-    BL_CUDA(cudaFuncSetAttribute(k_panel_factor<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 pf_bytes));
+    BL_CUDA(ensure_smem_limit((const void*)k_panel_factor<F>, pf_bytes));
     // every dirty panel is factorized in the round that finds it (batch <= 4096)
     const int32_t max_dirty = std::max<int32_t>(1, std::min<int32_t>(npan, 4096));
     int32_t* chunk_rows = c.alloc<int32_t>((size_t)max_dirty * KB);

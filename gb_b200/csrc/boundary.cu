@@ -233,6 +233,8 @@ int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
             if (!rc) rc = plan_result(P, &outs[i]);
             if (P) plan_destroy(P);
             status[i] = rc;
+            if (rc && getenv("GBGPU_DEBUG"))
+                fprintf(stderr, "gbgpu batch matrix %d: status %d: %s\n", i, rc, gbgpu_last_error());
         }
     };
     std::vector<std::thread> pool;

@@ -1,5 +1,7 @@
 // internal.h -- host-side declarations shared by the library's translation units.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <string>
 
 #include "../../include/gbgpu.h"
@@ -15,6 +17,10 @@ struct Plan;
 
 void set_error(const std::string& s);
 void count_launch(long long n);
+// Raise the dynamic shared-memory limit of a kernel on the current device to
+// at least `bytes`.  The limit only ever grows and is changed under a lock,
+// so a launch in one host thread never sees another thread lower it.
+cudaError_t ensure_smem_limit(const void* kernel, int bytes);
 int device_init(int device, DeviceInfo* info);
 
 // mode 0: linear_algebra (reduce C|D rows by the known pivots, then reduced

@@ -22,6 +22,7 @@
 #include <climits>
 
 #include "common.cuh"
+#include "internal.h"
 #include "kernels.h"
 
 namespace gbgpu {
@@ -379,9 +380,7 @@ template <class F>
 cudaError_t launch_reduce_sparse(const SparseReduceArgs& a, const F& f, int grid, bool smem,
                                  int smem_bytes, cudaStream_t s) {
     if (smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_reduce_sparse<F, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             smem_bytes);
+        cudaError_t e = ensure_smem_limit((const void*)k_reduce_sparse<F, true>, smem_bytes);
         if (e != cudaSuccess) return e;
         k_reduce_sparse<F, true><<<grid, kReduceThreads, smem_bytes, s>>>(a, f);
     } else {
@@ -394,9 +393,7 @@ template <class F>
 cudaError_t launch_reduce_dense(const DenseReduceArgs& a, const F& f, int grid, bool smem,
                                 int smem_bytes, cudaStream_t s) {
     if (smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_reduce_dense<F, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             smem_bytes);
+        cudaError_t e = ensure_smem_limit((const void*)k_reduce_dense<F, true>, smem_bytes);
         if (e != cudaSuccess) return e;
         k_reduce_dense<F, true><<<grid, kReduceThreads, smem_bytes, s>>>(a, f);
     } else {

@@ -844,8 +844,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     }
     prm.err = err;
     prm.budget = 4000000000LL;  // about 2 s at 2 GHz per wait
-    cudaError_t e = cudaFuncSetAttribute(k_tc_submul<L, SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Cfg::SMEM_BYTES);
+    cudaError_t e = ensure_smem_limit((const void*)k_tc_submul<L, SMALL>, Cfg::SMEM_BYTES);
     if (e != cudaSuccess) {
         set_error(std::string("tc smem attribute: ") + cudaGetErrorString(e));
         return GBGPU_ECUDA;
