@@ -198,6 +198,12 @@ struct Plan {
     int32_t np = 0;
     int64_t onnz = 0;
     uint32_t errbits = 0;
+    // small matrices: one-CTA echelon + compaction, no host round trip in a
+    // run; its checks, counts and timings are read when the answer is taken
+    bool tiny = false;
+    int tiny_bytes = 0;
+    int64_t* tiny_counts = nullptr;  // [2]: rows, entries of the answer
+    bool pending = false;            // a tiny run whose results are not read yet
     gbgpu_stats stats{};
     cudaEvent_t ev[8] = {};
     long long launches = 0;
@@ -304,6 +310,17 @@ static int plan_alloc(Plan* P) {
             A(losers, P->n_work);
         }
     }
+    if (P->mode == 0 && !P->blocked && P->n_work > 0 && P->ncr > 0)
+        P->tiny_bytes = tiny_rref_bytes(P->n_work, P->ncr, P->dev.smem_optin);
+    P->tiny = P->tiny_bytes > 0;
+    if (P->tiny) {
+        // the answer has at most n_work rows of ncr entries
+        const size_t cap = (size_t)P->n_work * P->ncr;
+        A(tiny_counts, 2);
+        A(out_cols, cap);
+        A(out_vals, cap);
+        P->out_cap = (int64_t)cap;
+    }
     A(piv_of_col, width);
     A(pflag, width);
     A(ppos, width);
@@ -362,8 +379,14 @@ static int run_form(Plan* P, const F& f) {
     if (P->mode == 0)
         GB_LAUNCH(k_check_pivots<<<grid_for(P->ncl, T), T, 0, s>>>(P->ncl, P->piv_row, P->err));
     GB_CUDA(cudaEventRecord(P->ev[6], s));
-    GB_CUDA(cudaMemcpyAsync(&P->errbits, P->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    GB_CUDA(cudaStreamSynchronize(s));
+    if (P->tiny) {
+        // the checks' verdict is read with the answer; the kernels below skip
+        // their work when it flags the input
+        P->errbits = 0;
+    } else {
+        GB_CUDA(cudaMemcpyAsync(&P->errbits, P->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+    }
     GB_CUDA(cudaEventRecord(P->ev[7], s));
     if (P->errbits) {
         std::string msg;
@@ -448,11 +471,23 @@ static int run_form(Plan* P, const F& f) {
     sa.gacc = P->gacc;
     sa.queue = P->counters + 0;
     sa.work_count = P->work_count + 0;
+    sa.err = P->err;
     if (P->n_work > 0)
         GB_CALL(launch_reduce_sparse(sa, f, P->grid_sparse, P->smem_sparse, P->nc * 4, s));
     GB_CUDA(cudaEventRecord(P->ev[2], s));
 
-    if (P->mode == 0) {
+    if (P->tiny) {
+        // ---- small right block: echelon form and compaction in one CTA ------
+        GB_CALL(launch_tiny_rref(P->n_work, P->ncr, P->D, P->ld, P->lead, P->err, P->ncl,
+                                 P->offs, P->out_cols, P->out_vals, P->piv_of_col,
+                                 P->tiny_counts, P->tiny_bytes, s, f));
+        P->stats.echelon_rounds = 0;
+        GB_CUDA(cudaEventRecord(P->ev[3], s));
+        GB_CUDA(cudaEventRecord(P->ev[4], s));
+        GB_CUDA(cudaEventRecord(P->ev[5], s));
+        P->pending = true;
+        return GBGPU_OK;
+    } else if (P->mode == 0) {
         // ---- echelon rounds on the dense right block ------------------------
         GB_LAUNCH(k_fill_i32<<<grid_for(P->ncr, T), T, 0, s>>>(P->piv_of_col, P->ncr, -1));
         GB_LAUNCH(k_collect_nonzero<<<grid_for(P->n_work, T), T, 0, s>>>(
@@ -590,6 +625,32 @@ static int run_form(Plan* P, const F& f) {
     return GBGPU_OK;
 }
 
+int finish_stats(Plan* P);
+
+// a small-matrix run enqueues everything without waiting; its input checks,
+// answer size and statistics are read here, before the answer is used
+int settle(Plan* P) {
+    if (!P->pending) return GBGPU_OK;
+    P->pending = false;
+    int64_t counts[2] = {0, 0};
+    GB_CUDA(cudaMemcpyAsync(&P->errbits, P->err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            P->stream));
+    GB_CUDA(cudaMemcpyAsync(counts, P->tiny_counts, sizeof(counts), cudaMemcpyDeviceToHost,
+                            P->stream));
+    GB_CUDA(cudaStreamSynchronize(P->stream));
+    if (P->errbits) {
+        std::string msg;
+        const int rc = err_to_status(P->errbits, &msg);
+        set_error(msg);
+        P->np = 0;
+        P->onnz = 0;
+        return rc;
+    }
+    P->np = (int32_t)counts[0];
+    P->onnz = counts[1];
+    return finish_stats(P);
+}
+
 int plan_run(Plan* P) {
     P->launches = 0;
     int rc;
@@ -631,6 +692,12 @@ int plan_run(Plan* P) {
         }
     }
     if (rc) return rc;
+    if (P->pending) return GBGPU_OK;  // small matrix: settled when the answer is read
+    return finish_stats(P);
+}
+
+// statistics of the last run (waits for it)
+int finish_stats(Plan* P) {
     GB_CUDA(cudaEventSynchronize(P->ev[5]));
     int64_t wc[2] = {0, 0};
     GB_CUDA(cudaMemcpyAsync(wc, P->work_count, sizeof(wc), cudaMemcpyDeviceToHost, P->stream));
@@ -753,6 +820,7 @@ int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** o
 
 int plan_result(Plan* P, gbgpu_rows* out) {
     memset(out, 0, sizeof(*out));
+    if (int rc = settle(P)) return rc;
     GB_CUDA(cudaStreamSynchronize(P->stream));
     out->np = P->np;
     out->nnz = P->onnz;
@@ -781,6 +849,7 @@ int plan_result(Plan* P, gbgpu_rows* out) {
 // copy the answer into caller-provided host arrays (no allocation)
 int plan_result_into(Plan* P, int64_t* row_ptr, int32_t* cols, int32_t* vals, int64_t cap_rows,
                      int64_t cap_nnz, int32_t* np, int64_t* nnz) {
+    if (int rc = settle(P)) return rc;
     GB_CUDA(cudaStreamSynchronize(P->stream));
     *np = P->np;
     *nnz = P->onnz;
@@ -812,6 +881,7 @@ int plan_result_into_v(Plan* P, int64_t* row_ptr, int32_t* cols, void* vals, int
         set_error("val_bytes must be 4, 2 (p < 2^16) or 1 (p < 2^8)");
         return GBGPU_EINVAL;
     }
+    if (int rc = settle(P)) return rc;
     GB_CUDA(cudaStreamSynchronize(P->stream));
     *np = P->np;
     *nnz = P->onnz;
@@ -896,8 +966,10 @@ int gbgpu_plan_result_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, 
 
 int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {
     if (!plan || !stats) return GBGPU_EINVAL;
+    // a pending small-matrix run is settled first (its timings, its checks)
+    const int rc = settle(plan->impl);
     *stats = plan_stats(plan->impl);
-    return GBGPU_OK;
+    return rc;
 }
 
 void gbgpu_plan_destroy(gbgpu_plan* plan) {

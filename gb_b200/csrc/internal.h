@@ -33,5 +33,7 @@ int plan_result_into(Plan* P, int64_t* row_ptr, int32_t* cols, int32_t* vals, in
                      int64_t cap_nnz, int32_t* np, int64_t* nnz);
 void plan_destroy(Plan* P);
 const gbgpu_stats& plan_stats(const Plan* P);
+// waits for a pending small-matrix run and reads its checks and sizes
+int settle(Plan* P);
 
 }  // namespace gbgpu

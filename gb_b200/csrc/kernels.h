@@ -29,6 +29,7 @@ struct SparseReduceArgs {
     uint32_t* gacc;          // [grid][acc_stride] when the accumulator is global
     int32_t* queue;          // work counter, zero before the launch
     int64_t* work_count;     // pivot entries applied (statistics)
+    const uint32_t* err = nullptr;  // optional: the input checks' flags (nonzero: skip)
 };
 
 struct DenseReduceArgs {
@@ -75,6 +76,14 @@ cudaError_t launch_promote(int grid, int threads, cudaStream_t s, const int32_t*
                            const int32_t* n_cand, const int32_t* lead, int32_t* claim,
                            int32_t* piv_of_col, uint32_t* rows, int64_t ld, int32_t ncr,
                            int32_t* losers, int32_t* n_losers, const F& f);
+
+// one-CTA reduced row echelon form of a small dense block (see plain.cu)
+int tiny_rref_bytes(int32_t n, int32_t m, int smem_optin);
+template <class F>
+cudaError_t launch_tiny_rref(int32_t n, int32_t m, const uint32_t* D, int64_t ld,
+                             const int32_t* lead, const uint32_t* err, int32_t col_shift,
+                             int64_t* offs, int32_t* cols, int32_t* vals, int32_t* piv_of_col,
+                             int64_t* counts, int bytes, cudaStream_t s, const F& f);
 
 __global__ void k_claim(const int32_t* cand, const int32_t* n_cand, const int32_t* lead,
                         int32_t* claim);

@@ -135,6 +135,7 @@ k_reduce_sparse(SparseReduceArgs a, F f) {
     __shared__ int s_work;
     uint32_t* acc = SMEM ? s_acc : a.gacc + (size_t)blockIdx.x * a.acc_stride;
     const int tid = threadIdx.x, nt = blockDim.x;
+    if (a.err && *a.err) return;  // invalid input: nothing is read (uniform)
 
     for (;;) {
         if (tid == 0) s_work = atomicAdd(a.queue, 1);
@@ -412,6 +413,218 @@ cudaError_t launch_promote(int grid, int threads, cudaStream_t s, const int32_t*
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Small matrices: the reduced row echelon form of the whole n x m block D'
+// (rows with lead < 0 are zero) and its compaction to CSR in the shared
+// memory of ONE CTA, in one launch instead of echelon rounds, back
+// substitution and compaction (which cost a host round trip each).  Row r
+// belongs to warp r % 32.  A step takes the non-pivot row with the smallest
+// (lead, row) as the pivot (the pivots of the column-by-column search),
+// normalises it (one inverse, lane 0 of its warp), and every warp clears the
+// pivot column from its other rows, pivots included (Gauss-Jordan),
+// recomputing the leads of the non-pivot rows it changed.  Output: the pivot
+// rows in descending pivot-column order as CSR (columns + col_shift), their
+// offsets, piv_of_col, and counts[0..1] = rows, entries.  When the input
+// checks flagged an error nothing is read and the answer is empty.
+constexpr int kTinyThreads = 1024;
+
+// in-place exclusive prefix sum of a[0..n) in shared memory; returns the total
+__device__ int tiny_exscan(int* a, int n, int* tmp) {
+    for (int off = 1; off < n; off <<= 1) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = a[i] + (i >= off ? a[i - off] : 0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = tmp[i];
+        __syncthreads();
+    }
+    const int total = n > 0 ? a[n - 1] : 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = i > 0 ? a[i - 1] : 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = tmp[i];
+    __syncthreads();
+    return total;
+}
+
+struct TinyOut {
+    int32_t col_shift;
+    int64_t* offs;      // [rank + 1]
+    int32_t* cols;      // [entries]
+    int32_t* vals;      // [entries]
+    int32_t* piv_of_col;  // [m]
+    int64_t* counts;    // rows, entries
+};
+
+template <class F>
+__global__ void __launch_bounds__(kTinyThreads)
+k_tiny_rref(int32_t n, int32_t m, const uint32_t* __restrict__ D, int64_t ld,
+            const int32_t* __restrict__ lead_in, const uint32_t* err, TinyOut out, F f) {
+    extern __shared__ uint32_t tiny_smem[];
+    const int tld = m + 1;
+    uint32_t* T = tiny_smem;                                 // [n][m + 1]
+    int32_t* lead = (int32_t*)(tiny_smem + (size_t)n * tld);  // [n]
+    int32_t* pcol = lead + n;                                // [n] pivot column of a pivot row, -1
+    int32_t* rcnt = pcol + n;                                // [n] entries of a pivot row
+    int32_t* prow = rcnt + n;                                // [m] pivot row of a column, -1
+    int32_t* rank = prow + m;                                // [max(n, m)] scan space
+    int32_t* tmp = rank + max(n, m);                         // [max(n, m)]
+    __shared__ int s_min[kTinyThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kTinyThreads / 32;
+    if (*err) {  // invalid input: nothing is read, the answer is empty (uniform)
+        for (int c = tid; c < m; c += blockDim.x) out.piv_of_col[c] = -1;
+        if (tid == 0) {
+            out.offs[0] = 0;
+            out.counts[0] = 0;
+            out.counts[1] = 0;
+        }
+        return;
+    }
+    for (int c = tid; c < m; c += blockDim.x) prow[c] = -1;
+    for (int64_t t = tid; t < (int64_t)n * m; t += blockDim.x) {
+        const int r = (int)(t / m), c = (int)(t % m);
+        T[(size_t)r * tld + c] = D[(size_t)r * ld + c];
+    }
+    for (int r = tid; r < n; r += blockDim.x) {
+        lead[r] = lead_in[r] < 0 ? INT_MAX : lead_in[r];
+        pcol[r] = -1;
+    }
+    __syncthreads();
+    for (int step = 0; step < n; ++step) {
+        // smallest (lead, row) over the non-pivot rows of this warp
+        int key = INT_MAX;
+        for (int r = warp + NW * lane; r < n; r += NW * 32)
+            if (pcol[r] < 0 && lead[r] != INT_MAX) key = min(key, lead[r] * n + r);
+        for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+        if (lane == 0) s_min[warp] = key;
+        __syncthreads();
+        int best = s_min[0];
+#pragma unroll 8
+        for (int w = 1; w < NW; ++w) best = min(best, s_min[w]);
+        __syncthreads();  // everyone read s_min before the next step writes it
+        if (best == INT_MAX) break;  // uniform: rank reached
+        const int c = best / n, i = best % n;
+        uint32_t* pr = T + (size_t)i * tld;
+        if (warp == (i % NW)) {
+            // normalise the pivot row (its owner warp)
+            uint32_t inv = 0;
+            if (lane == 0) inv = f.inv(pr[c]);
+            inv = __shfl_sync(0xffffffffu, inv, 0);
+            const uint32_t ip = f.prep(inv);
+            for (int j = c + 1 + lane; j < m; j += 32) {
+                const uint32_t v = pr[j];
+                if (v) pr[j] = f.mulp(v, ip);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                pr[c] = 1u;
+                pcol[i] = c;
+                prow[c] = i;
+            }
+        }
+        __syncthreads();
+        // clear column c from this warp's other rows
+        for (int r = warp; r < n; r += NW) {
+            if (r == i) continue;
+            uint32_t* row = T + (size_t)r * tld;
+            const uint32_t mr = row[c];
+            if (mr == 0u) continue;  // uniform over the warp
+            const uint32_t mp = f.prep(mr);
+            const bool track = pcol[r] < 0;  // its lead was c: find the next one
+            int nl = INT_MAX;
+            for (int j0 = c + 1; j0 < m; j0 += 32) {
+                const int j = j0 + lane;
+                uint32_t y = 0u;
+                if (j < m) {
+                    const uint32_t v = pr[j];
+                    y = row[j];
+                    if (v) {
+                        y = f.mulsub(y, mp, v);
+                        row[j] = y;
+                    }
+                }
+                if (track && nl == INT_MAX) {
+                    const unsigned bal = __ballot_sync(0xffffffffu, y != 0u);
+                    if (bal) nl = j0 + __ffs(bal) - 1;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                row[c] = 0u;
+                if (track) lead[r] = nl;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+    // ---- compaction: pivot rows in descending pivot-column order ----
+    for (int r = warp; r < n; r += NW) {
+        const int c0 = pcol[r];
+        if (c0 < 0) continue;
+        const uint32_t* row = T + (size_t)r * tld;
+        int cnt = 0;
+        for (int j0 = c0; j0 < m; j0 += 32) {
+            const int j = j0 + lane;
+            cnt += __popc(__ballot_sync(0xffffffffu, j < m && row[j] != 0u));
+        }
+        if (lane == 0) rcnt[r] = cnt;
+    }
+    // rank of a pivot column = pivot columns to its right
+    for (int c = tid; c < m; c += blockDim.x) rank[c] = prow[m - 1 - c] >= 0 ? 1 : 0;
+    __syncthreads();
+    const int np = tiny_exscan(rank, m, tmp);  // rank[m-1-c] = pivots right of c
+    // entries per output row (rank order) -> offsets
+    for (int c = tid; c < m; c += blockDim.x) {
+        const int r = prow[c];
+        if (r >= 0) tmp[rank[m - 1 - c]] = rcnt[r];
+    }
+    __syncthreads();
+    for (int k = tid; k < np; k += blockDim.x) rcnt[k] = tmp[k];  // rcnt reused: [np]
+    __syncthreads();
+    const int nnz = tiny_exscan(rcnt, np, tmp);
+    for (int k = tid; k < np; k += blockDim.x) out.offs[k] = rcnt[k];
+    for (int c = tid; c < m; c += blockDim.x) out.piv_of_col[c] = prow[c];
+    if (tid == 0) {
+        out.offs[np] = nnz;
+        out.counts[0] = np;
+        out.counts[1] = nnz;
+    }
+    for (int r = warp; r < n; r += NW) {
+        const int c0 = pcol[r];
+        if (c0 < 0) continue;
+        const uint32_t* row = T + (size_t)r * tld;
+        int64_t pos = rcnt[rank[m - 1 - c0]];
+        for (int j0 = c0; j0 < m; j0 += 32) {
+            const int j = j0 + lane;
+            const uint32_t v = j < m ? row[j] : 0u;
+            const unsigned bal = __ballot_sync(0xffffffffu, v != 0u);
+            if (v) {
+                const int64_t q = pos + __popc(bal & ((1u << lane) - 1u));
+                out.cols[q] = j + out.col_shift;
+                out.vals[q] = (int32_t)v;
+            }
+            pos += __popc(bal);
+        }
+    }
+}
+
+// shared memory of k_tiny_rref for an n x m block (0: too large)
+int tiny_rref_bytes(int32_t n, int32_t m, int smem_optin) {
+    const int64_t mx = std::max(n, m);
+    const int64_t bytes = (int64_t)n * (m + 1) * 4 + (int64_t)n * 12 + (int64_t)m * 4 + mx * 8 + 64;
+    return bytes <= smem_optin - 4096 ? (int)bytes : 0;
+}
+
+template <class F>
+cudaError_t launch_tiny_rref(int32_t n, int32_t m, const uint32_t* D, int64_t ld,
+                             const int32_t* lead, const uint32_t* err, int32_t col_shift,
+                             int64_t* offs, int32_t* cols, int32_t* vals, int32_t* piv_of_col,
+                             int64_t* counts, int bytes, cudaStream_t s, const F& f) {
+    cudaError_t e = ensure_smem_limit((const void*)k_tiny_rref<F>, bytes);
+    if (e != cudaSuccess) return e;
+    const TinyOut o{col_shift, offs, cols, vals, piv_of_col, counts};
+    k_tiny_rref<F><<<1, kTinyThreads, bytes, s>>>(n, m, D, ld, lead, err, o, f);
+    return cudaGetLastError();
+}
+
 #define GBGPU_INSTANTIATE(F)                                                                   \
     template cudaError_t launch_reduce_sparse<F>(const SparseReduceArgs&, const F&, int, bool, \
                                                  int, cudaStream_t);                            \
@@ -420,7 +633,11 @@ cudaError_t launch_promote(int grid, int threads, cudaStream_t s, const int32_t*
     template cudaError_t launch_promote<F>(int, int, cudaStream_t, const int32_t*,             \
                                            const int32_t*, const int32_t*, int32_t*, int32_t*, \
                                            uint32_t*, int64_t, int32_t, int32_t*, int32_t*,    \
-                                           const F&);
+                                           const F&);                                          \
+    template cudaError_t launch_tiny_rref<F>(int32_t, int32_t, const uint32_t*, int64_t,       \
+                                             const int32_t*, const uint32_t*, int32_t,         \
+                                             int64_t*, int32_t*, int32_t*, int32_t*, int64_t*, \
+                                             int, cudaStream_t, const F&);
 GBGPU_INSTANTIATE(FieldSmall)
 GBGPU_INSTANTIATE(FieldMont)
 #undef GBGPU_INSTANTIATE
