@@ -466,7 +466,8 @@ k_tiny_rref(int32_t n, int32_t m, const uint32_t* __restrict__ D, int64_t ld,
     int32_t* prow = rcnt + n;                                // [m] pivot row of a column, -1
     int32_t* rank = prow + m;                                // [max(n, m)] scan space
     int32_t* tmp = rank + max(n, m);                         // [max(n, m)]
-    __shared__ int s_min[kTinyThreads / 32];
+    uint32_t* rinv = (uint32_t*)(tmp + max(n, m));           // [n] inverse of a row's lead entry
+    __shared__ int s_min[2][kTinyThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = kTinyThreads / 32;
     if (*err) {  // invalid input: nothing is read, the answer is empty (uniform)
@@ -484,50 +485,51 @@ k_tiny_rref(int32_t n, int32_t m, const uint32_t* __restrict__ D, int64_t ld,
         T[(size_t)r * tld + c] = D[(size_t)r * ld + c];
     }
     for (int r = tid; r < n; r += blockDim.x) {
-        lead[r] = lead_in[r] < 0 ? INT_MAX : lead_in[r];
+        const int l = lead_in[r] < 0 ? INT_MAX : lead_in[r];
+        lead[r] = l;
         pcol[r] = -1;
+        // inverse of the row's lead entry, ready for the step that picks it
+        rinv[r] = l == INT_MAX ? 0u : f.inv(T[(size_t)r * tld + l]);
     }
     __syncthreads();
-    for (int step = 0; step < n; ++step) {
-        // smallest (lead, row) over the non-pivot rows of this warp
+    // Pivot rows are normalised at the end (the entry at a pivot column never
+    // changes afterwards, pivot columns only grow); a step clears the pivot
+    // column with row_r -= (row_r[c] / a_i) row_i, the inverse of a_i being
+    // ready since row i's lead was last set.  Every warp publishes the key of
+    // its rows right after its own updates: one barrier per pivot.
+    auto warp_key = [&]() {
         int key = INT_MAX;
         for (int r = warp + NW * lane; r < n; r += NW * 32)
             if (pcol[r] < 0 && lead[r] != INT_MAX) key = min(key, lead[r] * n + r);
         for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
-        if (lane == 0) s_min[warp] = key;
-        __syncthreads();
-        int best = s_min[0];
+        return key;
+    };
+    {
+        const int key = warp_key();
+        if (lane == 0) s_min[0][warp] = key;
+    }
+    __syncthreads();
+    for (int step = 0; step < n; ++step) {
+        const int* sm = s_min[step & 1];
+        int best = sm[0];
 #pragma unroll 8
-        for (int w = 1; w < NW; ++w) best = min(best, s_min[w]);
-        __syncthreads();  // everyone read s_min before the next step writes it
+        for (int w = 1; w < NW; ++w) best = min(best, sm[w]);
         if (best == INT_MAX) break;  // uniform: rank reached
         const int c = best / n, i = best % n;
-        uint32_t* pr = T + (size_t)i * tld;
-        if (warp == (i % NW)) {
-            // normalise the pivot row (its owner warp)
-            uint32_t inv = 0;
-            if (lane == 0) inv = f.inv(pr[c]);
-            inv = __shfl_sync(0xffffffffu, inv, 0);
-            const uint32_t ip = f.prep(inv);
-            for (int j = c + 1 + lane; j < m; j += 32) {
-                const uint32_t v = pr[j];
-                if (v) pr[j] = f.mulp(v, ip);
-            }
-            __syncwarp();
-            if (lane == 0) {
-                pr[c] = 1u;
-                pcol[i] = c;
-                prow[c] = i;
-            }
+        const uint32_t* pr = T + (size_t)i * tld;
+        const uint32_t ainv = rinv[i];
+        if (warp == (i % NW) && lane == 0) {
+            pcol[i] = c;
+            prow[c] = i;
         }
-        __syncthreads();
-        // clear column c from this warp's other rows
+        __syncwarp();  // the owner warp's lanes see pcol[i]
+        // clear column c from this warp's other rows, pivots included
         for (int r = warp; r < n; r += NW) {
             if (r == i) continue;
             uint32_t* row = T + (size_t)r * tld;
             const uint32_t mr = row[c];
             if (mr == 0u) continue;  // uniform over the warp
-            const uint32_t mp = f.prep(mr);
+            const uint32_t mp = f.prep(f.mulmod(mr, ainv));
             const bool track = pcol[r] < 0;  // its lead was c: find the next one
             int nl = INT_MAX;
             for (int j0 = c + 1; j0 < m; j0 += 32) {
@@ -549,12 +551,31 @@ k_tiny_rref(int32_t n, int32_t m, const uint32_t* __restrict__ D, int64_t ld,
             __syncwarp();
             if (lane == 0) {
                 row[c] = 0u;
-                if (track) lead[r] = nl;
+                if (track) {
+                    lead[r] = nl;
+                    rinv[r] = nl == INT_MAX ? 0u : f.inv(row[nl]);
+                }
             }
             __syncwarp();
         }
+        const int key = warp_key();
+        if (lane == 0) s_min[(step + 1) & 1][warp] = key;
         __syncthreads();
     }
+    // normalise the pivot rows
+    for (int r = warp; r < n; r += NW) {
+        const int c0 = pcol[r];
+        if (c0 < 0) continue;
+        uint32_t* row = T + (size_t)r * tld;
+        const uint32_t ip = f.prep(rinv[r]);
+        for (int j = c0 + 1 + lane; j < m; j += 32) {
+            const uint32_t v = row[j];
+            if (v) row[j] = f.mulp(v, ip);
+        }
+        __syncwarp();
+        if (lane == 0) row[c0] = 1u;
+    }
+    __syncthreads();
     // ---- compaction: pivot rows in descending pivot-column order ----
     for (int r = warp; r < n; r += NW) {
         const int c0 = pcol[r];
@@ -609,7 +630,7 @@ k_tiny_rref(int32_t n, int32_t m, const uint32_t* __restrict__ D, int64_t ld,
 // shared memory of k_tiny_rref for an n x m block (0: too large)
 int tiny_rref_bytes(int32_t n, int32_t m, int smem_optin) {
     const int64_t mx = std::max(n, m);
-    const int64_t bytes = (int64_t)n * (m + 1) * 4 + (int64_t)n * 12 + (int64_t)m * 4 + mx * 8 + 64;
+    const int64_t bytes = (int64_t)n * (m + 1) * 4 + (int64_t)n * 16 + (int64_t)m * 4 + mx * 8 + 64;
     return bytes <= smem_optin - 4096 ? (int)bytes : 0;
 }
 
