@@ -130,22 +130,35 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
 }
 
 // ---------------------------------------------------------------------------
-// Two tile shapes per limb count.  The large one (one CTA per SM) serves long
-// K; the small one (K <= 256, two CTAs per SM, TMEM <= 256 columns each) lets
-// one CTA's loads and MMAs overlap the other's D read-modify-write when the
-// epilogue dominates.
-template <int L, bool SMALL = false>
+// Tile shapes (SHAPE):
+//   TC_BIG   long K: 128 x BN tiles, one CTA per SM; one- and two-limb shapes
+//            keep their accumulators twice (the next tile's MMAs run while the
+//            epilogue drains the last) when 2 x NW x BN fits the 512 TMEM
+//            columns: 128 x 256 for L = 1; L = 2 keeps 128 x 128 once (more
+//            reuse per operand byte), L = 3, 4 keep 128 x 64 once;
+//   TC_MID   two limbs, K up to 1536: 128 x 64 tiles, accumulators twice;
+//   TC_SMALL K <= 256, one or two limbs: 128 x 128/64 tiles, two CTAs per SM
+//            (TMEM <= 256 columns each), so one CTA's loads and MMAs overlap
+//            the other's epilogue.
+constexpr int TC_BIG = 0, TC_SMALL = 1, TC_MID = 2;
+
+template <int L, int SHAPE = TC_BIG>
 struct TcCfg {
+    static constexpr bool SMALL = SHAPE == TC_SMALL;
     static constexpr int BM = 128;
     static constexpr int BK = 128;  // bytes of K per stage (one swizzle row)
-    static constexpr int BN = SMALL ? (L == 1 ? 128 : 64) : (L == 1 ? 256 : (L == 2 ? 128 : 64));
+    static constexpr int BN =
+        SMALL ? (L == 1 ? 128 : 64) : (L == 1 ? 256 : (L == 2 && SHAPE == TC_BIG ? 128 : 64));
     static constexpr int NW = 2 * L - 1;
+    // accumulator sets in TMEM (see the shapes above)
+    static constexpr int ACC_BUFS = (!SMALL && 2 * (2 * L - 1) * BN <= 512) ? 2 : 1;
     static constexpr int A_BYTES = BM * BK;
     static constexpr int B_BYTES = BN * BK;
     static constexpr int STAGE_BYTES = L * (A_BYTES + B_BYTES);
-    static constexpr int STAGES = SMALL ? 1 : (L == 1 ? 4 : (L == 2 ? 3 : 2));
+    static constexpr int STAGES = SMALL ? 1 : (L == 1 ? 4 : (L == 2 ? (BN == 128 ? 3 : 4) : 2));
+    static constexpr int ACC_COLS = ACC_BUFS * NW * BN;
     static constexpr int TMEM_COLS =
-        NW * BN <= 64 ? 64 : (NW * BN <= 128 ? 128 : (NW * BN <= 256 ? 256 : 512));
+        ACC_COLS <= 64 ? 64 : (ACC_COLS <= 128 ? 128 : (ACC_COLS <= 256 ? 256 : 512));
     // epilogue warps: two per TMEM lane quarter (each half of the columns) for
     // the one-CTA-per-SM shapes with one or two limbs, one otherwise
     static constexpr int EPI_WARPS = (!SMALL && L <= 2) ? 8 : 4;
@@ -173,6 +186,7 @@ struct TcCfg {
     static_assert(!SMALL || L <= 2, "small tiles for one or two limbs only");
     static_assert(!SMALL || 2 * TMEM_COLS <= 512, "two small CTAs share the TMEM");
     static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
+    static_assert(ACC_COLS <= 512, "TMEM columns");
 };
 
 // tiles of one batch item are visited in groups of TC_GROUP_M row tiles, all
@@ -199,24 +213,25 @@ struct TcParams {
     long long budget;
 };
 
-template <int L, bool SMALL>
-__global__ void __launch_bounds__(TcCfg<L, SMALL>::THREADS, TcCfg<L, SMALL>::MIN_CTAS)
+template <int L, int SHAPE>
+__global__ void __launch_bounds__(TcCfg<L, SHAPE>::THREADS, TcCfg<L, SHAPE>::MIN_CTAS)
 k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const TcParams prm) {
-    using C = TcCfg<L, SMALL>;
+    using C = TcCfg<L, SHAPE>;
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte aligned tile region (shared-window address)
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* gbase = smem_raw + (base - raw);
     uint64_t* bars = (uint64_t*)(gbase + C::BAR_OFF);
-    // bars: full[STAGES], empty[STAGES], tmem_full, tmem_empty; then tmem slot, abort flag
+    // bars: full[STAGES], empty[STAGES], tmem_full[ACC_BUFS], tmem_empty[ACC_BUFS];
+    // then tmem slot, abort flag
     const uint32_t bar0 = smem_u32(bars);
     auto full_bar = [&](int s) { return bar0 + 8u * s; };
     auto empty_bar = [&](int s) { return bar0 + 8u * (C::STAGES + s); };
-    const uint32_t tfull_bar = bar0 + 8u * (2 * C::STAGES);
-    const uint32_t tempty_bar = bar0 + 8u * (2 * C::STAGES + 1);
-    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 2 * C::STAGES + 2);
+    auto tfull_bar = [&](int b) { return bar0 + 8u * (2 * C::STAGES + b); };
+    auto tempty_bar = [&](int b) { return bar0 + 8u * (2 * C::STAGES + C::ACC_BUFS + b); };
+    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 2 * C::STAGES + 2 * C::ACC_BUFS);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -283,8 +298,10 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             mbar_init(full_bar(s), 1);
             mbar_init(empty_bar(s), 1);
         }
-        mbar_init(tfull_bar, 1);
-        mbar_init(tempty_bar, C::EPI_WARPS);
+        for (int b = 0; b < C::ACC_BUFS; ++b) {
+            mbar_init(tfull_bar(b), 1);
+            mbar_init(tempty_bar(b), C::EPI_WARPS);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -365,9 +382,10 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     const int s = it % C::STAGES;
                     const uint32_t ph = (it / C::STAGES) & 1;
                     const int pk = j % C::PANEL_KB;
-                    if (pk == 0 && pc > 0) {
-                        // accumulators are free once the epilogue read the last panel
-                        if (*abort_flag || !mbar_wait(tempty_bar, (pc - 1) & 1, prm.budget)) {
+                    const int ab = pc % C::ACC_BUFS, au = pc / C::ACC_BUFS;
+                    if (pk == 0 && au > 0) {
+                        // this accumulator set is free once the epilogue read its last panel
+                        if (*abort_flag || !mbar_wait(tempty_bar(ab), (au - 1) & 1, prm.budget)) {
                             *abort_flag = 1;
                             stop = true;
                             break;
@@ -392,13 +410,14 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                                 const uint64_t bd = umma_desc_sw128(
                                     st + L * C::A_BYTES + jj * C::B_BYTES + kk * 32);
                                 const uint32_t acc = (pk == 0 && kk == 0 && first_pair) ? 0u : 1u;
-                                tc_mma_i8(tmem + (uint32_t)(w * C::BN), ad, bd, C::IDESC, acc);
+                                tc_mma_i8(tmem + (uint32_t)(ab * C::NW * C::BN + w * C::BN), ad, bd,
+                                          C::IDESC, acc);
                             }
                         }
                     }
                     tc_commit(empty_bar(s));
                     if (pk == C::PANEL_KB - 1 || j == n_it - 1) {
-                        tc_commit(tfull_bar);
+                        tc_commit(tfull_bar(ab));
                         ++pc;
                     }
                     ++it;
@@ -456,8 +475,10 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 }
             };
             for (int panel = 0; panel < npanels; ++panel, ++pc) {
+                const int ab = pc % C::ACC_BUFS, au = pc / C::ACC_BUFS;
+                const uint32_t acc_base = (uint32_t)(ab * C::NW * C::BN);
                 bool ok = true;
-                if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar, pc & 1, prm.budget);
+                if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar(ab), au & 1, prm.budget);
                 ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
                 if (!ok) {
                     if (lane == 0) *abort_flag = 1;
@@ -481,7 +502,8 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 #pragma unroll
                     for (int w = 0; w < C::NW; ++w) {
                         uint32_t a[32];
-                        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(w * C::BN + c0), a);
+                        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + acc_base + (uint32_t)(w * C::BN + c0),
+                                  a);
                         const uint32_t cw = prm.cw[w];
 #pragma unroll
                         for (int j = 0; j < 32; ++j) {
@@ -510,7 +532,7 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(tempty_bar);
+                if (lane == 0) mbar_arrive(tempty_bar(ab));
             }
         }
     }
@@ -784,10 +806,10 @@ static int num_sms() {
     return n;
 }
 
-template <int L, bool SMALL>
+template <int L, int SHAPE>
 static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t* err,
                   long long* launches) {
-    using Cfg = TcCfg<L, SMALL>;
+    using Cfg = TcCfg<L, SHAPE>;
     const int32_t Mp = (g.M + Cfg::BM - 1) / Cfg::BM * Cfg::BM;
     const int32_t Np = (g.N + Cfg::BN - 1) / Cfg::BN * Cfg::BN;
     const int32_t Kp = (g.K + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
@@ -844,7 +866,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     }
     prm.err = err;
     prm.budget = 4000000000LL;  // about 2 s at 2 GHz per wait
-    cudaError_t e = ensure_smem_limit((const void*)k_tc_submul<L, SMALL>, Cfg::SMEM_BYTES);
+    cudaError_t e = ensure_smem_limit((const void*)k_tc_submul<L, SHAPE>, Cfg::SMEM_BYTES);
     if (e != cudaSuccess) {
         set_error(std::string("tc smem attribute: ") + cudaGetErrorString(e));
         return GBGPU_ECUDA;
@@ -863,7 +885,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
     }
-    k_tc_submul<L, SMALL><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
+    k_tc_submul<L, SHAPE><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, s>>>(ma, mb, prm);
     ++*launches;
     if (prof) {
         cudaEventRecord(e1, s);
@@ -907,13 +929,14 @@ int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err
     const bool small = g.K <= 256;  // at most two K steps: the small tile shape
     switch (limbs_for(g.p)) {
         case 1:
-            return small ? tc_run<1, true>(g, planes, s, err, launches)
-                         : tc_run<1, false>(g, planes, s, err, launches);
+            return small ? tc_run<1, TC_SMALL>(g, planes, s, err, launches)
+                         : tc_run<1, TC_BIG>(g, planes, s, err, launches);
         case 2:
-            return small ? tc_run<2, true>(g, planes, s, err, launches)
-                         : tc_run<2, false>(g, planes, s, err, launches);
-        case 3: return tc_run<3, false>(g, planes, s, err, launches);
-        default: return tc_run<4, false>(g, planes, s, err, launches);
+            return small            ? tc_run<2, TC_SMALL>(g, planes, s, err, launches)
+                   : g.K <= 1536    ? tc_run<2, TC_MID>(g, planes, s, err, launches)
+                                    : tc_run<2, TC_BIG>(g, planes, s, err, launches);
+        case 3: return tc_run<3, TC_BIG>(g, planes, s, err, launches);
+        default: return tc_run<4, TC_BIG>(g, planes, s, err, launches);
     }
 }
 
