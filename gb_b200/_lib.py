@@ -69,7 +69,7 @@ EXPORTS = [
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
     "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into", "gbgpu_dense_rref",
-    "gbgpu_plan_result_into_v",
+    "gbgpu_plan_result_into_v", "gbgpu_plan_run_into_v",
 ]
 
 _lib = None
@@ -97,6 +97,8 @@ def load(path: str = LIB_PATH):
                                            C.c_int64, C.c_int64, _PI32, _PI64]
     lib.gbgpu_plan_result_into_v.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_int32, C.c_int64, C.c_int64, _PI32, _PI64]
+    lib.gbgpu_plan_run_into_v.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int32, C.c_int64, C.c_int64, _PI32, _PI64]
     lib.gbgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.gbgpu_plan_destroy.restype = None
     lib.gbgpu_reduce_batch.argtypes = [C.c_int32, C.POINTER(Csr), C.POINTER(Options),

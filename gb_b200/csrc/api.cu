@@ -204,6 +204,10 @@ struct Plan {
     int tiny_bytes = 0;
     int64_t* tiny_counts = nullptr;  // [2]: rows, entries of the answer
     bool pending = false;            // a tiny run whose results are not read yet
+    // answer streamed to host arrays during the run (gbgpu_plan_run_into_v)
+    StreamOut* stream_req = nullptr;
+    bool streamed = false;
+    cudaStream_t s_out = nullptr;
     gbgpu_stats stats{};
     cudaEvent_t ev[8] = {};
     long long launches = 0;
@@ -222,6 +226,10 @@ struct Plan {
         return GBGPU_OK;
     }
     ~Plan() {
+        if (s_out) {
+            cudaStreamSynchronize(s_out);
+            cudaStreamDestroy(s_out);
+        }
         for (void* q : bufs) cudaFreeAsync(q, stream);
         if (stream) cudaStreamSynchronize(stream);
         for (auto& e : ev)
@@ -429,6 +437,7 @@ static int run_form(Plan* P, const F& f) {
         bo.piv_of_col = P->piv_of_col;
         bo.ms_event_schur = P->ev[2];
         bo.ms_event_echelon = P->ev[3];
+        bo.stream_out = P->stream_req;
         const int rc = blocked_reduce(bi, &bo, &launches);
         if (rc) {
             blocked_release(&bo, s);
@@ -440,7 +449,11 @@ static int run_form(Plan* P, const F& f) {
         P->stats.dense_rows = bo.dense_rows;
         P->stats.echelon_rounds = bo.echelon_rounds;
         GB_CUDA(cudaEventRecord(P->ev[4], s));
-        if (P->np > 0) {
+        P->streamed = bo.stream_out != nullptr;
+        if (P->streamed) {
+            // the answer went to host memory block by block
+            P->onnz = bo.stream_out->nnz;
+        } else if (P->np > 0) {
             GB_LAUNCH(k_pivot_flags<<<grid_for(P->ncr, T), T, 0, s>>>(P->ncr, P->piv_of_col, 1,
                                                                        P->pflag));
             size_t bytes = P->cub_bytes;
@@ -591,8 +604,8 @@ static int run_form(Plan* P, const F& f) {
 
     // ---- compaction -----------------------------------------------------------
     const int32_t shift = P->mode == 0 ? P->ncl : 0;
-    P->onnz = 0;
-    if (P->np > 0) {
+    if (!P->streamed) P->onnz = 0;
+    if (P->np > 0 && !P->streamed) {
         GB_LAUNCH(k_row_nnz<<<grid_for((int64_t)P->np * 32, T), T, 0, s>>>(
             P->np, P->pivcol, P->piv_of_col, final_rows, rows_ld, width, P->counts));
         GB_CUDA(cudaMemsetAsync(P->counts + P->np, 0, sizeof(int64_t), s));
@@ -653,6 +666,7 @@ int settle(Plan* P) {
 
 int plan_run(Plan* P) {
     P->launches = 0;
+    P->streamed = false;
     int rc;
     GemmProfile prof;
     if (P->profile) {
@@ -821,6 +835,10 @@ int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** o
 int plan_result(Plan* P, gbgpu_rows* out) {
     memset(out, 0, sizeof(*out));
     if (int rc = settle(P)) return rc;
+    if (P->streamed) {
+        set_error("the last run delivered its answer through gbgpu_plan_run_into_v");
+        return GBGPU_EINVAL;
+    }
     GB_CUDA(cudaStreamSynchronize(P->stream));
     out->np = P->np;
     out->nnz = P->onnz;
@@ -850,6 +868,10 @@ int plan_result(Plan* P, gbgpu_rows* out) {
 int plan_result_into(Plan* P, int64_t* row_ptr, int32_t* cols, int32_t* vals, int64_t cap_rows,
                      int64_t cap_nnz, int32_t* np, int64_t* nnz) {
     if (int rc = settle(P)) return rc;
+    if (P->streamed) {
+        set_error("the last run delivered its answer through gbgpu_plan_run_into_v");
+        return GBGPU_EINVAL;
+    }
     GB_CUDA(cudaStreamSynchronize(P->stream));
     *np = P->np;
     *nnz = P->onnz;
@@ -882,6 +904,10 @@ int plan_result_into_v(Plan* P, int64_t* row_ptr, int32_t* cols, void* vals, int
         return GBGPU_EINVAL;
     }
     if (int rc = settle(P)) return rc;
+    if (P->streamed) {
+        set_error("the last run delivered its answer through gbgpu_plan_run_into_v");
+        return GBGPU_EINVAL;
+    }
     GB_CUDA(cudaStreamSynchronize(P->stream));
     *np = P->np;
     *nnz = P->onnz;
@@ -910,6 +936,49 @@ int plan_result_into_v(Plan* P, int64_t* row_ptr, int32_t* cols, void* vals, int
         }
         GB_CUDA(cudaStreamSynchronize(P->stream));
     }
+    return GBGPU_OK;
+}
+
+// run and deliver the answer into host arrays; on the blocked form the
+// back substitution's finished blocks are copied while the rest is computed
+int plan_run_into_v(Plan* P, int64_t* row_ptr, int32_t* cols, void* vals, int32_t vb,
+                    int64_t cap_rows, int64_t cap_nnz, int32_t* np, int64_t* nnz) {
+    if (!(vb == 1 || vb == 2 || vb == 4) || (vb < 4 && (int64_t)P->p >= ((int64_t)1 << (8 * vb)))) {
+        set_error("val_bytes must be 4, 2 (p < 2^16) or 1 (p < 2^8)");
+        return GBGPU_EINVAL;
+    }
+    if (!P->blocked || P->mode != 0 || !row_ptr || !cols || !vals) {
+        int rc = plan_run(P);
+        if (rc) return rc;
+        return plan_result_into_v(P, row_ptr, cols, vals, vb, cap_rows, cap_nnz, np, nnz);
+    }
+    if (!P->s_out) GB_CUDA(cudaStreamCreateWithFlags(&P->s_out, cudaStreamNonBlocking));
+    StreamOut so;
+    so.col_shift = P->ncl;
+    so.offs = P->offs;
+    so.h_cols = cols;
+    so.h_vals = vals;
+    so.val_bytes = vb;
+    so.cap_nnz = cap_nnz;
+    so.s_out = P->s_out;
+    P->stream_req = &so;
+    int rc = plan_run(P);
+    P->stream_req = nullptr;
+    cudaError_t e = cudaStreamSynchronize(P->s_out);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+        set_error(std::string("answer copy: ") + cudaGetErrorString(e));
+        return GBGPU_ECUDA;
+    }
+    *np = P->np;
+    *nnz = P->onnz;
+    if ((int64_t)P->np + 1 > cap_rows || so.overflow) {
+        set_error("result buffers too small");
+        return GBGPU_ERANGE;
+    }
+    GB_CUDA(cudaMemcpyAsync(row_ptr, P->offs, sizeof(int64_t) * (P->np + 1),
+                            cudaMemcpyDeviceToHost, P->stream));
+    GB_CUDA(cudaStreamSynchronize(P->stream));
     return GBGPU_OK;
 }
 
@@ -962,6 +1031,15 @@ int gbgpu_plan_result_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, 
     if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
     return plan_result_into_v(plan->impl, row_ptr, cols, vals, val_bytes, cap_rows, cap_nnz, np,
                               nnz);
+}
+
+int gbgpu_plan_run_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, void* vals,
+                          int32_t val_bytes, int64_t cap_rows, int64_t cap_nnz, int32_t* np,
+                          int64_t* nnz) {
+    if (!plan || !np || !nnz) return GBGPU_EINVAL;
+    if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
+    return plan_run_into_v(plan->impl, row_ptr, cols, vals, val_bytes, cap_rows, cap_nnz, np,
+                           nnz);
 }
 
 int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {

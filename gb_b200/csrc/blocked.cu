@@ -814,6 +814,28 @@ static int neg_inverse_big(Ctx& c, const F& f, const uint32_t* src, int64_t lds,
     return GBGPU_OK;
 }
 
+// out[k] = in[n - 1 - k]
+__global__ void k_reverse_i32(int32_t n, const int32_t* __restrict__ in, int32_t* out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        out[k] = in[n - 1 - k];
+}
+
+// offs[k] = base + loc[k]
+__global__ void k_offs_write(int32_t n, const int64_t* __restrict__ loc, int64_t base,
+                             int64_t* offs) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        offs[k] = base + loc[k];
+}
+
+// values narrowed to vb (1 or 2) bytes
+__global__ void k_narrow_vals(int64_t n, const int32_t* __restrict__ in, int32_t vb, uint8_t* out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (vb == 1) out[i] = (uint8_t)in[i];
+        else ((uint16_t*)out)[i] = (uint16_t)in[i];
+    }
+}
+
 // Rows t_rows[0 .. rows) of M (leading dimension ld, ncols columns) are
 // reduced by the pivot rows u_rows[0 .. n_p) of M (sorted by lead, monic,
 // zero left of their leads, pivot columns pc ascending):
@@ -1168,6 +1190,73 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         BL_CUDA(cudaStreamSynchronize(s));
         BL_LAUNCH(k_gather_rows<<<grid_of(r), 256, 0, s>>>(r, pc, piv_of_col, prow, counters + 2));
         // echelon rows prow[0 .. r), ascending lead, reduced in place
+        StreamOut* so = out->stream_out;
+        int32_t* pcd = nullptr;          // pivot columns, descending (the answer's order)
+        int64_t* cnt = nullptr;          // [NB + 1] entries per row of a block
+        int64_t* loc = nullptr;          // [NB + 1] their exclusive scan
+        void* cscan = nullptr;
+        size_t cscan_bytes = 0;
+        cudaEvent_t blk_ev = nullptr;
+        if (so) {
+            pcd = c.alloc<int32_t>(r);
+            cnt = c.alloc<int64_t>(nb_for(r) + 1);
+            loc = c.alloc<int64_t>(nb_for(r) + 1);
+            cub::DeviceScan::ExclusiveSum(nullptr, cscan_bytes, cnt, loc, nb_for(r) + 1, s);
+            cscan = c.alloc<uint8_t>(cscan_bytes);
+            if (!pcd || !cnt || !loc || !cscan) return GBGPU_ENOMEM;
+            BL_LAUNCH(k_reverse_i32<<<grid_of(r), 256, 0, s>>>(r, pc, pcd));
+            BL_CUDA(cudaEventCreateWithFlags(&blk_ev, cudaEventDisableTiming));
+            so->nnz = 0;
+            so->overflow = false;
+        }
+        // block b's answer rows [r - b NB - kb, r - b NB): compacted and sent
+        auto send_block = [&](int b, int kb) -> int {
+            const int64_t out0 = (int64_t)r - ((int64_t)b * nb_for(r) + kb);
+            BL_LAUNCH(k_row_nnz<<<grid_of((int64_t)kb * 32), 256, 0, s>>>(
+                kb, pcd + out0, piv_of_col, Dp, ld, ncr, cnt));
+            BL_CUDA(cudaMemsetAsync(cnt + kb, 0, sizeof(int64_t), s));
+            size_t bytes = cscan_bytes;
+            BL_CUDA(cub::DeviceScan::ExclusiveSum(cscan, bytes, cnt, loc, kb + 1, s));
+            ++c.launches;
+            int64_t blk = 0;
+            BL_CUDA(cudaMemcpyAsync(&blk, loc + kb, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            BL_CUDA(cudaStreamSynchronize(s));
+            BL_LAUNCH(k_offs_write<<<grid_of(kb + 1), 256, 0, s>>>(kb + 1, loc, so->nnz,
+                                                                   so->offs + out0));
+            if (blk > 0) {
+                int32_t *bc = nullptr, *bv = nullptr;
+                uint8_t* bw = nullptr;
+                const int vb = so->val_bytes;
+                if (cudaMallocAsync((void**)&bc, sizeof(int32_t) * blk, s) != cudaSuccess ||
+                    cudaMallocAsync((void**)&bv, sizeof(int32_t) * blk, s) != cudaSuccess ||
+                    (vb < 4 && cudaMallocAsync((void**)&bw, (size_t)vb * blk, s) != cudaSuccess)) {
+                    set_error("answer block allocation failed");
+                    return GBGPU_ENOMEM;
+                }
+                BL_LAUNCH(k_row_write<<<grid_of((int64_t)kb * 32), 256, 0, s>>>(
+                    kb, pcd + out0, piv_of_col, Dp, ld, ncr, loc, so->col_shift, bc, bv));
+                if (vb < 4)
+                    BL_LAUNCH(k_narrow_vals<<<grid_of(blk), 256, 0, s>>>(blk, bv, vb, bw));
+                cudaStream_t fs = s;
+                if (!so->overflow && so->nnz + blk <= so->cap_nnz) {
+                    BL_CUDA(cudaEventRecord(blk_ev, s));
+                    BL_CUDA(cudaStreamWaitEvent(so->s_out, blk_ev, 0));
+                    BL_CUDA(cudaMemcpyAsync(so->h_cols + so->nnz, bc, sizeof(int32_t) * blk,
+                                            cudaMemcpyDeviceToHost, so->s_out));
+                    BL_CUDA(cudaMemcpyAsync((uint8_t*)so->h_vals + (size_t)so->nnz * vb,
+                                            vb < 4 ? (void*)bw : (void*)bv, (size_t)vb * blk,
+                                            cudaMemcpyDeviceToHost, so->s_out));
+                    fs = so->s_out;  // freed once copied
+                } else {
+                    so->overflow = true;
+                }
+                cudaFreeAsync(bc, fs);
+                cudaFreeAsync(bv, fs);
+                if (bw) cudaFreeAsync(bw, fs);
+            }
+            so->nnz += blk;
+            return GBGPU_OK;
+        };
         const int32_t NB = nb_for(r);
         const int64_t bstride = (int64_t)NB * (NB + 1);
         const int32_t nb = (r + NB - 1) / NB;
@@ -1206,7 +1295,12 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             BL_CHECK(gemm_args(c, g));
             BL_LAUNCH(k_scatter_rows_dense<<<grid_of((int64_t)kb * (ncr - c0)), 256, 0, s>>>(
                 kb, rows_k, ncr - c0, Y + c0, ld, Dp + c0, ld));
+            if (so) BL_CHECK(send_block(b, kb));
         }
+        if (blk_ev) cudaEventDestroy(blk_ev);
+    } else if (out->stream_out) {
+        out->stream_out->nnz = 0;
+        BL_CUDA(cudaMemsetAsync(out->stream_out->offs, 0, sizeof(int64_t), s));
     }
     return GBGPU_OK;
 }

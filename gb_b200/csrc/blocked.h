@@ -21,7 +21,25 @@ struct BlockedInput {
     int32_t* err;             // device status word of the tensor-core kernels
 };
 
+// Streaming of the answer while the back substitution runs: each finished
+// block of pivot rows (the output is in descending pivot order, so the last
+// block comes first) is compacted into CSR and copied to host memory on a
+// second stream, overlapping the copies with the remaining blocks.
+struct StreamOut {
+    int32_t col_shift = 0;
+    int64_t* offs = nullptr;     // device [rank + 1]: row offsets of the answer (filled)
+    int32_t* h_cols = nullptr;   // host destinations (pinned for full speed)
+    void* h_vals = nullptr;
+    int32_t val_bytes = 4;       // 4, 2 or 1 bytes per host value
+    int64_t cap_nnz = 0;
+    cudaStream_t s_out = nullptr;
+    // results
+    int64_t nnz = 0;             // entries of the answer
+    bool overflow = false;       // host arrays too small: nothing was copied
+};
+
 struct BlockedOutput {
+    StreamOut* stream_out = nullptr;  // optional (see StreamOut)
     int32_t* piv_of_col = nullptr;  // [ncr], filled: reduced row of each pivot column or -1
     uint32_t* rows = nullptr;       // reduced rows (row piv_of_col[c] of `rows`), ld below
     int64_t ld = 0;

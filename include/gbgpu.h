@@ -211,6 +211,16 @@ int gbgpu_plan_result_into(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
 int gbgpu_plan_result_into_v(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
                              void *vals, int32_t val_bytes, int64_t cap_rows,
                              int64_t cap_nnz, int32_t *np, int64_t *nnz);
+/* Run and deliver the answer into caller host arrays (values of val_bytes
+ * bytes, as gbgpu_plan_result_into_v).  On the blocked forms the finished
+ * blocks of the back substitution are compacted and copied while the rest is
+ * still computed, so most of the device-to-host copy overlaps the reduction.
+ * Arrays too small: GBGPU_ERANGE with *np / *nnz set (run again with larger
+ * arrays).  After a streamed run the gbgpu_plan_result* calls return
+ * GBGPU_EINVAL until the next gbgpu_plan_run. */
+int gbgpu_plan_run_into_v(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
+                          void *vals, int32_t val_bytes, int64_t cap_rows,
+                          int64_t cap_nnz, int32_t *np, int64_t *nnz);
 int gbgpu_plan_stats(const gbgpu_plan *plan, gbgpu_stats *stats);
 void gbgpu_plan_destroy(gbgpu_plan *plan);
 

@@ -256,3 +256,35 @@ def test_narrow_values_in_and_out(form, p, vb):
     bad = _lib.Csr(m.p, m.laopt, m.nr, m.ncl, m.ncr, m.row_ptr.ctypes.data, m.cols.ctypes.data,
                    vals_in.ctypes.data, 3)
     assert lib.gbgpu_plan_create(C.byref(bad), C.byref(opt), C.byref(h)) == _lib.GBGPU_EINVAL
+
+
+@pytest.mark.parametrize("p,vb", [(65521, 2), (2147483647, 4)])
+def test_run_into_streams_the_answer(p, vb):
+    """gbgpu_plan_run_into_v: the answer copied block by block during the
+    back substitution equals the oracle's; too-small arrays give ERANGE with the
+    sizes; after a streamed run the result calls refuse until the next run."""
+    m = synth.staircase(1500, 700, 1400, p, seed=13)
+    want, _ = oracle.oracle_la(m)
+    lib = _lib.load()
+    vdt = np.uint16 if vb == 2 else np.int32
+    plan = la.Plan(m, form=_lib.FORM_TENSOR)
+    npv, nnz = C.c_int32(), C.c_int64()
+    rc = lib.gbgpu_plan_run_into_v(plan._h, None, None, None, vb, 0, 0, C.byref(npv), C.byref(nnz))
+    assert rc == _lib.GBGPU_ERANGE and npv.value == want.np and nnz.value == want.nnz
+    rp = np.zeros(npv.value + 1, dtype=np.int64)
+    cols = np.zeros(nnz.value, dtype=np.int32)
+    vals = np.zeros(nnz.value, dtype=vdt)
+    small = np.zeros(4, dtype=np.int32)
+    rc = lib.gbgpu_plan_run_into_v(plan._h, rp.ctypes.data, small.ctypes.data, small.ctypes.data,
+                                   vb, rp.shape[0], 1, C.byref(npv), C.byref(nnz))
+    assert rc == _lib.GBGPU_ERANGE and nnz.value == want.nnz
+    for _ in range(2):
+        _lib.check(lib.gbgpu_plan_run_into_v(plan._h, rp.ctypes.data, cols.ctypes.data,
+                                             vals.ctypes.data, vb, rp.shape[0], cols.shape[0],
+                                             C.byref(npv), C.byref(nnz)))
+        check_same(ReducedRows(rp, cols, vals.astype(np.int64).astype(np.int32)), want)
+    with pytest.raises(_lib.GbgpuError):
+        plan.result()
+    plan.run()
+    check_same(plan.result(), want)
+    plan.close()
