@@ -379,6 +379,18 @@ __global__ void k_collect_pending(int32_t t, const int32_t* __restrict__ lead,
         if (lead[r] >= 0 && !is_piv[r]) pend[atomicAdd(n_pend, 1)] = r;
 }
 
+// the round's new pivots: count = last exclusive-scan position + last flag,
+// and their rows in ascending pivot-column order
+__global__ void k_new_pivots(int32_t ncr, const int32_t* __restrict__ wflag,
+                             const int32_t* __restrict__ wpos, const int32_t* __restrict__ pc,
+                             const int32_t* __restrict__ piv_of_col, int32_t* n_new,
+                             int32_t* prow) {
+    const int32_t n = ncr > 0 ? wpos[ncr - 1] + wflag[ncr - 1] : 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        prow[i] = piv_of_col[pc[i]];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_new = n;
+}
+
 // pending flags for an ordered compaction (rows in ascending order)
 __global__ void k_pending_flags(int32_t t, const int32_t* __restrict__ lead,
                                 const uint8_t* __restrict__ is_piv, uint8_t* flag) {
@@ -419,17 +431,19 @@ __global__ void k_bucket_sorted(int32_t n, const int32_t* __restrict__ key,
 
 // rows per lead column and per 128-column panel; a panel is "dirty" when
 // two pending rows share a lead in it
-__global__ void k_lead_hist(int32_t n, const int32_t* __restrict__ pend,
+__global__ void k_lead_hist(const int32_t* __restrict__ n_dev, const int32_t* __restrict__ pend,
                             const int32_t* __restrict__ lead, int32_t* hist, int32_t* pcnt) {
+    const int32_t n = *n_dev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int32_t l = lead[pend[i]];
         atomicAdd(&hist[l], 1);
         atomicAdd(&pcnt[l / KB], 1);
     }
 }
-__global__ void k_dirty_panels(int32_t n, const int32_t* __restrict__ pend,
+__global__ void k_dirty_panels(const int32_t* __restrict__ n_dev, const int32_t* __restrict__ pend,
                                const int32_t* __restrict__ lead, const int32_t* __restrict__ hist,
                                int32_t* pdirty) {
+    const int32_t n = *n_dev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int32_t l = lead[pend[i]];
         if (hist[l] > 1) pdirty[l / KB] = 1;
@@ -437,9 +451,10 @@ __global__ void k_dirty_panels(int32_t n, const int32_t* __restrict__ pend,
 }
 
 // rows of collision-free panels have leads of their own: they are pivots
-__global__ void k_claim_clean(int32_t n, const int32_t* __restrict__ pend,
+__global__ void k_claim_clean(const int32_t* __restrict__ n_dev, const int32_t* __restrict__ pend,
                               const int32_t* __restrict__ lead, const int32_t* __restrict__ pdirty,
                               int32_t* piv_of_col, uint8_t* is_piv, int32_t* wflag) {
+    const int32_t n = *n_dev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int32_t r = pend[i], l = lead[r];
         if (!pdirty[l / KB]) {
@@ -495,10 +510,11 @@ __global__ void k_register_chunks(const int32_t* __restrict__ n_piv,
 // scale row rows[i] by the inverse of its entry at column cols[i] (one CTA
 // per row)
 template <class F>
-__global__ void k_normalize_at(int32_t n, const int32_t* __restrict__ rows,
+__global__ void k_normalize_at(const int32_t* __restrict__ n_dev, const int32_t* __restrict__ rows,
                                const int32_t* __restrict__ cols, int32_t ncols, uint32_t* M,
                                int64_t ld, F f) {
     __shared__ uint32_t s_inv;
+    const int32_t n = *n_dev;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         uint32_t* row = M + (size_t)rows[i] * ld;
         const int32_t c0 = cols[i];
@@ -1049,28 +1065,30 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     int rounds = 0;
     bool first = true;
     while (t > 0 && ncr > 0) {
+        // pending rows, lead histogram, clean panels claimed, dirty panels
+        // flagged -- all sized on the device; one host round trip reads the
+        // count and the dirty flags
         int32_t n_pend = 0;
         BL_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int32_t), s));
         BL_CHECK(collect_pending(counters));
+        BL_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * ncr, s));
+        BL_CUDA(cudaMemsetAsync(pcnt, 0, sizeof(int32_t) * npan, s));
+        BL_CUDA(cudaMemsetAsync(pdirty, 0, sizeof(int32_t) * npan, s));
+        BL_CUDA(cudaMemsetAsync(wflag, 0, sizeof(int32_t) * ncr, s));
+        BL_LAUNCH(k_lead_hist<<<grid_of(t), 256, 0, s>>>(counters, pend, lead, hist, pcnt));
+        BL_LAUNCH(k_dirty_panels<<<grid_of(t), 256, 0, s>>>(counters, pend, lead, hist, pdirty));
+        BL_LAUNCH(k_claim_clean<<<grid_of(t), 256, 0, s>>>(counters, pend, lead, pdirty,
+                                                            piv_of_col, is_piv, wflag));
+        // dirty panels, leftmost first, at most max_dirty of them this round
+        std::vector<int32_t> h_dirty(npan);
         BL_CUDA(cudaMemcpyAsync(&n_pend, counters, 4, cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaMemcpyAsync(h_dirty.data(), pdirty, sizeof(int32_t) * npan,
+                                cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
         if (first) out->dense_rows = n_pend;
         first = false;
         if (n_pend == 0) break;
         ++rounds;
-        BL_CUDA(cudaMemsetAsync(hist, 0, sizeof(int32_t) * ncr, s));
-        BL_CUDA(cudaMemsetAsync(pcnt, 0, sizeof(int32_t) * npan, s));
-        BL_CUDA(cudaMemsetAsync(pdirty, 0, sizeof(int32_t) * npan, s));
-        BL_CUDA(cudaMemsetAsync(wflag, 0, sizeof(int32_t) * ncr, s));
-        BL_LAUNCH(k_lead_hist<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, hist, pcnt));
-        BL_LAUNCH(k_dirty_panels<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, hist, pdirty));
-        BL_LAUNCH(k_claim_clean<<<grid_of(n_pend), 256, 0, s>>>(n_pend, pend, lead, pdirty,
-                                                                 piv_of_col, is_piv, wflag));
-        // dirty panels, leftmost first, at most max_dirty of them this round
-        std::vector<int32_t> h_dirty(npan);
-        BL_CUDA(cudaMemcpyAsync(h_dirty.data(), pdirty, sizeof(int32_t) * npan,
-                                cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaStreamSynchronize(s));
         std::vector<int32_t> h_dpanel, h_dslot(npan, -1);
         for (int32_t p = 0; p < npan && (int32_t)h_dpanel.size() < max_dirty; ++p) {
             if (h_dirty[p]) {
@@ -1142,25 +1160,22 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
         BL_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wflag, wpos, ncr, s));
         ++c.launches;
         BL_LAUNCH(k_compact_cols<<<grid_of(ncr), 256, 0, s>>>(ncr, wflag, wpos, pc));
-        int32_t last_pos = 0, last_flag = 0;
-        BL_CUDA(cudaMemcpyAsync(&last_pos, wpos + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaMemcpyAsync(&last_flag, wflag + ncr - 1, 4, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaStreamSynchronize(s));
-        const int32_t n_new = last_pos + last_flag;
-        if (trace_rounds()) fprintf(stderr, "gbgpu echelon round %d: new pivots %d\n", rounds, n_new);
-        BL_LAUNCH(k_gather_rows<<<grid_of(n_new), 256, 0, s>>>(n_new, pc, piv_of_col, prow,
-                                                               counters + 2));
-        BL_LAUNCH(k_normalize_at<F><<<std::max(1, std::min(n_new, 148 * 8)), 256, 0, s>>>(
-            n_new, prow, pc, ncr, Dp, ld, f));
-        // the rest: eliminated against every pivot of the round
-        int32_t n_rest = 0;
+        BL_LAUNCH(k_new_pivots<<<grid_of(ncr), 256, 0, s>>>(ncr, wflag, wpos, pc, piv_of_col,
+                                                           counters + 2, prow));
+        BL_LAUNCH(k_normalize_at<F><<<std::min(t, 148 * 8), 256, 0, s>>>(counters + 2, prow, pc,
+                                                                         ncr, Dp, ld, f));
+        // the rest: eliminated against every pivot of the round; one host
+        // round trip reads both counts and the pivot columns
         BL_CHECK(collect_pending(counters + 3));
-        BL_CUDA(cudaMemcpyAsync(&n_rest, counters + 3, 4, cudaMemcpyDeviceToHost, s));
+        int32_t cnt[2] = {0, 0};
+        std::vector<int32_t> h_pc((size_t)ncr);
+        BL_CUDA(cudaMemcpyAsync(cnt, counters + 2, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * ncr, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaStreamSynchronize(s));
+        const int32_t n_new = cnt[0], n_rest = cnt[1];
+        if (trace_rounds()) fprintf(stderr, "gbgpu echelon round %d: new pivots %d\n", rounds, n_new);
         if (n_rest == 0) break;
-        std::vector<int32_t> h_pc(n_new);
-        BL_CUDA(cudaMemcpyAsync(h_pc.data(), pc, sizeof(int32_t) * n_new, cudaMemcpyDeviceToHost, s));
-        BL_CUDA(cudaStreamSynchronize(s));
+        h_pc.resize((size_t)n_new);
         BL_CHECK(eliminate(c, f, Dp, ld, pend, n_rest, ncr, prow, n_new, pc, h_pc));
         BL_LAUNCH(k_row_leads<<<grid_of((int64_t)n_rest * 32), 256, 0, s>>>(n_rest, pend, ncr, Dp,
                                                                              ld, lead, 1));
