@@ -37,6 +37,13 @@ CONFIG = {"nru": 20000, "nrl": 5000, "ncr": 20000, "p": 65521, "dmin": 0.02, "dm
           "seed": 1}
 METRIC = "GF(p) matrix reductions/s (20000x5000 A|B/C|D, 40000 cols, p=65521, bit-exact)"
 INT8_PEAK_TOPS = 3040.7  # torch._int_mm 8192^3 int8, best of 10, measured on this pool
+# DRAM traffic of the tensor-core GEMM on the staircase workload: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum summed over the 82 k_tc_submul
+# launches of one reduction (4665.9 MB read + 647.8 MB written), per launch.
+# A one-pass metric capture of this exact workload; the kernel's traffic does
+# not depend on the clocks or the timing, so it is reported, not re-measured.
+GEMM_TRAFFIC_PER_LAUNCH = (4665.9e6 + 647.8e6) / 82
+GEMM_TRAFFIC_LAUNCHES = 82
 UNIT = "matrices/s"
 
 
@@ -63,14 +70,48 @@ def dist_env():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML read every 10 ms from a thread (the library nvidia-smi reads),
+    or nvidia-smi every 200 ms where NVML cannot be opened.  Reads only."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []  # (sm MHz, max sm MHz, reasons bitmask)
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def __enter__(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+        except Exception:
+            nv = None
+        if nv is not None:
+            self.stop = threading.Event()
+
+            def loop():
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                while True:
+                    self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                         nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    if self.stop.wait(0.01):
+                        break
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return self
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -85,6 +126,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -94,19 +138,27 @@ class Clocks:
 
     def summary(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.thread is not None:
+            if self.samples:
+                out["sm_mhz"] = statistics.median(x[0] for x in self.samples)
+                out["sm_max_mhz"] = max(x[1] for x in self.samples)
+                out["reasons"] = sorted({n for x in self.samples for n, bit in self.REASONS
+                                         if x[2] & bit})
+            out["samples"] = len(self.samples)
+            out["source"] = "nvml, 10 ms"
+            return out
         try:
             rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l]
             os.unlink(self.path)
-        except OSError:
+        except (OSError, TypeError):
             return out
         sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in rows:
             if len(r) < 9:
                 continue
-            for n, v in zip(names, r[5:9]):
+            for (n, _), v in zip(self.REASONS, r[5:9]):
                 if v.strip() == "Active":
                     reasons.add(n)
         if sm:
@@ -115,6 +167,7 @@ class Clocks:
             out["sm_max_mhz"] = max(mx)
         out["reasons"] = sorted(reasons)
         out["samples"] = len(sm)
+        out["source"] = "nvidia-smi, 200 ms"
         return out
 
 
@@ -294,7 +347,12 @@ def main():
                 "peak": INT8_PEAK_TOPS, "unit": "TOPS (int8)", "frac": tops / INT8_PEAK_TOPS,
                 "peak_source": "measured: torch._int_mm 8192^3 int8 on this pool (no int8 "
                                "figure in MEASURED_PEAKS.json)",
-                "traffic": None, "launches": pst["gemm_launches"],
+                "traffic": (GEMM_TRAFFIC_PER_LAUNCH
+                            if pst["gemm_launches"] == GEMM_TRAFFIC_LAUNCHES and args.scale == 1.0
+                            else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, bytes per "
+                                  "launch averaged over the GEMM launches of one reduction",
+                "launches": pst["gemm_launches"],
                 "ms_all_launches": pst["gemm_ms"], "int8_ops_all_launches": pst["gemm_int8_ops"],
                 "avg_launch_ms": pst["gemm_ms"] / max(pst["gemm_launches"], 1)}
     line = {

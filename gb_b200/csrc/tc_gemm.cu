@@ -474,9 +474,27 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     return ri >= 0 ? Dz + (size_t)ri * prm.ldd : nullptr;
                 }
             };
+            // D values of a 32 x 32 block (row r, this lane's column)
+            auto load_d = [&](int c0, uint32_t (&dv)[32]) {
+                const int gn = n0 + c0 + lane;
+                const bool col_ok = gn < prm.N;
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    const uint32_t* rp = drow(r);
+                    dv[r] = (rp && col_ok) ? rp[gn] : 0u;
+                }
+            };
             for (int panel = 0; panel < npanels; ++panel, ++pc) {
                 const int ab = pc % C::ACC_BUFS, au = pc / C::ACC_BUFS;
                 const uint32_t acc_base = (uint32_t)(ab * C::NW * C::BN);
+                // the first block's D values do not depend on the accumulators:
+                // their loads are in flight while the MMAs finish (this lane
+                // wrote the same addresses in the previous panel, if any).
+                // Three and four limbs have no registers to spare for it; with
+                // two CTAs per SM the other CTA's epilogue covers the wait.
+                constexpr bool EARLY_D = L <= 2 && !C::SMALL;
+                uint32_t dv[32];
+                if constexpr (EARLY_D) load_d(cbeg, dv);
                 bool ok = true;
                 if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar(ab), au & 1, prm.budget);
                 ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -489,13 +507,8 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 for (int c0 = cbeg; c0 < cbeg + COLS; c0 += 32) {
                     const int gn = n0 + c0 + lane;
                     const bool col_ok = gn < prm.N;
-                    // D values of the block (row r, column gn), issued before the fold
-                    uint32_t dv[32];
-#pragma unroll
-                    for (int r = 0; r < 32; ++r) {
-                        const uint32_t* rp = drow(r);
-                        dv[r] = (rp && col_ok) ? rp[gn] : 0u;
-                    }
+                    // D values of the later blocks, issued before the fold
+                    if (!EARLY_D || c0 != cbeg) load_d(c0, dv);
                     uint32_t v[32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) v[j] = 0;
