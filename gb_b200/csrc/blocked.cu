@@ -304,7 +304,7 @@ __global__ void k_gather_cols(int32_t rows, int32_t n, const uint32_t* __restric
     }
 }
 
-// dst row i = src row rows[i] (n columns)
+// dst row i = src row rows[i] (n columns; a negative index: a zero row)
 __global__ void k_gather_rows_dense(int32_t nrows, const int32_t* __restrict__ rows, int32_t n,
                                     const uint32_t* __restrict__ src, int64_t lds, uint32_t* dst,
                                     int64_t ldd) {
@@ -313,7 +313,8 @@ __global__ void k_gather_rows_dense(int32_t nrows, const int32_t* __restrict__ r
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = t / n;
         const int j = (int)(t % n);
-        dst[i * ldd + j] = src[(int64_t)rows[i] * lds + j];
+        const int32_t r = rows[i];
+        dst[i * ldd + j] = r >= 0 ? src[(int64_t)r * lds + j] : 0u;
     }
 }
 
@@ -479,15 +480,20 @@ __global__ void k_bucket_dirty(int32_t n, const int32_t* __restrict__ pend,
     }
 }
 
-// row list of the pivot rows of every chunk (the others -1): only the pivot
-// rows take the panel transformation; the rest are cleared later by the
-// round's elimination against all new pivots
+// row lists of the pivot rows of every chunk, packed to the front (the rest
+// -1): only the pivot rows take the panel transformation, as rows 0..n_piv of
+// the product -- D row k is the chunk row of pivot k, A row k the row of I - E
+// at that row's chunk position -- so that the GEMM's row quarters past n_piv
+// hold no row and skip their epilogue.  The other chunk rows are cleared later
+// by the round's elimination against all new pivots.
 __global__ void k_pivot_rowlist(const int32_t* __restrict__ n_piv, const int32_t* __restrict__ piv_pos,
-                                const int32_t* __restrict__ chunk_rows, int32_t* drows) {
+                                const int32_t* __restrict__ chunk_rows, int32_t* drows,
+                                int32_t* arows) {
     const int d = blockIdx.x;
     for (int k = threadIdx.x; k < n_piv[d]; k += blockDim.x) {
         const int32_t pos = piv_pos[d * KB + k];
-        drows[d * KB + pos] = chunk_rows[d * KB + pos];
+        drows[d * KB + k] = chunk_rows[d * KB + pos];
+        arows[d * KB + k] = pos;
     }
 }
 
@@ -1038,6 +1044,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     int32_t* piv_colb = c.alloc<int32_t>((size_t)max_dirty * KB);
     int32_t* n_piv = c.alloc<int32_t>(max_dirty);
     int32_t* piv_rows = c.alloc<int32_t>((size_t)max_dirty * KB);
+    int32_t* piv_arows = c.alloc<int32_t>((size_t)max_dirty * KB);
     // ordered compaction of the pending rows and the stable (panel, row) sort
     // that fills the chunks: the same rows, in the same order, on every run
     uint8_t* pflag = c.alloc<uint8_t>(t);
@@ -1052,7 +1059,7 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
     void* sel_tmp = c.alloc<uint8_t>(sel_bytes);
     void* sort_tmp = c.alloc<uint8_t>(sort_bytes);
     if (!chunk_rows || !cursor || !imeB || !piv_pos || !piv_colb || !n_piv || !piv_rows ||
-        !pflag || !pkey || !pkey_sorted || !prow_sorted || !sel_tmp || !sort_tmp)
+        !piv_arows || !pflag || !pkey || !pkey_sorted || !prow_sorted || !sel_tmp || !sort_tmp)
         return GBGPU_ENOMEM;
     // pending rows (nonzero, not pivots) into pend[0 .. *count), ascending
     auto collect_pending = [&](int32_t* count) -> int {
@@ -1127,15 +1134,47 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             // the elimination against the round's pivots below clears them.
             BL_LAUNCH(k_fill_i32<<<grid_of((int64_t)n_dirty * KB), 256, 0, s>>>(
                 piv_rows, n_dirty * KB, -1));
-            BL_LAUNCH(k_pivot_rowlist<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, chunk_rows, piv_rows));
-            TcGemmArgs g{c.p, KB, width, KB, imeB, KB, Dp + j0, ld, Dp + j0, ld};
-            g.batch = n_dirty;
-            g.sA = (int64_t)KB * KB;
-            g.b_rows = chunk_rows;
-            g.sBr = KB;
-            g.d_rows = piv_rows;
-            g.sDr = KB;
-            BL_CHECK(gemm_args(c, g));
+            BL_LAUNCH(k_fill_i32<<<grid_of((int64_t)n_dirty * KB), 256, 0, s>>>(
+                piv_arows, n_dirty * KB, -1));
+            BL_LAUNCH(k_pivot_rowlist<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, chunk_rows, piv_rows,
+                                                             piv_arows));
+            if (c.form != GBGPU_FORM_PLAIN) {
+                TcGemmArgs g{c.p, KB, width, KB, imeB, KB, Dp + j0, ld, Dp + j0, ld};
+                g.batch = n_dirty;
+                g.sA = (int64_t)KB * KB;
+                g.a_rows = piv_arows;
+                g.sAr = KB;
+                g.b_rows = chunk_rows;
+                g.sBr = KB;
+                g.d_rows = piv_rows;
+                g.sDr = KB;
+                BL_CHECK(gemm_args(c, g));
+            } else {
+                // The CUDA-core product reads its operands where they lie, and
+                // a tile may read chunk rows that another tile of the same
+                // launch has already rewritten: the chunk rows are copied
+                // first (groups of chunks, at most 256 MB of copies at once).
+                const int64_t per = (int64_t)KB * width;
+                const int32_t group = (int32_t)std::max<int64_t>(
+                    1, std::min<int64_t>(n_dirty, (256ll << 20) / (per * 4)));
+                uint32_t* oldc = c.alloc<uint32_t>((size_t)group * per);
+                if (!oldc) return GBGPU_ENOMEM;
+                for (int32_t d0 = 0; d0 < n_dirty; d0 += group) {
+                    const int32_t nb = std::min(group, n_dirty - d0);
+                    BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)nb * per), 256, 0, s>>>(
+                        nb * KB, chunk_rows + (size_t)d0 * KB, width, Dp + j0, ld, oldc, width));
+                    TcGemmArgs g{c.p, KB, width, KB, imeB + (size_t)d0 * KB * KB, KB, oldc, width,
+                                 Dp + j0, ld};
+                    g.batch = nb;
+                    g.sA = (int64_t)KB * KB;
+                    g.sB = per;
+                    g.a_rows = piv_arows + (size_t)d0 * KB;
+                    g.sAr = KB;
+                    g.d_rows = piv_rows + (size_t)d0 * KB;
+                    g.sDr = KB;
+                    BL_CHECK(gemm_args(c, g));
+                }
+            }
             BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
                                                                 piv_of_col, is_piv, wflag));
             if (trace_rounds()) {

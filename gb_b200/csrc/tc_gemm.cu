@@ -455,6 +455,7 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             const int m0 = mt * C::BM, n0 = nt * C::BN;
             const int gm = m0 + row;
             uint32_t* Dz = prm.D + (size_t)z * prm.sD;
+            bool rows_here;  // any of this warp's 32 rows is written
             {
                 int32_t ri = -1;
                 if (gm < prm.M) ri = prm.d_rows ? prm.d_rows[(size_t)z * prm.sDr + gm] : gm;
@@ -463,7 +464,8 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     rowp[lane] = ri >= 0 ? Dz + (size_t)ri * prm.ldd : nullptr;
                 else
                     rowi[lane] = ri;
-                __syncwarp();
+                rows_here = __any_sync(0xffffffffu, ri >= 0);
+                __syncwarp();  // the row table is visible to the whole warp
             }
             // row r of the tile in D (nullptr: not written)
             auto drow = [&](int r) -> uint32_t* {
@@ -494,7 +496,9 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                 // two CTAs per SM the other CTA's epilogue covers the wait.
                 constexpr bool EARLY_D = L <= 2 && !C::SMALL;
                 uint32_t dv[32];
-                if constexpr (EARLY_D) load_d(cbeg, dv);
+                if constexpr (EARLY_D) {
+                    if (rows_here) load_d(cbeg, dv);
+                }
                 bool ok = true;
                 if (lane == 0) ok = !*abort_flag && mbar_wait(tfull_bar(ab), au & 1, prm.budget);
                 ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -504,7 +508,9 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     break;
                 }
                 tc_fence_after();
-                for (int c0 = cbeg; c0 < cbeg + COLS; c0 += 32) {
+                // a warp with no row to write keeps only its place in the
+                // accumulator handshake
+                for (int c0 = cbeg; rows_here && c0 < cbeg + COLS; c0 += 32) {
                     const int gn = n0 + c0 + lane;
                     const bool col_ok = gn < prm.N;
                     // D values of the later blocks, issued before the fold
