@@ -39,10 +39,10 @@ METRIC = "GF(p) matrix reductions/s (20000x5000 A|B/C|D, 40000 cols, p=65521, bi
 INT8_PEAK_TOPS = 3040.7  # torch._int_mm 8192^3 int8, best of 10, measured on this pool
 # DRAM traffic of the tensor-core GEMM on the staircase workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum summed over the 82 k_tc_submul
-# launches of one reduction (4665.9 MB read + 647.8 MB written), per launch.
+# launches of one reduction (4665.2 MB read + 651.8 MB written), per launch.
 # A one-pass metric capture of this exact workload; the kernel's traffic does
 # not depend on the clocks or the timing, so it is reported, not re-measured.
-GEMM_TRAFFIC_PER_LAUNCH = (4665.9e6 + 647.8e6) / 82
+GEMM_TRAFFIC_PER_LAUNCH = (4665.2e6 + 651.8e6) / 82
 GEMM_TRAFFIC_LAUNCHES = 82
 UNIT = "matrices/s"
 
