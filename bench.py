@@ -209,11 +209,21 @@ def cpu_reference(mat, steps: int, budget_s: float = 20.0):
         times.append(secs)
     t = statistics.median(times)
     share = keep.shape[0] / nrl
-    return {"value": share / t, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": (f"reference la option 1 (oracle/_ref, {threads} OpenMP threads) on all "
-                       f"{mat.ncl} known pivots + {keep.shape[0]} of {nrl} C|D rows "
-                       f"(every {int(round(1 / frac))}th), median of {len(times)} calls "
-                       f"{t:.3f}s, extrapolated linearly to all {nrl} rows")}
+    out = {"value": share / t, "unit": UNIT, "cores": threads, "kind": "reference",
+           "sample": (f"reference la option 1 (oracle/_ref, {threads} OpenMP threads) on all "
+                      f"{mat.ncl} known pivots + {keep.shape[0]} of {nrl} C|D rows "
+                      f"(every {int(round(1 / frac))}th), median of {len(times)} calls "
+                      f"{t:.3f}s, extrapolated linearly to all {nrl} rows")}
+    # the same la on one thread, on a quarter of that sample (one call)
+    if threads > 1:
+        stride1 = 4 * max(1, int(round(1 / frac)))
+        keep1 = np.arange(0, nrl, stride1)
+        _, secs1 = oracle.ref_la(mat.subset(keep1), 1, nthreads=1)
+        out["one_thread"] = {
+            "value": (keep1.shape[0] / nrl) / secs1, "unit": UNIT, "cores": 1,
+            "sample": (f"all {mat.ncl} known pivots + {keep1.shape[0]} of {nrl} C|D rows "
+                       f"(every {stride1}th), one call {secs1:.3f}s, extrapolated linearly")}
+    return out
 
 
 def run_reference_arm(args):
