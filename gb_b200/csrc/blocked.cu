@@ -550,12 +550,14 @@ __global__ void k_normalize_at(const int32_t* __restrict__ n_dev, const int32_t*
 // eight threads (adjacent lanes).  A step takes the non-pivot row with the
 // smallest (lead, index) as the next pivot -- the same pivot the column-by-
 // column search finds -- and updates exactly the other non-pivot rows with that
-// lead: row_r -= (P[r][c] / P[i][c]) row_i on the columns after c and on E.
-// Pivot rows are not scaled (they are normalised after the round).  Column c
-// is never read again, so it is not written, and the multipliers need no
-// barrier; the updated rows recompute their leads from the values they wrote
-// and publish their keys for the next step.  Two barriers per pivot: the
-// minimum's and the pivot inverse's (one thread, Fermat).
+// lead, fraction-free: row_r <- P[i][c] row_r - P[r][c] row_i on the columns
+// after c and on E (a nonzero multiple of the usual update: the same zero
+// pattern, hence the same leads and pivots, and no inverse on the sequential
+// path).  Pivot rows are not scaled (they are normalised after the round).
+// Column c is never read again, so it is not written; the pivot row is not
+// written in the step that chooses it, so the updates need no barrier of their
+// own.  The updated rows recompute their leads from the values they wrote and
+// publish their keys for the next step: one barrier per pivot.
 constexpr int PF_GROUPS = 8;     // threads (adjacent lanes) per row in k_panel_factor
 constexpr int PF_LD = KB + 8;    // row stride of P and E: conflict-free for 8 lanes per row
 
@@ -577,7 +579,6 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     uint32_t(*P)[PF_LD] = (uint32_t(*)[PF_LD])pf_smem;
     uint32_t(*E)[PF_LD] = (uint32_t(*)[PF_LD])(pf_smem + KB * PF_LD);
     __shared__ int s_min[2][KB * PF_GROUPS / 32];  // double-buffered block minimum
-    __shared__ uint32_t s_inv;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int r = tid / PF_GROUPS, g = tid % PF_GROUPS;  // row and column group of this thread
@@ -614,12 +615,11 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
         if (tid == 0) {
             piv_pos[k] = i;
             piv_col[k] = col0 + c;
-            s_inv = f.inv(P[i][c]);
         }
-        __syncthreads();
         if (r == i) my_piv = true;
         if (!my_piv && my_lead == c) {
-            const uint32_t mp = f.prep(f.mulmod(P[r][c], s_inv));
+            const uint32_t ap = f.prep(P[i][c]);  // the pivot's lead value
+            const uint32_t mp = f.prep(P[r][c]);  // this row's value in column c
             int nl = INT_MAX;
             // four independent columns per pass (loads first, then stores)
             for (int cc = c + 1 + g; cc < bw; cc += 4 * PF_GROUPS) {
@@ -633,9 +633,10 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int col = cc + u * PF_GROUPS;
-                    if (col < bw) {
-                        const uint32_t y = v[u] ? f.mulsub(x[u], mp, v[u]) : x[u];
-                        if (v[u]) P[r][col] = y;
+                    if (col < bw && (x[u] | v[u])) {
+                        const uint32_t ax = x[u] ? f.mulp(x[u], ap) : 0u;
+                        const uint32_t y = v[u] ? f.mulsub(ax, mp, v[u]) : ax;
+                        P[r][col] = y;
                         if (y != 0u && col < nl) nl = col;
                     }
                 }
@@ -646,12 +647,15 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
                 for (int u = 0; u < 4; ++u) {
                     const int col = cc + u * PF_GROUPS;
                     v[u] = col < n ? E[i][col] : 0u;
-                    x[u] = col < n && v[u] ? E[r][col] : 0u;
+                    x[u] = col < n ? E[r][col] : 0u;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int col = cc + u * PF_GROUPS;
-                    if (col < n && v[u]) E[r][col] = f.mulsub(x[u], mp, v[u]);
+                    if (col < n && (x[u] | v[u])) {
+                        const uint32_t ax = x[u] ? f.mulp(x[u], ap) : 0u;
+                        E[r][col] = v[u] ? f.mulsub(ax, mp, v[u]) : ax;
+                    }
                 }
             }
             nl = min(nl, __shfl_xor_sync(grp, nl, 1));

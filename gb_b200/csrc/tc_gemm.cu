@@ -569,11 +569,14 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 // ---------------------------------------------------------------------------
 // limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded; row m
 // of A is A + a_rows[m] lda when a_rows is given (negative: a zero row).
-// Every thread splits 16 consecutive k of one row (one 16-byte store per limb).
+// Every thread splits 16 consecutive k of one row (one 16-byte store per limb);
+// with `vec` (A and its row and batch strides 16-byte aligned) a full group is
+// read as four 16-byte loads.
 __global__ void __launch_bounds__(256)
 k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
              const int32_t* __restrict__ a_rows, int64_t sAr, int32_t M, int32_t K, int32_t Mp,
-             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t fstride) {
+             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t fstride,
+             int32_t vec) {
     // batch item blockIdx.y
     A += (size_t)blockIdx.y * sA;
     if (a_rows) a_rows += (size_t)blockIdx.y * sAr;
@@ -590,11 +593,22 @@ k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
         const uint32_t* row = src >= 0 ? A + (size_t)src * lda : nullptr;
         uint32_t v[16];
         uint32_t any = 0;
+        if (vec && row && k + 16 <= K) {
+            const uint4* r4 = (const uint4*)(row + k);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            v[i] = (row && k + i < K) ? row[k + i] : 0u;
-            any |= v[i];
+            for (int q = 0; q < 4; ++q) {
+                const uint4 w = r4[q];
+                v[4 * q] = w.x;
+                v[4 * q + 1] = w.y;
+                v[4 * q + 2] = w.z;
+                v[4 * q + 3] = w.w;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = (row && k + i < K) ? row[k + i] : 0u;
         }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) any |= v[i];
         if (flags && any) flags[(size_t)(m / 128) * fstride + k / 128] = 1;
         for (int l = 0; l < L; ++l) {
             uint32_t w[4];
@@ -848,8 +862,9 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         const int64_t total = (int64_t)Mp * (Kp / 16);
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256,
                                                                        148 * 32 / nb + 1));
+        const int32_t vec = ((uintptr_t)g.A % 16 == 0) && g.lda % 4 == 0 && g.sA % 4 == 0;
         k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.a_rows, g.sAr, g.M, g.K,
-                                                    Mp, Kp, L, Ap, fa, nkbp);
+                                                    Mp, Kp, L, Ap, fa, nkbp, vec);
         dim3 gb(Np / 64, Kp / 128, nb);
         k_split_cols<<<gb, 256, L * 64 * SPLIT_ROW, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K,
                                                           g.N, Np, Kp, L, Bp, fb, Cfg::BN, nkbp);
