@@ -21,3 +21,41 @@ def test_every_workload_has_a_runner():
     assert callable(b.main)
     assert callable(b.run_reference_arm)
     assert b.make_matrix(0.02).nr > 0
+
+
+def test_clock_summary_reports_median_and_throttle_reasons():
+    b = _bench()
+    clk = b.Clocks(0)
+    clk.thread = object()  # the NVML sampler ran: summarise its samples
+    clk.samples = [(1965, 1965, 0x0), (1950, 1965, 0x4), (1965, 1965, 0x4), (1800, 1965, 0x40)]
+    out = clk.summary()
+    assert out["sm_mhz"] == 1957.5 and out["sm_max_mhz"] == 1965
+    assert out["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
+    assert out["samples"] == 4
+
+
+def test_clock_summary_reads_nvidia_smi_csv(tmp_path):
+    b = _bench()
+    clk = b.Clocks(0)
+    path = tmp_path / "clocks.csv"
+    path.write_text("0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active\n"
+                    "0, 1320, 1965, 1000.2, 0x4, Not Active, Not Active, Not Active, Active\n"
+                    "0, 1400, 1965, 998.0, 0x4, Active, Not Active, Not Active, Active\n")
+    clk.path = str(path)
+    out = clk.summary()
+    assert out["sm_mhz"] == 1400 and out["sm_max_mhz"] == 1965 and out["samples"] == 3
+    assert out["reasons"] == ["hw_slowdown", "sw_power_cap"]
+
+
+def test_cpu_baseline_states_both_thread_counts():
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference build absent")
+    b = _bench()
+    from gb_b200 import synth
+    mat = synth.staircase(800, 200, 800, 65521, seed=3)
+    cb = b.cpu_reference(mat, 1, budget_s=0.5)
+    assert cb["kind"] == "reference" and cb["value"] > 0 and cb["cores"] >= 1
+    if cb["cores"] > 1:
+        one = cb["one_thread"]
+        assert one["cores"] == 1 and one["value"] > 0 and "C|D rows" in one["sample"]
