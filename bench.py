@@ -255,12 +255,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
-    ap.add_argument("--workload", default="staircase", choices=["staircase", "dense", "rref", "batch", "f4"],
+    ap.add_argument("--workload", default="staircase",
+                    choices=["staircase", "dense", "rref", "batch", "f4", "multimod"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
                          "rref: RREF of a rank-3n/4 n x n block; batch: 2 x 128 independent "
                          "matrices through the batch entry point; f4: the captured la calls "
-                         "of the dense F4 systems")
+                         "of the dense F4 systems; multimod: an integer matrix reduced over Q "
+                         "from its GF(p) images")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
@@ -277,6 +279,9 @@ def main():
         return
     if args.workload == "f4":
         run_f4_captures(args)
+        return
+    if args.workload == "multimod":
+        run_multimod(args)
         return
 
     import torch
@@ -657,6 +662,76 @@ def run_f4_captures(args):
             "data": "reference-captured F4 matrices (tests/golden/mats)",
             "config": {"workload": "f4 captures: dense_quadratic_7 (p=32003) + "
                                    "dense_cubic_5_p31 (p=2^31-1)", "systems": systems}}
+    print(json.dumps(line), flush=True)
+
+
+def multimod_matrix():
+    """The integer system of the multi-modular workload: the staircase
+    structure (400 known pivots, 100 rows to reduce, 300 right columns,
+    density U[2%, 5%]) with integer coefficients in [-64, 64] \\ {0}."""
+    from gb_b200 import multimod, synth
+    m = synth.integer_staircase(400, 100, 300, bound=1 << 6, dmin=0.02, dmax=0.05, seed=1)
+    return multimod.IntegerMacaulay.from_matrix(m, vals=m.vals.astype(np.int64))
+
+
+def multimod_cpu_reference(mat, primes_used: int, lift_s: float, sample: int = 8):
+    """The same computation with the reference's la (oracle/_ref, all host
+    threads) for the GF(p) images: `sample` images timed, scaled to the
+    primes the GPU run used, plus the same host lift."""
+    import oracle
+    from gb_b200 import multimod
+    threads = os.cpu_count() or 1
+    gen = multimod.primes_below_2_31()
+    secs = []
+    while len(secs) < sample:
+        img = multimod.image(mat, next(gen))
+        if img is not None:
+            secs.append(oracle.ref_la(img, 1, nthreads=threads)[1])
+    per = statistics.median(secs)
+    total = per * primes_used + lift_s
+    return {"value": 1.0 / total, "unit": "systems/s", "cores": threads, "kind": "reference",
+            "sample": (f"reference la option 1 (oracle/_ref, {threads} threads) on {sample} "
+                       f"GF(p) images, median {per * 1e3:.2f} ms, x {primes_used} primes, "
+                       f"+ the same host lift {lift_s:.2f} s")}
+
+
+def run_multimod(args):
+    """Row (f) 3 of the scope: an integer Macaulay matrix reduced over Q.
+    One step = gb_b200.multimod.reduce_over_q: GF(p) images for the largest
+    primes below 2^31, reduced 16 at a time by gbgpu_reduce_batch, lifted by
+    CRT + rational reconstruction on the host and certified by one more prime.
+    Wall clock (the host lift is part of the step); the lifted answer's image
+    is checked against the oracle for one prime."""
+    from gb_b200 import _lib, multimod
+    _lib.load()
+    mat = multimod_matrix()
+    multimod.reduce_over_q(mat, batch=16)  # warm
+    ts, st, res = [], {}, None
+    for _ in range(max(1, args.steps)):
+        st = {}
+        t0 = time.perf_counter()
+        res = multimod.reduce_over_q(mat, batch=16, stats=st)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    line = {"metric": "rational reductions/s (multi-modular, integer staircase 400+100 x 700)",
+            "value": 1.0 / t, "unit": "systems/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 residues mod 31-bit primes; host big integers",
+            "data": "synthetic (seeded integer staircase, coefficients in [-64, 64])",
+            "config": {"workload": "multimod: integer staircase nru=400 nrl=100 ncr=300",
+                       "primes_used": res.primes_used, "rank": res.np,
+                       "answer_entries": int(res.row_ptr[-1]),
+                       "seconds": {k: round(v, 4) for k, v in st.items()
+                                   if isinstance(v, float)},
+                       "lifts": st.get("lifts"), "primes_tried": st.get("primes_tried")}}
+    if not args.no_cpu:
+        import oracle
+        p = next(multimod.primes_below_2_31())
+        img = multimod.image(mat, p)
+        line["verified_image_vs_oracle"] = bool(
+            img is not None and res.image(p).equals(oracle.oracle_la(img)[0]))
+        line["cpu_baseline"] = multimod_cpu_reference(mat, st.get("primes_tried", 0),
+                                                      st.get("lift_s", 0.0))
     print(json.dumps(line), flush=True)
 
 

@@ -3,6 +3,11 @@ import glob
 import json
 import os
 
+from fractions import Fraction
+
+import numpy as np
+
+from gb_b200 import multimod, synth
 from gb_b200.matrix import ReducedRows, load_captures
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -36,3 +41,36 @@ def as_rows(mat):
 def kat_normalize():
     with open(os.path.join(GOLDEN, "kat_normalize_row.json")) as fh:
         return json.load(fh)
+
+
+def exact_answer(mat: multimod.IntegerMacaulay):
+    """Rows of the reduced row echelon form over Q whose pivot lies in the
+    right block, restricted to it, descending lead (pure Python, small cases)."""
+    nr, nc = mat.nr, mat.ncl + mat.ncr
+    M = [[Fraction(0)] * nc for _ in range(nr)]
+    for i in range(nr):
+        for k in range(int(mat.row_ptr[i]), int(mat.row_ptr[i + 1])):
+            M[i][int(mat.cols[k])] = Fraction(int(mat.vals[k]))
+    piv_row = 0
+    pivots = []
+    for c in range(nc):
+        r = next((r for r in range(piv_row, nr) if M[r][c] != 0), None)
+        if r is None:
+            continue
+        M[piv_row], M[r] = M[r], M[piv_row]
+        inv = 1 / M[piv_row][c]
+        M[piv_row] = [v * inv for v in M[piv_row]]
+        for rr in range(nr):
+            if rr != piv_row and M[rr][c] != 0:
+                f = M[rr][c]
+                M[rr] = [a - f * b for a, b in zip(M[rr], M[piv_row])]
+        pivots.append((c, piv_row))
+        piv_row += 1
+    rows = [(c, M[r]) for c, r in pivots if c >= mat.ncl]
+    rows.sort(key=lambda t: -t[0])
+    return [[(j, v) for j, v in enumerate(row) if j >= mat.ncl and v != 0] for _, row in rows]
+
+
+def small_integer_matrix(seed=1, bound=1 << 6):
+    m = synth.integer_staircase(40, 15, 30, bound=bound, dmin=0.05, dmax=0.15, seed=seed)
+    return multimod.IntegerMacaulay.from_matrix(m, vals=m.vals.astype(np.int64))

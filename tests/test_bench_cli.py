@@ -20,7 +20,9 @@ def test_every_workload_has_a_runner():
     assert callable(b.run_dense)
     assert callable(b.main)
     assert callable(b.run_reference_arm)
+    assert callable(b.run_multimod)
     assert b.make_matrix(0.02).nr > 0
+    assert b.multimod_matrix().nr == 500
 
 
 def test_clock_summary_reports_median_and_throttle_reasons():
@@ -59,3 +61,13 @@ def test_cpu_baseline_states_both_thread_counts():
     if cb["cores"] > 1:
         one = cb["one_thread"]
         assert one["cores"] == 1 and one["value"] > 0 and "C|D rows" in one["sample"]
+
+
+def test_multimod_cpu_baseline_scales_the_sampled_images():
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference build absent")
+    b = _bench()
+    cb = b.multimod_cpu_reference(b.multimod_matrix(), primes_used=100, lift_s=1.0, sample=2)
+    assert cb["kind"] == "reference" and 0 < cb["value"] < 1.0
+    assert "x 100 primes" in cb["sample"]

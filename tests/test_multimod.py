@@ -1,0 +1,122 @@
+"""The multi-modular driver's host logic (no GPU): GF(p) images of integer
+matrices, the lucky-pattern choice, CRT + rational reconstruction, and the
+lifted answer against an exact rational elimination.  The per-prime answers
+come from the oracle here; the GPU path is tested in test_gpu_multimod.py."""
+from fractions import Fraction
+
+import numpy as np
+
+import oracle
+from gb_b200 import multimod, synth
+from helpers import exact_answer, small_integer_matrix
+
+
+def oracle_answers(mat, primes):
+    ps, ans = [], []
+    for p in primes:
+        img = multimod.image(mat, p)
+        if img is None:
+            continue
+        r, _ = oracle.oracle_la(img)
+        ps.append(p)
+        ans.append(r)
+    return ps, ans
+
+
+def test_image_is_monic_and_drops_vanishing_entries():
+    mat = multimod.IntegerMacaulay(
+        2, 2, np.array([0, 2, 5], dtype=np.int64), np.array([0, 2, 1, 2, 3], dtype=np.int32),
+        np.array([3, 7, 5, 10, 11], dtype=np.int64))
+    img = multimod.image(mat, 5)
+    assert img is None  # 5 divides the lead of row 1
+    img = multimod.image(mat, 7)  # row 0: 3, 7 -> 1, 0 (dropped)
+    assert list(img.row_ptr) == [0, 1, 4] and list(img.vals[img.row_ptr[:-1]]) == [1, 1]
+    assert list(img.cols) == [0, 1, 2, 3]
+    # row 1 scaled by 5^-1 mod 7 = 3: 5, 10, 11 -> 1, 2, 5
+    assert list(img.vals[1:]) == [1, 2, 5]
+
+
+def test_ratrecon_and_crt_round_trip():
+    from gb_b200.matrix import ReducedRows
+    primes = list(synth.largest_primes_below(1 << 31, 4))
+    fracs = [(3, 7), (-22, 9), (123456789, 987654), (-1, 2 ** 40 + 15)]
+    # one answer row [1, f_0, f_1, ...] at columns 10, 11, ... per prime
+    lifter = None
+    for p in primes:
+        vals = [1] + [a * pow(b, p - 2, p) % p for a, b in fracs]
+        ans = ReducedRows(np.array([0, len(vals)]), np.arange(10, 10 + len(vals)),
+                          np.array(vals))
+        if lifter is None:
+            lifter = multimod.Lifter(ans, p)
+        else:
+            lifter.add(ans, p)
+    got = lifter.lift()
+    assert got.fractions() == [[(10, Fraction(1))] +
+                               [(11 + k, Fraction(a, b)) for k, (a, b) in enumerate(fracs)]]
+    assert multimod._ratrecon(0, lifter.m, 10) == (0, 1)
+
+
+def test_lift_matches_exact_rational_answer():
+    mat = small_integer_matrix()
+    want = exact_answer(mat)
+    primes = list(synth.largest_primes_below(1 << 31, 40))
+    ps, ans = oracle_answers(mat, primes)
+    got = None
+    for k in range(2, len(ps) + 1):
+        got = multimod.combine(ps[:k], ans[:k])
+        if got is not None and got.image(ps[-1]).equals(ans[-1]):
+            break
+    assert got is not None
+    assert got.fractions() == want
+    # every image of the lifted answer is the GF(p) answer
+    for p, a in zip(ps, ans):
+        assert got.image(p).equals(a)
+
+
+def test_lucky_pattern_skips_a_rank_deficient_prime():
+    p0 = 2147483647
+    # known pivot [1 | 0 0]; C rows [1 | 1 0], [1 | 5 p0]: the Schur complement
+    # [[1, 0], [5, p0]] has determinant p0 -- rank 2 over Q, 1 mod p0
+    mat = multimod.IntegerMacaulay(
+        1, 2, np.array([0, 1, 3, 6], dtype=np.int64),
+        np.array([0, 0, 1, 0, 1, 2], dtype=np.int32),
+        np.array([1, 1, 1, 1, 5, p0], dtype=np.int64))
+    primes = [p0] + list(synth.largest_primes_below(p0, 3))
+    ps, ans = oracle_answers(mat, primes)
+    assert [len(multimod._pattern(a)) for a in ans] == [1, 2, 2, 2]
+    pat = multimod.lucky_pattern(ans)
+    assert pat == (1, 2)
+    sel = [i for i, a in enumerate(ans) if multimod._pattern(a) == pat]
+    got = multimod.combine([ps[i] for i in sel], [ans[i] for i in sel])
+    assert got.fractions() == [[(2, Fraction(1))], [(1, Fraction(1))]]
+    assert got.fractions() == exact_answer(mat)
+
+
+def test_unreconstructible_residues_ask_for_more_primes():
+    mat = small_integer_matrix(seed=2, bound=1 << 20)
+    ps, ans = oracle_answers(mat, list(synth.largest_primes_below(1 << 31, 2)))
+    # one 31-bit prime cannot hold the answer's fractions
+    assert multimod.combine(ps[:1], ans[:1]) is None
+
+
+def _oracle_batch(mats, form=0, device=0):
+    out = [oracle.oracle_la(m)[0] for m in mats]
+    return out, [0] * len(out)
+
+
+def test_driver_loop_with_oracle_images(monkeypatch):
+    """reduce_over_q's batching, pattern choice, incremental lift and check,
+    with the GPU batch call replaced by the oracle (host logic only)."""
+    from gb_b200 import la
+    monkeypatch.setattr(la, "reduce_batch", _oracle_batch)
+    mat = small_integer_matrix()
+    got = multimod.reduce_over_q(mat, batch=5)
+    assert got.fractions() == exact_answer(mat)
+    p0 = 2147483647  # the first prime tried is rank deficient for this matrix
+    mat = multimod.IntegerMacaulay(
+        1, 2, np.array([0, 1, 3, 6], dtype=np.int64),
+        np.array([0, 0, 1, 0, 1, 2], dtype=np.int32),
+        np.array([1, 1, 1, 1, 5, p0], dtype=np.int64))
+    for batch in (1, 2, 4):
+        got = multimod.reduce_over_q(mat, batch=batch)
+        assert got.fractions() == [[(2, Fraction(1))], [(1, Fraction(1))]]
