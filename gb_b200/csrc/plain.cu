@@ -484,6 +484,7 @@ k_tiny_rref(int32_t n, int32_t m, const uint32_t* __restrict__ D, int64_t ld,
         const int r = (int)(t / m), c = (int)(t % m);
         T[(size_t)r * tld + c] = D[(size_t)r * ld + c];
     }
+    __syncthreads();  // the lead entries below were loaded by other threads
     for (int r = tid; r < n; r += blockDim.x) {
         const int l = lead_in[r] < 0 ? INT_MAX : lead_in[r];
         lead[r] = l;

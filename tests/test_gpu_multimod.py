@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from gb_b200 import multimod
-from helpers import exact_answer, small_integer_matrix
+from tests.helpers import exact_answer, small_integer_matrix
 
 pytestmark = pytest.mark.gpu
 

@@ -64,6 +64,23 @@ def test_gpu_wide_matrix_global_accumulators():
         check_same(la.linear_algebra(m, form=form), want)
 
 
+def test_gpu_small_path_repeatable_on_wide_blocks():
+    """The one-CTA echelon of the small-matrix path on 100 x 300 right blocks
+    (several load passes per thread before the lead inverses are taken): every
+    run, single and batched, equals the oracle, for primes near 2^31 and 2^16."""
+    base = synth.integer_staircase(400, 100, 300, bound=1 << 6, dmin=0.02, dmax=0.05, seed=1)
+    primes = synth.largest_primes_below(1 << 31, 12) + synth.largest_primes_below(1 << 16, 4)
+    imgs = [synth.image_mod(base, p) for p in primes]
+    wants = [oracle.oracle_la(m)[0] for m in imgs]
+    for _ in range(3):
+        for m, want in zip(imgs, wants):
+            check_same(la.linear_algebra(m), want)
+        got, status = la.reduce_batch(imgs)
+        assert status == [0] * len(imgs)
+        for g, want in zip(got, wants):
+            check_same(g, want)
+
+
 @pytest.mark.parametrize("p", [251, 65521, 1000003, 2147483647])
 def test_gpu_blocked_many_rounds(p):
     # many C|D rows on few leads with a rank-deficient right block: several

@@ -8,7 +8,7 @@ import numpy as np
 
 import oracle
 from gb_b200 import multimod, synth
-from helpers import exact_answer, small_integer_matrix
+from tests.helpers import exact_answer, small_integer_matrix
 
 
 def oracle_answers(mat, primes):
