@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgbgpu.so")
+LIFT_LIB = os.path.join(HERE, "libgblift.so")  # host-only helper of gb_b200/multimod.py
 OBJDIR = os.path.join(REPO, "_build", "gbgpu")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -66,7 +67,20 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    build_lift(verbose=verbose, force=force)
     return LIB
+
+
+def build_lift(verbose: bool = False, force: bool = False) -> str:
+    """libgblift.so: the host-side Chinese remaindering of the multi-modular
+    driver (plain C++, g++)."""
+    src = os.path.join(CSRC, "lift.cpp")
+    if force or _stale(LIFT_LIB, [src]):
+        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", src, "-o", LIFT_LIB]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return LIFT_LIB
 
 
 if __name__ == "__main__":

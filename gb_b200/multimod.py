@@ -38,6 +38,7 @@ two bounded numbers.
 from __future__ import annotations
 
 import dataclasses
+import os
 from fractions import Fraction
 from math import gcd, isqrt
 from typing import Iterable, List, Optional, Sequence, Tuple
@@ -180,16 +181,20 @@ def lucky_pattern(answers: Sequence[ReducedRows]) -> Tuple[int, ...]:
     return min(pats, key=lambda t: (-len(t), t))
 
 
-def _dense(rows: ReducedRows, order: Sequence[int], col_index: dict) -> np.ndarray:
-    """Answer rows as a dense array over the union support (rows in the
-    order of their pivot columns ``order``)."""
-    out = np.zeros((len(order), len(col_index)), dtype=np.int64)
-    row_of = {int(rows.cols[rows.row_ptr[i]]): i for i in range(rows.np)}
-    for r, lead in enumerate(order):
-        i = row_of[lead]
-        a, b = int(rows.row_ptr[i]), int(rows.row_ptr[i + 1])
-        idx = [col_index[int(c)] for c in rows.cols[a:b]]
-        out[r, idx] = rows.vals[a:b]
+def _dense(rows: ReducedRows, order: Sequence[int], support: np.ndarray) -> np.ndarray:
+    """Answer rows as a dense array over the sorted column list ``support``
+    (which holds every column of the answer), rows in the order of their
+    pivot columns ``order``."""
+    out = np.zeros((len(order), support.shape[0]), dtype=np.int64)
+    if rows.np == 0:
+        return out
+    leads = rows.cols[rows.row_ptr[:-1]].astype(np.int64)
+    order_arr = np.asarray(order, dtype=np.int64)
+    # position of every answer row in `order` (descending leads)
+    pos = np.searchsorted(-order_arr, -leads)
+    nnz = rows.nnz
+    row_of_entry = np.repeat(pos, np.diff(rows.row_ptr))
+    out[row_of_entry, np.searchsorted(support, rows.cols[:nnz])] = rows.vals[:nnz]
     return out
 
 
@@ -209,45 +214,80 @@ def _ratrecon(x: int, m: int, bound: int) -> Optional[Tuple[int, int]]:
     return a, b
 
 
+_lift = None
+
+
+def _lift_lib():
+    """libgblift.so (built with the package; compiled here if missing)."""
+    global _lift
+    if _lift is None:
+        import ctypes as C
+        from . import build
+        if not os.path.exists(build.LIFT_LIB):
+            build.build_lift()
+        lib = C.CDLL(build.LIFT_LIB)
+        lib.gblift_crt_add.argtypes = [C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                       C.c_void_p, C.c_uint32, C.c_uint32]
+        lib.gblift_crt_add.restype = C.c_int
+        _lift = lib
+    return _lift
+
+
 class Lifter:
     """Incremental Chinese remaindering of the answers of one pivot pattern:
     the residues of every entry (dense over the union of the answers'
-    columns) as one integer in [0, M), M the product of the primes added."""
+    columns) as one integer in [0, M), M the product of the primes added,
+    held as little-endian 64-bit limbs and updated by libgblift.so
+    (x <- x + M ((r - x) M^-1 mod p))."""
 
     def __init__(self, answer: ReducedRows, p: int):
         self.pattern = _pattern(answer)
         self.order = sorted(self.pattern, reverse=True)  # answer rows: descending lead
-        self.support: List[int] = []
-        self.col_index: dict = {}
-        self.x = np.zeros((len(self.order), 0), dtype=object)
+        self.support = np.zeros(0, dtype=np.int64)  # sorted columns of the entries
+        self.nl = 4  # limbs per entry
+        self.x = np.zeros((len(self.order), 0, self.nl), dtype=np.uint64)
         self.m = 1
         self.primes: List[int] = []
         self.hard: Optional[Tuple[int, int]] = None  # the entry that failed to lift last
         self.add(answer, p)
 
     def _grow(self, answer: ReducedRows) -> None:
-        new = sorted({int(c) for c in answer.cols[: answer.nnz]} - set(self.col_index))
-        if not new:
+        cols = np.unique(answer.cols[: answer.nnz].astype(np.int64))
+        new = np.setdiff1d(cols, self.support, assume_unique=True)
+        if new.shape[0] == 0:
             return
         # a column no earlier answer had is 0 modulo every earlier prime
-        self.support = sorted(self.support + new)
-        self.col_index = {c: k for k, c in enumerate(self.support)}
-        old = self.x
-        self.x = np.zeros((len(self.order), len(self.support)), dtype=object)
-        self.x[...] = 0
-        if old.shape[1]:
-            keep = [self.col_index[c] for c in sorted(set(self.support) - set(new))]
-            self.x[:, keep] = old
+        support = np.union1d(self.support, new)
+        keep = np.searchsorted(support, self.support)
+        x = np.zeros((len(self.order), support.shape[0], self.nl), dtype=np.uint64)
+        x[:, keep, :] = self.x
+        self.support, self.x = support, x
 
     def add(self, answer: ReducedRows, p: int) -> None:
         """x <- the integer in [0, M p) that is x mod M and the answer mod p."""
         self._grow(answer)
-        r = _dense(answer, self.order, self.col_index)
-        xm = (self.x % p).astype(np.int64) if self.x.size else np.zeros(r.shape, dtype=np.int64)
-        t = ((r - xm) % p) * pow(self.m % p, p - 2, p) % p
-        self.x = self.x + t.astype(object) * self.m
+        r = np.ascontiguousarray(_dense(answer, self.order, self.support), dtype=np.int64)
+        m_len = max(1, (self.m.bit_length() + 63) // 64)
+        if m_len + 1 > self.nl:  # room for M p
+            x = np.zeros(self.x.shape[:2] + (2 * self.nl,), dtype=np.uint64)
+            x[:, :, : self.nl] = self.x
+            self.x, self.nl = x, 2 * self.nl
+        mlimbs = np.frombuffer(self.m.to_bytes(8 * m_len, "little"), dtype=np.uint64).copy()
+        n = int(r.size)
+        if n:
+            rc = _lift_lib().gblift_crt_add(n, self.nl, self.x.ctypes.data, mlimbs.ctypes.data,
+                                            m_len, r.ctypes.data, p,
+                                            pow(self.m % p, p - 2, p))
+            if rc != 0:
+                raise RuntimeError("gblift_crt_add rejected its arguments")
         self.m *= p
         self.primes.append(p)
+
+    def _row_values(self, r: int) -> List[int]:
+        raw = self.x[r].tobytes()
+        w = 8 * self.nl
+        return [int.from_bytes(raw[k * w:(k + 1) * w], "little")
+                for k in range(self.support.shape[0])]
 
     def lift(self) -> Optional[RationalRows]:
         """Rational reconstruction of every entry, or None when some entry has
@@ -258,21 +298,25 @@ class Lifter:
         symmetric range with |y| <= sqrt(M/2) and y = d x (mod M) after
         cancelling is the reconstruction (it is unique within those bounds),
         at the cost of one multiplication; only the others run the extended
-        Euclid.  The entry that failed last time is tried first."""
+        Euclid.  The entry that failed last time is tried first, then the
+        rows from the last."""
         m = self.m
         bound = _isqrt((m - 1) // 2)
         half = m // 2
-        nrows, ncols = self.x.shape
+        nrows, ncols = len(self.order), int(self.support.shape[0])
         if self.hard is not None and self.hard[0] < nrows and self.hard[1] < ncols:
-            v = int(self.x[self.hard])
+            v = int.from_bytes(self.x[self.hard].tobytes(), "little")
             if v and _ratrecon(v, m, bound) is None:
                 return None
-        ptr = [0]
-        cols, num, den = [], [], []
+        # the last rows (smallest leads) carry the largest fractions: they go
+        # first, so that a lift that needs more primes stops early
+        per_row: List[Tuple[List[int], List[int], List[int]]] = [([], [], [])] * nrows
         d = 1
-        for r in range(nrows):
+        for r in range(nrows - 1, -1, -1):
+            xs = self._row_values(r)
+            rc, rn, rd = [], [], []
             for k in range(ncols):
-                v = int(self.x[r, k])
+                v = xs[k]
                 if v == 0:
                     continue
                 y = v * d % m
@@ -291,9 +335,16 @@ class Lifter:
                         return None
                     lcm = d // gcd(d, q[1]) * q[1]
                     d = lcm if lcm <= bound else q[1]
-                cols.append(self.support[k])
-                num.append(q[0])
-                den.append(q[1])
+                rc.append(int(self.support[k]))
+                rn.append(q[0])
+                rd.append(q[1])
+            per_row[r] = (rc, rn, rd)
+        ptr = [0]
+        cols, num, den = [], [], []
+        for rc, rn, rd in per_row:
+            cols += rc
+            num += rn
+            den += rd
             ptr.append(len(cols))
         return RationalRows(np.array(ptr, dtype=np.int64), np.array(cols, dtype=np.int32),
                             np.array(num, dtype=object), np.array(den, dtype=object),

@@ -8,6 +8,7 @@ import numpy as np
 
 import oracle
 from gb_b200 import multimod, synth
+from gb_b200.matrix import ReducedRows
 from tests.helpers import exact_answer, small_integer_matrix
 
 
@@ -120,3 +121,30 @@ def test_driver_loop_with_oracle_images(monkeypatch):
     for batch in (1, 2, 4):
         got = multimod.reduce_over_q(mat, batch=batch)
         assert got.fractions() == [[(2, Fraction(1))], [(1, Fraction(1))]]
+
+
+def test_native_crt_matches_python_integers():
+    """libgblift.so's x <- x + M ((r - x) M^-1 mod p) against Python integers,
+    across limb boundaries and with residues at both ends of [0, p)."""
+    rng = np.random.default_rng(5)
+    primes = synth.largest_primes_below(1 << 31, 12)
+    n = 257
+    want = [0] * n
+    lifter = None
+    m = 1
+    for k, p in enumerate(primes):
+        r = rng.integers(0, p, size=n)
+        r[:3] = [0, p - 1, 1]
+        ans = ReducedRows(np.arange(n + 1), np.arange(10, 10 + n), r.astype(np.int32))
+        # one answer row per entry keeps the pattern fixed: leads 10 .. 10 + n - 1
+        if lifter is None:
+            lifter = multimod.Lifter(ans, p)
+        else:
+            lifter.add(ans, p)
+        want = [w + m * (((int(ri) - w) * pow(m, -1, p)) % p) for w, ri in zip(want, r)]
+        m *= p
+        # answer row i (lead 10 + i) is row n - 1 - i of the lift (descending
+        # leads), its entry column i of the support
+        got = [int.from_bytes(lifter.x[n - 1 - i, i].tobytes(), "little") for i in range(n)]
+        assert got == want, f"after {k + 1} primes"
+    assert lifter.m == m and lifter.nl * 64 >= m.bit_length() + 64
