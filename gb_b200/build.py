@@ -76,7 +76,7 @@ def build_lift(verbose: bool = False, force: bool = False) -> str:
     driver (plain C++, g++)."""
     src = os.path.join(CSRC, "lift.cpp")
     if force or _stale(LIFT_LIB, [src]):
-        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", src, "-o", LIFT_LIB]
+        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", src, "-o", LIFT_LIB]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

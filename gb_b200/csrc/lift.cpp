@@ -13,31 +13,19 @@
 // reduction), so no limb needs a division.
 #include <stdint.h>
 
+#include <algorithm>
+#include <thread>
 #include <vector>
 
 namespace {
 
 uint64_t mod128(unsigned __int128 v, uint32_t p) { return (uint64_t)(v % p); }
 
-}  // namespace
-
-extern "C" {
-
-// x: n entries of nl limbs; m: M as m_len limbs (m_len + 1 <= nl, M < 2^(64 m_len));
-// r: n residues in [0, p); minv = M^-1 mod p.  Returns 0, or -1 when the
-// limbs cannot hold M p (nl too small) or an argument is out of range.
-int gblift_crt_add(int64_t n, int32_t nl, uint64_t* x, const uint64_t* m, int32_t m_len,
-                   const int64_t* r, uint32_t p, uint32_t minv) {
-    if (n < 0 || nl <= 0 || m_len < 1 || m_len + 1 > nl || p < 2) return -1;
-    // 2^(32 j) mod p for the 2 m_len + 2 halves an entry below M p can have
-    const int halves = 2 * (m_len + 1);
-    std::vector<uint64_t> pw(halves);
-    uint64_t w = 1 % p;
-    for (int j = 0; j < halves; ++j) {
-        pw[j] = w;
-        w = (w << 32) % p;
-    }
-    for (int64_t e = 0; e < n; ++e) {
+// entries [e0, e1) of gblift_crt_add
+void crt_add_range(int64_t e0, int64_t e1, int32_t nl, uint64_t* x, const uint64_t* m,
+                   int32_t m_len, const int64_t* r, uint32_t p, uint32_t minv,
+                   const uint64_t* pw) {
+    for (int64_t e = e0; e < e1; ++e) {
         uint64_t* xe = x + e * (int64_t)nl;
         unsigned __int128 acc = 0;
         for (int i = 0; i < m_len; ++i) {  // x < M: limbs at and above m_len are 0
@@ -59,6 +47,42 @@ int gblift_crt_add(int64_t n, int32_t nl, uint64_t* x, const uint64_t* m, int32_
             xe[i] = (uint64_t)v;
             carry = (uint64_t)(v >> 64);
         }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// x: n entries of nl limbs; m: M as m_len limbs (m_len + 1 <= nl, M < 2^(64 m_len));
+// r: n residues in [0, p); minv = M^-1 mod p.  Returns 0, or -1 when the
+// limbs cannot hold M p (nl too small) or an argument is out of range.
+int gblift_crt_add(int64_t n, int32_t nl, uint64_t* x, const uint64_t* m, int32_t m_len,
+                   const int64_t* r, uint32_t p, uint32_t minv) {
+    if (n < 0 || nl <= 0 || m_len < 1 || m_len + 1 > nl || p < 2) return -1;
+    // 2^(32 j) mod p for the 2 m_len + 2 halves an entry below M p can have
+    const int halves = 2 * (m_len + 1);
+    std::vector<uint64_t> pw(halves);
+    uint64_t w = 1 % p;
+    for (int j = 0; j < halves; ++j) {
+        pw[j] = w;
+        w = (w << 32) % p;
+    }
+    // entries split over the host's threads (each entry is independent)
+    const int64_t grain = 4096;
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t nt = std::min<int64_t>(hw, (n + grain - 1) / grain);
+    if (nt <= 1) {
+        crt_add_range(0, n, nl, x, m, m_len, r, p, minv, pw.data());
+    } else {
+        std::vector<std::thread> pool;
+        const int64_t per = (n + nt - 1) / nt;
+        for (int64_t t = 0; t < nt; ++t) {
+            const int64_t e0 = t * per, e1 = std::min(n, e0 + per);
+            if (e0 < e1)
+                pool.emplace_back(crt_add_range, e0, e1, nl, x, m, m_len, r, p, minv, pw.data());
+        }
+        for (auto& th : pool) th.join();
     }
     return 0;
 }

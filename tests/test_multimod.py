@@ -148,3 +148,25 @@ def test_native_crt_matches_python_integers():
         got = [int.from_bytes(lifter.x[n - 1 - i, i].tobytes(), "little") for i in range(n)]
         assert got == want, f"after {k + 1} primes"
     assert lifter.m == m and lifter.nl * 64 >= m.bit_length() + 64
+
+
+def test_native_crt_threads_over_many_entries():
+    """gblift_crt_add on 20000 entries (split over host threads) equals the
+    Python integer update, entry for entry."""
+    rng = np.random.default_rng(9)
+    lib = multimod._lift_lib()
+    n, nl = 20000, 4
+    x = np.zeros((n, nl), dtype=np.uint64)
+    want = [0] * n
+    m = 1
+    for p in synth.largest_primes_below(1 << 31, 5):
+        r = rng.integers(0, p, size=n).astype(np.int64)
+        m_len = max(1, (m.bit_length() + 63) // 64)
+        ml = np.frombuffer(m.to_bytes(8 * m_len, "little"), dtype=np.uint64).copy()
+        assert lib.gblift_crt_add(n, nl, x.ctypes.data, ml.ctypes.data, m_len, r.ctypes.data,
+                                  p, pow(m % p, p - 2, p)) == 0
+        want = [w + m * (((int(ri) - w) * pow(m, -1, p)) % p) for w, ri in zip(want, r)]
+        m *= p
+    got = [int.from_bytes(x[i].tobytes(), "little") for i in range(n)]
+    assert got == want
+    assert lib.gblift_crt_add(n, 1, x.ctypes.data, ml.ctypes.data, 1, r.ctypes.data, 7, 1) == -1
