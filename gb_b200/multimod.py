@@ -74,8 +74,9 @@ class IntegerMacaulay:
 @dataclasses.dataclass
 class RationalRows:
     """The answer over Q: ``np`` rows in CSR form (columns as in
-    :class:`ReducedRows`), entry k = num[k] / den[k] in lowest terms with
-    den[k] > 0.  Leads are 1."""
+    :class:`ReducedRows`), entry k = num[k] / den[k] with den[k] > 0.  The
+    entries of a row share denominators where they can, so a fraction need
+    not be in lowest terms (``fractions()`` reduces them).  Leads are 1."""
 
     row_ptr: np.ndarray  # int64 [np + 1]
     cols: np.ndarray  # int32 [nnz]
@@ -294,11 +295,11 @@ class Lifter:
         none yet (more primes needed).
 
         Entries of an echelon form mostly share their denominators, so every
-        entry first tries the last denominator found: y = x d mod M in the
-        symmetric range with |y| <= sqrt(M/2) and y = d x (mod M) after
-        cancelling is the reconstruction (it is unique within those bounds),
-        at the cost of one multiplication; only the others run the extended
-        Euclid.  The entry that failed last time is tried first, then the
+        entry first tries the denominators found so far (their lcm while it
+        stays within the bound): y = x d mod M in the symmetric range with
+        |y| <= sqrt(M/2) makes y/d the reconstruction (unique within those
+        bounds; kept over d, not reduced), at the cost of one multiplication;
+        only the others run the extended Euclid.  The entry that failed last time is tried first, then the
         rows from the last."""
         m = self.m
         bound = _isqrt((m - 1) // 2)
@@ -324,10 +325,10 @@ class Lifter:
                     y -= m
                 q = None
                 if -bound <= y <= bound:
-                    g = gcd(y, d)
-                    a, b = y // g, d // g
-                    if (b * v - a) % m == 0:
-                        q = (a, b)
+                    # y = d v (mod M) by construction, |y| and d within the
+                    # bounds: the same number as the reconstruction of v,
+                    # written over the shared denominator d
+                    q = (y, d)
                 if q is None:
                     q = _ratrecon(v, m, bound)
                     if q is None:
