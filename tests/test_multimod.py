@@ -170,3 +170,22 @@ def test_native_crt_threads_over_many_entries():
     got = [int.from_bytes(x[i].tobytes(), "little") for i in range(n)]
     assert got == want
     assert lib.gblift_crt_add(n, 1, x.ctypes.data, ml.ctypes.data, 1, r.ctypes.data, 7, 1) == -1
+
+
+def test_lifter_grows_its_columns_when_an_entry_vanishes_mod_p():
+    """An entry that is 0 modulo the first prime (absent from that answer) and
+    nonzero modulo the next ones is lifted from residue 0 at the first prime."""
+    primes = synth.largest_primes_below(1 << 31, 6)
+    frac = Fraction(primes[0] * 5, 7)  # vanishes modulo primes[0]
+    lifter = None
+    for p in primes:
+        v = frac.numerator * pow(frac.denominator, p - 2, p) % p
+        cols, vals = ([20, 21], [1, v]) if v else ([20], [1])
+        ans = ReducedRows(np.array([0, len(cols)]), np.array(cols), np.array(vals))
+        if lifter is None:
+            lifter = multimod.Lifter(ans, p)
+            assert list(lifter.support) == [20]
+        else:
+            lifter.add(ans, p)
+    assert list(lifter.support) == [20, 21]
+    assert lifter.lift().fractions() == [[(20, Fraction(1)), (21, frac)]]
