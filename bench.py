@@ -36,14 +36,13 @@ sys.path.insert(0, REPO)
 CONFIG = {"nru": 20000, "nrl": 5000, "ncr": 20000, "p": 65521, "dmin": 0.02, "dmax": 0.05,
           "seed": 1}
 METRIC = "GF(p) matrix reductions/s (20000x5000 A|B/C|D, 40000 cols, p=65521, bit-exact)"
-INT8_PEAK_TOPS = 3040.7  # torch._int_mm 8192^3 int8, best of 10, measured on this pool
-# DRAM traffic of the tensor-core GEMM on the staircase workload: ncu
-# dram__bytes_read.sum + dram__bytes_write.sum summed over the 82 k_tc_submul
-# launches of one reduction (4665.2 MB read + 651.8 MB written), per launch.
-# A one-pass metric capture of this exact workload; the kernel's traffic does
-# not depend on the clocks or the timing, so it is reported, not re-measured.
-GEMM_TRAFFIC_PER_LAUNCH = (4665.2e6 + 651.8e6) / 82
-GEMM_TRAFFIC_LAUNCHES = 82
+# DRAM traffic of the tensor-core GEMM per executed int8 operation, from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the k_tc_submul
+# launches of one reduction of a 0.5-scale copy of the workload; the line's
+# per-launch traffic scales it by the operations one launch executes here.
+GEMM_TRAFFIC_PER_OP = (4665.2e6 + 651.8e6) / 5.118e12
+GEMM_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the GEMM launches "
+                       "of one reduction, bytes per int8 op, times this run's ops per launch")
 UNIT = "matrices/s"
 
 
@@ -186,62 +185,66 @@ def algorithmic_bytes_schur(mat, work_entries: int, ncr: int) -> int:
     return rows_in + work_entries * (4 + cb) + int(lens.shape[0]) * ncr * 4
 
 
-def cpu_reference(mat, steps: int, budget_s: float = 20.0):
-    """The reference's own la (oracle/_ref, la option 1, all host threads) on
-    a bounded sample: all known pivots and a stride-selected subset of the
-    C|D rows.  Matrices/s is extrapolated linearly in the number of C|D rows
-    (the dense tail grows faster, so this favours the CPU)."""
+def reference_call(mat, threads: int):
+    """One call of the reference's own la (oracle/_ref, la option 1,
+    src/la_ff_32.c:1804) on the WHOLE matrix: (answer, seconds of the call,
+    as the reference's realtime() measures it around the la call)."""
     import oracle
-    threads = os.cpu_count() or 1
-    nrl = mat.nr - mat.ncl
-    frac = 0.01
-    # calibrate the sample so one call takes a few seconds
-    while True:
-        keep = np.arange(0, nrl, max(1, int(round(1 / frac))))
-        sub = mat.subset(keep)
-        _, secs = oracle.ref_la(sub, 1, nthreads=threads)
-        if secs > budget_s / max(steps, 1) / 4 or frac >= 1.0:
-            break
-        frac = min(1.0, frac * 2)
-    times = [secs]
-    for _ in range(max(steps, 1) - 1):
-        _, secs = oracle.ref_la(sub, 1, nthreads=threads)
-        times.append(secs)
-    t = statistics.median(times)
-    share = keep.shape[0] / nrl
-    out = {"value": share / t, "unit": UNIT, "cores": threads, "kind": "reference",
-           "sample": (f"reference la option 1 (oracle/_ref, {threads} OpenMP threads) on all "
-                      f"{mat.ncl} known pivots + {keep.shape[0]} of {nrl} C|D rows "
-                      f"(every {int(round(1 / frac))}th), median of {len(times)} calls "
-                      f"{t:.3f}s, extrapolated linearly to all {nrl} rows")}
-    # the same la on one thread, on a quarter of that sample (one call)
-    if threads > 1:
-        stride1 = 4 * max(1, int(round(1 / frac)))
-        keep1 = np.arange(0, nrl, stride1)
-        _, secs1 = oracle.ref_la(mat.subset(keep1), 1, nthreads=1)
-        out["one_thread"] = {
-            "value": (keep1.shape[0] / nrl) / secs1, "unit": UNIT, "cores": 1,
-            "sample": (f"all {mat.ncl} known pivots + {keep1.shape[0]} of {nrl} C|D rows "
-                       f"(every {stride1}th), one call {secs1:.3f}s, extrapolated linearly")}
-    return out
+    return oracle.ref_la(mat, 1, nthreads=threads)
+
+
+def cpu_baseline_full(mat, threads: int, secs: float):
+    """cpu_baseline entry of one full reference call that took `secs`."""
+    return {"value": 1.0 / secs, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": (f"the whole matrix ({mat.ncl} known pivots, {mat.nr - mat.ncl} C|D "
+                       f"rows), one call of the reference la option 1 (oracle/_ref, "
+                       f"{threads} OpenMP threads): {secs:.3f} s; nothing extrapolated")}
 
 
 def run_reference_arm(args):
+    """The reference's own CPU la, timed on this host's cores: every timed step
+    reduces the whole matrix (no sample, no extrapolation).  The warm-up steps
+    reduce every 25th C|D row only (their time is not used)."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
+    threads = os.cpu_count() or 1
     mat = make_matrix()
-    cb = cpu_reference(mat, args.steps)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+    nrl = mat.nr - mat.ncl
+    warm = mat.subset(np.arange(0, nrl, 25))
+    for _ in range(args.warmup):
+        reference_call(warm, threads)
+    secs = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        secs.append(reference_call(mat, threads)[1])
+    wall = time.perf_counter() - t0
+    total = float(sum(secs))
+    value = args.steps / total
+    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+          "sample": (f"the whole matrix every step ({mat.ncl} known pivots, {nrl} C|D rows), "
+                     f"reference la option 1 (oracle/_ref, {threads} OpenMP threads); "
+                     f"{args.steps} calls, {total:.1f} s; warm-up steps on every 25th C|D row")}
+    if args.one_thread and threads > 1:
+        s1 = reference_call(mat, 1)[1]
+        cb["one_thread"] = {"value": 1.0 / s1, "unit": UNIT, "cores": 1,
+                            "sample": f"the whole matrix, one call on one thread: {s1:.1f} s"}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": workload_name(), "la_option": 1,
-                       "l2": "input larger than L2"},
-            "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+            "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": config_dict(), "la_option": 1,
+            "cpu_baseline": cb, "wall_s_timed": wall,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def config_dict():
+    """The `config` object both arms print (identical, so the two lines name
+    the same workload)."""
+    return {"workload": workload_name(), "l2": "inputs (CSR ~230 MB) larger than L2; "
+                                               "no flush needed"}
 
 
 def main():
@@ -267,6 +270,8 @@ def main():
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
                     help="1: check the timed form's answer against the sparse-row form")
+    ap.add_argument("--one-thread", type=int, default=1,
+                    help="reference arm: also time one full call on one thread")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -328,8 +333,8 @@ def main():
         ref_plan.close()
 
     # ---- end to end through gbgpu_reduce with pinned host buffers ---------
-    e2e_s, h2d, d2h, e2e_out = (_e2e(lib, mat, args, local) if not args.no_e2e
-                                else (float("nan"), 0, 0, None))
+    e2e_s, h2d, d2h, e2e_out, e2e_steps = (_e2e(lib, mat, args, local) if not args.no_e2e
+                                           else (float("nan"), 0, 0, None, 0))
     e2e_ok = None
     if e2e_out is not None:
         (rp, cc, vv), npv, nnz, vb = e2e_out
@@ -358,29 +363,33 @@ def main():
         pst = prof.stats()
         prof.close()
         tops = pst["gemm_int8_ops"] / (pst["gemm_ms"] * 1e-3) / 1e12 if pst["gemm_ms"] else 0.0
+        peak, peak_src, peaks = _int8_peak()
+        n_l = max(pst["gemm_launches"], 1)
         roof = {"bound": "tensor", "kernel": "k_tc_submul", "achieved": tops,
-                "peak": INT8_PEAK_TOPS, "unit": "TOPS (int8)", "frac": tops / INT8_PEAK_TOPS,
-                "peak_source": "measured: torch._int_mm 8192^3 int8 on this pool (no int8 "
-                               "figure in MEASURED_PEAKS.json)",
-                "traffic": (GEMM_TRAFFIC_PER_LAUNCH
-                            if pst["gemm_launches"] == GEMM_TRAFFIC_LAUNCHES and args.scale == 1.0
-                            else None),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, bytes per "
-                                  "launch averaged over the GEMM launches of one reduction",
+                "peak": peak, "unit": "TOPS (int8)", "frac": tops / peak,
+                "peak_source": peak_src, "peaks_seen": peaks,
+                "traffic": (GEMM_TRAFFIC_PER_OP * pst["gemm_int8_ops"] / n_l
+                            if args.scale == 1.0 else None),
+                "traffic_source": GEMM_TRAFFIC_SOURCE,
                 "launches": pst["gemm_launches"],
                 "ms_all_launches": pst["gemm_ms"], "int8_ops_all_launches": pst["gemm_int8_ops"],
-                "avg_launch_ms": pst["gemm_ms"] / max(pst["gemm_launches"], 1)}
+                "avg_launch_ms": pst["gemm_ms"] / n_l}
+    cfg = config_dict()
+    if args.scale != 1.0:
+        cfg["scale"] = args.scale
+    if ws > 1:
+        cfg["parallelism"] = f"replicas x{ws}"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (mod p, exact)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8 limbs on the int8 tensor cores (s32 accumulation), u32 residues mod p",
         "data": "synthetic (seeded, gb_b200.synth.staircase)",
-        "config": {"workload": workload_name(),
-                   "form": {1: "plain", 2: "tensor", 3: "blocked-plain"}.get(form_used, "?"),
-                   "l2": "inputs (CSR ~230 MB) larger than L2; no flush needed",
-                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+        "config": cfg,
+        "form": {1: "plain", 2: "tensor", 3: "blocked-plain"}.get(form_used, "?"),
         "e2e": {"value": ws / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "answer_equals_device_answer": e2e_ok},
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                "answer_equals_device_answer": e2e_ok},
         "gpu_launches": int(launches),
         "roofline": roof,
         "stages_ms": {k: stats[k] for k in ("ms_classify", "ms_check", "ms_schur", "ms_echelon",
@@ -390,12 +399,17 @@ def main():
         "verified_against_plain_form": verified,
     }
     line["clocks"] = clk.summary()
-    if args.scale != 1.0:
-        line["config"]["scale"] = args.scale
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu and args.scale == 1.0:
+        # the reference's la on the whole matrix, once, outside the timed
+        # region: its answer checks the GPU's bit for bit, its time is the
+        # CPU baseline
+        threads = os.cpu_count() or 1
         try:
-            line["cpu_baseline"] = cpu_reference(mat, 3)
+            ref_ans, secs = reference_call(mat, threads)
+            line["verified_against_reference"] = bool(ref_ans.equals(answer))
+            line["cpu_baseline"] = cpu_baseline_full(mat, threads, secs)
         except Exception as e:  # reference build absent on this host
+            line["verified_against_reference"] = None
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {e}"}
     if rank == 0:
@@ -409,7 +423,7 @@ def _e2e(lib, mat, args, device):
     gbgpu_plan_create (H2D of the CSR from pinned host memory),
     gbgpu_plan_run_into_v (the reduction, with the D2H of the answer into pinned
     host memory overlapping its back substitution), gbgpu_plan_destroy -- all
-    inside the timed region, every step.  Values
+    inside the timed region, every one of the `steps` steps.  Values
     travel at the reference's own coefficient width (cf_8 / cf_16 / cf_32:
     1, 2 or 4 bytes).  Returns (seconds per step, H2D bytes, D2H bytes)."""
     import torch
@@ -448,7 +462,7 @@ def _e2e(lib, mat, args, device):
             torch.empty(max(nnz, 1), dtype=tdt).pin_memory())
     one(bufs)  # warm
     torch.cuda.synchronize()
-    steps = max(2, min(args.steps, 5))
+    steps = max(1, args.steps)
     t0 = time.perf_counter()
     for _ in range(steps):
         one(bufs)
@@ -456,7 +470,7 @@ def _e2e(lib, mat, args, device):
     h2d = mat.row_ptr.nbytes + mat.cols.nbytes + mat.nnz * vb
     d2h = (npv + 1) * 8 + nnz * (4 + vb)
     # the answer that crossed the bus is the device answer
-    return e2e_s, h2d, d2h, (bufs, npv, nnz, vb)
+    return e2e_s, h2d, d2h, (bufs, npv, nnz, vb), steps
 
 
 def run_dense(args):
@@ -535,14 +549,15 @@ def run_dense(args):
 
     ms_t = timed(_lib.FORM_TENSOR, args.steps)
     ops = 2.0 * n ** 3
+    peak8, peak8_src, _ = _int8_peak()
     line = {"metric": "exact modular GEMM throughput (D - A B mod p)", "value": ops / ms_t / 1e9,
             "unit": "modular TOPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": f"u32 residues, {L} u8 limbs", "data": "synthetic",
             "config": {"workload": f"dense GEMM n={n} p={p}", "limbs": L},
             "roofline": {"bound": "tensor", "achieved": L * L * ops / ms_t / 1e9,
-                         "peak": INT8_PEAK_TOPS, "unit": "TOPS",
-                         "frac": L * L * ops / ms_t / 1e9 / INT8_PEAK_TOPS}}
+                         "peak": peak8, "unit": "TOPS", "peak_source": peak8_src,
+                         "frac": L * L * ops / ms_t / 1e9 / peak8}}
     if n <= 8192:
         ms_p = timed(_lib.FORM_PLAIN, 1)
         line["plain_ms"] = ms_p
@@ -748,6 +763,44 @@ def _peaks():
             return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def _int8_peak():
+    """The int8 tensor peak the GEMM roofline divides by: the larger of
+    (a) torch._int_mm on 8192^3 int8 (cuBLAS), timed here with CUDA events,
+    best of 10 after warm-up, and (b) twice the dense bf16 burst figure of
+    MEASURED_PEAKS.json (the sm_100 int8 rate is twice bf16), when present.
+    Taking the larger keeps the fraction conservative."""
+    import torch
+    seen = {}
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = float("inf")
+        for _ in range(10):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        seen["int_mm_8192"] = 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+        del a, b
+    except Exception:  # no int8 GEMM in this torch build
+        pass
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            seen["2x_bf16_burst"] = 2.0 * float(json.load(fh)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        pass
+    if not seen:
+        return 3362.6, "fallback (2 x 1681 bf16 TFLOP/s)", seen
+    key = max(seen, key=seen.get)
+    src = {"int_mm_8192": "measured in this run: torch._int_mm 8192^3 int8, best of 10",
+           "2x_bf16_burst": "2 x bf16_tflops of MEASURED_PEAKS.json"}[key]
+    return seen[key], src, seen
 
 
 if __name__ == "__main__":

@@ -1,25 +1,26 @@
 // noalloc.cu -- the one entry point of libgbgpu.so that allocates nothing.
 //
-// Some callers cannot allocate device memory once they are running: code
-// that runs inside a stream capture or under a memory budget fixed in
-// advance, or a host program that hands the library pointers into a pool it
-// manages itself and forbids any other cudaMalloc / cudaFree.  For them,
-// gbgpu_dense_submul_noalloc performs the same exact modular GEMM as
-// gbgpu_dense_submul (tensor-core form) but takes its scratch memory -- the
-// 8-bit limb planes of A and B and the kernel's status word -- from one
+// Some callers cannot allocate device memory once they are running: a
+// service that reserves its whole device-memory budget at start-up and must
+// not exceed it later, or a host program that hands the library pointers
+// into a pool it manages itself and forbids any other cudaMalloc / cudaFree
+// (a second allocator in the process would fragment or overrun its pool).
+// For them, gbgpu_dense_submul_noalloc performs the same exact modular GEMM
+// as gbgpu_dense_submul (tensor-core form) but takes its scratch memory --
+// the 8-bit limb planes of A and B and the kernel's status word -- from one
 // file-scope device array of kNoAllocScratchBytes bytes instead of
 // allocating it.
 //
 // The array lives on every GPU that loads the library, from load until the
 // process exits.  In host code its name is only a host-side stand-in, never
-// a device address, so its device address is looked up once per device with
-// cudaGetSymbolAddress (with that device current) the first time the entry
-// point runs on it, and cached.  That first call should therefore come before
-// any stream capture.  All calls share the one array and it keeps the last
-// call's contents: the status word is cleared by every call, the limb planes
-// are fully rewritten (zero padding included).  Calls that overlap on the GPU
-// (different streams or threads) race on it and must be serialised by the
-// caller.
+// a device address, so its device address is looked up with
+// cudaGetSymbolAddress (with that device current) by the first call on each
+// device, and cached for the life of the process; calls on a device after a
+// cudaDeviceReset of it are therefore not supported.  All calls share the
+// one array and it keeps the last call's contents: the status word is
+// cleared by every call, the limb planes are fully rewritten (zero padding
+// included).  Calls that overlap on the GPU (different streams or threads)
+// race on it and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -179,3 +179,34 @@ def dense_lowrank(n_rows: int, n_cols: int, rank: int, p: int, seed: int = 0) ->
         hi = (L[:, k0:k0 + step] @ r_hi[k0:k0 + step, :]) % p
         out = (out + lo + ((hi << 16) % p)) % p
     return out
+
+
+def dense_block_macaulay(D: np.ndarray, p: int, laopt: int = 1) -> MacaulayMatrix:
+    """A Macaulay matrix whose answer is the reduced row echelon form of the
+    dense residue block ``D`` (r x m): r known pivots [e_i | 0] followed by r
+    rows [e_i | D_i] (lead i, coefficient 1).  Its Schur complement is D
+    itself, so a la call on it runs exactly the dense echelon and
+    interreduction of the D block (src/la_ff_32.c:1217 and :1181 for la option
+    1); the answer's columns are those of D shifted by r."""
+    D = np.asarray(D, dtype=np.int64)
+    r, m = D.shape
+    nz = D != 0
+    lens = nz.sum(axis=1).astype(np.int64)
+    ptr = np.zeros(2 * r + 1, dtype=np.int64)
+    ptr[1:r + 1] = np.arange(1, r + 1)
+    ptr[r + 1:] = r + np.cumsum(1 + lens)
+    nnz = int(ptr[-1])
+    cols = np.empty(nnz, dtype=np.int32)
+    vals = np.empty(nnz, dtype=np.int32)
+    cols[:r] = np.arange(r)
+    vals[:r] = 1
+    starts = ptr[r:2 * r]
+    cols[starts] = np.arange(r)
+    vals[starts] = 1
+    ri, ci = np.nonzero(nz)
+    # position of entry k of row i: starts[i] + 1 + (rank of k within row i)
+    within = np.arange(ri.shape[0]) - np.repeat(np.concatenate(([0], np.cumsum(lens)[:-1])), lens)
+    at = starts[ri] + 1 + within
+    cols[at] = r + ci
+    vals[at] = D[ri, ci]
+    return MacaulayMatrix(p, r, m, ptr, cols, vals, laopt)

@@ -266,19 +266,20 @@ int gbgpu_dense_rref(int32_t p, int32_t rows, int32_t cols, uint32_t *D,
                      int64_t ld, int32_t *rank, int32_t *piv_cols,
                      const gbgpu_options *opt);
 
-/* Allocation-free variant of gbgpu_dense_submul (tensor-core form, odd p):
- * for callers that may not call cudaMalloc / cudaFree once they run (inside
- * a stream capture, under a device-memory budget fixed in advance, or in a
- * host program whose allocator owns all device memory).  No counterpart in
- * the reference.  Its scratch (the 8-bit limb planes of A and B and a status
- * word) is one fixed 32 MiB device array inside the library, present on every
- * GPU that loads it until the process exits; requests whose limb planes need
- * more than 32 MiB - 256 bytes are rejected with GBGPU_ERANGE.  The first call
- * on a device looks the array's address up (cudaGetSymbolAddress), so make it
- * before any stream capture.  Calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller.  Device pointers; runs on
- * `stream` (NULL: legacy default stream) and returns when the result is
- * complete. */
+/* Allocation-free variant of gbgpu_dense_submul (tensor-core form, odd p),
+ * for callers that must not allocate device memory once they run: a service
+ * whose device-memory budget is reserved up front, or a host program whose
+ * own allocator owns all device memory and forbids other cudaMalloc /
+ * cudaFree calls.  No counterpart in the reference.  Its scratch (the 8-bit
+ * limb planes of A and B and a status word) is one fixed 32 MiB device array
+ * inside the library, present on every GPU that loads it until the process
+ * exits; requests whose limb planes need more than 32 MiB - 256 bytes are
+ * rejected with GBGPU_ERANGE.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) and caches it for the life of the
+ * process, so calls may not follow a cudaDeviceReset of that device.  Calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  Device pointers; runs on `stream` (NULL: legacy default
+ * stream), waits for it and returns when the result is complete. */
 int gbgpu_dense_submul_noalloc(int32_t p, int32_t M, int32_t N, int32_t K,
                                const uint32_t *A, int64_t lda,
                                const uint32_t *B, int64_t ldb, uint32_t *D,

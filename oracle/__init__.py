@@ -24,7 +24,7 @@ from gb_b200.matrix import MacaulayMatrix, ReducedRows
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgbref.so")
-# gb compiled with the integration recipe of INTEGRATION.md (linked to libgbgpu.so)
+# gb compiled with its two linear-algebra call sites rerouted to libgbgpu.so (linked to it)
 GB_GPU_SO = os.path.join(HERE, "_ref", "libgb_gpu.so")
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -217,7 +217,7 @@ def gb_gpu_available() -> bool:
 
 
 def gb_gpu_f4(case: dict):
-    """F4 of gb compiled with the INTEGRATION.md recipe: every linear-algebra
+    """F4 of gb compiled with the two-macro drop-in recipe: every linear-algebra
     call goes to libgbgpu.so.  Returns (lens, cfs, exps) of the basis."""
     global _gb_gpu
     if _gb_gpu is None:

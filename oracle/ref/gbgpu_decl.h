@@ -1,5 +1,6 @@
-/* Declarations force-included into gb's unity build for the integration
- * recipe of INTEGRATION.md: gb's own headers define mat_t / bs_t / stat_t, so
+/* Declarations force-included into gb's unity build when its two
+ * linear-algebra call sites are rerouted to libgbgpu.so by two -D macros:
+ * gb's own headers define mat_t / bs_t / stat_t, so
  * the GPU entry points are declared here with void pointers. */
 void gbgpu_linear_algebra(void *mat, const void *bs, void *st);
 void gbgpu_interreduce_matrix_rows(void *mat, void *bs, const void *st);

@@ -74,3 +74,40 @@ def exact_answer(mat: multimod.IntegerMacaulay):
 def small_integer_matrix(seed=1, bound=1 << 6):
     m = synth.integer_staircase(40, 15, 30, bound=bound, dmin=0.05, dmax=0.15, seed=seed)
     return multimod.IntegerMacaulay.from_matrix(m, vals=m.vals.astype(np.int64))
+
+
+def matvec_mod(M, x, p: int, chunk: int = 1024) -> np.ndarray:
+    """(M x) mod p exactly for residue matrices M (rows x n, any integer
+    dtype, entries < p < 2^31) and residue vectors x: every product is
+    reduced before the row sums (each < 2^62, sums of n < 2^32 of them stay
+    below 2^63)."""
+    M = np.asarray(M)
+    x = np.asarray(x, dtype=np.int64)
+    out = np.empty(M.shape[0], dtype=np.int64)
+    for r0 in range(0, M.shape[0], chunk):
+        blk = M[r0:r0 + chunk].astype(np.int64)
+        out[r0:r0 + chunk] = ((blk * x[None, :]) % p).sum(axis=1) % p
+    return out
+
+
+def vecmat_mod(a, B, p: int, chunk: int = 512) -> np.ndarray:
+    """(a B) mod p exactly for a residue vector a (K) and matrix B (K x N)."""
+    a = np.asarray(a, dtype=np.int64)
+    B = np.asarray(B)
+    out = np.zeros(B.shape[1], dtype=np.int64)
+    for k0 in range(0, B.shape[0], chunk):
+        blk = B[k0:k0 + chunk].astype(np.int64)
+        out = (out + ((blk * a[k0:k0 + chunk, None]) % p).sum(axis=0)) % p
+    return out
+
+
+def dense_rref_rows(R, rank: int, piv_cols, shift: int) -> ReducedRows:
+    """The first ``rank`` rows of a dense RREF (ascending pivots) as the
+    reference's answer rows: descending lead order, columns + ``shift``."""
+    R = np.asarray(R)[:rank][::-1]
+    nz = R != 0
+    lens = nz.sum(axis=1)
+    ptr = np.zeros(rank + 1, dtype=np.int64)
+    np.cumsum(lens, out=ptr[1:])
+    ri, ci = np.nonzero(nz)
+    return ReducedRows(ptr, (ci + shift).astype(np.int32), R[ri, ci].astype(np.int32))

@@ -105,7 +105,7 @@ def test_dense_lowrank_rank():
 
 @pytest.mark.skipif(not oracle.gb_gpu_available(), reason="integration build absent")
 def test_integration_recipe_build_links_to_library():
-    """The INTEGRATION.md recipe reroutes only the two call sites: the gb build
+    """The two-macro drop-in recipe reroutes only the two call sites: the gb build
     exports f4_julia and imports exactly the two GPU entry points."""
     out = subprocess.run(["nm", "-D", oracle.GB_GPU_SO], capture_output=True, text=True,
                          check=True).stdout

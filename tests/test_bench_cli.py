@@ -49,18 +49,27 @@ def test_clock_summary_reads_nvidia_smi_csv(tmp_path):
     assert out["reasons"] == ["hw_slowdown", "sw_power_cap"]
 
 
-def test_cpu_baseline_states_both_thread_counts():
+def test_reference_call_reduces_the_whole_matrix():
+    """The CPU baseline is one call of the reference la on the whole matrix:
+    its answer is the oracle's, and the baseline entry states the call's
+    time and thread count without extrapolating."""
     import oracle
     if not oracle.ref_available():
         pytest.skip("reference build absent")
     b = _bench()
     from gb_b200 import synth
     mat = synth.staircase(800, 200, 800, 65521, seed=3)
-    cb = b.cpu_reference(mat, 1, budget_s=0.5)
-    assert cb["kind"] == "reference" and cb["value"] > 0 and cb["cores"] >= 1
-    if cb["cores"] > 1:
-        one = cb["one_thread"]
-        assert one["cores"] == 1 and one["value"] > 0 and "C|D rows" in one["sample"]
+    ans, secs = b.reference_call(mat, 2)
+    assert secs > 0 and ans.equals(oracle.oracle_la(mat)[0])
+    cb = b.cpu_baseline_full(mat, 2, secs)
+    assert cb["kind"] == "reference" and cb["cores"] == 2
+    assert abs(cb["value"] - 1.0 / secs) < 1e-9 and "nothing extrapolated" in cb["sample"]
+
+
+def test_both_arms_print_the_same_config():
+    b = _bench()
+    cfg = b.config_dict()
+    assert cfg["workload"] == b.workload_name() and set(cfg) == {"workload", "l2"}
 
 
 def test_multimod_cpu_baseline_scales_the_sampled_images():

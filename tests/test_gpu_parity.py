@@ -205,7 +205,7 @@ def test_f4_with_gpu_linear_algebra_matches_golden(case):
 @pytest.mark.skipif(not oracle.gb_gpu_available(), reason="integration build absent")
 @pytest.mark.parametrize("case", f4_cases(), ids=[c["name"] for c in f4_cases()])
 def test_integration_recipe_build_matches_golden(case):
-    """gb compiled exactly as INTEGRATION.md describes (two -D macros, no source
+    """gb compiled with the two-macro drop-in recipe (two -D macros, no source
     edit, linked against libgbgpu.so) reproduces every golden basis."""
     lens, cfs, exps = oracle.gb_gpu_f4(case)
     exp = case["expected"]

@@ -135,3 +135,41 @@ def test_oracle_rejects_contract_violations():
         nopiv.validate()
     with pytest.raises(ValueError):
         oracle.oracle_la(nopiv, 1)
+
+
+def _rref_python(D, p):
+    """Gauss-Jordan over GF(p) in plain Python (small blocks only)."""
+    R = [list(map(int, row)) for row in D]
+    piv, r = [], 0
+    for c in range(len(R[0]) if R else 0):
+        k = next((i for i in range(r, len(R)) if R[i][c] % p), None)
+        if k is None:
+            continue
+        R[r], R[k] = R[k], R[r]
+        inv = pow(R[r][c], p - 2, p)
+        R[r] = [v * inv % p for v in R[r]]
+        for i in range(len(R)):
+            if i != r and R[i][c]:
+                f = R[i][c]
+                R[i] = [(a - f * b) % p for a, b in zip(R[i], R[r])]
+        piv.append(c)
+        r += 1
+    return np.array(R, dtype=np.int64), r, piv
+
+
+@pytest.mark.parametrize("p", [101, 65521, 2147483647])
+def test_dense_block_embedding_yields_the_rref(p):
+    """The Macaulay embedding of a dense block (used to run the reference's dense
+    echelon on D blocks) has the block's RREF as its answer, in the oracle and
+    in the reference build."""
+    from gb_b200 import synth
+    from helpers import dense_rref_rows
+    D = synth.dense_lowrank(24, 30, 17, p, seed=4)
+    R, rank, piv = _rref_python(D, p)
+    want = dense_rref_rows(R, rank, piv, 24)
+    m = synth.dense_block_macaulay(D, p)
+    got, _ = oracle.oracle_la(m)
+    assert rank == 17 and got.equals(want), got.first_difference(want)
+    if oracle.ref_available():
+        ref, _ = oracle.ref_la(m, 1, nthreads=2)
+        assert ref.equals(want)

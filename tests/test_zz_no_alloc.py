@@ -1,11 +1,11 @@
 """GPU test of gbgpu_dense_submul_noalloc, the entry point that allocates
-nothing (for callers that may not call cudaMalloc/cudaFree while they run:
-inside a stream capture, under a fixed device-memory budget, or behind a
-host allocator that owns all device memory).  It must return exactly what
-gbgpu_dense_submul returns on the same inputs, on two calls in a row (the
-second call reuses the fixed scratch array the first one left behind), and
-reject work larger than its fixed scratch.  The file name makes pytest collect
-it last."""
+nothing, for callers that must not call cudaMalloc/cudaFree once they run (a
+device-memory budget reserved up front, or a host allocator that owns all
+device memory).  It must return exactly what gbgpu_dense_submul returns on the
+same inputs, on two calls in a row (the second call reuses the fixed scratch
+array the first one left behind), leave the device's allocations as they were,
+and reject work larger than its fixed scratch.  The file name makes pytest
+collect it last."""
 import ctypes as C
 
 import numpy as np
@@ -24,6 +24,20 @@ def _device_mats(torch, p, M, N, K, seed):
     return mk(M, K), mk(K, N), mk(M, N)
 
 
+def _pool_used_bytes(device: int):
+    """Bytes in use in the device's default stream-ordered memory pool (the
+    pool cudaMallocAsync draws from), or None where cuda-python is absent."""
+    try:
+        from cuda.bindings import runtime as rt
+    except ImportError:
+        return None
+    err, pool = rt.cudaDeviceGetDefaultMemPool(device)
+    if err != rt.cudaError_t.cudaSuccess:
+        return None
+    err, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    return int(used) if err == rt.cudaError_t.cudaSuccess else None
+
+
 def test_noalloc_matches_allocating_entry_point_twice():
     torch = pytest.importorskip("torch")
     lib = _lib.load()
@@ -34,9 +48,18 @@ def test_noalloc_matches_allocating_entry_point_twice():
         _lib.check(lib.gbgpu_dense_submul(p, M, N, K, A.data_ptr(), K, B.data_ptr(), N,
                                           D_ref.data_ptr(), N, C.byref(opt)))
         D_new = D.clone()
+        torch.cuda.synchronize()
+        torch_before = torch.cuda.memory_allocated()
+        free_before = torch.cuda.mem_get_info()[0]
+        pool_before = _pool_used_bytes(0)
         _lib.check(lib.gbgpu_dense_submul_noalloc(p, M, N, K, A.data_ptr(), K, B.data_ptr(), N,
                                                   D_new.data_ptr(), N, 0, None))
         torch.cuda.synchronize()
+        # nothing was allocated: torch's allocator, the driver's free memory and
+        # the stream-ordered pool all read as before the call
+        assert torch.cuda.memory_allocated() == torch_before
+        assert torch.cuda.mem_get_info()[0] == free_before
+        assert _pool_used_bytes(0) == pool_before
         assert torch.equal(D_new, D_ref), f"call {call}: results differ"
         assert not torch.equal(D_new, D)  # the update did something
 
