@@ -21,6 +21,8 @@ name.  Every generator is a pure function of its arguments and seed
 """
 from __future__ import annotations
 
+import itertools
+
 import numpy as np
 
 from .matrix import MacaulayMatrix
@@ -210,3 +212,36 @@ def dense_block_macaulay(D: np.ndarray, p: int, laopt: int = 1) -> MacaulayMatri
     cols[at] = r + ci
     vals[at] = D[ri, ci]
     return MacaulayMatrix(p, r, m, ptr, cols, vals, laopt)
+
+
+def monomials_drl_desc(nvars: int, maxdeg: int):
+    """All exponent vectors of total degree <= maxdeg, in descending DRL order
+    (degree first, then the smaller exponent of the last differing variable
+    is larger, src/order.c:239-267) -- the term order gb's input expects."""
+    mons = [e for d in range(maxdeg + 1)
+            for e in itertools.product(range(d + 1), repeat=nvars) if sum(e) == d]
+    return sorted(mons, key=lambda e: (sum(e), tuple(-x for x in reversed(e))), reverse=True)
+
+
+def dense_system(nvars: int, ngens: int, maxdeg: int, p: int, seed: int):
+    """`ngens` polynomials in `nvars` variables, each with every monomial of
+    degree <= maxdeg and coefficients uniform in [1, p-1] (seeded), as gb's
+    f4_julia takes them: (term counts, coefficients, exponent vectors)."""
+    rng = np.random.default_rng(seed)
+    mons = monomials_drl_desc(nvars, maxdeg)
+    lens, cfs, exps = [], [], []
+    for _ in range(ngens):
+        lens.append(len(mons))
+        cfs += rng.integers(1, p, size=len(mons)).tolist()
+        for e in mons:
+            exps += list(e)
+    return lens, cfs, exps
+
+
+def f4_case(name: str, nvars: int, ngens: int, maxdeg: int, p: int, la_option: int,
+            seed: int, nr_threads: int = 1) -> dict:
+    """The f4_julia arguments of a dense system (DRL, no final reduction)."""
+    lens, cfs, exps = dense_system(nvars, ngens, maxdeg, p, seed)
+    return {"name": name, "nr_vars": nvars, "nr_gens": ngens, "ht_size": 12, "field_char": p,
+            "mon_order": 0, "nr_threads": nr_threads, "la_option": la_option, "reduce_gb": 0,
+            "max_nr_pairs": 0, "reset_hash_table": 0, "lens": lens, "cfs": cfs, "exps": exps}

@@ -23,6 +23,8 @@
  */
 #include <stddef.h>
 #include <stdint.h>
+#include <string.h>
+#include <unistd.h>
 
 struct mat_t;
 struct bs_t;
@@ -148,6 +150,109 @@ static void gbref_write_answer(FILE *f, const mat_t *mat, int ff_bits)
     gbref_write_rows(f, mat->r, np, gbref_mat_table(mat, ff_bits), ff_bits);
 }
 
+/* Comparison mode: every la call of an F4 run goes to an implementation
+ * under test (cmp_la, e.g. the GPU library's gbgpu_linear_algebra; NULL: the
+ * reference's own function again) AND, on a deep copy of the matrix, to the
+ * reference's own linear_algebra; the two answers are compared row by row
+ * (np, lengths, columns, coefficients) and one line per call goes to the log:
+ *   call K nr NR nc NC ncl NCL ncr NCR nrl NRL np NP ref_np RNP ref_s T gpu_s T equal E
+ * Once the reference calls have taken more than `budget_s` seconds in total
+ * the process ends (_exit(0)) right after logging, so that a large F4 run is
+ * compared round by round up to a fixed CPU budget. */
+static void gbref_free_mat_output(mat_t *mat, int ff_bits, int32_t np);
+static int gbref_cmp_on = 0;
+static gbref_la_fn gbref_cmp_la = NULL;
+static double gbref_cmp_budget = 0.0;
+static double gbref_cmp_spent = 0.0;
+static int64_t gbref_cmp_calls = 0;
+static FILE *gbref_cmp_log = NULL;
+
+int gbref_set_compare(void *cmp_la, double budget_s, const char *log_path)
+{
+    if (gbref_cmp_log) {
+        fclose(gbref_cmp_log);
+        gbref_cmp_log = NULL;
+    }
+    gbref_cmp_on = 0;
+    if (log_path == NULL || log_path[0] == '\0') return 0;
+    gbref_cmp_log = fopen(log_path, "w");
+    if (!gbref_cmp_log) return -1;
+    gbref_cmp_la = (gbref_la_fn)cmp_la;
+    gbref_cmp_budget = budget_s;
+    gbref_cmp_spent = 0.0;
+    gbref_cmp_calls = 0;
+    gbref_cmp_on = 1;
+    return 0;
+}
+
+static mat_t *gbref_copy_mat(const mat_t *mat)
+{
+    int32_t i;
+    mat_t *c = (mat_t *)malloc(sizeof(mat_t));
+    *c = *mat;
+    c->r = (hm_t **)malloc((size_t)(mat->nr > 0 ? mat->nr : 1) * sizeof(hm_t *));
+    for (i = 0; i < mat->nr; ++i) {
+        const size_t n = (size_t)mat->r[i][2] + 3;
+        c->r[i] = (hm_t *)malloc(n * sizeof(hm_t));
+        memcpy(c->r[i], mat->r[i], n * sizeof(hm_t));
+    }
+    c->cf_8 = NULL;
+    c->cf_16 = NULL;
+    c->cf_32 = NULL;
+    c->cf_qq = NULL;
+    c->cf_ab_qq = NULL;
+    return c;
+}
+
+static int gbref_same_answer(const mat_t *a, const mat_t *b, int ff_bits)
+{
+    int32_t i, j;
+    void *const *ta = gbref_mat_table(a, ff_bits);
+    void *const *tb = gbref_mat_table(b, ff_bits);
+    if (a->np != b->np) return 0;
+    for (i = 0; i < a->np; ++i) {
+        const hm_t *ra = a->r[i], *rb = b->r[i];
+        if (ra[2] != rb[2]) return 0;
+        for (j = 0; j < ra[2]; ++j) {
+            if (ra[3 + j] != rb[3 + j]) return 0;
+            if (gbref_cf(ta, ff_bits, ra[0], j) != gbref_cf(tb, ff_bits, rb[0], j)) return 0;
+        }
+    }
+    return 1;
+}
+
+static void gbref_compare_call(mat_t *mat, const bs_t *bs, stat_t *st)
+{
+    mat_t *ref = gbref_copy_mat(mat);
+    stat_t st_ref = *st;
+    const int32_t nr = mat->nr, nc = mat->nc, ncl = mat->ncl, ncr = mat->ncr,
+                  nrl = mat->nrl;
+    double t0 = realtime();
+    (linear_algebra)(ref, bs, &st_ref);
+    double t1 = realtime();
+    if (gbref_cmp_la) {
+        gbref_cmp_la(mat, bs, st);
+    } else {
+        (linear_algebra)(mat, bs, st);
+    }
+    double t2 = realtime();
+    const int eq = gbref_same_answer(mat, ref, st->ff_bits);
+    gbref_cmp_spent += t1 - t0;
+    fprintf(gbref_cmp_log,
+            "call %lld nr %d nc %d ncl %d ncr %d nrl %d np %d ref_np %d ref_s %.6f "
+            "gpu_s %.6f equal %d\n",
+            (long long)gbref_cmp_calls++, nr, nc, ncl, ncr, nrl, mat->np, ref->np, t1 - t0,
+            t2 - t1, eq);
+    fflush(gbref_cmp_log);
+    gbref_free_mat_output(ref, st->ff_bits, ref->np);
+    free(ref);
+    if (gbref_cmp_budget > 0.0 && gbref_cmp_spent > gbref_cmp_budget) {
+        fprintf(gbref_cmp_log, "stop budget %.3f\n", gbref_cmp_spent);
+        fclose(gbref_cmp_log);
+        _exit(0);
+    }
+}
+
 void gbref_hook_linear_algebra(struct mat_t *mat, const struct bs_t *bs,
                                struct stat_t *st)
 {
@@ -161,7 +266,9 @@ void gbref_hook_linear_algebra(struct mat_t *mat, const struct bs_t *bs,
         }
     }
     double t0 = realtime();
-    if (gbref_ext_la) {
+    if (gbref_cmp_on) {
+        gbref_compare_call(mat, bs, st);
+    } else if (gbref_ext_la) {
         gbref_ext_la(mat, bs, st);
     } else {
         (linear_algebra)(mat, bs, st);

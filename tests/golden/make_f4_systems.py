@@ -21,40 +21,17 @@ in [1, p-1], terms in descending DRL order as gb's input expects):
 from __future__ import annotations
 
 import glob
-import itertools
 import json
 import os
 import sys
 import tempfile
-
-import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 import oracle  # noqa: E402
 from gb_b200.matrix import Capture, read_gbm, save_captures  # noqa: E402
-
-
-def monomials_drl_desc(nvars: int, maxdeg: int):
-    """All exponent vectors of total degree <= maxdeg, in descending DRL order
-    (degree first, then the smaller exponent of the last differing variable
-    is larger, src/order.c:239-267)."""
-    mons = [e for d in range(maxdeg + 1)
-            for e in itertools.product(range(d + 1), repeat=nvars) if sum(e) == d]
-    return sorted(mons, key=lambda e: (sum(e), tuple(-x for x in reversed(e))), reverse=True)
-
-
-def dense_system(nvars: int, ngens: int, maxdeg: int, p: int, seed: int):
-    rng = np.random.default_rng(seed)
-    mons = monomials_drl_desc(nvars, maxdeg)
-    lens, cfs, exps = [], [], []
-    for _ in range(ngens):
-        lens.append(len(mons))
-        cfs += rng.integers(1, p, size=len(mons)).tolist()
-        for e in mons:
-            exps += list(e)
-    return lens, cfs, exps
+from gb_b200.synth import f4_case  # noqa: E402
 
 
 SYSTEMS = [
@@ -68,12 +45,8 @@ def main() -> None:
     os.makedirs(os.path.join(HERE, "f4"), exist_ok=True)
     os.makedirs(os.path.join(HERE, "mats"), exist_ok=True)
     for sysdef in SYSTEMS:
-        lens, cfs, exps = dense_system(sysdef["nvars"], sysdef["ngens"], sysdef["maxdeg"],
-                                       sysdef["p"], sysdef["seed"])
-        case = {"name": sysdef["name"], "nr_vars": sysdef["nvars"], "nr_gens": sysdef["ngens"],
-                "ht_size": 12, "field_char": sysdef["p"], "mon_order": 0, "nr_threads": 1,
-                "la_option": sysdef["la_option"], "reduce_gb": 0, "max_nr_pairs": 0,
-                "reset_hash_table": 0, "lens": lens, "cfs": cfs, "exps": exps}
+        case = f4_case(sysdef["name"], sysdef["nvars"], sysdef["ngens"], sysdef["maxdeg"],
+                       sysdef["p"], sysdef["la_option"], sysdef["seed"])
         with tempfile.TemporaryDirectory() as cap:
             blen, bcf, bexp = oracle.ref_f4(case, capture_dir=cap)
             caps = []

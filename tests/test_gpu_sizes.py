@@ -94,3 +94,29 @@ def test_dense_rref_8192_matches_reference(p):
     want, _ = oracle.ref_la(synth.dense_block_macaulay(D0, p), 1, nthreads=THREADS)
     assert rank.value == want.np == r
     assert got.equals(want), got.first_difference(want)
+
+
+@needs_ref
+def test_f4_dense_cubic_10_p31_every_la_call_matches_reference(tmp_path):
+    """F4 on the dense cubic system in 10 variables (10 polynomials, all 286
+    monomials of degree <= 3, p = 2^31 - 1, la option 1) with gb's own host
+    code: every la call (src/f4.c:306) goes to libgbgpu.so and, on a copy of
+    the matrix, to the reference la; the answers must agree bit for bit.  The
+    run is compared round by round until the reference calls have used 40 s
+    (the reference cannot finish this system); the largest matrix reached is
+    checked to be at least 40000 rows (round 8: 42358 x 72876 with this seed)."""
+    import subprocess
+    import sys
+    from oracle.f4_compare import parse_log
+    log = tmp_path / "calls.log"
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run([sys.executable, "-m", "oracle.f4_compare", "--nvars", "10", "--ngens", "10",
+                    "--maxdeg", "3", "--p", "2147483647", "--la-option", "1", "--seed", "10",
+                    "--budget", "40", "--log", str(log), "--impl", "gpu"],
+                   check=True, cwd=repo, timeout=1500)
+    res = parse_log(str(log))
+    calls = res["calls"]
+    assert calls, res
+    bad = [c for c in calls if not c["equal"]]
+    assert not bad, bad
+    assert max(c["nr"] for c in calls) >= 40000, calls

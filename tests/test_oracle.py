@@ -8,6 +8,8 @@
   reference build, and the oracle agrees with the reference build on seeded
   synthetic matrices (when oracle/_ref was built here).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -173,3 +175,30 @@ def test_dense_block_embedding_yields_the_rref(p):
     if oracle.ref_available():
         ref, _ = oracle.ref_la(m, 1, nthreads=2)
         assert ref.equals(want)
+
+
+def test_f4_compare_harness_self_check_and_budget(tmp_path):
+    """The round-by-round comparison harness (oracle/f4_compare.py, the
+    reference hook's compare mode): comparing the reference with itself logs
+    every la call as equal, and a budget stops the run after the call that
+    exceeds it."""
+    import subprocess
+    import sys
+    from oracle.f4_compare import parse_log
+    if not oracle.ref_available():
+        pytest.skip("reference build absent")
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    args = [sys.executable, "-m", "oracle.f4_compare", "--nvars", "4", "--ngens", "4",
+            "--maxdeg", "3", "--p", "65521", "--la-option", "2", "--seed", "3",
+            "--impl", "reference", "--threads", "2"]
+    full = tmp_path / "full.log"
+    subprocess.run(args + ["--budget", "1000", "--log", str(full)], check=True, cwd=repo,
+                   timeout=300)
+    res = parse_log(str(full))
+    assert res["end"] == "done" and len(res["calls"]) >= 5
+    assert all(c["equal"] == 1 and c["np"] == c["ref_np"] for c in res["calls"])
+    cut = tmp_path / "cut.log"
+    subprocess.run(args + ["--budget", "1e-9", "--log", str(cut)], check=True, cwd=repo,
+                   timeout=300)
+    res = parse_log(str(cut))
+    assert len(res["calls"]) == 1 and res["end"].startswith("stop budget")
