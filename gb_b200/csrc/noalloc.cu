@@ -12,7 +12,9 @@
 // allocating it.
 //
 // The array lives on every GPU that loads the library, from load until the
-// process exits.  In host code its name is only a host-side stand-in, never
+// process exits; the CUDA driver sets its memory aside when it loads the
+// library's device code on that GPU (with lazy module loading, during the
+// first call that needs it), not this entry point.  In host code its name is only a host-side stand-in, never
 // a device address, so its device address is looked up with
 // cudaGetSymbolAddress (with that device current) by the first call on each
 // device, and cached for the life of the process; calls on a device after a

@@ -15,6 +15,8 @@ from gb_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 
+SCRATCH_BYTES = 32 << 20  # the library's fixed scratch array
+
 
 def _device_mats(torch, p, M, N, K, seed):
     g = torch.Generator(device="cuda")
@@ -55,11 +57,18 @@ def test_noalloc_matches_allocating_entry_point_twice():
         _lib.check(lib.gbgpu_dense_submul_noalloc(p, M, N, K, A.data_ptr(), K, B.data_ptr(), N,
                                                   D_new.data_ptr(), N, 0, None))
         torch.cuda.synchronize()
-        # nothing was allocated: torch's allocator, the driver's free memory and
-        # the stream-ordered pool all read as before the call
+        # nothing was allocated: torch's allocator and the stream-ordered pool
+        # read as before the call.  The driver's free memory may drop once, by
+        # at most the library's fixed 32 MiB scratch array, when the first call
+        # makes the driver load that array on this GPU (lazy module loading);
+        # after that it must not move.
         assert torch.cuda.memory_allocated() == torch_before
-        assert torch.cuda.mem_get_info()[0] == free_before
         assert _pool_used_bytes(0) == pool_before
+        drop = free_before - torch.cuda.mem_get_info()[0]
+        if call == 0:
+            assert 0 <= drop <= SCRATCH_BYTES + (2 << 20), drop
+        else:
+            assert drop == 0, drop
         assert torch.equal(D_new, D_ref), f"call {call}: results differ"
         assert not torch.equal(D_new, D)  # the update did something
 
