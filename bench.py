@@ -635,48 +635,60 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def run_f4_captures(args):
-    """The linear-algebra calls of F4 on the dense systems (reference-captured
-    matrices under tests/golden/mats): dense_quadratic_7 (7 quadratics in 7
-    variables, p = 32003, la option 2) and dense_cubic_5_p31 (5 cubics in 5
-    variables, p = 2^31 - 1, la option 1).  Each step reduces every captured
-    matrix of a system once through gbgpu_reduce (host CSR in, host rows out,
-    the call the drop-in makes); every answer is compared with the reference's
-    captured answer.  The CPU column is the reference's la on the same calls."""
-    from gb_b200 import _lib, la
-    from gb_b200.matrix import load_captures
-    _lib.load()
-    systems = {}
+def f4_systems_timing(steps: int, cpu: bool = True) -> dict:
+    """The la calls of F4 on the dense systems (tests/golden/f4: dense_quadratic_7,
+    7 quadratics in 7 variables over 32003, la option 2; dense_cubic_5_p31, 5
+    cubics in 5 variables over 2^31 - 1, la option 1), made by gb's own host
+    code (the reference build, src/f4.c:190) and timed where they happen: the
+    hook at src/f4.c:306 measures each call with the reference's realtime().
+    GPU: the hook calls gbgpu_linear_algebra (the drop-in, host rows in and
+    malloc'ed rows out); CPU: the reference's own la, with the case's thread
+    count.  Every run's basis is checked against the golden one."""
+    import oracle
+    from gb_b200 import la
+    lib = oracle._load_ref()
+    fn = la.function_address("gbgpu_linear_algebra")
+    out = {}
     for name in ("dense_quadratic_7", "dense_cubic_5_p31"):
-        caps = load_captures(os.path.join(REPO, "tests", "golden", "mats", name + ".npz"))
-        caps = [c for c in caps if c.kind == 0]
-        for c in caps:  # warm
-            la.linear_algebra(c.mat)
-        ts = []
-        for _ in range(max(1, args.steps)):
-            t0 = time.perf_counter()
-            for c in caps:
-                ans = la.linear_algebra(c.mat)
-                assert ans.equals(c.answer), name
-            ts.append(time.perf_counter() - t0)
-        entry = {"matrices": len(caps), "largest": max([c.mat.nr, c.mat.nc] for c in caps),
-                 "gpu_ms_per_system": statistics.median(ts) * 1e3}
-        if not args.no_cpu:
-            import oracle
-            threads = os.cpu_count() or 1
-            cpu = sum(oracle.ref_la(c.mat, c.mat.laopt, nthreads=threads)[1] for c in caps)
-            entry["cpu_reference_ms_per_system"] = cpu * 1e3
-            entry["cpu_threads"] = threads
-        systems[name] = entry
+        with open(os.path.join(REPO, "tests", "golden", "f4", name + ".json")) as fh:
+            case = json.load(fh)
+        exp = case["expected"]
+
+        def one(la_fn):
+            s0, c0 = lib.gbref_hook_seconds(), lib.gbref_hook_calls()
+            lens, cfs, exps = oracle.ref_f4(case, la_fn=la_fn)
+            ok = (lens.tolist() == exp["tlen"] and cfs.tolist() == exp["tcf"]
+                  and exps.tolist() == exp["texp"])
+            return lib.gbref_hook_seconds() - s0, lib.gbref_hook_calls() - c0, ok
+
+        one(fn)  # warm: library load, sessions, kernels
+        g = [one(fn) for _ in range(max(1, steps))]
+        entry = {"la_calls": g[0][1], "largest": case.get("max_matrix"),
+                 "gpu_ms_per_system": 1e3 * statistics.median(x[0] for x in g),
+                 "basis_equals_golden": all(x[2] for x in g)}
+        if cpu:
+            r = [one(None) for _ in range(max(1, steps))]
+            entry["cpu_reference_ms_per_system"] = 1e3 * statistics.median(x[0] for x in r)
+            entry["cpu_threads"] = case["nr_threads"]
+        out[name] = entry
+    return out
+
+
+def run_f4_captures(args):
+    """Config-1 style workload: the la calls of F4 on the dense systems, timed
+    at the call site (see f4_systems_timing)."""
+    from gb_b200 import _lib
+    _lib.load()
+    systems = f4_systems_timing(args.steps, cpu=not args.no_cpu)
     ms = sum(v["gpu_ms_per_system"] for v in systems.values())
-    n = sum(v["matrices"] for v in systems.values())
-    line = {"metric": "F4 linear-algebra calls/s (reference-captured dense systems, end to end)",
+    n = sum(v["la_calls"] for v in systems.values())
+    line = {"metric": "F4 linear-algebra calls/s (dense systems, at the src/f4.c:306 call site)",
             "value": n / (ms * 1e-3), "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
             "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 (mod p, exact)",
-            "data": "reference-captured F4 matrices (tests/golden/mats)",
-            "config": {"workload": "f4 captures: dense_quadratic_7 (p=32003) + "
-                                   "dense_cubic_5_p31 (p=2^31-1)", "systems": systems}}
+            "data": "dense systems of tests/golden/f4 (seeded coefficients)",
+            "config": {"workload": "f4: dense_quadratic_7 (p=32003, la 2) + "
+                                   "dense_cubic_5_p31 (p=2^31-1, la 1)", "systems": systems}}
     print(json.dumps(line), flush=True)
 
 

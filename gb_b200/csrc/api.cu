@@ -29,6 +29,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "kernels.h"
+#include "small.h"
 #include "tc_gemm.h"
 
 namespace gbgpu {
@@ -238,7 +239,7 @@ struct Plan {
     }
 };
 
-static int err_to_status(uint32_t bits, std::string* msg) {
+int err_to_status(uint32_t bits, std::string* msg) {
     if (!bits) return GBGPU_OK;
     std::string s = "input breaks the mat_t contract:";
     if (bits & kErrEmptyRow) s += " empty row;";
@@ -1056,9 +1057,66 @@ void gbgpu_plan_destroy(gbgpu_plan* plan) {
     delete plan;
 }
 
+// host CSR of a gbgpu_csr into the small path's staging (values widened)
+static void fill_from_csr(void* ctx, int64_t* row_ptr, int32_t* cols, uint32_t* vals) {
+    const gbgpu_csr* m = (const gbgpu_csr*)ctx;
+    const int64_t nnz = m->row_ptr[m->nr];
+    memcpy(row_ptr, m->row_ptr, sizeof(int64_t) * (size_t)(m->nr + 1));
+    memcpy(cols, m->cols, sizeof(int32_t) * (size_t)nnz);
+    const int vb = val_bytes_of(m);
+    if (vb == 4) {
+        memcpy(vals, m->vals, sizeof(int32_t) * (size_t)nnz);
+    } else if (vb == 2) {
+        const uint16_t* v = (const uint16_t*)m->vals;
+        for (int64_t k = 0; k < nnz; ++k) vals[k] = v[k];
+    } else {
+        const uint8_t* v = (const uint8_t*)m->vals;
+        for (int64_t k = 0; k < nnz; ++k) vals[k] = v[k];
+    }
+}
+
+// small matrices take the one-pass path of small.cu (AUTO or the sparse-row
+// form, library stream, no profiling); *handled tells whether it ran
+static int reduce_small(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows* out,
+                        bool* handled) {
+    *handled = false;
+    gbgpu_options o{};
+    if (opt) o = *opt;
+    if (!(o.form == GBGPU_FORM_AUTO || o.form == GBGPU_FORM_PLAIN) || o.stream || o.profile)
+        return GBGPU_OK;
+    if (!m || m->p < 2 || m->nr <= 0 || !m->row_ptr || !m->cols || !m->vals) return GBGPU_OK;
+    const int vb = val_bytes_of(m);
+    if (!(vb == 1 || vb == 2 || vb == 4) || (vb < 4 && (int64_t)m->p >= ((int64_t)1 << (8 * vb))))
+        return GBGPU_OK;
+    if (m->row_ptr[0] != 0 || m->row_ptr[m->nr] < 0) return GBGPU_OK;
+    if (!small_eligible(m->nr, m->ncl, m->ncr, o.device)) return GBGPU_OK;
+    *handled = true;
+    SmallInput in{m->p, m->nr, m->ncl, m->ncr, m->row_ptr[m->nr], o.device, fill_from_csr,
+                  (void*)m};
+    SmallAnswer a;
+    int rc = small_reduce(in, &a);
+    if (rc) return rc;
+    out->np = a.np;
+    out->nnz = a.nnz;
+    out->row_ptr = (int64_t*)malloc(sizeof(int64_t) * (size_t)(a.np + 1));
+    out->cols = (int32_t*)malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(a.nnz, 1));
+    out->vals = (int32_t*)malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(a.nnz, 1));
+    if (!out->row_ptr || !out->cols || !out->vals) {
+        gbgpu_rows_free(out);
+        return GBGPU_ENOMEM;
+    }
+    memcpy(out->row_ptr, a.offs, sizeof(int64_t) * (size_t)(a.np + 1));
+    memcpy(out->cols, a.cols, sizeof(int32_t) * (size_t)a.nnz);
+    memcpy(out->vals, a.vals, sizeof(int32_t) * (size_t)a.nnz);
+    return GBGPU_OK;
+}
+
 int gbgpu_reduce(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows* out) {
     if (!out) return GBGPU_EINVAL;
     memset(out, 0, sizeof(*out));
+    bool handled = false;
+    int rs = reduce_small(m, opt, out, &handled);
+    if (handled) return rs;
     Plan* P = nullptr;
     int rc = plan_create(m, opt, 0, &P);
     if (rc) return rc;

@@ -23,6 +23,7 @@
 
 #include "../../include/gbgpu.h"
 #include "internal.h"
+#include "small.h"
 
 using namespace gbgpu;
 
@@ -75,8 +76,10 @@ void gather_rows(gbgpu_hm_t* const* rows, int32_t nr, const void* const* tab, in
 }
 
 // CSR answer -> malloc'ed reference rows and coefficient arrays
-int store_rows(gbgpu_mat_t* mat, int bits, const gbgpu_rows& out) {
-    const int32_t np = out.np;
+int store_rows_raw(gbgpu_mat_t* mat, int bits, int32_t np, const int64_t* row_ptr,
+                   const int32_t* ocols, const int32_t* ovals) {
+    const gbgpu_rows out{np, np > 0 ? row_ptr[np] : 0, const_cast<int64_t*>(row_ptr),
+                         const_cast<int32_t*>(ocols), const_cast<int32_t*>(ovals)};
     gbgpu_hm_t** r = (gbgpu_hm_t**)malloc(sizeof(gbgpu_hm_t*) * (size_t)std::max(np, 1));
     void** cf = (void**)malloc(sizeof(void*) * (size_t)std::max(np, 1));
     if (!r || !cf) return GBGPU_ENOMEM;
@@ -115,6 +118,34 @@ int store_rows(gbgpu_mat_t* mat, int bits, const gbgpu_rows& out) {
     return GBGPU_OK;
 }
 
+int store_rows(gbgpu_mat_t* mat, int bits, const gbgpu_rows& out) {
+    return store_rows_raw(mat, bits, out.np, out.row_ptr, out.cols, out.vals);
+}
+
+// mat->r rows -> the small path's pinned staging (coefficients reduced into
+// [0, p) as gather_rows does)
+struct GatherCtx {
+    const gbgpu_mat_t* mat;
+    const void* const* tab;
+    int bits;
+    int32_t p;
+};
+void fill_from_rows(void* ctx, int64_t* ptr, int32_t* cols, uint32_t* vals) {
+    const GatherCtx& g = *(const GatherCtx*)ctx;
+    const int32_t nr = g.mat->nr;
+    ptr[0] = 0;
+    for (int32_t i = 0; i < nr; ++i) {
+        const gbgpu_hm_t* r = g.mat->r[i];
+        const int64_t off = ptr[i], len = r[2];
+        ptr[i + 1] = off + len;
+        memcpy(cols + off, r + 3, sizeof(int32_t) * (size_t)len);
+        for (int64_t j = 0; j < len; ++j) {
+            int32_t v = load_cf(g.tab, g.bits, r[0], j) % g.p;
+            vals[off + j] = (uint32_t)(v < 0 ? v + g.p : v);
+        }
+    }
+}
+
 gbgpu_options shim_options() {
     gbgpu_options o{};
     o.form = GBGPU_FORM_AUTO;
@@ -132,20 +163,32 @@ int gbgpu_linear_algebra_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_st
     if (!mat || !bs || !st) return GBGPU_EINVAL;
     const double ct0 = cpu_seconds(), rt0 = wall_seconds();
     const int bits = coef_bits(st);
-    std::vector<int64_t> ptr;
-    std::vector<int32_t> cols, vals;
-    gather_rows(mat->r, mat->nr, bs_table(bs, bits), bits, st->fc, ptr, cols, vals);
-    gbgpu_csr m{st->fc, st->laopt, mat->nr, mat->ncl, mat->ncr, ptr.data(), cols.data(),
-                vals.data()};
     gbgpu_options o = shim_options();
-    gbgpu_rows out{};
-    int rc = gbgpu_reduce(&m, &o, &out);
-    if (rc) return rc;
-    // the la functions free their input rows (src/la_ff_16.c:665, :688-691, :804)
-    for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
-    rc = store_rows(mat, bits, out);
-    gbgpu_rows_free(&out);
-    if (rc) return rc;
+    int rc;
+    if (st->fc >= 2 && small_eligible(mat->nr, mat->ncl, mat->ncr, o.device)) {
+        // small matrix: rows gathered straight into pinned staging, one pass
+        int64_t nnz = 0;
+        for (int32_t i = 0; i < mat->nr; ++i) nnz += mat->r[i][2];
+        GatherCtx g{mat, bs_table(bs, bits), bits, st->fc};
+        SmallInput in{st->fc, mat->nr, mat->ncl, mat->ncr, nnz, o.device, fill_from_rows, &g};
+        SmallAnswer a;
+        if ((rc = small_reduce(in, &a))) return rc;
+        // the la functions free their input rows (src/la_ff_16.c:665, :688-691, :804)
+        for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
+        if ((rc = store_rows_raw(mat, bits, a.np, a.offs, a.cols, a.vals))) return rc;
+    } else {
+        std::vector<int64_t> ptr;
+        std::vector<int32_t> cols, vals;
+        gather_rows(mat->r, mat->nr, bs_table(bs, bits), bits, st->fc, ptr, cols, vals);
+        gbgpu_csr m{st->fc, st->laopt, mat->nr, mat->ncl, mat->ncr, ptr.data(), cols.data(),
+                    vals.data()};
+        gbgpu_rows out{};
+        if ((rc = gbgpu_reduce(&m, &o, &out))) return rc;
+        for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
+        rc = store_rows(mat, bits, out);
+        gbgpu_rows_free(&out);
+        if (rc) return rc;
+    }
     // the sparse options also reset the row count (src/la_ff_16.c:734)
     const int32_t lo = st->laopt;
     if (!(lo == 1 || lo == 42 || lo == 43)) mat->nr = mat->sz = mat->np;

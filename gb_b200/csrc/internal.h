@@ -22,6 +22,9 @@ void count_launch(long long n);
 // so a launch in one host thread never sees another thread lower it.
 cudaError_t ensure_smem_limit(const void* kernel, int bytes);
 int device_init(int device, DeviceInfo* info);
+// GBGPU_EINVAL with a description of the contract violations in `bits`
+// (the error bits of the device-side input checks), GBGPU_OK for none
+int err_to_status(uint32_t bits, std::string* msg);
 
 // mode 0: linear_algebra (reduce C|D rows by the known pivots, then reduced
 // echelon form of the right block); mode 1: full interreduction of rows with

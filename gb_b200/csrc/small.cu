@@ -1,0 +1,438 @@
+// small.cu -- one-pass reduction of small Macaulay matrices (the la calls of
+// the early F4 rounds and of small systems), built for latency.
+//
+// A general plan (api.cu) creates a stream, allocates a dozen buffers, runs
+// ten or more launches and copies in and out through pageable memory; for a
+// matrix of a few hundred rows that overhead is most of the call.  Here every
+// host thread keeps one session per device (a stream, a device arena, pinned
+// input staging and mapped pinned output memory, all grown to a high-water
+// mark and reused), and a call is
+//
+//   rows gathered into pinned staging  ->  one host-to-device copy
+//   k_small_prep      (1 CTA)   input checks, known pivots, ordered C|D row list
+//   k_reduce_rows_warp          one warp per C|D row, dense accumulator of the
+//                               row in shared memory, known pivots applied in
+//                               column order (src/la_ff_16.c:289-351 / :102-190)
+//   k_tiny_rref       (1 CTA)   reduced echelon form of the right block and its
+//                               compaction (plain.cu), written straight into
+//                               mapped host memory
+//   one 4-byte copy of the checks' verdict, one stream synchronisation.
+//
+// The answer is the canonical one of every other path (descending leads,
+// monic, columns ascending).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/gbgpu.h"
+#include "common.cuh"
+#include "internal.h"
+#include "kernels.h"
+#include "small.h"
+
+namespace gbgpu {
+
+constexpr int kPrepThreads = 1024;
+constexpr int kSmallMaxLeft = 12288;  // left columns: the prep kernel's pivot table in smem
+constexpr int kRowWarpsMax = 16;      // warps (rows) per CTA of k_reduce_rows_warp
+
+// ---------------------------------------------------------------------------
+// kernels
+
+// Input checks (the contract k_check_rows enforces), the known pivot of every
+// left column (first row with that lead, src/la_ff_16.c:762-772), the check
+// that every left column has one, and the C|D rows in row order -- one CTA.
+__global__ void __launch_bounds__(kPrepThreads)
+k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __restrict__ row_ptr,
+             const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals,
+             int32_t* piv_row, int32_t* work, int32_t* n_work, uint32_t* err) {
+    extern __shared__ int32_t prep_tab[];  // [ncl]: first row of each lead
+    __shared__ uint32_t s_err;
+    __shared__ int s_warp[kPrepThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kPrepThreads / 32;
+    for (int c = tid; c < ncl; c += blockDim.x) prep_tab[c] = INT_MAX;
+    if (tid == 0) s_err = 0;
+    __syncthreads();
+    for (int i = warp; i < nr; i += NW) {
+        const int64_t b = row_ptr[i], e = row_ptr[i + 1];
+        uint32_t bad = 0;
+        if (e <= b) {
+            bad |= kErrEmptyRow;
+        } else {
+            const int32_t lead = cols[b];
+            if (lead < 0 || lead >= ncl) bad |= kErrLeadRange;
+            if (vals[b] != 1u) bad |= kErrNotMonic;
+            for (int64_t k = b + lane; k < e; k += 32) {
+                const int32_t c = cols[k];
+                const uint32_t v = vals[k];
+                if (c < lead || c >= nc || (k > b && c == lead)) bad |= kErrColRange;
+                if (v == 0u || v >= p) bad |= kErrCoefRange;
+            }
+            if (lane == 0 && lead >= 0 && lead < ncl) atomicMin(&prep_tab[lead], i);
+        }
+        for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        if (lane == 0 && bad) atomicOr(&s_err, bad);
+    }
+    __syncthreads();
+    for (int c = tid; c < ncl; c += blockDim.x) {
+        const int32_t r = prep_tab[c];
+        if (r == INT_MAX) atomicOr(&s_err, kErrMissingPivot);
+        piv_row[c] = r;
+    }
+    // rows that are not the known pivot of their lead, in row order
+    int base = 0;
+    for (int r0 = 0; r0 < nr; r0 += kPrepThreads) {
+        const int i = r0 + tid;
+        int f = 0;
+        if (i < nr) {
+            const int64_t b = row_ptr[i];
+            if (row_ptr[i + 1] > b) {
+                const int32_t lead = cols[b];
+                if (lead >= 0 && lead < ncl) f = prep_tab[lead] != i;
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) s_warp[warp] = __popc(bal);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < NW; ++w) {
+            const int c = s_warp[w];
+            before += w < warp ? c : 0;
+            total += c;
+        }
+        if (f) work[base + before + __popc(bal & ((1u << lane) - 1u))] = i;
+        base += total;
+        __syncthreads();  // s_warp is rewritten by the next chunk
+    }
+    __syncthreads();
+    if (tid == 0) {
+        *n_work = base;
+        *err = s_err;
+    }
+}
+
+// One warp per C|D row: the row is scattered into a dense accumulator of nc
+// residues in shared memory, then the known pivots are applied in column
+// order -- the next column to clear is the first nonzero left column after
+// the last one cleared (a warp ballot over 32 columns at a time); the pivot
+// row (monic, its lead skipped) is applied by the 32 lanes in coalesced
+// strides (distinct columns, no conflicts).  The right block is written out
+// dense with its lead.  Nothing is read when the checks flagged the input.
+template <class F>
+__global__ void __launch_bounds__(kRowWarpsMax * 32)
+k_reduce_rows_warp(int32_t n_rows, const int32_t* __restrict__ work,
+                   const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
+                   const uint32_t* __restrict__ vals, const int32_t* __restrict__ piv_row,
+                   int32_t ncl, int32_t nc, int32_t stride, uint32_t* out, int64_t ld,
+                   int32_t* out_lead, const uint32_t* err, F f) {
+    extern __shared__ __align__(16) uint32_t rw_acc[];
+    if (*err) return;  // invalid input: nothing is read (uniform)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wpc = blockDim.x >> 5;
+    uint32_t* acc = rw_acc + (size_t)warp * stride;
+    const int32_t ncr = nc - ncl;
+    for (int w = blockIdx.x * wpc + warp; w < n_rows; w += gridDim.x * wpc) {
+        const int32_t r = work[w];
+        const int64_t rb = row_ptr[r], re = row_ptr[r + 1];
+        const int32_t lead = cols[rb];
+        for (int c = (lead & ~3) + 4 * lane; c < stride; c += 128)
+            *(uint4*)(acc + c) = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+        for (int64_t k = rb + lane; k < re; k += 32) acc[cols[k]] = vals[k];
+        __syncwarp();
+        int last = lead - 1;
+        for (;;) {
+            int found = -1;
+            for (int base = last + 1; base < ncl; base += 32) {
+                const int c = base + lane;
+                const unsigned bal = __ballot_sync(0xffffffffu, c < ncl && acc[c] != 0u);
+                if (bal) {
+                    found = base + __ffs(bal) - 1;
+                    break;
+                }
+            }
+            if (found < 0) break;
+            const uint32_t m = f.prep(acc[found]);
+            const int32_t pr = piv_row[found];
+            const int64_t pb = row_ptr[pr] + 1, pe = row_ptr[pr + 1];
+            for (int64_t k = pb + lane; k < pe; k += 32) {
+                const int32_t c = cols[k];
+                acc[c] = f.mulsub(acc[c], m, vals[k]);
+            }
+            last = found;
+            __syncwarp();
+        }
+        uint32_t* o = out + (size_t)w * ld;
+        int first = -1;
+        for (int j0 = 0; j0 < ncr; j0 += 32) {
+            const int j = j0 + lane;
+            const uint32_t v = j < ncr ? acc[ncl + j] : 0u;
+            if (j < ncr) o[j] = v;
+            const unsigned bal = __ballot_sync(0xffffffffu, v != 0u);
+            if (first < 0 && bal) first = j0 + __ffs(bal) - 1;
+        }
+        if (lane == 0) out_lead[w] = first;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+namespace {
+
+struct Session {
+    DeviceInfo dev{};
+    cudaStream_t s = nullptr;
+    void* dmem = nullptr;  // device arena
+    size_t dcap = 0;
+    uint8_t* hin = nullptr;  // pinned input staging
+    size_t hin_cap = 0;
+    uint8_t* hout = nullptr;  // mapped pinned output
+    size_t hout_cap = 0;
+    uint32_t* herr = nullptr;  // pinned: the checks' verdict
+    ~Session() {
+        // runs at thread exit; at process exit the runtime may already be
+        // gone, which these calls tolerate
+        if (s) cudaStreamSynchronize(s);
+        if (dmem) cudaFree(dmem);
+        if (hin) cudaFreeHost(hin);
+        if (hout) cudaFreeHost(hout);
+        if (herr) cudaFreeHost(herr);
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+constexpr int kMaxDev = 64;
+struct Sessions {
+    Session* by_dev[kMaxDev] = {};
+    ~Sessions() {
+        for (auto*& x : by_dev) {
+            delete x;
+            x = nullptr;
+        }
+    }
+};
+thread_local Sessions t_sessions;
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int grow_device(Session& S, size_t need) {
+    if (need <= S.dcap) return GBGPU_OK;
+    const size_t cap = std::max(need, S.dcap * 2);
+    if (S.dmem) {
+        cudaStreamSynchronize(S.s);
+        cudaFree(S.dmem);
+        S.dmem = nullptr;
+        S.dcap = 0;
+    }
+    if (cudaMalloc(&S.dmem, cap) != cudaSuccess) {
+        set_error("small-matrix arena allocation failed");
+        return GBGPU_ENOMEM;
+    }
+    S.dcap = cap;
+    return GBGPU_OK;
+}
+
+int grow_host(uint8_t** buf, size_t* capv, size_t need, unsigned flags, cudaStream_t s) {
+    if (need <= *capv) return GBGPU_OK;
+    const size_t cap = std::max(need, *capv * 2);
+    if (*buf) {
+        cudaStreamSynchronize(s);
+        cudaFreeHost(*buf);
+        *buf = nullptr;
+        *capv = 0;
+    }
+    if (cudaHostAlloc((void**)buf, cap, flags) != cudaSuccess) {
+        set_error("small-matrix pinned staging allocation failed");
+        return GBGPU_ENOMEM;
+    }
+    *capv = cap;
+    return GBGPU_OK;
+}
+
+int session_for(int device, Session** out) {
+    if (device < 0 || device >= kMaxDev) {
+        set_error("device ordinal out of range");
+        return GBGPU_ENODEV;
+    }
+    Session*& S = t_sessions.by_dev[device];
+    if (!S) {
+        Session* n = new Session();
+        int rc = device_init(device, &n->dev);
+        if (rc) {
+            delete n;
+            return rc;
+        }
+        if (cudaStreamCreateWithFlags(&n->s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaHostAlloc((void**)&n->herr, 64, cudaHostAllocDefault) != cudaSuccess) {
+            delete n;
+            set_error("small-matrix session set-up failed");
+            return GBGPU_ECUDA;
+        }
+        S = n;
+    }
+    *out = S;
+    return GBGPU_OK;
+}
+
+// the device current on entry is made current again on return
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// rows (warps) per CTA of k_reduce_rows_warp and the accumulator stride
+int rows_warps(int32_t nc, const DeviceInfo& dev, int32_t* stride) {
+    *stride = (int32_t)round_up((size_t)std::max(nc, 1), 4);
+    const int per = *stride * 4;
+    const int fit = (dev.smem_optin - 2048) / per;
+    return std::min(kRowWarpsMax, fit);
+}
+
+}  // namespace
+
+bool small_eligible(int32_t nr, int32_t ncl, int32_t ncr, int device) {
+    if (nr <= 0 || ncl < 0 || ncr <= 0 || nr < ncl || ncl > kSmallMaxLeft) return false;
+    DeviceGuard guard;
+    DeviceInfo dev{};
+    if (device_init(device, &dev)) return false;
+    int32_t stride = 0;
+    if (rows_warps(ncl + ncr, dev, &stride) < 4) return false;
+    const int32_t n_work = nr - ncl;
+    return n_work == 0 || tiny_rref_bytes(n_work, ncr, dev.smem_optin) > 0;
+}
+
+int small_reduce(const SmallInput& in, SmallAnswer* ans) {
+    DeviceGuard guard;
+    Session* S = nullptr;
+    int rc = session_for(in.device, &S);
+    if (rc) return rc;
+    const int32_t nr = in.nr, ncl = in.ncl, ncr = in.ncr, nc = ncl + ncr;
+    const int32_t n_work = nr - ncl;
+    const int64_t nnz = in.nnz;
+    const int64_t ld = (int64_t)round_up((size_t)std::max(ncr, 1), 4);
+    // pinned staging: row_ptr | cols | vals (copied to the arena's start)
+    const size_t b_ptr = sizeof(int64_t) * (size_t)(nr + 1);
+    const size_t o_cols = round_up(b_ptr, 16);
+    const size_t o_vals = round_up(o_cols + 4 * (size_t)nnz, 16);
+    const size_t in_bytes = round_up(o_vals + 4 * (size_t)nnz, 16);
+    if ((rc = grow_host(&S->hin, &S->hin_cap, in_bytes, cudaHostAllocDefault, S->s))) return rc;
+    // every call ends with a synchronisation, so the staging is free to refill
+    in.fill(in.ctx, (int64_t*)S->hin, (int32_t*)(S->hin + o_cols), (uint32_t*)(S->hin + o_vals));
+    // device arena
+    const size_t o_piv = round_up(in_bytes, 256);
+    const size_t o_work = round_up(o_piv + 4 * (size_t)std::max(ncl, 1), 256);
+    const size_t o_cnt = round_up(o_work + 4 * (size_t)nr, 256);  // n_work, err
+    const size_t o_D = round_up(o_cnt + 64, 256);
+    const size_t o_lead = round_up(o_D + 4 * (size_t)std::max(n_work, 1) * ld, 256);
+    const size_t o_poc = round_up(o_lead + 4 * (size_t)std::max(n_work, 1), 256);
+    const size_t d_bytes = round_up(o_poc + 4 * (size_t)ncr, 256);
+    if ((rc = grow_device(*S, d_bytes))) return rc;
+    uint8_t* d = (uint8_t*)S->dmem;
+    const int64_t* d_ptr = (const int64_t*)d;
+    const int32_t* d_cols = (const int32_t*)(d + o_cols);
+    const uint32_t* d_vals = (const uint32_t*)(d + o_vals);
+    int32_t* d_piv = (int32_t*)(d + o_piv);
+    int32_t* d_work = (int32_t*)(d + o_work);
+    int32_t* d_nwork = (int32_t*)(d + o_cnt);
+    uint32_t* d_err = (uint32_t*)(d + o_cnt + 16);
+    uint32_t* d_D = (uint32_t*)(d + o_D);
+    int32_t* d_lead = (int32_t*)(d + o_lead);
+    int32_t* d_poc = (int32_t*)(d + o_poc);
+    // mapped output: counts | offs | cols | vals
+    const size_t cap = (size_t)std::max(n_work, 0) * ncr;
+    const size_t h_offs = 64;
+    const size_t h_cols = round_up(h_offs + 8 * (size_t)(std::max(n_work, 0) + 1), 16);
+    const size_t h_vals = round_up(h_cols + 4 * std::max<size_t>(cap, 1), 16);
+    const size_t out_bytes = round_up(h_vals + 4 * std::max<size_t>(cap, 1), 16);
+    if ((rc = grow_host(&S->hout, &S->hout_cap, out_bytes, cudaHostAllocMapped, S->s))) return rc;
+    uint8_t* hd = nullptr;
+    if (cudaHostGetDevicePointer((void**)&hd, S->hout, 0) != cudaSuccess) {
+        set_error("mapped output pointer unavailable");
+        return GBGPU_ECUDA;
+    }
+    int64_t* h_counts = (int64_t*)S->hout;
+    h_counts[0] = 0;
+    h_counts[1] = 0;
+
+    cudaStream_t s = S->s;
+    long long launches = 0;
+    if (cudaMemcpyAsync(d, S->hin, in_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        set_error("small-matrix input copy failed");
+        return GBGPU_ECUDA;
+    }
+    const int prep_bytes = 4 * std::max(ncl, 1);
+    if (ensure_smem_limit((const void*)k_small_prep, prep_bytes) != cudaSuccess) {
+        set_error("prep kernel shared memory");
+        return GBGPU_ECUDA;
+    }
+    k_small_prep<<<1, kPrepThreads, prep_bytes, s>>>(nr, ncl, nc, (uint32_t)in.p, d_ptr, d_cols,
+                                                     d_vals, d_piv, d_work, d_nwork, d_err);
+    ++launches;
+    if (n_work > 0) {
+        int32_t stride = 0;
+        const int wpc = rows_warps(nc, S->dev, &stride);
+        const int bytes = wpc * stride * 4;
+        const int grid = std::max(1, std::min((n_work + wpc - 1) / wpc, S->dev.sms * 4));
+        const int tb = tiny_rref_bytes(n_work, ncr, S->dev.smem_optin);
+        auto run = [&](auto f) -> int {
+            using Fd = decltype(f);
+            if (ensure_smem_limit((const void*)k_reduce_rows_warp<Fd>, bytes) != cudaSuccess) {
+                set_error("row kernel shared memory");
+                return GBGPU_ECUDA;
+            }
+            k_reduce_rows_warp<Fd><<<grid, wpc * 32, bytes, s>>>(
+                n_work, d_work, d_ptr, d_cols, d_vals, d_piv, ncl, nc, stride, d_D, ld, d_lead,
+                d_err, f);
+            ++launches;
+            cudaError_t e = launch_tiny_rref(n_work, ncr, d_D, ld, d_lead, d_err, ncl,
+                                             (int64_t*)(hd + h_offs), (int32_t*)(hd + h_cols),
+                                             (int32_t*)(hd + h_vals), d_poc, (int64_t*)hd, tb,
+                                             s, f);
+            ++launches;
+            if (e != cudaSuccess) {
+                set_error(std::string("small-matrix launch: ") + cudaGetErrorString(e));
+                return GBGPU_ECUDA;
+            }
+            return GBGPU_OK;
+        };
+        rc = (uint32_t)in.p < 65536u ? run(FieldSmall::make((uint32_t)in.p))
+                                     : run(FieldMont::make((uint32_t)in.p));
+        if (rc) return rc;
+    } else {
+        ((int64_t*)(S->hout + h_offs))[0] = 0;
+    }
+    count_launch(launches);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S->herr, d_err, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(std::string("small-matrix run: ") + cudaGetErrorString(e));
+        return GBGPU_ECUDA;
+    }
+    if (*S->herr) {
+        std::string msg;
+        rc = err_to_status(*S->herr, &msg);
+        set_error(msg);
+        return rc;
+    }
+    ans->np = n_work > 0 ? (int32_t)h_counts[0] : 0;
+    ans->nnz = n_work > 0 ? h_counts[1] : 0;
+    ans->offs = (const int64_t*)(S->hout + h_offs);
+    ans->cols = (const int32_t*)(S->hout + h_cols);
+    ans->vals = (const int32_t*)(S->hout + h_vals);
+    return GBGPU_OK;
+}
+
+}  // namespace gbgpu
