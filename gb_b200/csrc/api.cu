@@ -177,6 +177,9 @@ struct Plan {
     uint32_t* gacc = nullptr;
     int grid_sparse = 0;
     bool smem_sparse = true, smem_dense = true;
+    // team-per-row known-pivot reduction (plain.cu k_reduce_team)
+    int team_bytes = 0, grid_team = 0;
+    longlong2* pext = nullptr;
     // echelon
     int32_t* piv_of_col = nullptr;
     int32_t* claim = nullptr;
@@ -277,8 +280,10 @@ static int plan_alloc(Plan* P) {
 #define A(ptr, n) \
     if ((rc = P->alloc(&P->ptr, (size_t)(n)))) return rc
     A(row_ptr, P->nr + 1);
-    A(cols, P->nnz);
-    A(vals, P->nnz);
+    // 16 entries of padding: the team kernel stages pivot rows in whole
+    // 16-byte groups, reading up to 3 entries past a row's end
+    A(cols, P->nnz + 16);
+    A(vals, P->nnz + 16);
     A(piv_row, P->nc);
     A(flag, P->nr);
     A(work, P->nr);
@@ -340,6 +345,12 @@ static int plan_alloc(Plan* P) {
     const int64_t smem_cap = std::min<int64_t>(P->dev.smem_optin - 1024, 200 * 1024);
     P->smem_sparse = (int64_t)P->nc * 4 <= smem_cap;
     P->smem_dense = (int64_t)P->ncr * 4 <= smem_cap;
+    P->team_bytes = team_smem_bytes(P->nc, P->dev.smem_optin);
+    if (P->team_bytes > 0 && !P->blocked) {
+        A(pext, P->mode == 0 ? std::max(P->ncl, 1) : std::max(P->nc, 1));
+        const int per_sm = std::max(1, std::min(8, (P->dev.smem_optin - 1024) / (P->team_bytes + 3072)));
+        P->grid_team = std::max(1, std::min<int>(P->n_work, P->dev.sms * per_sm));
+    }
     P->grid_sparse = std::max(1, std::min<int>(P->n_work, P->dev.sms * (P->smem_sparse ? 1 : 2)));
     if (P->smem_sparse) {
         // two CTAs per SM when two accumulators fit
@@ -486,8 +497,15 @@ static int run_form(Plan* P, const F& f) {
     sa.queue = P->counters + 0;
     sa.work_count = P->work_count + 0;
     sa.err = P->err;
-    if (P->n_work > 0)
-        GB_CALL(launch_reduce_sparse(sa, f, P->grid_sparse, P->smem_sparse, P->nc * 4, s));
+    if (P->n_work > 0) {
+        if (P->pext) {
+            GB_LAUNCH(k_pivot_extents<<<grid_for(sa.piv_limit, T), T, 0, s>>>(
+                sa.piv_limit, P->piv_row, P->row_ptr, P->pext));
+            GB_CALL(launch_reduce_team(sa, P->pext, f, P->grid_team, P->team_bytes, s));
+        } else {
+            GB_CALL(launch_reduce_sparse(sa, f, P->grid_sparse, P->smem_sparse, P->nc * 4, s));
+        }
+    }
     GB_CUDA(cudaEventRecord(P->ev[2], s));
 
     if (P->tiny) {

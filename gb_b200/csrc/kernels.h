@@ -68,6 +68,14 @@ __global__ void k_gather_rows(int32_t n, const int32_t* pivcol, const int32_t* p
 template <class F>
 cudaError_t launch_reduce_sparse(const SparseReduceArgs& a, const F& f, int grid, bool smem,
                                  int smem_bytes, cudaStream_t s);
+// the team-per-row form of the known-pivot reduction (pivot rows staged in
+// shared memory ahead of use); pext from k_pivot_extents
+__global__ void k_pivot_extents(int32_t n, const int32_t* piv_row, const int64_t* row_ptr,
+                                longlong2* ext);
+int team_smem_bytes(int32_t nc, int smem_optin);
+template <class F>
+cudaError_t launch_reduce_team(const SparseReduceArgs& a, const longlong2* pext, const F& f,
+                               int grid, int smem_bytes, cudaStream_t s);
 template <class F>
 cudaError_t launch_reduce_dense(const DenseReduceArgs& a, const F& f, int grid, bool smem,
                                 int smem_bytes, cudaStream_t s);

@@ -194,6 +194,217 @@ k_reduce_sparse(SparseReduceArgs a, F f) {
 }
 
 // ---------------------------------------------------------------------------
+// 2'. the same reduction by a team of warps per row with the pivot rows staged
+// in shared memory ahead of use.
+//
+// One CTA (kTeamThreads) per row, the row's dense accumulator in shared
+// memory.  The known pivots are applied in column order like the reference's
+// reduce_dense_row_by_old_pivots (src/la_ff_16.c:289-351): the next pivot is
+// the first nonzero column after the last one cleared.  Each step costs two
+// barriers and no global round trip on its critical path: the cols/vals of the
+// next two pivot rows the accumulator predicts (the next nonzero columns as it
+// stands) are already being copied into a three-slot ring by cp.async while
+// the current one is applied; a wrong prediction (an update created or
+// cancelled a nonzero before the predicted column) drains the ring and
+// restarts it at the true next pivot.  Pivot-row extents come from a window of
+// 256 columns staged in shared memory.  The staged copies read whole 16-byte
+// groups around each row, so cols/vals carry at least 4 elements of padding.
+constexpr int kTeamThreads = 256;
+constexpr int kStageLen = 2048;  // entries of one staged pivot row (longer rows: tail from global)
+constexpr int kStages = 3;
+constexpr int kExtWin = 256;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// ext[c] = {first applied entry, end} of the pivot row of column c (its lead
+// entry excluded), {-1, -1} when column c has no pivot
+__global__ void k_pivot_extents(int32_t n, const int32_t* __restrict__ piv_row,
+                                const int64_t* __restrict__ row_ptr, longlong2* ext) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int32_t r = piv_row[c];
+        ext[c] = r == INT_MAX ? make_longlong2(-1, -1)
+                              : make_longlong2(row_ptr[r] + 1, row_ptr[r + 1]);
+    }
+}
+
+template <class F, bool CHECK>
+__global__ void __launch_bounds__(kTeamThreads, 1)
+k_reduce_team(SparseReduceArgs a, const longlong2* __restrict__ pext, F f) {
+    extern __shared__ __align__(16) uint32_t t_smem[];
+    uint32_t* st_cols = t_smem;                          // [kStages][kStageLen]
+    uint32_t* st_vals = t_smem + kStages * kStageLen;    // [kStages][kStageLen]
+    uint32_t* acc = t_smem + 2 * kStages * kStageLen;    // [nc]
+    __shared__ longlong2 s_ext[kExtWin];
+    __shared__ int s_scratch[kTeamThreads / 32];
+    __shared__ int s_work;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int limit = a.piv_limit;
+    if (a.err && *a.err) return;  // invalid input: nothing is read (uniform)
+    int wb = -kExtWin;            // first column of the extents window
+
+    // first column c >= from, c < limit, with acc[c] != 0 (and a pivot when
+    // CHECK), -1 if none: every warp computes it from the same data
+    auto scan = [&](int from) -> int {
+        for (int base = from & ~3; base < limit; base += 128) {
+            const int c0 = base + 4 * lane;
+            uint32_t bits = 0;
+            if (c0 < a.nc) {
+                const uint4 v = *(const uint4*)(acc + c0);
+                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c = c0 + j;
+                    bool nz = w[j] != 0u && c >= from && c < limit;
+                    if (CHECK && nz) nz = a.piv_row[c] != INT_MAX;
+                    bits |= nz ? (1u << j) : 0u;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, bits != 0u);
+            if (bal) {
+                const int l = __ffs(bal) - 1;
+                const uint32_t b = __shfl_sync(0xffffffffu, bits, l);
+                return base + 4 * l + __ffs(b) - 1;
+            }
+        }
+        return -1;
+    };
+    // extents of column c through the shared window (uniform call: barriers)
+    auto extent = [&](int c) -> longlong2 {
+        if (c < wb || c >= wb + kExtWin) {
+            __syncthreads();
+            wb = c;
+            if (wb + tid < limit) s_ext[tid] = pext[wb + tid];
+            __syncthreads();
+        }
+        return s_ext[c - wb];
+    };
+    // copy the pivot row of column c into ring slot `slot`; one commit group
+    // per call for every thread (empty for c < 0)
+    int slot_off[kStages], slot_lim[kStages];
+    long long slot_x[kStages], slot_len[kStages];
+    auto issue = [&](int c, int slot) {
+        if (c >= 0) {
+            const longlong2 e = extent(c);
+            const long long x0 = e.x & ~3ll, y0 = (e.y + 3) & ~3ll;
+            const int n = (int)min(y0 - x0, (long long)kStageLen);
+            slot_off[slot] = (int)(e.x - x0);
+            slot_lim[slot] = n - (int)(e.x - x0);
+            slot_x[slot] = e.x;
+            slot_len[slot] = e.y - e.x;
+            uint32_t* dc = st_cols + slot * kStageLen;
+            uint32_t* dv = st_vals + slot * kStageLen;
+            for (int i = 4 * tid; i < n; i += 4 * kTeamThreads) {
+                cp_async16(dc + i, a.cols + x0 + i);
+                cp_async16(dv + i, a.vals + x0 + i);
+            }
+        }
+        cp_async_commit();
+    };
+
+    for (;;) {
+        if (tid == 0) s_work = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int w = s_work;
+        __syncthreads();
+        if (w >= a.n_work) break;
+        const int32_t r = a.work[w];
+        const int64_t rb = a.row_ptr[r], re = a.row_ptr[r + 1];
+        const int32_t lead = a.cols[rb];
+        for (int c = (min(lead, a.emit_from) & ~3) + 4 * tid; c < a.nc; c += 4 * kTeamThreads)
+            *(uint4*)(acc + c) = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        for (int64_t k = rb + tid; k < re; k += kTeamThreads) acc[a.cols[k]] = a.vals[k];
+        __syncthreads();
+        long long applied = 0;
+        int cur = scan(lead + a.skip_lead);
+        if (cur >= 0) {
+            // ring: cur in slot s0, two predictions behind it
+            int s0 = 0, q1 = scan(cur + 1), q2 = q1 >= 0 ? scan(q1 + 1) : -1;
+            issue(cur, 0);
+            issue(q1, 1);
+            issue(q2, 2);
+            for (;;) {
+                cp_async_wait<2>();  // this thread's copies of `cur` have landed
+                __syncthreads();     // ... and every thread's
+                const uint32_t m = f.prep(acc[cur]);
+                const uint32_t* sc = st_cols + s0 * kStageLen + slot_off[s0];
+                const uint32_t* sv = st_vals + s0 * kStageLen + slot_off[s0];
+                const int len = (int)slot_len[s0], lim = slot_lim[s0];
+                const long long x = slot_x[s0];
+                for (int k = tid; k < len; k += kTeamThreads) {
+                    uint32_t col, v;
+                    if (k < lim) {
+                        col = sc[k];
+                        v = sv[k];
+                    } else {
+                        col = (uint32_t)a.cols[x + k];
+                        v = a.vals[x + k];
+                    }
+                    acc[col] = f.mulsub(acc[col], m, v);
+                }
+                applied += len + 1;
+                __syncthreads();  // the step's updates are complete
+                if (tid == 0) acc[cur] = 0u;  // read by nobody before the row is emitted
+                const int nxt = scan(cur + 1);
+                if (nxt < 0) break;
+                const int s1 = (s0 + 1) % kStages, s2 = (s0 + 2) % kStages;
+                if (nxt == q1) {
+                    // prediction held: slot s0 is free (its copies landed)
+                    const int q3 = q2 >= 0 ? scan(q2 + 1) : scan(nxt + 1);
+                    cur = nxt;
+                    q1 = q2;
+                    q2 = q3;
+                    issue(q2, s0);
+                    s0 = s1;
+                    (void)s2;
+                } else {
+                    // mispredicted: let the copies in flight land, restart the ring
+                    cp_async_wait<0>();
+                    __syncthreads();
+                    cur = nxt;
+                    q1 = scan(cur + 1);
+                    q2 = q1 >= 0 ? scan(q1 + 1) : -1;
+                    s0 = 0;
+                    issue(cur, 0);
+                    issue(q1, 1);
+                    issue(q2, 2);
+                }
+            }
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (tid == 0 && applied) atomicAdd((unsigned long long*)a.work_count,
+                                           (unsigned long long)applied);
+        // write the window [emit_from, emit_from + emit_width) and its lead
+        uint32_t* out = a.out + (size_t)w * a.out_ld;
+        int first = INT_MAX;
+        for (int k = tid; k < a.emit_width; k += kTeamThreads) {
+            const uint32_t v = acc[a.emit_from + k];
+            out[k] = v;
+            if (v != 0u && k < first) first = k;
+        }
+        first = block_min(first, s_scratch);
+        if (tid == 0) a.out_lead[w] = first == INT_MAX ? -1 : first;
+    }
+}
+
+// shared memory of k_reduce_team for nc columns (0: too large for one CTA)
+int team_smem_bytes(int32_t nc, int smem_optin) {
+    const int64_t b = (int64_t)2 * kStages * kStageLen * 4 + (((int64_t)nc + 3) & ~3ll) * 4;
+    return b + 4096 <= smem_optin ? (int)b : 0;
+}
+
+// ---------------------------------------------------------------------------
 // 3./4. reduction of dense rows by dense (echelon) pivot rows
 //
 // mode kUntilFree: reduce row r (in place in `rows`) by the pivots of its
@@ -377,6 +588,21 @@ __global__ void k_row_write(int32_t np, const int32_t* __restrict__ pivcol,
 
 // ---------------------------------------------------------------------------
 // host launchers: every kernel is launched from this translation unit
+template <class F>
+cudaError_t launch_reduce_team(const SparseReduceArgs& a, const longlong2* pext, const F& f,
+                               int grid, int smem_bytes, cudaStream_t s) {
+    if (a.skip_lead) {
+        cudaError_t e = ensure_smem_limit((const void*)k_reduce_team<F, true>, smem_bytes);
+        if (e != cudaSuccess) return e;
+        k_reduce_team<F, true><<<grid, kTeamThreads, smem_bytes, s>>>(a, pext, f);
+    } else {
+        cudaError_t e = ensure_smem_limit((const void*)k_reduce_team<F, false>, smem_bytes);
+        if (e != cudaSuccess) return e;
+        k_reduce_team<F, false><<<grid, kTeamThreads, smem_bytes, s>>>(a, pext, f);
+    }
+    return cudaGetLastError();
+}
+
 template <class F>
 cudaError_t launch_reduce_sparse(const SparseReduceArgs& a, const F& f, int grid, bool smem,
                                  int smem_bytes, cudaStream_t s) {
@@ -648,6 +874,8 @@ cudaError_t launch_tiny_rref(int32_t n, int32_t m, const uint32_t* D, int64_t ld
 }
 
 #define GBGPU_INSTANTIATE(F)                                                                   \
+    template cudaError_t launch_reduce_team<F>(const SparseReduceArgs&, const longlong2*,      \
+                                               const F&, int, int, cudaStream_t);              \
     template cudaError_t launch_reduce_sparse<F>(const SparseReduceArgs&, const F&, int, bool, \
                                                  int, cudaStream_t);                            \
     template cudaError_t launch_reduce_dense<F>(const DenseReduceArgs&, const F&, int, bool,   \
