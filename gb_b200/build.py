@@ -18,6 +18,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgbgpu.so")
 LIFT_LIB = os.path.join(HERE, "libgblift.so")  # host-only helper of gb_b200/multimod.py
+SYNTH_LIB = os.path.join(HERE, "libgbsynth.so")  # host-only generator of gb_b200/synth.py
 OBJDIR = os.path.join(REPO, "_build", "gbgpu")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -68,6 +69,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     build_lift(verbose=verbose, force=force)
+    build_synth(verbose=verbose, force=force)
     return LIB
 
 
@@ -81,6 +83,18 @@ def build_lift(verbose: bool = False, force: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     return LIFT_LIB
+
+
+def build_synth(verbose: bool = False, force: bool = False) -> str:
+    """libgbsynth.so: the host generator of the large synthetic staircase
+    matrices (plain C++, g++)."""
+    src = os.path.join(CSRC, "synth.cpp")
+    if force or _stale(SYNTH_LIB, [src]):
+        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", src, "-o", SYNTH_LIB]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return SYNTH_LIB
 
 
 if __name__ == "__main__":

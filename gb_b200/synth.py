@@ -245,3 +245,45 @@ def f4_case(name: str, nvars: int, ngens: int, maxdeg: int, p: int, la_option: i
     return {"name": name, "nr_vars": nvars, "nr_gens": ngens, "ht_size": 12, "field_char": p,
             "mon_order": 0, "nr_threads": nr_threads, "la_option": la_option, "reduce_gb": 0,
             "max_nr_pairs": 0, "reset_hash_table": 0, "lens": lens, "cfs": cfs, "exps": exps}
+
+
+
+_SYNTH_LIB = None
+
+
+def staircase_native(nru: int, nrl: int, ncr: int, p: int, dmin: float, dmax: float,
+                     band: float = 4.0, seed: int = 1, laopt: int = 1,
+                     threads: int = 0) -> MacaulayMatrix:
+    """The banded A|B/C|D structure of ``staircase`` drawn by the host
+    generator libgbsynth.so (gb_b200/csrc/synth.cpp; host threads, one random
+    stream per row, so the matrix does not depend on the thread count): for
+    the batched workloads, whose matrices reach hundreds of millions of
+    entries.  Inside each band the columns are one draw per equal stratum."""
+    import ctypes as C
+    import os
+    global _SYNTH_LIB
+    if _SYNTH_LIB is None:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgbsynth.so")
+        lib = C.CDLL(path)
+        lib.gbsynth_staircase_layout.restype = C.c_int64
+        lib.gbsynth_staircase_layout.argtypes = [C.c_int32] * 3 + [C.c_double] * 3 + [
+            C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p]
+        lib.gbsynth_staircase_fill.argtypes = [C.c_int32] * 4 + [C.c_double] * 3 + [
+            C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _SYNTH_LIB = lib
+    lib = _SYNTH_LIB
+    threads = threads or (os.cpu_count() or 1)
+    nr = nru + nrl
+    ptr = np.empty(nr + 1, dtype=np.int64)
+    order = np.empty(max(nr, 1), dtype=np.int32)
+    nnz = lib.gbsynth_staircase_layout(nru, nrl, ncr, dmin, dmax, band, seed, threads,
+                                       ptr.ctypes.data, order.ctypes.data)
+    if nnz < 0:
+        raise ValueError("bad staircase parameters")
+    cols = np.empty(max(nnz, 1), dtype=np.int32)
+    vals = np.empty(max(nnz, 1), dtype=np.int32)
+    if lib.gbsynth_staircase_fill(nru, nrl, ncr, p, dmin, dmax, band, seed, threads,
+                                  ptr.ctypes.data, order.ctypes.data, cols.ctypes.data,
+                                  vals.ctypes.data) != 0:
+        raise ValueError("bad staircase parameters")
+    return MacaulayMatrix(p, nru, ncr, ptr, cols[:nnz], vals[:nnz], laopt)
