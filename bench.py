@@ -565,74 +565,198 @@ def run_dense(args):
     print(json.dumps(line), flush=True)
 
 
-def batch_matrices(n_images: int = 128, n_mixed: int = 128, seed: int = 5):
-    """The two batches of the batched workload:
-    (a) one integer system (staircase structure, 2400 x 600, 3600 columns,
-        coefficients in [-2^20, 2^20]) reduced modulo the n_images largest
-        primes below 2^31 -- same structure, different coefficients;
-    (b) n_mixed staircase matrices over p = 32003 with total rows log-uniform
-        in [500, 5000] (a fifth of them C|D rows), columns 1.5-3 x rows,
-        density U[1%, 10%]."""
+BATCH_IMAGE_SYSTEM = {"nvars": 8, "ngens": 8, "maxdeg": 2, "bound": 1 << 20, "seed": 20}
+
+
+def integer_quadratic_system():
+    """The integer system of the batched workload: 8 polynomials in 8
+    variables, each with all 45 monomials of degree <= 2 (descending DRL), the
+    coefficients uniform in [-2^20, 2^20] without 0 (seeded)."""
     from gb_b200 import synth
-    base = synth.integer_staircase(2400, 600, 2400, seed=seed)
-    imgs = [synth.image_mod(base, q) for q in synth.largest_primes_below(1 << 31, n_images)]
+    c = BATCH_IMAGE_SYSTEM
+    rng = np.random.default_rng(c["seed"])
+    mons = synth.monomials_drl_desc(c["nvars"], c["maxdeg"])
+    ints = rng.integers(1, c["bound"] + 1, size=c["ngens"] * len(mons))
+    ints = np.where(rng.random(ints.shape[0]) < 0.5, -ints, ints)
+    exps = [x for _ in range(c["ngens"]) for e in mons for x in e]
+    return [len(mons)] * c["ngens"], ints, exps
+
+
+def f4_prime_images(n_primes: int, threads: int):
+    """The CPU-baseline leg of the batched workload's first half: gb's F4 (the
+    reference build, src/f4.c:190, la option 1) on the integer system reduced
+    modulo each of the n_primes largest primes below 2^31, every la call
+    captured by the hook at src/f4.c:306.  Returns, per prime, the largest la
+    call (the matrix of the batch), the reference's answer to it and the
+    reference la's time for that call (all host threads)."""
+    import glob
+    import oracle
+    from gb_b200 import synth
+    from gb_b200.matrix import read_gbm
+    lens, ints, exps = integer_quadratic_system()
+    c = BATCH_IMAGE_SYSTEM
+    out = []
+    for q in synth.largest_primes_below(1 << 31, n_primes):
+        case = {"name": f"img{q}", "nr_vars": c["nvars"], "nr_gens": c["ngens"], "ht_size": 12,
+                "field_char": q, "mon_order": 0, "nr_threads": threads, "la_option": 1,
+                "reduce_gb": 0, "max_nr_pairs": 0, "reset_hash_table": 0, "lens": lens,
+                "cfs": [int(x) % q for x in ints], "exps": exps}
+        with tempfile.TemporaryDirectory() as d:
+            oracle.ref_f4(case, capture_dir=d)
+            caps = [read_gbm(open(f, "rb").read()) for f in sorted(glob.glob(d + "/*.gbm"))]
+        _, mat, ans, _ = max((x for x in caps if x[0] == 0), key=lambda x: x[1].nr * x[1].nc)
+        _, secs = oracle.ref_la(mat, 1, nthreads=threads)
+        out.append((mat, ans, secs))
+    return out
+
+
+def mixed_staircases(n: int, seed: int = 5, p: int = 32003):
+    """The second half: n banded A|B/C|D matrices over p with total rows
+    log-uniform in [500, 50000] (a fifth of them rows to reduce), columns
+    1.5-3 x rows, row density U[1%, 10%] (gb_b200.synth.staircase_native)."""
+    from gb_b200 import synth
     rng = np.random.default_rng(seed)
-    mixed = []
-    for i in range(n_mixed):
-        rows = int(np.exp(rng.uniform(np.log(500), np.log(5000))))
+    mats = []
+    for i in range(n):
+        rows = int(np.exp(rng.uniform(np.log(500), np.log(50000))))
         nrl = max(1, rows // 5)
         nru = rows - nrl
         ncr = max(16, int(rows * rng.uniform(1.5, 3.0)) - nru)
-        mixed.append(synth.staircase(nru, nrl, ncr, 32003, 0.01, 0.10, seed=seed * 1000 + i))
-    return imgs, mixed
+        d = float(rng.uniform(0.01, 0.10))
+        mats.append(synth.staircase_native(nru, nrl, ncr, p, d, d, seed=seed * 1000 + i))
+    return mats
+
+
+def _rows_copy(r):
+    """A ReducedRows copy of one gbgpu_rows answer (the library still owns it)."""
+    from gb_b200.matrix import ReducedRows
+    n, nnz = r.np, r.nnz
+    return ReducedRows(np.ctypeslib.as_array(r.row_ptr, shape=(n + 1,)).copy(),
+                       np.ctypeslib.as_array(r.cols, shape=(max(nnz, 1),))[:nnz].copy(),
+                       np.ctypeslib.as_array(r.vals, shape=(max(nnz, 1),))[:nnz].copy())
 
 
 def run_batch(args):
-    """Batched workload: 2 x 128 independent matrices through gbgpu_reduce_batch
-    (host CSR in, host rows out), timed end to end on the host clock around the
-    call (the call returns when every answer is in host memory)."""
+    """Batched workload: 256 matrices in one gbgpu_reduce_batch call (host CSR
+    in, host rows out), wall clock around the call (it returns when every
+    answer is in host memory):
+      * 128 images: the largest la call of F4 on one integer quadratic system
+        modulo each of the 128 largest primes below 2^31 (f4_prime_images;
+        small matrices: one persistent launch with a device work queue);
+      * 128 mixed: banded staircases over 32003, 500-50000 rows
+        (mixed_staircases; the blocked tensor-core form, host workers).
+    Every image's answer is checked against the reference's answer to that
+    call, and the mixed matrices up to 5000 rows against the reference la,
+    which is also the CPU baseline on exactly those matrices (whole matrices,
+    nothing extrapolated).  With --gpus N (torchrun) the batch is split across
+    the ranks by estimated work (gb_b200.dist.shard_batch), every rank reduces
+    its shard, and the time is the maximum over the ranks."""
+    import ctypes as Cc
     import torch
-    from gb_b200 import _lib, la
-    _lib.load()
-    imgs, mixed = batch_matrices()
-    out = {}
-    for name, mats in (("prime images", imgs), ("mixed sizes p=32003", mixed)):
-        la.reduce_batch(mats[:4])  # warm
-        ts = []
-        for _ in range(max(1, args.steps)):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            res, st = la.reduce_batch(mats)
-            ts.append(time.perf_counter() - t0)
-            assert all(x == 0 for x in st), st
-        sec = statistics.median(ts)
-        # spot check: the batched answers equal single-matrix reductions
-        for i in (0, len(mats) // 2, len(mats) - 1):
-            assert res[i].equals(la.linear_algebra(mats[i])), (name, i)
-        entry = {"matrices": len(mats), "seconds": sec, "matrices_per_s": len(mats) / sec,
-                 "rows_total": int(sum(m.nr for m in mats)),
-                 "nnz_total": int(sum(m.nnz for m in mats))}
-        if not args.no_cpu:
-            # the reference's la (oracle/_ref, option 1, all host threads) on
-            # every 16th matrix of the batch, scaled to the whole batch
-            import oracle
-            threads = os.cpu_count() or 1
-            sample = mats[::16]
-            cpu = sum(oracle.ref_la(m, 1, nthreads=threads)[1] for m in sample)
-            entry["cpu_reference_matrices_per_s"] = len(sample) / cpu
-            entry["cpu_sample"] = f"{len(sample)} of {len(mats)} matrices, {threads} threads"
-        out[name] = entry
-    n = sum(v["matrices"] for v in out.values())
-    sec = sum(v["seconds"] for v in out.values())
-    line = {"metric": "batched GF(p) matrix reductions/s (end to end, host CSR in/out)",
-            "value": n / sec, "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32 (mod p, exact)",
-            "data": "synthetic (seeded staircase batches)",
-            "config": {"workload": "batch: 128 images of one integer system mod the largest "
-                                   "primes < 2^31 + 128 mixed-size matrices over 32003",
-                       "batches": out}}
-    print(json.dumps(line), flush=True)
+    from gb_b200 import _lib, dist, la
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    lib = _lib.load()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    images = f4_prime_images(128, threads)
+    mixed = mixed_staircases(128)
+    gen_s = time.perf_counter() - t0
+    mats = [m for m, _, _ in images] + mixed
+    mine = dist.shard_batch(mats, ws)[rank] if ws > 1 else list(range(len(mats)))
+    sel = [mats[i] for i in mine]
+    n_sel = max(len(sel), 1)
+    csrs = (_lib.Csr * n_sel)(*[la._csr(m) for m in sel])
+    opt = _lib.Options(_lib.FORM_AUTO, local, 1, 0, None)
+
+    def batch(cs, n):
+        outs = (_lib.Rows * max(n, 1))()
+        status = (Cc.c_int32 * max(n, 1))()
+        t = time.perf_counter()
+        _lib.check(lib.gbgpu_reduce_batch(n, cs, Cc.byref(opt), outs,
+                                          Cc.cast(status, Cc.POINTER(Cc.c_int32))))
+        return time.perf_counter() - t, outs, [int(status[i]) for i in range(n)]
+
+    def free(outs, n):
+        for i in range(n):
+            lib.gbgpu_rows_free(Cc.byref(outs[i]))
+
+    few = (_lib.Csr * 8)(*[la._csr(m) for m in mats[:8]])
+    _, wo, _ = batch(few, 8)  # warm-up: kernels, sessions
+    free(wo, 8)
+    if ws > 1:
+        torch.distributed.barrier()
+    launches0 = lib.gbgpu_kernel_launches()
+    times, outs, status = [], None, None
+    for _ in range(max(1, args.steps)):
+        if outs is not None:
+            free(outs, len(sel))
+        dt, outs, status = batch(csrs, len(sel))
+        times.append(dt)
+    launches = lib.gbgpu_kernel_launches() - launches0
+    sec = dist.max_over_ranks(float(statistics.median(times)), device="cuda")
+    failed = [s for s in status if s != 0]
+    checked = ok = 0
+    for k, i in enumerate(mine):
+        if i < len(images):
+            checked += 1
+            ok += int(_rows_copy(outs[k]).equals(images[i][1]))
+    small = [(k, i) for k, i in enumerate(mine) if i >= len(images) and mats[i].nr <= 5000]
+    cpu_s = gpu_small_s = 0.0
+    if small and rank == 0 and not args.no_cpu:
+        import oracle
+        sc = (_lib.Csr * len(small))(*[la._csr(mats[i]) for _, i in small])
+        gpu_small_s, so, _ = batch(sc, len(small))
+        for j, (k, i) in enumerate(small):
+            ref, secs = oracle.ref_la(mats[i], 1, nthreads=threads)
+            cpu_s += secs
+            checked += 1
+            ok += int(_rows_copy(outs[k]).equals(ref) and _rows_copy(so[j]).equals(ref))
+        free(so, len(small))
+    # one mid-size staircase (the largest of <= 12000 rows) also through the
+    # sparse-row form, an independent code path: the same answer
+    plain_ok = None
+    mid = [(k, i) for k, i in enumerate(mine) if i >= len(images) and mats[i].nr <= 12000]
+    if mid:
+        k, i = max(mid, key=lambda x: mats[x[1]].nr)
+        plain_ok = bool(la.linear_algebra(mats[i], form=_lib.FORM_PLAIN).equals(
+            _rows_copy(outs[k])))
+    free(outs, len(sel))
+    img_cpu = sum(x[2] for x in images)
+    line = {"metric": "batched GF(p) matrix reductions/s (256 uneven matrices, host CSR in/out)",
+            "value": len(mats) / sec, "unit": "matrices/s", "n_gpus": ws, "steps": len(times),
+            "warmup": 1, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "u32 residues (u8 limbs on the tensor cores in the blocked form)",
+            "data": "synthetic: F4 la calls of one integer quadratic system mod 128 primes + "
+                    "128 banded staircases (seeded)",
+            "config": {"workload": "batch: 128 F4 prime images (8 quadratics in 8 variables, "
+                                   "coefficients in [-2^20, 2^20], the 128 largest primes "
+                                   "< 2^31) + 128 staircases over 32003, 500-50000 rows, "
+                                   "columns 1.5-3x, density 1-10%",
+                       "parallelism": f"batch split over {ws} ranks" if ws > 1 else "single GPU"},
+            "gpu_launches": int(launches), "failed": failed,
+            "rows_total": int(sum(m.nr for m in mats)),
+            "nnz_total": int(sum(m.nnz for m in mats)),
+            "largest": max([m.nr, m.nc] for m in mats),
+            "image_shape": [images[0][0].nr, images[0][0].nc], "generate_s": gen_s,
+            "answers_checked": checked, "answers_equal_reference": ok == checked,
+            "largest_mid_size_equals_plain_form": plain_ok}
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = {
+            "value": (len(images) + len(small)) / (img_cpu + cpu_s), "unit": "matrices/s",
+            "cores": threads, "kind": "reference",
+            "sample": (f"the reference la (oracle/_ref, {threads} threads) on the 128 images "
+                       f"({img_cpu:.2f} s) and on the {len(small)} staircases of <= 5000 rows "
+                       f"({cpu_s:.2f} s), whole matrices; the GPU takes {gpu_small_s:.3f} s "
+                       f"for those staircases in one batch call")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
 
 
 def f4_systems_timing(steps: int, cpu: bool = True) -> dict:

@@ -1001,6 +1001,24 @@ int plan_run_into_v(Plan* P, int64_t* row_ptr, int32_t* cols, void* vals, int32_
     return GBGPU_OK;
 }
 
+// host CSR of a gbgpu_csr into the small path's staging (values widened)
+void fill_from_csr_vals(void* ctx, int64_t* row_ptr, int32_t* cols, uint32_t* vals) {
+    const gbgpu_csr* m = (const gbgpu_csr*)ctx;
+    const int64_t nnz = m->row_ptr[m->nr];
+    memcpy(row_ptr, m->row_ptr, sizeof(int64_t) * (size_t)(m->nr + 1));
+    memcpy(cols, m->cols, sizeof(int32_t) * (size_t)nnz);
+    const int vb = m->val_bytes ? m->val_bytes : 4;
+    if (vb == 4) {
+        memcpy(vals, m->vals, sizeof(int32_t) * (size_t)nnz);
+    } else if (vb == 2) {
+        const uint16_t* v = (const uint16_t*)m->vals;
+        for (int64_t k = 0; k < nnz; ++k) vals[k] = v[k];
+    } else {
+        const uint8_t* v = (const uint8_t*)m->vals;
+        for (int64_t k = 0; k < nnz; ++k) vals[k] = v[k];
+    }
+}
+
 void plan_destroy(Plan* P) { delete P; }
 const gbgpu_stats& plan_stats(const Plan* P) { return P->stats; }
 
@@ -1075,24 +1093,6 @@ void gbgpu_plan_destroy(gbgpu_plan* plan) {
     delete plan;
 }
 
-// host CSR of a gbgpu_csr into the small path's staging (values widened)
-static void fill_from_csr(void* ctx, int64_t* row_ptr, int32_t* cols, uint32_t* vals) {
-    const gbgpu_csr* m = (const gbgpu_csr*)ctx;
-    const int64_t nnz = m->row_ptr[m->nr];
-    memcpy(row_ptr, m->row_ptr, sizeof(int64_t) * (size_t)(m->nr + 1));
-    memcpy(cols, m->cols, sizeof(int32_t) * (size_t)nnz);
-    const int vb = val_bytes_of(m);
-    if (vb == 4) {
-        memcpy(vals, m->vals, sizeof(int32_t) * (size_t)nnz);
-    } else if (vb == 2) {
-        const uint16_t* v = (const uint16_t*)m->vals;
-        for (int64_t k = 0; k < nnz; ++k) vals[k] = v[k];
-    } else {
-        const uint8_t* v = (const uint8_t*)m->vals;
-        for (int64_t k = 0; k < nnz; ++k) vals[k] = v[k];
-    }
-}
-
 // small matrices take the one-pass path of small.cu (AUTO or the sparse-row
 // form, library stream, no profiling); *handled tells whether it ran
 static int reduce_small(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows* out,
@@ -1109,7 +1109,7 @@ static int reduce_small(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows
     if (m->row_ptr[0] != 0 || m->row_ptr[m->nr] < 0) return GBGPU_OK;
     if (!small_eligible(m->nr, m->ncl, m->ncr, o.device)) return GBGPU_OK;
     *handled = true;
-    SmallInput in{m->p, m->nr, m->ncl, m->ncr, m->row_ptr[m->nr], o.device, fill_from_csr,
+    SmallInput in{m->p, m->nr, m->ncl, m->ncr, m->row_ptr[m->nr], o.device, fill_from_csr_vals,
                   (void*)m};
     SmallAnswer a;
     int rc = small_reduce(in, &a);

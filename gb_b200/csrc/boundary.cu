@@ -18,6 +18,8 @@
 #include <ctime>
 #include <sys/time.h>
 #include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -245,6 +247,17 @@ void gbgpu_interreduce_matrix_rows(gbgpu_mat_t* mat, gbgpu_bs_t* bs, const gbgpu
     }
 }
 
+// a batch matrix the one-launch small-matrix kernel takes
+static bool batch_small(const gbgpu_csr& m, const gbgpu_options* opt) {
+    if (opt && !(opt->form == GBGPU_FORM_AUTO || opt->form == GBGPU_FORM_PLAIN)) return false;
+    if (opt && opt->profile) return false;
+    if (m.p < 2 || m.nr <= 0 || !m.row_ptr || !m.cols || !m.vals || m.row_ptr[0] != 0) return false;
+    const int vb = m.val_bytes ? m.val_bytes : 4;
+    if (!(vb == 1 || vb == 2 || vb == 4) || (vb < 4 && (int64_t)m.p >= ((int64_t)1 << (8 * vb))))
+        return false;
+    return small_batch_bytes(m.nr, m.ncl, m.ncr, opt ? opt->device : 0) > 0;
+}
+
 int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
                        gbgpu_rows* outs, int32_t* status) {
     if (n < 0 || (n > 0 && (!ms || !outs || !status))) return GBGPU_EINVAL;
@@ -252,21 +265,62 @@ int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
         memset(&outs[i], 0, sizeof(gbgpu_rows));
         status[i] = GBGPU_OK;
     }
-    // A few host workers, each reducing one matrix at a time on a stream of
-    // its own: the reductions of different matrices overlap on the device
-    // (their host round trips and small launches interleave), and at most
-    // `workers` matrices hold device memory at once.
+    // The small matrices of the batch go to ONE persistent launch (small.cu,
+    // a device work queue over the matrices); the others are reduced by a few
+    // host workers, each one matrix at a time on a stream of its own, so
+    // that their host round trips and small launches interleave on the device
+    // (and at most `workers` of them hold device memory at once).  The small
+    // launch runs on the calling thread while the workers run.
+    std::vector<int32_t> small_idx, big_idx;
+    for (int32_t i = 0; i < n; ++i)
+        (batch_small(ms[i], opt) ? small_idx : big_idx).push_back(i);
     int workers = 4;
     if (const char* w = getenv("GBGPU_BATCH_WORKERS")) workers = std::max(1, atoi(w));
-    workers = std::min<int>(workers, std::max<int32_t>(n, 1));
+    workers = std::min<int>(workers, std::max<int>((int)big_idx.size(), 1));
     const int device = opt ? opt->device : 0;
     std::atomic<int32_t> next{0};
+    const int32_t n_big = (int32_t)big_idx.size();
+    // device-memory gate: the matrices in flight together stay within 60% of
+    // the memory free when the batch starts (one matrix always runs)
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(device) == cudaSuccess) cudaMemGetInfo(&free_b, &total_b);
+    const double budget = 0.6 * (double)free_b;
+    double in_flight = 0.0;
+    std::mutex gate_mu;
+    std::condition_variable gate_cv;
+    auto estimate = [&](const gbgpu_csr& m) {
+        const double t = std::max(0, m.nr - m.ncl), nc = (double)m.ncl + m.ncr;
+        const double nnz = m.nr > 0 && m.row_ptr ? (double)m.row_ptr[m.nr] : 0.0;
+        return nnz * 12.0 + (t + m.ncl) * nc * 4.0 + 2.0 * (t + m.ncr) * m.ncl +
+               t * (double)m.ncr * 8.0;
+    };
     auto work = [&]() {
         if (cudaSetDevice(device) != cudaSuccess) {
-            for (int32_t i; (i = next.fetch_add(1)) < n;) status[i] = GBGPU_ECUDA;
+            for (int32_t k; (k = next.fetch_add(1)) < n_big;) status[big_idx[k]] = GBGPU_ECUDA;
             return;
         }
-        for (int32_t i; (i = next.fetch_add(1)) < n;) {
+        for (int32_t k; (k = next.fetch_add(1)) < n_big;) {
+            const int32_t i = big_idx[k];
+            const double need = estimate(ms[i]);
+            {
+                std::unique_lock<std::mutex> lock(gate_mu);
+                gate_cv.wait(lock, [&] { return in_flight == 0.0 || in_flight + need <= budget; });
+                in_flight += need;
+            }
+            struct Release {
+                std::mutex& mu;
+                std::condition_variable& cv;
+                double& fl;
+                double n;
+                ~Release() {
+                    {
+                        std::lock_guard<std::mutex> lock(mu);
+                        fl -= n;
+                        if (fl < 1.0) fl = 0.0;
+                    }
+                    cv.notify_all();
+                }
+            } release{gate_mu, gate_cv, in_flight, need};
             gbgpu_options o{};
             if (opt) o = *opt;
             o.stream = nullptr;  // the plan creates its own stream
@@ -281,8 +335,20 @@ int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
         }
     };
     std::vector<std::thread> pool;
-    for (int k = 1; k < workers; ++k) pool.emplace_back(work);
-    work();
+    if (n_big > 0)
+        for (int k = 0; k < workers; ++k) pool.emplace_back(work);
+    if (!small_idx.empty()) {
+        std::vector<const gbgpu_csr*> sm;
+        for (int32_t i : small_idx) sm.push_back(&ms[i]);
+        std::vector<gbgpu_rows> so(sm.size());
+        std::vector<int32_t> ss(sm.size(), GBGPU_OK);
+        for (auto& r : so) memset(&r, 0, sizeof(r));
+        int rc = small_batch((int32_t)sm.size(), sm.data(), device, so.data(), ss.data());
+        for (size_t k = 0; k < sm.size(); ++k) {
+            outs[small_idx[k]] = so[k];
+            status[small_idx[k]] = rc ? rc : ss[k];
+        }
+    }
     for (auto& th : pool) th.join();
     return GBGPU_OK;
 }

@@ -27,12 +27,14 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/gbgpu.h"
 #include "common.cuh"
 #include "internal.h"
 #include "kernels.h"
 #include "small.h"
+#include "tiny.cuh"
 
 namespace gbgpu {
 
@@ -46,11 +48,12 @@ constexpr int kRowWarpsMax = 16;      // warps (rows) per CTA of k_reduce_rows_w
 // Input checks (the contract k_check_rows enforces), the known pivot of every
 // left column (first row with that lead, src/la_ff_16.c:762-772), the check
 // that every left column has one, and the C|D rows in row order -- one CTA.
-__global__ void __launch_bounds__(kPrepThreads)
-k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __restrict__ row_ptr,
-             const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals,
-             int32_t* piv_row, int32_t* work, int32_t* n_work, uint32_t* err) {
-    extern __shared__ int32_t prep_tab[];  // [ncl]: first row of each lead
+__device__ void small_prep_body(int32_t nr, int32_t ncl, int32_t nc, uint32_t p,
+                                const int64_t* __restrict__ row_ptr,
+                                const int32_t* __restrict__ cols,
+                                const uint32_t* __restrict__ vals, int32_t* piv_row,
+                                int32_t* work, int32_t* n_work, uint32_t* err,
+                                int32_t* prep_tab /* smem [ncl] */) {
     __shared__ uint32_t s_err;
     __shared__ int s_warp[kPrepThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -116,6 +119,14 @@ k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __r
     }
 }
 
+__global__ void __launch_bounds__(kPrepThreads)
+k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __restrict__ row_ptr,
+             const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals,
+             int32_t* piv_row, int32_t* work, int32_t* n_work, uint32_t* err) {
+    extern __shared__ int32_t prep_smem[];  // [ncl]: first row of each lead
+    small_prep_body(nr, ncl, nc, p, row_ptr, cols, vals, piv_row, work, n_work, err, prep_smem);
+}
+
 // One warp per C|D row: the row is scattered into a dense accumulator of nc
 // residues in shared memory, then the known pivots are applied in column
 // order -- the next column to clear is the first nonzero left column after
@@ -123,20 +134,20 @@ k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __r
 // row (monic, its lead skipped) is applied by the 32 lanes in coalesced
 // strides (distinct columns, no conflicts).  The right block is written out
 // dense with its lead.  Nothing is read when the checks flagged the input.
+// rows w = first, first + step, ... (< n_rows) by the calling warp, whose
+// accumulator is acc (stride entries, 16-byte aligned)
 template <class F>
-__global__ void __launch_bounds__(kRowWarpsMax * 32)
-k_reduce_rows_warp(int32_t n_rows, const int32_t* __restrict__ work,
-                   const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
-                   const uint32_t* __restrict__ vals, const int32_t* __restrict__ piv_row,
-                   int32_t ncl, int32_t nc, int32_t stride, uint32_t* out, int64_t ld,
-                   int32_t* out_lead, const uint32_t* err, F f) {
-    extern __shared__ __align__(16) uint32_t rw_acc[];
-    if (*err) return;  // invalid input: nothing is read (uniform)
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wpc = blockDim.x >> 5;
-    uint32_t* acc = rw_acc + (size_t)warp * stride;
+__device__ void rows_warp_body(int32_t n_rows, int w0, int step,
+                               const int32_t* __restrict__ work,
+                               const int64_t* __restrict__ row_ptr,
+                               const int32_t* __restrict__ cols,
+                               const uint32_t* __restrict__ vals,
+                               const int32_t* __restrict__ piv_row, int32_t ncl, int32_t nc,
+                               int32_t stride, uint32_t* out, int64_t ld, int32_t* out_lead,
+                               F f, uint32_t* acc) {
+    const int lane = threadIdx.x & 31;
     const int32_t ncr = nc - ncl;
-    for (int w = blockIdx.x * wpc + warp; w < n_rows; w += gridDim.x * wpc) {
+    for (int w = w0; w < n_rows; w += step) {
         const int32_t r = work[w];
         const int64_t rb = row_ptr[r], re = row_ptr[r + 1];
         const int32_t lead = cols[rb];
@@ -160,7 +171,22 @@ k_reduce_rows_warp(int32_t n_rows, const int32_t* __restrict__ work,
             const uint32_t m = f.prep(acc[found]);
             const int32_t pr = piv_row[found];
             const int64_t pb = row_ptr[pr] + 1, pe = row_ptr[pr + 1];
-            for (int64_t k = pb + lane; k < pe; k += 32) {
+            // four entries per lane at a time (distinct columns: loads first)
+            int64_t k = pb + lane;
+            for (; k + 96 < pe; k += 128) {
+                int32_t c[4];
+                uint32_t v[4], y[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    c[u] = cols[k + 32 * u];
+                    v[u] = vals[k + 32 * u];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) y[u] = acc[c[u]];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[c[u]] = f.mulsub(y[u], m, v[u]);
+            }
+            for (; k < pe; k += 32) {
                 const int32_t c = cols[k];
                 acc[c] = f.mulsub(acc[c], m, vals[k]);
             }
@@ -178,6 +204,135 @@ k_reduce_rows_warp(int32_t n_rows, const int32_t* __restrict__ work,
         }
         if (lane == 0) out_lead[w] = first;
         __syncwarp();
+    }
+}
+
+template <class F>
+__global__ void __launch_bounds__(kRowWarpsMax * 32)
+k_reduce_rows_warp(int32_t n_rows, const int32_t* __restrict__ work,
+                   const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
+                   const uint32_t* __restrict__ vals, const int32_t* __restrict__ piv_row,
+                   int32_t ncl, int32_t nc, int32_t stride, uint32_t* out, int64_t ld,
+                   int32_t* out_lead, const uint32_t* err, F f) {
+    extern __shared__ __align__(16) uint32_t rw_acc[];
+    if (*err) return;  // invalid input: nothing is read (uniform)
+    const int warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+    rows_warp_body(n_rows, blockIdx.x * wpc + warp, gridDim.x * wpc, work, row_ptr, cols, vals,
+                   piv_row, ncl, nc, stride, out, ld, out_lead, f,
+                   rw_acc + (size_t)warp * stride);
+}
+
+
+// ---------------------------------------------------------------------------
+// batches: every small matrix of a batch in ONE launch.  Each CTA takes the
+// next matrix from a device work queue and runs the three phases above on it
+// (checks and classification, warp-per-row known-pivot reduction into its
+// scratch, one-CTA echelon and compaction into mapped host memory), so the
+// uneven small matrices of a batch share one persistent launch.
+
+struct BatchItem {
+    int32_t p, nr, ncl, ncr;
+    int64_t in_off, cols_off, vals_off;  // bytes into the input buffer
+    int64_t scr_off;                     // bytes into the scratch buffer
+    int64_t out_off;                     // bytes into the mapped output
+    FieldSmall fs;
+    FieldMont fm;
+};
+
+// scratch of one matrix: piv_row [ncl] | work [nr] | n_work, err | D [n_work][ld] |
+// lead [n_work] | piv_of_col [ncr]
+struct ScrLayout {
+    int64_t piv, work, cnt, D, lead, poc, bytes, ld;
+};
+__host__ __device__ inline int64_t rup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+__host__ __device__ inline ScrLayout scr_layout(int32_t nr, int32_t ncl, int32_t ncr) {
+    ScrLayout L;
+    const int64_t nw = nr - ncl > 0 ? nr - ncl : 1;
+    L.ld = rup(ncr > 0 ? ncr : 1, 4);
+    L.piv = 0;
+    L.work = rup(4 * (int64_t)(ncl > 0 ? ncl : 1), 256);
+    L.cnt = L.work + rup(4 * (int64_t)nr, 256);
+    L.D = L.cnt + 256;
+    L.lead = L.D + rup(4 * nw * L.ld, 256);
+    L.poc = L.lead + rup(4 * nw, 256);
+    L.bytes = L.poc + rup(4 * (int64_t)(ncr > 0 ? ncr : 1), 256);
+    return L;
+}
+// mapped output of one matrix: counts[2], err | offs [n_work + 1] | cols | vals
+struct OutLayout {
+    int64_t offs, cols, vals, bytes;
+};
+__host__ __device__ inline OutLayout out_layout(int32_t nr, int32_t ncl, int32_t ncr) {
+    OutLayout L;
+    const int64_t nw = nr - ncl > 0 ? nr - ncl : 0;
+    const int64_t cap = nw * (ncr > 0 ? ncr : 0);
+    L.offs = 32;
+    L.cols = rup(L.offs + 8 * (nw + 1), 16);
+    L.vals = rup(L.cols + 4 * (cap > 0 ? cap : 1), 16);
+    L.bytes = rup(L.vals + 4 * (cap > 0 ? cap : 1), 256);
+    return L;
+}
+
+__global__ void __launch_bounds__(kPrepThreads)
+k_batch_small(int32_t n, const BatchItem* __restrict__ items, const uint8_t* __restrict__ in,
+              uint8_t* scr, uint8_t* out, int32_t* queue, int32_t smem_bytes) {
+    extern __shared__ __align__(16) uint8_t bt_smem[];
+    __shared__ int s_item;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int i = s_item;
+        __syncthreads();
+        if (i >= n) break;
+        const BatchItem it = items[i];
+        const int32_t nr = it.nr, ncl = it.ncl, ncr = it.ncr, nc = ncl + ncr;
+        const int64_t* row_ptr = (const int64_t*)(in + it.in_off);
+        const int32_t* cols = (const int32_t*)(in + it.cols_off);
+        const uint32_t* vals = (const uint32_t*)(in + it.vals_off);
+        const ScrLayout S = scr_layout(nr, ncl, ncr);
+        uint8_t* sb = scr + it.scr_off;
+        int32_t* piv = (int32_t*)(sb + S.piv);
+        int32_t* work = (int32_t*)(sb + S.work);
+        int32_t* nwork = (int32_t*)(sb + S.cnt);
+        uint32_t* err = (uint32_t*)(sb + S.cnt + 16);
+        uint32_t* D = (uint32_t*)(sb + S.D);
+        int32_t* lead = (int32_t*)(sb + S.lead);
+        int32_t* poc = (int32_t*)(sb + S.poc);
+        const OutLayout O = out_layout(nr, ncl, ncr);
+        uint8_t* ob = out + it.out_off;
+        int64_t* counts = (int64_t*)ob;
+        small_prep_body(nr, ncl, nc, (uint32_t)it.p, row_ptr, cols, vals, piv, work, nwork, err,
+                        (int32_t*)bt_smem);
+        __syncthreads();  // prep's global writes are visible to the block
+        const uint32_t e = *err;
+        const int32_t n_work = nr - ncl;
+        if (e == 0 && n_work > 0) {
+            const int32_t stride = (int32_t)rup(nc > 0 ? nc : 1, 4);
+            const int wpc = min(kPrepThreads / 32, smem_bytes / (stride * 4));
+            const TinyOut to{ncl, (int64_t*)(ob + O.offs), (int32_t*)(ob + O.cols),
+                             (int32_t*)(ob + O.vals), poc, counts};
+            uint32_t* acc = (uint32_t*)bt_smem + (size_t)warp * stride;
+            if ((uint32_t)it.p < 65536u) {
+                if (warp < wpc)
+                    rows_warp_body(n_work, warp, wpc, work, row_ptr, cols, vals, piv, ncl, nc,
+                                   stride, D, S.ld, lead, it.fs, acc);
+                __syncthreads();
+                tiny_rref_body(n_work, ncr, D, S.ld, lead, err, to, it.fs, (uint32_t*)bt_smem);
+            } else {
+                if (warp < wpc)
+                    rows_warp_body(n_work, warp, wpc, work, row_ptr, cols, vals, piv, ncl, nc,
+                                   stride, D, S.ld, lead, it.fm, acc);
+                __syncthreads();
+                tiny_rref_body(n_work, ncr, D, S.ld, lead, err, to, it.fm, (uint32_t*)bt_smem);
+            }
+        } else if (tid == 0) {
+            counts[0] = 0;
+            counts[1] = 0;
+            ((int64_t*)(ob + O.offs))[0] = 0;
+        }
+        if (tid == 0) counts[2] = (int64_t)e;
+        __syncthreads();  // the shared memory is reused by the next matrix
     }
 }
 
@@ -432,6 +587,132 @@ int small_reduce(const SmallInput& in, SmallAnswer* ans) {
     ans->offs = (const int64_t*)(S->hout + h_offs);
     ans->cols = (const int32_t*)(S->hout + h_cols);
     ans->vals = (const int32_t*)(S->hout + h_vals);
+    return GBGPU_OK;
+}
+
+
+int small_batch_bytes(int32_t nr, int32_t ncl, int32_t ncr, int device) {
+    if (nr <= 0 || ncl < 0 || ncr <= 0 || nr < ncl || ncl > kSmallMaxLeft) return 0;
+    DeviceGuard guard;
+    DeviceInfo dev{};
+    if (device_init(device, &dev)) return 0;
+    const int64_t stride = rup(ncl + ncr, 4);
+    const int64_t rows = 4 * 4 * stride;  // at least four row warps
+    const int32_t n_work = nr - ncl;
+    const int64_t tiny = n_work > 0 ? tiny_rref_bytes(n_work, ncr, dev.smem_optin) : 1;
+    if (tiny <= 0) return 0;
+    const int64_t need = std::max<int64_t>({4 * (int64_t)std::max(ncl, 1), rows, tiny});
+    return need + 2048 <= dev.smem_optin ? (int)need : 0;
+}
+
+int small_batch(int32_t n, const gbgpu_csr* const* ms, int device, gbgpu_rows* outs,
+                int32_t* status) {
+    if (n <= 0) return GBGPU_OK;
+    DeviceGuard guard;
+    DeviceInfo dev{};
+    int rc = device_init(device, &dev);
+    if (rc) return rc;
+    std::vector<BatchItem> items((size_t)n);
+    int64_t in_bytes = 0, scr_bytes = 0, out_bytes = 0;
+    int smem = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        const gbgpu_csr* m = ms[i];
+        BatchItem& it = items[i];
+        it.p = m->p;
+        it.nr = m->nr;
+        it.ncl = m->ncl;
+        it.ncr = m->ncr;
+        const int64_t nnz = m->row_ptr[m->nr];
+        it.in_off = in_bytes;
+        it.cols_off = rup(it.in_off + 8 * (int64_t)(m->nr + 1), 16);
+        it.vals_off = rup(it.cols_off + 4 * nnz, 16);
+        in_bytes = rup(it.vals_off + 4 * nnz, 256);
+        it.scr_off = scr_bytes;
+        scr_bytes += scr_layout(m->nr, m->ncl, m->ncr).bytes;
+        it.out_off = out_bytes;
+        out_bytes += out_layout(m->nr, m->ncl, m->ncr).bytes;
+        it.fs = FieldSmall::make((uint32_t)std::max(m->p, 2));
+        it.fm = FieldMont::make((uint32_t)(m->p | 1));  // used only for odd p >= 2^16
+        smem = std::max(smem, small_batch_bytes(m->nr, m->ncl, m->ncr, device));
+    }
+    smem = std::min(dev.smem_optin - 2048, std::max(smem, 4 * 4 * 1024));
+    uint8_t *h_in = nullptr, *h_out = nullptr, *d_out = nullptr, *d_in = nullptr;
+    BatchItem* d_items = nullptr;
+    int32_t* d_queue = nullptr;
+    cudaStream_t s = nullptr;
+    auto cleanup = [&]() {
+        if (s) cudaStreamSynchronize(s);
+        if (d_in) cudaFree(d_in);
+        if (h_in) cudaFreeHost(h_in);
+        if (h_out) cudaFreeHost(h_out);
+        if (s) cudaStreamDestroy(s);
+    };
+    // device: input | scratch | items | queue
+    const int64_t o_scr = rup(in_bytes, 256), o_items = rup(o_scr + scr_bytes, 256);
+    const int64_t o_queue = rup(o_items + (int64_t)sizeof(BatchItem) * n, 256);
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaHostAlloc((void**)&h_in, (size_t)std::max<int64_t>(in_bytes, 16), 0) != cudaSuccess ||
+        cudaHostAlloc((void**)&h_out, (size_t)std::max<int64_t>(out_bytes, 256),
+                      cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&d_out, h_out, 0) != cudaSuccess ||
+        cudaMalloc((void**)&d_in, (size_t)(o_queue + 256)) != cudaSuccess) {
+        cleanup();
+        set_error("small-matrix batch: allocation failed");
+        return GBGPU_ENOMEM;
+    }
+    for (int32_t i = 0; i < n; ++i) {
+        const gbgpu_csr* m = ms[i];
+        fill_from_csr_vals((void*)m, (int64_t*)(h_in + items[i].in_off),
+                           (int32_t*)(h_in + items[i].cols_off),
+                           (uint32_t*)(h_in + items[i].vals_off));
+    }
+    d_items = (BatchItem*)(d_in + o_items);
+    d_queue = (int32_t*)(d_in + o_queue);
+    cudaError_t e = cudaMemcpyAsync(d_in, h_in, (size_t)in_bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_items, items.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_queue, 0, sizeof(int32_t), s);
+    if (e == cudaSuccess) e = ensure_smem_limit((const void*)k_batch_small, smem);
+    if (e == cudaSuccess) {
+        const int per_sm = std::max(1, std::min(2, (dev.smem_optin - 1024) / (smem + 1024)));
+        const int grid = std::max(1, std::min(n, dev.sms * per_sm));
+        k_batch_small<<<grid, kPrepThreads, smem, s>>>(n, d_items, d_in, d_in + o_scr, d_out,
+                                                       d_queue, smem);
+        count_launch(1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(std::string("small-matrix batch: ") + cudaGetErrorString(e));
+        for (int32_t i = 0; i < n; ++i) status[i] = GBGPU_ECUDA;
+        cleanup();
+        return GBGPU_OK;
+    }
+    for (int32_t i = 0; i < n; ++i) {
+        const uint8_t* ob = h_out + items[i].out_off;
+        const OutLayout O = out_layout(items[i].nr, items[i].ncl, items[i].ncr);
+        const int64_t* counts = (const int64_t*)ob;
+        if (counts[2]) {
+            std::string msg;
+            status[i] = err_to_status((uint32_t)counts[2], &msg);
+            continue;
+        }
+        gbgpu_rows& r = outs[i];
+        r.np = (int32_t)counts[0];
+        r.nnz = counts[1];
+        r.row_ptr = (int64_t*)malloc(sizeof(int64_t) * (size_t)(r.np + 1));
+        r.cols = (int32_t*)malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(r.nnz, 1));
+        r.vals = (int32_t*)malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(r.nnz, 1));
+        if (!r.row_ptr || !r.cols || !r.vals) {
+            status[i] = GBGPU_ENOMEM;
+            continue;
+        }
+        memcpy(r.row_ptr, ob + O.offs, sizeof(int64_t) * (size_t)(r.np + 1));
+        memcpy(r.cols, ob + O.cols, sizeof(int32_t) * (size_t)r.nnz);
+        memcpy(r.vals, ob + O.vals, sizeof(int32_t) * (size_t)r.nnz);
+        status[i] = GBGPU_OK;
+    }
+    cleanup();
     return GBGPU_OK;
 }
 

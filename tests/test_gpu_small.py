@@ -81,3 +81,39 @@ def test_small_path_rejects_contract_violations():
     assert ei.value.code == _lib.GBGPU_EINVAL and "coefficient" in str(ei.value)
     # a good matrix right after a rejected one is reduced correctly
     assert la.linear_algebra(m).equals(oracle.oracle_la(m)[0])
+
+
+def test_batch_of_small_matrices_is_one_launch():
+    """A batch of small matrices (uneven shapes, several primes, one that
+    breaks the contract) is reduced in ONE persistent launch with a device
+    work queue; every answer equals the oracle's, the bad matrix alone fails."""
+    lib = _lib.load()
+    mats = []
+    for i in range(40):
+        p = PRIMES[i % len(PRIMES)]
+        mats.append(synth.random_macaulay(20 + 7 * i, 10 + 3 * i, 30 + 5 * i, p, density=0.15,
+                                          seed=100 + i, dup_rows=min(3, 10 + 3 * i)))
+    bad = mats[7]
+    mats[7] = MacaulayMatrix(bad.p, bad.ncl, bad.ncr, bad.row_ptr, bad.cols, bad.vals.copy())
+    mats[7].vals[mats[7].row_ptr[2] + 1] = 0  # zero coefficient
+    before = lib.gbgpu_kernel_launches()
+    outs, status = la.reduce_batch(mats)
+    assert lib.gbgpu_kernel_launches() - before == 1
+    for i, m in enumerate(mats):
+        if i == 7:
+            assert status[i] == _lib.GBGPU_EINVAL and outs[i] is None
+            continue
+        assert status[i] == 0, (i, status[i])
+        want, _ = oracle.oracle_la(m)
+        assert outs[i].equals(want), (i, outs[i].first_difference(want))
+
+
+def test_batch_mixed_small_and_blocked():
+    mats = [synth.random_macaulay(30, 20, 40, 32003, density=0.2, seed=1),
+            synth.staircase(1200, 400, 1500, 65521, seed=2),
+            synth.random_macaulay(50, 30, 60, 2147483647, density=0.2, seed=3),
+            synth.staircase(900, 300, 1000, 2147483647, seed=4)]
+    outs, status = la.reduce_batch(mats)
+    assert list(status) == [0, 0, 0, 0]
+    for m, o in zip(mats, outs):
+        assert o.equals(oracle.oracle_la(m)[0])
