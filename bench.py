@@ -684,6 +684,12 @@ def run_batch(args):
         for i in range(n):
             lib.gbgpu_rows_free(Cc.byref(outs[i]))
 
+    # the tile shapes of the tensor-core GEMM, tuned on this GPU for this run
+    tune_path = os.path.join(tempfile.gettempdir(), f"gbgpu_shapes_{os.getpid()}.txt")
+    tuned = None
+    if lib.gbgpu_autotune(local, tune_path.encode()) == 0:
+        with open(tune_path) as fh:
+            tuned = [l.strip() for l in fh if not l.startswith("#")]
     few = (_lib.Csr * 8)(*[la._csr(m) for m in mats[:8]])
     _, wo, _ = batch(few, 8)  # warm-up: kernels, sessions
     free(wo, 8)
@@ -744,7 +750,8 @@ def run_batch(args):
             "largest": max([m.nr, m.nc] for m in mats),
             "image_shape": [images[0][0].nr, images[0][0].nc], "generate_s": gen_s,
             "answers_checked": checked, "answers_equal_reference": ok == checked,
-            "largest_mid_size_equals_plain_form": plain_ok}
+            "largest_mid_size_equals_plain_form": plain_ok,
+            "tuned_tile_shapes": tuned}
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = {
             "value": (len(images) + len(small)) / (img_cpu + cpu_s), "unit": "matrices/s",

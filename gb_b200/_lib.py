@@ -69,7 +69,7 @@ EXPORTS = [
     "gbgpu_plan_stats", "gbgpu_plan_destroy", "gbgpu_reduce_batch", "gbgpu_layout",
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
     "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into", "gbgpu_dense_rref",
-    "gbgpu_plan_result_into_v", "gbgpu_plan_run_into_v",
+    "gbgpu_plan_result_into_v", "gbgpu_plan_run_into_v", "gbgpu_autotune",
 ]
 
 _lib = None
@@ -113,6 +113,7 @@ def load(path: str = LIB_PATH):
         C.c_void_p]
     lib.gbgpu_dense_rref.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
                                      _PI32, C.c_void_p, C.POINTER(Options)]
+    lib.gbgpu_autotune.argtypes = [C.c_int32, C.c_char_p]
     lib.gbgpu_last_error.restype = C.c_char_p
     lib.gbgpu_kernel_launches.restype = C.c_int64
     _lib = lib

@@ -959,16 +959,24 @@ int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err
         set_error("tensor-core path needs an odd prime");
         return GBGPU_EINVAL;
     }
+    return tc_submul_shape(g, workspace, s, err, launches, tc_shape_for(limbs_for(g.p), g.K));
+}
+
+// the shapes: 0 big, 1 small (K <= 256, L <= 2), 2 mid (L = 2); any other
+// request falls back to the big shape
+int tc_submul_shape(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
+                    long long* launches, int shape) {
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.batch <= 0) return GBGPU_OK;
     uint8_t* planes = (uint8_t*)workspace;
-    const bool small = g.K <= 256;  // at most two K steps: the small tile shape
+    const bool small = shape == 1 && g.K <= 256;
     switch (limbs_for(g.p)) {
         case 1:
             return small ? tc_run<1, TC_SMALL>(g, planes, s, err, launches)
                          : tc_run<1, TC_BIG>(g, planes, s, err, launches);
         case 2:
-            return small            ? tc_run<2, TC_SMALL>(g, planes, s, err, launches)
-                   : g.K <= 1536    ? tc_run<2, TC_MID>(g, planes, s, err, launches)
-                                    : tc_run<2, TC_BIG>(g, planes, s, err, launches);
+            return small         ? tc_run<2, TC_SMALL>(g, planes, s, err, launches)
+                   : shape == 2  ? tc_run<2, TC_MID>(g, planes, s, err, launches)
+                                 : tc_run<2, TC_BIG>(g, planes, s, err, launches);
         case 3: return tc_run<3, TC_BIG>(g, planes, s, err, launches);
         default: return tc_run<4, TC_BIG>(g, planes, s, err, launches);
     }

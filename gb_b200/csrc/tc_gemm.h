@@ -51,6 +51,11 @@ size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K, int32_t b
 // bounded wait expired
 int tc_submul(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
               long long* launches);
+// the same with an explicit tile shape (0 big, 1 small, 2 mid; tune.cu)
+int tc_submul_shape(const TcGemmArgs& g, void* workspace, cudaStream_t s, int32_t* err,
+                    long long* launches, int shape);
+// the tile shape the autotuner's cache (or the built-in rule) picks for L, K
+int tc_shape_for(int L, int K);
 // CUDA-core path (any p)
 int plain_submul(const TcGemmArgs& g, cudaStream_t s, long long* launches);
 

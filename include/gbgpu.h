@@ -285,6 +285,16 @@ int gbgpu_dense_submul_noalloc(int32_t p, int32_t M, int32_t N, int32_t K,
                                const uint32_t *B, int64_t ldb, uint32_t *D,
                                int64_t ldd, int32_t device, void *stream);
 
+/* ---- autotuning -------------------------------------------------------- */
+/* Times every tile shape of the tensor-core GEMM for every limb count the
+ * shapes differ in (1 and 2) and every band of reduction depths K on this
+ * device, and writes the fastest shape per (limbs, K band) to the cache file
+ * `path` (NULL: $GBGPU_TUNE_FILE, else $HOME/.cache/gbgpu/gemm_shapes.txt),
+ * which every later process reads at its first GEMM; this process uses the
+ * result at once.  No counterpart in the reference (it has no GPU code); the
+ * tuned choice never changes a result, only its speed.  About 2 s. */
+int gbgpu_autotune(int32_t device, const char *path);
+
 /* ---- misc ------------------------------------------------------------ */
 /* Fills out[0..n) with sizeof/offsetof values of the mirrored structs in
  * the order the test-suite compares; returns how many it knows. */

@@ -133,3 +133,26 @@ def test_dense_rref_exact(form, p, rows, cols, rank):
     assert pc.cpu().numpy()[: rk.value].tolist() == piv
     assert np.array_equal(got[: rk.value], want)
     assert not got[rk.value:].any()
+
+
+def test_autotune_writes_a_cache_and_keeps_results_exact(tmp_path, monkeypatch):
+    """gbgpu_autotune times the tile shapes on this GPU, writes one valid line
+    per (limbs, K band) it tuned, and the GEMMs after it stay exact."""
+    lib = _lib.load()
+    path = tmp_path / "shapes.txt"
+    _lib.check(lib.gbgpu_autotune(0, str(path).encode()))
+    lines = [l.split() for l in path.read_text().splitlines() if not l.startswith("#")]
+    assert len(lines) >= 9
+    for L, kmax, shape in lines:
+        assert int(L) in (1, 2) and int(shape) in (0, 1, 2)
+        if int(shape) == 1:
+            assert int(kmax) <= 256
+        if int(shape) == 2:
+            assert int(L) == 2
+    for p, M, N, K in [(251, 300, 520, 700), (65521, 257, 130, 333), (65521, 200, 300, 2000)]:
+        rng = np.random.default_rng(K)
+        A = rng.integers(0, p, size=(M, K), dtype=np.int64)
+        B = rng.integers(0, p, size=(K, N), dtype=np.int64)
+        D = rng.integers(0, p, size=(M, N), dtype=np.int64)
+        got = run(_lib.FORM_TENSOR, p, A, B, D)
+        assert np.array_equal(got, exact_submul(D, A, B, p))
