@@ -70,6 +70,8 @@ EXPORTS = [
     "gbgpu_last_error", "gbgpu_kernel_launches", "gbgpu_dense_submul", "gbgpu_dense_submul_host",
     "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into", "gbgpu_dense_rref",
     "gbgpu_plan_result_into_v", "gbgpu_plan_run_into_v", "gbgpu_autotune",
+    "gbgpu_convert_hashes_to_columns_flat", "gbgpu_convert_hashes_to_columns",
+    "gbgpu_sort_matrix_rows",
 ]
 
 _lib = None
@@ -114,6 +116,8 @@ def load(path: str = LIB_PATH):
     lib.gbgpu_dense_rref.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
                                      _PI32, C.c_void_p, C.POINTER(Options)]
     lib.gbgpu_autotune.argtypes = [C.c_int32, C.c_char_p]
+    lib.gbgpu_convert_hashes_to_columns_flat.argtypes = [C.c_int32, C.c_int32] + [
+        C.c_void_p] * 3 + [C.c_int32, C.c_int32] + [C.c_void_p] * 7 + [C.c_int32]
     lib.gbgpu_last_error.restype = C.c_char_p
     lib.gbgpu_kernel_launches.restype = C.c_int64
     _lib = lib

@@ -287,3 +287,64 @@ def staircase_native(nru: int, nrl: int, ncr: int, p: int, dmin: float, dmax: fl
                                   vals.ctypes.data) != 0:
         raise ValueError("bad staircase parameters")
     return MacaulayMatrix(p, nru, ncr, ptr, cols[:nnz], vals[:nnz], laopt)
+
+
+def f4_round(nv: int, maxdeg: int, n_cols: int, nr: int, n_piv: int, row_len: int,
+             seed: int = 0):
+    """Synthetic input of one F4 round's conversion step: n_cols distinct
+    monomials in nv variables of degree <= maxdeg (the secondary hash table,
+    hash index = position + 1), the first n_piv of them marked as lead
+    monomials of known pivots (idx 2, the rest 1), and nr rows of about
+    row_len distinct hash indices each whose first entry (the lead term) is a
+    pivot monomial.  Returns dict(nv, exps [n][nv] int16, deg, idx, row_ptr,
+    hashes)."""
+    from math import comb
+    if n_cols > comb(nv + maxdeg, maxdeg):
+        raise ValueError("fewer monomials of that degree than columns asked for")
+    rng = np.random.default_rng(seed)
+    mons = set()
+    for _ in range(64 * n_cols):
+        if len(mons) >= n_cols:
+            break
+        d = int(rng.integers(0, maxdeg + 1))
+        mons.add(tuple(int(x) for x in rng.multinomial(d, [1.0 / nv] * nv)))
+    if len(mons) < n_cols:
+        raise ValueError("could not draw enough distinct monomials")
+    mons = sorted(mons)
+    rng.shuffle(mons)
+    exps = np.array(mons, dtype=np.int16).reshape(n_cols, nv)
+    deg = exps.sum(axis=1).astype(np.int32)
+    idx = np.ones(n_cols, dtype=np.int32)
+    idx[:n_piv] = 2
+    perm = rng.permutation(n_cols)  # table order differs from the pivot marks
+    exps, deg, idx = exps[perm], deg[perm], idx[perm]
+    piv_hashes = np.flatnonzero(idx == 2) + 1
+    ptr = [0]
+    hashes = []
+    for i in range(nr):
+        lead = int(piv_hashes[i]) if i < len(piv_hashes) else int(rng.choice(piv_hashes))
+        k = max(1, int(rng.integers(max(1, row_len // 2), row_len + row_len // 2 + 1)))
+        k = min(k, n_cols)
+        cand = np.unique(rng.integers(1, n_cols + 1, size=2 * k + 8))
+        cand = cand[cand != lead]
+        rest = rng.permutation(cand)[:k - 1]
+        hashes.append(np.concatenate([[lead], rest]))
+        ptr.append(ptr[-1] + hashes[-1].shape[0])
+    return {"nv": nv, "exps": np.ascontiguousarray(exps), "deg": deg, "idx": idx,
+            "row_ptr": np.array(ptr, dtype=np.int64),
+            "hashes": np.concatenate(hashes).astype(np.int32)}
+
+
+def column_order_key(exps: np.ndarray, deg: np.ndarray, idx: np.ndarray, mo: int) -> list:
+    """Sort keys of the reference's column order (hcm_cmp, src/order.c:153-235)
+    for monomials given by rows of exps: pivot monomials (idx 2) first, then
+    DRL (mo 0): higher degree first, then the smaller exponent of the last
+    variable where they differ; LEX (mo 1): the larger exponent of the first
+    variable where they differ."""
+    keys = []
+    for e, d, i in zip(exps.tolist(), deg.tolist(), idx.tolist()):
+        if mo == 1:
+            keys.append((-i,) + tuple(-x for x in e))
+        else:
+            keys.append((-i, -d) + tuple(reversed(e)))
+    return keys

@@ -83,6 +83,22 @@ typedef struct gbgpu_stat_t { /* stat_t, src/data.h:157-211 */
     int32_t info_level, gen_pbm_file;
 } gbgpu_stat_t;
 
+/* hd_t and ht_t, src/data.h:69-97 (the hash data and the hash table) */
+typedef struct gbgpu_hd_t {
+    int32_t val, sdm, deg, idx;
+} gbgpu_hd_t;
+
+typedef struct gbgpu_ht_t {
+    int16_t **ev;        /* exponent vectors, exp_t = int16_t */
+    gbgpu_hd_t *hd;
+    int32_t *hmap;
+    int32_t eld, esz, hsz, nv;
+    int32_t *dm;
+    int32_t ndv, bpv;
+    int32_t *rn;
+    uint32_t rsd;
+} gbgpu_ht_t;
+
 /* Replaces `linear_algebra(mat, bs, st)` at src/f4.c:306 for every la option
  * (the function-pointer table of src/io.c:581-780).  Same contract as the
  * reference (src/la_ff_16.c:1430-1507): reads mat->r rows and bs->cf_X
@@ -102,6 +118,23 @@ void gbgpu_linear_algebra(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
  * order and sets mat->np = mat->nr. */
 void gbgpu_interreduce_matrix_rows(gbgpu_mat_t *mat, gbgpu_bs_t *bs,
                                    const gbgpu_stat_t *st);
+
+/* Replaces `convert_hashes_to_columns(&hcm, mat, st, sht)` at src/f4.c:299
+ * (src/convert.c:30-135): the columns of the round are the monomials
+ * 1 .. sht->eld-1 of the secondary hash table, ordered as the reference's
+ * hcm_cmp orders them (src/order.c:153-235; st->mo 0 DRL, 1 LEX) on the
+ * device; *hcmp (realloc'ed) receives the hash of every column, sht->hd[h].idx
+ * the column of hash h, every row's entries their columns, and mat->nru /
+ * ncl / nrl / ncr and st->num_rowsred are set as the reference sets them.
+ * The rows of mat->r also come back in the order of sort_matrix_rows
+ * (lead column, then length), so that the reference's sort which follows
+ * finds them sorted.  Prints the status and exits on error. */
+void gbgpu_convert_hashes_to_columns(int32_t **hcmp, gbgpu_mat_t *mat, gbgpu_stat_t *st,
+                                     gbgpu_ht_t *sht);
+/* Replaces `sort_matrix_rows(mat)` at src/f4.c:300 (src/order.c:125-131):
+ * rows by (lead column, length) on the device; rows that tie keep their
+ * order. */
+void gbgpu_sort_matrix_rows(gbgpu_mat_t *mat);
 
 /* Same as the two above but returning a status instead of exiting. */
 int gbgpu_linear_algebra_status(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
@@ -284,6 +317,23 @@ int gbgpu_dense_submul_noalloc(int32_t p, int32_t M, int32_t N, int32_t K,
                                const uint32_t *A, int64_t lda,
                                const uint32_t *B, int64_t ldb, uint32_t *D,
                                int64_t ldd, int32_t device, void *stream);
+
+/* ---- the step before the linear algebra -------------------------------- */
+/* convert_hashes_to_columns + sort_matrix_rows (src/convert.c:30-135,
+ * src/order.c:98-131) on flat host arrays: the n monomials of one round
+ * (exps[n][nv], total degrees deg[n], idx[n] = 2 for the lead monomials of
+ * known pivots, 1 otherwise; monomial i has hash index i + 1) and nr rows of
+ * hash indices (row_ptr[nr + 1], hashes[nnz], first entry = lead term); mo 0
+ * DRL, 1 LEX.  Outputs: hcm[n] (hash index of every column, in column order),
+ * *ncl (columns of known pivots), row_order[nr] (input row of every output
+ * row), out_row_ptr[nr + 1] and out_cols[nnz] (the rows in that order, every
+ * entry's column, entries in input order).  Rows tie-broken by input order. */
+int gbgpu_convert_hashes_to_columns_flat(int32_t nv, int32_t n, const int16_t *exps,
+                                         const int32_t *deg, const int32_t *idx, int32_t mo,
+                                         int32_t nr, const int64_t *row_ptr,
+                                         const int32_t *hashes, int32_t *hcm, int32_t *ncl,
+                                         int32_t *row_order, int64_t *out_row_ptr,
+                                         int32_t *out_cols, int32_t device);
 
 /* ---- autotuning -------------------------------------------------------- */
 /* Times every tile shape of the tensor-core GEMM for every limb count the

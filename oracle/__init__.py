@@ -26,6 +26,8 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgbref.so")
 # gb compiled with its two linear-algebra call sites rerouted to libgbgpu.so (linked to it)
 GB_GPU_SO = os.path.join(HERE, "_ref", "libgb_gpu.so")
+# the same with the hash -> column mapping and row sort rerouted too (ref/gb_gpu_full.c)
+GB_GPU_FULL_SO = os.path.join(HERE, "_ref", "libgb_gpu_full.so")
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
@@ -225,6 +227,22 @@ def gb_gpu_f4(case: dict):
     return _run_f4(_gb_gpu, case)
 
 
+_gb_gpu_full = None
+
+
+def gb_gpu_full_available() -> bool:
+    return os.path.exists(GB_GPU_FULL_SO)
+
+
+def gb_gpu_full_f4(case: dict):
+    """F4 of gb with the linear algebra AND the conversion / row sort before it
+    on libgbgpu.so (ref/gb_gpu_full.c).  Returns (lens, cfs, exps)."""
+    global _gb_gpu_full
+    if _gb_gpu_full is None:
+        _gb_gpu_full = _f4_binding(C.CDLL(GB_GPU_FULL_SO))
+    return _run_f4(_gb_gpu_full, case)
+
+
 def ref_f4(case: dict, la_fn=None, ir_fn=None, capture_dir: Optional[str] = None):
     """Run the reference's F4 (f4_julia, src/f4.c:190) on a golden case.
 
@@ -240,3 +258,32 @@ def ref_f4(case: dict, la_fn=None, ir_fn=None, capture_dir: Optional[str] = None
     finally:
         lib.gbref_set_la(None, None)
         lib.gbref_set_capture(None)
+
+
+def ref_convert(nv: int, exps: np.ndarray, deg: np.ndarray, idx: np.ndarray, mo: int,
+                row_ptr: np.ndarray, hashes: np.ndarray):
+    """The reference's convert_hashes_to_columns + sort_matrix_rows
+    (src/convert.c:30-135, src/order.c:125-131) on one round's flat data.
+    Returns (hcm, ncl, row_order, out_cols, seconds)."""
+    lib = _load_ref()
+    n = int(exps.shape[0])
+    nr = int(row_ptr.shape[0] - 1)
+    exps = np.ascontiguousarray(exps, dtype=np.int16)
+    deg = np.ascontiguousarray(deg, dtype=np.int32)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    hashes = np.ascontiguousarray(hashes, dtype=np.int32)
+    hcm = np.zeros(max(n, 1), dtype=np.int32)
+    order = np.zeros(max(nr, 1), dtype=np.int32)
+    cols = np.zeros(max(int(row_ptr[-1]), 1), dtype=np.int32)
+    ncl = C.c_int32()
+    secs = C.c_double()
+    lib.gbref_convert_csr.argtypes = [C.c_int32, C.c_int32] + [C.c_void_p] * 3 + [
+        C.c_int32, C.c_int32] + [C.c_void_p] * 2 + [C.c_void_p, C.POINTER(C.c_int32)] + [
+        C.c_void_p] * 2 + [C.POINTER(C.c_double)]
+    rc = lib.gbref_convert_csr(nv, n, exps.ctypes.data, deg.ctypes.data, idx.ctypes.data, mo, nr,
+                               row_ptr.ctypes.data, hashes.ctypes.data, hcm.ctypes.data,
+                               C.byref(ncl), order.ctypes.data, cols.ctypes.data, C.byref(secs))
+    if rc != 0:
+        raise RuntimeError("reference conversion failed")
+    return hcm[:n], ncl.value, order[:nr], cols[:int(row_ptr[-1])], secs.value

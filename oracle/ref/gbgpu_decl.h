@@ -4,3 +4,5 @@
  * the GPU entry points are declared here with void pointers. */
 void gbgpu_linear_algebra(void *mat, const void *bs, void *st);
 void gbgpu_interreduce_matrix_rows(void *mat, void *bs, const void *st);
+void gbgpu_convert_hashes_to_columns(void *hcmp, void *mat, void *st, void *sht);
+void gbgpu_sort_matrix_rows(void *mat);

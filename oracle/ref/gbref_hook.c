@@ -532,3 +532,79 @@ int gbref_interreduce_csr(int32_t p, int32_t nr, int32_t nc,
 }
 
 void gbref_free(void *ptr) { free(ptr); }
+
+/* The reference's convert_hashes_to_columns (src/convert.c:30-135) followed
+ * by sort_matrix_rows (src/order.c:125-131) on a flat description of one F4
+ * round: the secondary hash table's monomials 1..n (exponents exps[n][nv],
+ * total degrees deg[n], idx[n] = 2 for the lead monomials of known pivots,
+ * 1 otherwise) and nr rows of hash indices (row_ptr, hashes; the first entry
+ * of a row is its lead term).  Outputs: hcm[n] (the hash of every column, in
+ * column order), *ncl, row_order[nr] (input row of every row after the sort)
+ * and out_cols (the rows' column indices, rows in the sorted order, entries
+ * in their input order).  mo: 0 DRL, 1 LEX. */
+int gbref_convert_csr(int32_t nv, int32_t n, const int16_t *exps, const int32_t *deg,
+                      const int32_t *idx, int32_t mo, int32_t nr, const int64_t *row_ptr,
+                      const int32_t *hashes, int32_t *hcm_out, int32_t *ncl_out,
+                      int32_t *row_order, int32_t *out_cols, double *seconds)
+{
+    int32_t i, j;
+    stat_t *st = (stat_t *)calloc(1, sizeof(stat_t));
+    st->mo = mo;
+    st->nthrds = 1;
+    st->fc = 65521;
+    st->ff_bits = 32;
+    st->laopt = 2;
+    set_function_pointers(st);
+    ht_t *sht = (ht_t *)calloc(1, sizeof(ht_t));
+    sht->nv = nv;
+    sht->eld = n + 1;
+    sht->esz = n + 1;
+    sht->hd = (hd_t *)calloc((size_t)n + 1, sizeof(hd_t));
+    sht->ev = (exp_t **)calloc((size_t)n + 1, sizeof(exp_t *));
+    exp_t *block = (exp_t *)calloc((size_t)(n + 1) * (size_t)(nv > 0 ? nv : 1), sizeof(exp_t));
+    for (i = 0; i <= n; ++i) sht->ev[i] = block + (size_t)i * nv;
+    for (i = 0; i < n; ++i) {
+        for (j = 0; j < nv; ++j) sht->ev[i + 1][j] = exps[(size_t)i * nv + j];
+        sht->hd[i + 1].deg = deg[i];
+        sht->hd[i + 1].idx = idx[i];
+    }
+    mat_t *mat = (mat_t *)calloc(1, sizeof(mat_t));
+    mat->r = (hm_t **)malloc((size_t)(nr > 0 ? nr : 1) * sizeof(hm_t *));
+    for (i = 0; i < nr; ++i) {
+        const int64_t len = row_ptr[i + 1] - row_ptr[i];
+        hm_t *row = (hm_t *)malloc((size_t)(len + 3) * sizeof(hm_t));
+        row[0] = i; /* tags the input row through the sort */
+        row[1] = (hm_t)(len % UNROLL);
+        row[2] = (hm_t)len;
+        memcpy(row + 3, hashes + row_ptr[i], (size_t)len * sizeof(int32_t));
+        mat->r[i] = row;
+    }
+    mat->nr = nr;
+    mat->sz = nr;
+    mat->nc = n;
+    hl_t *hcm = NULL;
+    double t0 = realtime();
+    convert_hashes_to_columns(&hcm, mat, st, sht);
+    sort_matrix_rows(mat);
+    double t1 = realtime();
+    if (seconds) *seconds = t1 - t0;
+    for (i = 0; i < n; ++i) hcm_out[i] = hcm[i];
+    *ncl_out = mat->ncl;
+    int64_t off = 0;
+    for (i = 0; i < nr; ++i) {
+        const hm_t *row = mat->r[i];
+        row_order[i] = row[0];
+        memcpy(out_cols + off, row + 3, (size_t)row[2] * sizeof(int32_t));
+        off += row[2];
+        free(mat->r[i]);
+    }
+    free(mat->r);
+    free(mat);
+    free(hcm);
+    free(block);
+    free(sht->ev);
+    free(sht->hd);
+    free(sht);
+    free(st);
+    return 0;
+}

@@ -202,3 +202,30 @@ def test_f4_compare_harness_self_check_and_budget(tmp_path):
                    timeout=300)
     res = parse_log(str(cut))
     assert len(res["calls"]) == 1 and res["end"].startswith("stop budget")
+
+
+@pytest.mark.parametrize("mo", [0, 1])
+def test_reference_conversion_matches_restated_order(mo):
+    """The reference's convert_hashes_to_columns + sort_matrix_rows (through
+    the test build) orders columns as the restated comparator of
+    synth.column_order_key says and rows by (lead column, length); this pins
+    the order the device conversion reproduces."""
+    from gb_b200 import synth
+    r = synth.f4_round(5, 6, 300, 200, 80, 20, seed=mo + 1)
+    hcm, ncl, order, cols, _ = oracle.ref_convert(r["nv"], r["exps"], r["deg"], r["idx"], mo,
+                                                  r["row_ptr"], r["hashes"])
+    keys = synth.column_order_key(r["exps"], r["deg"], r["idx"], mo)
+    want = [h + 1 for h in sorted(range(len(keys)), key=lambda h: keys[h])]
+    assert hcm.tolist() == want and ncl == int((r["idx"] == 2).sum())
+    col_of = np.empty(len(keys) + 1, dtype=np.int64)
+    col_of[hcm] = np.arange(len(keys))
+    ptr = r["row_ptr"]
+    lead = col_of[r["hashes"][ptr[:-1]]]
+    lens = np.diff(ptr)
+    got_keys = [(int(lead[i]), int(lens[i])) for i in order]
+    assert got_keys == sorted(got_keys) and sorted(order.tolist()) == list(range(len(lens)))
+    off = 0
+    for i in order:
+        seg = r["hashes"][ptr[i]:ptr[i + 1]]
+        assert cols[off:off + seg.shape[0]].tolist() == col_of[seg].tolist()
+        off += seg.shape[0]
