@@ -681,6 +681,84 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
 
 
 
+// The panel transformation of every factorized chunk on CUDA cores: the pivot
+// rows of chunk d become E_d old over the columns from the first dirty panel
+// on, as  D[row of pivot k] = old[pos_k] - sum_j (I - E_d)[pos_k][j] old[j]
+// (ime = I - E_d from k_panel_factor; pos_k = the pivot's chunk position).
+// A block stages the old values of the chunk's n rows for 64 columns and the
+// (I - E) rows of its pivots in shared memory, then every thread forms the
+// new values of four pivots in one column: 64-bit sums without reduction
+// (p < 2^16: each product < 2^32, at most 128 of them; otherwise the column
+// value in 16-bit halves), one reduction per result.  Reads happen before any
+// write of the same columns (a block owns its columns of the chunk), so the
+// update is in place.  Only the chunk's pivot rows are written.
+constexpr int PA_COLS = 64;
+constexpr int PA_THREADS = 256;
+constexpr int PA_PIV = 4;
+
+template <bool WIDE>
+__global__ void __launch_bounds__(PA_THREADS)
+k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0,
+              const int32_t* __restrict__ chunk_rows, const int32_t* __restrict__ dpanel,
+              const int32_t* __restrict__ cursor, const uint32_t* __restrict__ ime_b,
+              const int32_t* __restrict__ n_piv_b, const int32_t* __restrict__ arows_b,
+              const int32_t* __restrict__ drows_b, uint32_t p) {
+    extern __shared__ uint32_t pa_smem[];
+    uint32_t(*T)[PA_COLS] = (uint32_t(*)[PA_COLS])pa_smem;  // [KB][PA_COLS]
+    uint32_t* A = pa_smem + KB * PA_COLS;                   // [np][KB]
+    const int d = blockIdx.y;
+    const int n = min(cursor[d], KB), np = n_piv_b[d];
+    const int c0 = j0 + blockIdx.x * PA_COLS;
+    const int pj = dpanel[d] * KB;
+    if (np == 0 || c0 + PA_COLS <= pj || c0 >= ncr) return;  // uniform
+    const int32_t* rows = chunk_rows + (size_t)d * KB;
+    for (int t = threadIdx.x; t < n * PA_COLS; t += PA_THREADS) {
+        const int j = t / PA_COLS, c = t % PA_COLS, col = c0 + c;
+        T[j][c] = col < ncr ? Dp[(size_t)rows[j] * ld + col] : 0u;
+    }
+    const uint32_t* ime = ime_b + (size_t)d * KB * KB;
+    const int32_t* pos = arows_b + (size_t)d * KB;
+    for (int t = threadIdx.x; t < np * n; t += PA_THREADS) {
+        const int k = t / n, j = t % n;
+        A[k * KB + j] = ime[(size_t)pos[k] * KB + j];
+    }
+    __syncthreads();
+    const uint64_t m = ~0ull / p;
+    const int c = threadIdx.x % PA_COLS, g = threadIdx.x / PA_COLS;
+    const int col = c0 + c;
+    const int32_t* drows = drows_b + (size_t)d * KB;
+    for (int k0 = g * PA_PIV; k0 < np; k0 += (PA_THREADS / PA_COLS) * PA_PIV) {
+        uint64_t lo[PA_PIV], hi[PA_PIV];
+#pragma unroll
+        for (int q = 0; q < PA_PIV; ++q) lo[q] = hi[q] = 0;
+        const int kq = min(PA_PIV, np - k0);
+        for (int j = 0; j < n; ++j) {
+            const uint32_t v = T[j][c];
+            if (v == 0u) continue;
+            const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
+#pragma unroll
+            for (int q = 0; q < PA_PIV; ++q) {
+                if (q < kq) {
+                    const uint32_t a = A[(k0 + q) * KB + j];
+                    lo[q] += (uint64_t)a * vl;
+                    if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
+                }
+            }
+        }
+        if (col < ncr) {
+#pragma unroll
+            for (int q = 0; q < PA_PIV; ++q) {
+                if (q < kq) {
+                    const int k = k0 + q;
+                    const uint32_t s = WIDE ? fold_lohi(lo[q], hi[q], p, m) : mod64(lo[q], p, m);
+                    const uint32_t old = T[pos[k]][c];
+                    Dp[(size_t)drows[k] * ld + col] = old >= s ? old - s : old + (p - s);
+                }
+            }
+        }
+    }
+}
+
 // dst block b (NB x NB, leading dimension NB, block stride NB (NB + 1)) =
 // src block b (nb_b x nb_b at src + b stride_src, leading dimension lds),
 // identity-padded; nb_b = NB except for the last block
@@ -1142,42 +1220,22 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
                 piv_arows, n_dirty * KB, -1));
             BL_LAUNCH(k_pivot_rowlist<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, chunk_rows, piv_rows,
                                                              piv_arows));
-            if (c.form != GBGPU_FORM_PLAIN) {
-                TcGemmArgs g{c.p, KB, width, KB, imeB, KB, Dp + j0, ld, Dp + j0, ld};
-                g.batch = n_dirty;
-                g.sA = (int64_t)KB * KB;
-                g.a_rows = piv_arows;
-                g.sAr = KB;
-                g.b_rows = chunk_rows;
-                g.sBr = KB;
-                g.d_rows = piv_rows;
-                g.sDr = KB;
-                BL_CHECK(gemm_args(c, g));
-            } else {
-                // The CUDA-core product reads its operands where they lie, and
-                // a tile may read chunk rows that another tile of the same
-                // launch has already rewritten: the chunk rows are copied
-                // first (groups of chunks, at most 256 MB of copies at once).
-                const int64_t per = (int64_t)KB * width;
-                const int32_t group = (int32_t)std::max<int64_t>(
-                    1, std::min<int64_t>(n_dirty, (256ll << 20) / (per * 4)));
-                uint32_t* oldc = c.alloc<uint32_t>((size_t)group * per);
-                if (!oldc) return GBGPU_ENOMEM;
-                for (int32_t d0 = 0; d0 < n_dirty; d0 += group) {
-                    const int32_t nb = std::min(group, n_dirty - d0);
-                    BL_LAUNCH(k_gather_rows_dense<<<grid_of((int64_t)nb * per), 256, 0, s>>>(
-                        nb * KB, chunk_rows + (size_t)d0 * KB, width, Dp + j0, ld, oldc, width));
-                    TcGemmArgs g{c.p, KB, width, KB, imeB + (size_t)d0 * KB * KB, KB, oldc, width,
-                                 Dp + j0, ld};
-                    g.batch = nb;
-                    g.sA = (int64_t)KB * KB;
-                    g.sB = per;
-                    g.a_rows = piv_arows + (size_t)d0 * KB;
-                    g.sAr = KB;
-                    g.d_rows = piv_rows + (size_t)d0 * KB;
-                    g.sDr = KB;
-                    BL_CHECK(gemm_args(c, g));
-                }
+            {
+                // pivot rows of every chunk <- E_d old (CUDA cores, in place)
+                const bool wide = c.p >= 65536u;
+                const int bytes = (KB * PA_COLS + KB * KB) * (int)sizeof(uint32_t);
+                const void* kern = wide ? (const void*)k_panel_apply<true>
+                                        : (const void*)k_panel_apply<false>;
+                BL_CUDA(ensure_smem_limit(kern, bytes));
+                const dim3 grid((unsigned)((width + PA_COLS - 1) / PA_COLS), (unsigned)n_dirty);
+                if (wide)
+                    BL_LAUNCH(k_panel_apply<true><<<grid, PA_THREADS, bytes, s>>>(
+                        Dp, ld, ncr, j0, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
+                        piv_rows, c.p));
+                else
+                    BL_LAUNCH(k_panel_apply<false><<<grid, PA_THREADS, bytes, s>>>(
+                        Dp, ld, ncr, j0, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
+                        piv_rows, c.p));
             }
             BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
                                                                 piv_of_col, is_piv, wflag));
