@@ -685,16 +685,18 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
 // rows of chunk d become E_d old over the columns from the first dirty panel
 // on, as  D[row of pivot k] = old[pos_k] - sum_j (I - E_d)[pos_k][j] old[j]
 // (ime = I - E_d from k_panel_factor; pos_k = the pivot's chunk position).
-// A block stages the old values of the chunk's n rows for 64 columns and the
-// (I - E) rows of its pivots in shared memory, then every thread forms the
-// new values of four pivots in one column: 64-bit sums without reduction
-// (p < 2^16: each product < 2^32, at most 128 of them; otherwise the column
-// value in 16-bit halves), one reduction per result.  Reads happen before any
-// write of the same columns (a block owns its columns of the chunk), so the
-// update is in place.  Only the chunk's pivot rows are written.
+// A block walks PA_TILES tiles of 64 columns of one chunk: it stages the old
+// values of the chunk's n rows for a tile in shared memory, then every thread
+// forms the new values of four pivots in one column, reading the (I - E) rows
+// through the L1 cache (all lanes of a warp read the same entry): 64-bit sums
+// without reduction (p < 2^16: each product < 2^32, at most 128 of them;
+// otherwise the column value in 16-bit halves), one reduction per result.
+// Reads happen before any write of the same columns (a block owns its columns
+// of the chunk), so the update is in place.  Only pivot rows are written.
 constexpr int PA_COLS = 64;
 constexpr int PA_THREADS = 256;
 constexpr int PA_PIV = 4;
+constexpr int PA_TILES = 4;
 
 template <bool WIDE>
 __global__ void __launch_bounds__(PA_THREADS)
@@ -703,56 +705,59 @@ k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0,
               const int32_t* __restrict__ cursor, const uint32_t* __restrict__ ime_b,
               const int32_t* __restrict__ n_piv_b, const int32_t* __restrict__ arows_b,
               const int32_t* __restrict__ drows_b, uint32_t p) {
-    extern __shared__ uint32_t pa_smem[];
-    uint32_t(*T)[PA_COLS] = (uint32_t(*)[PA_COLS])pa_smem;  // [KB][PA_COLS]
-    uint32_t* A = pa_smem + KB * PA_COLS;                   // [np][KB]
+    __shared__ uint32_t T[KB][PA_COLS];
+    __shared__ int32_t s_rows[KB], s_pos[KB], s_drow[KB];
     const int d = blockIdx.y;
     const int n = min(cursor[d], KB), np = n_piv_b[d];
-    const int c0 = j0 + blockIdx.x * PA_COLS;
     const int pj = dpanel[d] * KB;
-    if (np == 0 || c0 + PA_COLS <= pj || c0 >= ncr) return;  // uniform
-    const int32_t* rows = chunk_rows + (size_t)d * KB;
-    for (int t = threadIdx.x; t < n * PA_COLS; t += PA_THREADS) {
-        const int j = t / PA_COLS, c = t % PA_COLS, col = c0 + c;
-        T[j][c] = col < ncr ? Dp[(size_t)rows[j] * ld + col] : 0u;
+    if (np == 0) return;  // uniform
+    for (int t = threadIdx.x; t < KB; t += PA_THREADS) {
+        s_rows[t] = t < n ? chunk_rows[(size_t)d * KB + t] : 0;
+        s_pos[t] = t < np ? arows_b[(size_t)d * KB + t] : 0;
+        s_drow[t] = t < np ? drows_b[(size_t)d * KB + t] : 0;
     }
     const uint32_t* ime = ime_b + (size_t)d * KB * KB;
-    const int32_t* pos = arows_b + (size_t)d * KB;
-    for (int t = threadIdx.x; t < np * n; t += PA_THREADS) {
-        const int k = t / n, j = t % n;
-        A[k * KB + j] = ime[(size_t)pos[k] * KB + j];
-    }
-    __syncthreads();
     const uint64_t m = ~0ull / p;
     const int c = threadIdx.x % PA_COLS, g = threadIdx.x / PA_COLS;
-    const int col = c0 + c;
-    const int32_t* drows = drows_b + (size_t)d * KB;
-    for (int k0 = g * PA_PIV; k0 < np; k0 += (PA_THREADS / PA_COLS) * PA_PIV) {
-        uint64_t lo[PA_PIV], hi[PA_PIV];
-#pragma unroll
-        for (int q = 0; q < PA_PIV; ++q) lo[q] = hi[q] = 0;
-        const int kq = min(PA_PIV, np - k0);
-        for (int j = 0; j < n; ++j) {
-            const uint32_t v = T[j][c];
-            if (v == 0u) continue;
-            const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
+    for (int tile = 0; tile < PA_TILES; ++tile) {
+        const int c0 = j0 + (blockIdx.x * PA_TILES + tile) * PA_COLS;
+        if (c0 >= ncr) break;                // uniform
+        if (c0 + PA_COLS <= pj) continue;    // uniform: the chunk rows are zero here
+        __syncthreads();  // the row lists are in place / the last tile's readers are done
+        for (int t = threadIdx.x; t < n * PA_COLS; t += PA_THREADS) {
+            const int j = t / PA_COLS, cc = t % PA_COLS, col = c0 + cc;
+            T[j][cc] = col < ncr ? Dp[(size_t)s_rows[j] * ld + col] : 0u;
+        }
+        __syncthreads();
+        const int col = c0 + c;
+        for (int k0 = g * PA_PIV; k0 < np; k0 += (PA_THREADS / PA_COLS) * PA_PIV) {
+            uint64_t lo[PA_PIV], hi[PA_PIV];
+            const uint32_t* ar[PA_PIV];
 #pragma unroll
             for (int q = 0; q < PA_PIV; ++q) {
-                if (q < kq) {
-                    const uint32_t a = A[(k0 + q) * KB + j];
+                lo[q] = hi[q] = 0;
+                ar[q] = ime + (size_t)s_pos[min(k0 + q, np - 1)] * KB;
+            }
+            for (int j = 0; j < n; ++j) {
+                const uint32_t v = T[j][c];
+                const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
+#pragma unroll
+                for (int q = 0; q < PA_PIV; ++q) {
+                    const uint32_t a = __ldg(ar[q] + j);
                     lo[q] += (uint64_t)a * vl;
                     if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
                 }
             }
-        }
-        if (col < ncr) {
+            if (col < ncr) {
 #pragma unroll
-            for (int q = 0; q < PA_PIV; ++q) {
-                if (q < kq) {
+                for (int q = 0; q < PA_PIV; ++q) {
                     const int k = k0 + q;
-                    const uint32_t s = WIDE ? fold_lohi(lo[q], hi[q], p, m) : mod64(lo[q], p, m);
-                    const uint32_t old = T[pos[k]][c];
-                    Dp[(size_t)drows[k] * ld + col] = old >= s ? old - s : old + (p - s);
+                    if (k < np) {
+                        const uint32_t s =
+                            WIDE ? fold_lohi(lo[q], hi[q], p, m) : mod64(lo[q], p, m);
+                        const uint32_t old = T[s_pos[k]][c];
+                        Dp[(size_t)s_drow[k] * ld + col] = old >= s ? old - s : old + (p - s);
+                    }
                 }
             }
         }
@@ -1223,17 +1228,14 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             {
                 // pivot rows of every chunk <- E_d old (CUDA cores, in place)
                 const bool wide = c.p >= 65536u;
-                const int bytes = (KB * PA_COLS + KB * KB) * (int)sizeof(uint32_t);
-                const void* kern = wide ? (const void*)k_panel_apply<true>
-                                        : (const void*)k_panel_apply<false>;
-                BL_CUDA(ensure_smem_limit(kern, bytes));
-                const dim3 grid((unsigned)((width + PA_COLS - 1) / PA_COLS), (unsigned)n_dirty);
+                const int tiles = (width + PA_COLS - 1) / PA_COLS;
+                const dim3 grid((unsigned)((tiles + PA_TILES - 1) / PA_TILES), (unsigned)n_dirty);
                 if (wide)
-                    BL_LAUNCH(k_panel_apply<true><<<grid, PA_THREADS, bytes, s>>>(
+                    BL_LAUNCH(k_panel_apply<true><<<grid, PA_THREADS, 0, s>>>(
                         Dp, ld, ncr, j0, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
                         piv_rows, c.p));
                 else
-                    BL_LAUNCH(k_panel_apply<false><<<grid, PA_THREADS, bytes, s>>>(
+                    BL_LAUNCH(k_panel_apply<false><<<grid, PA_THREADS, 0, s>>>(
                         Dp, ld, ncr, j0, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
                         piv_rows, c.p));
             }
