@@ -697,6 +697,7 @@ constexpr int PA_COLS = 64;
 constexpr int PA_THREADS = 256;
 constexpr int PA_PIV = 4;
 constexpr int PA_TILES = 4;
+constexpr int PA_AST = 3072;  // (I - E) entries kept in shared memory
 
 template <bool WIDE>
 __global__ void __launch_bounds__(PA_THREADS)
@@ -706,6 +707,7 @@ k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0,
               const int32_t* __restrict__ n_piv_b, const int32_t* __restrict__ arows_b,
               const int32_t* __restrict__ drows_b, uint32_t p) {
     __shared__ uint32_t T[KB][PA_COLS];
+    __shared__ uint32_t s_a[PA_AST];
     __shared__ int32_t s_rows[KB], s_pos[KB], s_drow[KB];
     const int d = blockIdx.y;
     const int n = min(cursor[d], KB), np = n_piv_b[d];
@@ -717,6 +719,14 @@ k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0,
         s_drow[t] = t < np ? drows_b[(size_t)d * KB + t] : 0;
     }
     const uint32_t* ime = ime_b + (size_t)d * KB * KB;
+    // the (I - E) rows of the block's pivots, n entries each, in shared memory
+    // when they fit (else read through L1)
+    const bool in_smem = np * n <= PA_AST;
+    if (in_smem)
+        for (int t = threadIdx.x; t < np * n; t += PA_THREADS) {
+            const int k = t / n, j = t % n;
+            s_a[t] = ime[(size_t)arows_b[(size_t)d * KB + k] * KB + j];
+        }
     const uint64_t m = ~0ull / p;
     const int c = threadIdx.x % PA_COLS, g = threadIdx.x / PA_COLS;
     for (int tile = 0; tile < PA_TILES; ++tile) {
@@ -732,20 +742,36 @@ k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0,
         const int col = c0 + c;
         for (int k0 = g * PA_PIV; k0 < np; k0 += (PA_THREADS / PA_COLS) * PA_PIV) {
             uint64_t lo[PA_PIV], hi[PA_PIV];
-            const uint32_t* ar[PA_PIV];
 #pragma unroll
-            for (int q = 0; q < PA_PIV; ++q) {
-                lo[q] = hi[q] = 0;
-                ar[q] = ime + (size_t)s_pos[min(k0 + q, np - 1)] * KB;
-            }
-            for (int j = 0; j < n; ++j) {
-                const uint32_t v = T[j][c];
-                const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
+            for (int q = 0; q < PA_PIV; ++q) lo[q] = hi[q] = 0;
+            if (in_smem) {
+                const uint32_t* ar = s_a + (size_t)k0 * n;
+                const int kq = min(PA_PIV, np - k0);
+#pragma unroll 4
+                for (int j = 0; j < n; ++j) {
+                    const uint32_t v = T[j][c];
+                    const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
 #pragma unroll
-                for (int q = 0; q < PA_PIV; ++q) {
-                    const uint32_t a = __ldg(ar[q] + j);
-                    lo[q] += (uint64_t)a * vl;
-                    if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
+                    for (int q = 0; q < PA_PIV; ++q) {
+                        const uint32_t a = q < kq ? ar[q * n + j] : 0u;
+                        lo[q] += (uint64_t)a * vl;
+                        if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
+                    }
+                }
+            } else {
+                const uint32_t* ar[PA_PIV];
+#pragma unroll
+                for (int q = 0; q < PA_PIV; ++q)
+                    ar[q] = ime + (size_t)s_pos[min(k0 + q, np - 1)] * KB;
+                for (int j = 0; j < n; ++j) {
+                    const uint32_t v = T[j][c];
+                    const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
+#pragma unroll
+                    for (int q = 0; q < PA_PIV; ++q) {
+                        const uint32_t a = __ldg(ar[q] + j);
+                        lo[q] += (uint64_t)a * vl;
+                        if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
+                    }
                 }
             }
             if (col < ncr) {
