@@ -37,12 +37,15 @@ CONFIG = {"nru": 20000, "nrl": 5000, "ncr": 20000, "p": 65521, "dmin": 0.02, "dm
           "seed": 1}
 METRIC = "GF(p) matrix reductions/s (20000x5000 A|B/C|D, 40000 cols, p=65521, bit-exact)"
 # DRAM traffic of the tensor-core GEMM per executed int8 operation, from an ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the k_tc_submul
-# launches of one reduction of a 0.5-scale copy of the workload; the line's
-# per-launch traffic scales it by the operations one launch executes here.
-GEMM_TRAFFIC_PER_OP = (4665.2e6 + 651.8e6) / 5.118e12
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the 47 k_tc_submul
+# launches of one reduction of the half-scale copy of the workload
+# (10000 x 2500, 20000 columns: 719.7 MB read + 24.3 MB written for 6.432e11
+# int8 ops); the line's per-launch traffic scales it by the operations one
+# launch of the full workload executes.
+GEMM_TRAFFIC_PER_OP = (719.7e6 + 24.3e6) / 6.43196518400e11
 GEMM_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the GEMM launches "
-                       "of one reduction, bytes per int8 op, times this run's ops per launch")
+                       "of one half-scale reduction, bytes per int8 op, times this run's ops "
+                       "per launch")
 UNIT = "matrices/s"
 
 
@@ -352,7 +355,7 @@ def main():
         alg = algorithmic_bytes_schur(mat, work_sparse, mat.ncr)
         peak, peak_src = _peaks()
         achieved = alg / (sch * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "k_reduce_sparse", "achieved": achieved, "peak": peak,
+        roof = {"bound": "hbm", "kernel": "k_reduce_team", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                 "traffic": None, "alg_bytes_per_launch": alg, "launch_ms": sch}
     else:
