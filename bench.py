@@ -273,7 +273,7 @@ def main():
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
                     help="1: check the timed form's answer against the sparse-row form")
-    ap.add_argument("--one-thread", type=int, default=1,
+    ap.add_argument("--one-thread", type=int, default=0,
                     help="reference arm: also time one full call on one thread")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -371,6 +371,14 @@ int gbgpu_layout(int64_t* out, int32_t n) {
         (int64_t)offsetof(gbgpu_stat_t, num_zerored), (int64_t)offsetof(gbgpu_stat_t, fc),
         (int64_t)offsetof(gbgpu_stat_t, laopt), (int64_t)offsetof(gbgpu_stat_t, nthrds),
         (int64_t)offsetof(gbgpu_stat_t, ff_bits), (int64_t)offsetof(gbgpu_stat_t, info_level),
+        (int64_t)offsetof(gbgpu_stat_t, mo), (int64_t)offsetof(gbgpu_stat_t, num_rowsred),
+        (int64_t)offsetof(gbgpu_stat_t, convert_ctime),
+        (int64_t)offsetof(gbgpu_stat_t, convert_rtime),
+        (int64_t)sizeof(gbgpu_hd_t), (int64_t)offsetof(gbgpu_hd_t, deg),
+        (int64_t)offsetof(gbgpu_hd_t, idx),
+        (int64_t)sizeof(gbgpu_ht_t), (int64_t)offsetof(gbgpu_ht_t, ev),
+        (int64_t)offsetof(gbgpu_ht_t, hd), (int64_t)offsetof(gbgpu_ht_t, eld),
+        (int64_t)offsetof(gbgpu_ht_t, nv),
     };
     const int32_t k = (int32_t)(sizeof(v) / sizeof(v[0]));
     for (int32_t i = 0; i < k && i < n; ++i) out[i] = v[i];

@@ -329,6 +329,11 @@ int gbref_layout(int64_t *out, int n)
         (int64_t)offsetof(stat_t, num_zerored), (int64_t)offsetof(stat_t, fc),
         (int64_t)offsetof(stat_t, laopt), (int64_t)offsetof(stat_t, nthrds),
         (int64_t)offsetof(stat_t, ff_bits), (int64_t)offsetof(stat_t, info_level),
+        (int64_t)offsetof(stat_t, mo), (int64_t)offsetof(stat_t, num_rowsred),
+        (int64_t)offsetof(stat_t, convert_ctime), (int64_t)offsetof(stat_t, convert_rtime),
+        (int64_t)sizeof(hd_t), (int64_t)offsetof(hd_t, deg), (int64_t)offsetof(hd_t, idx),
+        (int64_t)sizeof(ht_t), (int64_t)offsetof(ht_t, ev), (int64_t)offsetof(ht_t, hd),
+        (int64_t)offsetof(ht_t, eld), (int64_t)offsetof(ht_t, nv),
     };
     int k = (int)(sizeof(v) / sizeof(v[0]));
     int i;
