@@ -262,7 +262,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
     ap.add_argument("--workload", default="staircase",
-                    choices=["staircase", "dense", "rref", "batch", "f4", "multimod"],
+                    choices=["staircase", "dense", "rref", "batch", "f4", "f4cubic10",
+                             "multimod"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
                          "rref: RREF of a rank-3n/4 n x n block; batch: 2 x 128 independent "
@@ -287,6 +288,9 @@ def main():
         return
     if args.workload == "f4":
         run_f4_captures(args)
+        return
+    if args.workload == "f4cubic10":
+        run_f4_cubic10(args)
         return
     if args.workload == "multimod":
         run_multimod(args)
@@ -823,6 +827,44 @@ def run_f4_captures(args):
             "data": "dense systems of tests/golden/f4 (seeded coefficients)",
             "config": {"workload": "f4: dense_quadratic_7 (p=32003, la 2) + "
                                    "dense_cubic_5_p31 (p=2^31-1, la 1)", "systems": systems}}
+    print(json.dumps(line), flush=True)
+
+
+def run_f4_cubic10(args, budget_s: float = 40.0):
+    """Config-3 workload: F4 on the dense cubic system in 10 variables (10
+    polynomials, all 286 monomials of degree <= 3, p = 2^31 - 1, la option 1)
+    with gb's own host code, every la call at src/f4.c:306 sent to the drop-in
+    gbgpu_linear_algebra and, on a copy, to the reference la (the CPU baseline
+    and checker), until the reference has used budget_s seconds
+    (oracle/f4_compare.py, a child process).  Reports every call's shape and
+    both times."""
+    import oracle.f4_compare as fc
+    log = os.path.join(tempfile.gettempdir(), f"f4cubic10_{os.getpid()}.log")
+    t0 = time.perf_counter()
+    subprocess.run([sys.executable, "-m", "oracle.f4_compare", "--nvars", "10", "--ngens", "10",
+                    "--maxdeg", "3", "--p", "2147483647", "--la-option", "1", "--seed", "10",
+                    "--budget", str(budget_s), "--log", log, "--impl", "gpu"],
+                   check=True, cwd=REPO, timeout=3600)
+    wall = time.perf_counter() - t0
+    res = fc.parse_log(log)
+    calls = res["calls"]
+    gpu_s = sum(c["gpu_s"] for c in calls)
+    ref_s = sum(c["ref_s"] for c in calls)
+    threads = os.cpu_count() or 1
+    line = {"metric": "F4 la calls of the 10-variable dense cubic over 2^31-1 (call site)",
+            "value": len(calls) / gpu_s if gpu_s else None, "unit": "matrices/s", "n_gpus": 1,
+            "steps": 1, "warmup": 0, "ms_per_step": gpu_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 residues, 4 u8 limbs",
+            "data": "synthetic (seeded dense cubic system, gb's own F4)",
+            "config": {"workload": "f4cubic10: 10 cubics in 10 variables, p=2^31-1, la 1, "
+                                   f"rounds until the reference has used {budget_s:.0f} s"},
+            "calls": [{k: c[k] for k in ("nr", "nc", "ncl", "ncr", "nrl", "np", "gpu_s",
+                                          "ref_s", "equal")} for c in calls],
+            "all_equal": all(c["equal"] for c in calls), "end": res["end"], "wall_s": wall,
+            "cpu_baseline": {"value": len(calls) / ref_s if ref_s else None,
+                             "unit": "matrices/s", "cores": threads, "kind": "reference",
+                             "sample": f"the reference la on the same {len(calls)} calls, "
+                                       f"{ref_s:.1f} s, {threads} threads"}}
     print(json.dumps(line), flush=True)
 
 
