@@ -607,9 +607,10 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
         int* sm = s_min[step & 1];
         if (lane == 0) sm[warp] = key;
         __syncthreads();  // also: the previous step's updates are visible
-        int best = sm[0];
-#pragma unroll
-        for (int w = 1; w < KB * PF_GROUPS / 32; ++w) best = min(best, sm[w]);
+        // the 32 warp minima: one read per lane, then a warp reduction
+        static_assert(KB * PF_GROUPS / 32 == 32, "one warp minimum per lane");
+        int best = sm[lane];
+        for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
         if (best == INT_MAX) break;  // uniform: no pivot left in the panel
         const int c = best / KB, i = best % KB;
         if (tid == 0) {

@@ -52,6 +52,7 @@ __device__ void tiny_rref_body(int32_t n, int32_t m, const uint32_t* __restrict_
     __shared__ int s_min[2][kTinyThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = kTinyThreads / 32;
+    static_assert(NW == 32, "one warp minimum per lane");
     if (*err) {  // invalid input: nothing is read, the answer is empty (uniform)
         for (int c = tid; c < m; c += blockDim.x) out.piv_of_col[c] = -1;
         if (tid == 0) {
@@ -94,9 +95,9 @@ __device__ void tiny_rref_body(int32_t n, int32_t m, const uint32_t* __restrict_
     __syncthreads();
     for (int step = 0; step < n; ++step) {
         const int* sm = s_min[step & 1];
-        int best = sm[0];
-#pragma unroll 8
-        for (int w = 1; w < NW; ++w) best = min(best, sm[w]);
+        // the NW (= 32) warp minima: one read per lane, then a warp reduction
+        int best = sm[lane];
+        for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
         if (best == INT_MAX) break;  // uniform: rank reached
         const int c = best / n, i = best % n;
         const uint32_t* pr = T + (size_t)i * tld;
