@@ -1032,9 +1032,11 @@ extern "C" {
 
 struct gbgpu_plan {
     Plan* impl;
+    int impl_device() const { return impl ? impl->device : -1; }
 };
 
 int gbgpu_plan_create(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_plan** plan) {
+    DeviceScope scope;
     if (!plan) return GBGPU_EINVAL;
     Plan* P = nullptr;
     int rc = plan_create(m, opt, 0, &P);
@@ -1044,17 +1046,20 @@ int gbgpu_plan_create(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_plan**
 }
 
 int gbgpu_plan_run(gbgpu_plan* plan) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan) return GBGPU_EINVAL;
     return plan_run(plan->impl);
 }
 
 int gbgpu_plan_result(gbgpu_plan* plan, gbgpu_rows* out) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan || !out) return GBGPU_EINVAL;
     return plan_result(plan->impl, out);
 }
 
 int gbgpu_plan_result_into(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, int32_t* vals,
                            int64_t cap_rows, int64_t cap_nnz, int32_t* np, int64_t* nnz) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan || !np || !nnz) return GBGPU_EINVAL;
     if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
     // NULL buffers with zero capacities query the sizes (GBGPU_ERANGE)
@@ -1064,6 +1069,7 @@ int gbgpu_plan_result_into(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, in
 int gbgpu_plan_result_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, void* vals,
                              int32_t val_bytes, int64_t cap_rows, int64_t cap_nnz, int32_t* np,
                              int64_t* nnz) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan || !np || !nnz) return GBGPU_EINVAL;
     if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
     return plan_result_into_v(plan->impl, row_ptr, cols, vals, val_bytes, cap_rows, cap_nnz, np,
@@ -1073,6 +1079,7 @@ int gbgpu_plan_result_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, 
 int gbgpu_plan_run_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, void* vals,
                           int32_t val_bytes, int64_t cap_rows, int64_t cap_nnz, int32_t* np,
                           int64_t* nnz) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan || !np || !nnz) return GBGPU_EINVAL;
     if ((!row_ptr || !cols || !vals) && (cap_rows > 0 || cap_nnz > 0)) return GBGPU_EINVAL;
     return plan_run_into_v(plan->impl, row_ptr, cols, vals, val_bytes, cap_rows, cap_nnz, np,
@@ -1080,6 +1087,7 @@ int gbgpu_plan_run_into_v(gbgpu_plan* plan, int64_t* row_ptr, int32_t* cols, voi
 }
 
 int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan || !stats) return GBGPU_EINVAL;
     // a pending small-matrix run is settled first (its timings, its checks)
     const int rc = settle(plan->impl);
@@ -1088,6 +1096,7 @@ int gbgpu_plan_stats(const gbgpu_plan* plan, gbgpu_stats* stats) {
 }
 
 void gbgpu_plan_destroy(gbgpu_plan* plan) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan) return;
     plan_destroy(plan->impl);
     delete plan;
@@ -1130,6 +1139,7 @@ static int reduce_small(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows
 }
 
 int gbgpu_reduce(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows* out) {
+    DeviceScope scope;
     if (!out) return GBGPU_EINVAL;
     memset(out, 0, sizeof(*out));
     bool handled = false;
@@ -1147,6 +1157,7 @@ int gbgpu_reduce(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows* out) 
 int gbgpu_interreduce(int32_t p, int32_t nr, int32_t nc, const int64_t* row_ptr,
                       const int32_t* cols, const int32_t* vals, const gbgpu_options* opt,
                       gbgpu_rows* out) {
+    DeviceScope scope;
     if (!out) return GBGPU_EINVAL;
     memset(out, 0, sizeof(*out));
     gbgpu_csr m{p, 2, nr, 0, nc, row_ptr, cols, vals};

@@ -162,6 +162,7 @@ gbgpu_options shim_options() {
 extern "C" {
 
 int gbgpu_linear_algebra_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_stat_t* st) {
+    DeviceScope scope;
     if (!mat || !bs || !st) return GBGPU_EINVAL;
     const double ct0 = cpu_seconds(), rt0 = wall_seconds();
     const int bits = coef_bits(st);
@@ -214,6 +215,7 @@ void gbgpu_linear_algebra(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_stat_t* 
 
 int gbgpu_interreduce_matrix_rows_status(gbgpu_mat_t* mat, gbgpu_bs_t* bs,
                                          const gbgpu_stat_t* st) {
+    DeviceScope scope;
     if (!mat || !bs || !st) return GBGPU_EINVAL;
     if (st->info_level > 1) printf("                        ");
     const int bits = coef_bits(st);
@@ -260,6 +262,7 @@ static bool batch_small(const gbgpu_csr& m, const gbgpu_options* opt) {
 
 int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
                        gbgpu_rows* outs, int32_t* status) {
+    DeviceScope scope;
     if (n < 0 || (n > 0 && (!ms || !outs || !status))) return GBGPU_EINVAL;
     for (int32_t i = 0; i < n; ++i) {
         memset(&outs[i], 0, sizeof(gbgpu_rows));

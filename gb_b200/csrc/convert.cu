@@ -394,6 +394,7 @@ void gbgpu_convert_hashes_to_columns(int32_t** hcmp, gbgpu_mat_t* mat, gbgpu_sta
 }
 
 int gbgpu_sort_matrix_rows_status(gbgpu_mat_t* mat) {
+    DeviceScope scope;
     if (!mat) return GBGPU_EINVAL;
     const int32_t nr = mat->nr;
     if (nr <= 1) return GBGPU_OK;

@@ -77,6 +77,7 @@ extern "C" {
 int gbgpu_dense_submul(int32_t p, int32_t M, int32_t N, int32_t K, const uint32_t* A,
                        int64_t lda, const uint32_t* B, int64_t ldb, uint32_t* D, int64_t ldd,
                        const gbgpu_options* opt) {
+    DeviceScope scope;
     int rc = check_args(p, M, N, K, lda, ldb, ldd);
     if (rc) return rc;
     DeviceInfo dev;
@@ -89,6 +90,7 @@ int gbgpu_dense_submul(int32_t p, int32_t M, int32_t N, int32_t K, const uint32_
 int gbgpu_dense_submul_host(int32_t p, int32_t M, int32_t N, int32_t K, const uint32_t* A,
                             int64_t lda, const uint32_t* B, int64_t ldb, uint32_t* D,
                             int64_t ldd, const gbgpu_options* opt) {
+    DeviceScope scope;
     int rc = check_args(p, M, N, K, lda, ldb, ldd);
     if (rc) return rc;
     DeviceInfo dev;
@@ -131,6 +133,7 @@ int gbgpu_dense_submul_host(int32_t p, int32_t M, int32_t N, int32_t K, const ui
 
 int gbgpu_dense_rref(int32_t p, int32_t rows, int32_t cols, uint32_t* D, int64_t ld,
                      int32_t* rank, int32_t* piv_cols, const gbgpu_options* opt) {
+    DeviceScope scope;
     if (p < 2 || rows < 0 || cols < 0 || ld < cols || !rank || (rows > 0 && cols > 0 && (!D || !piv_cols))) {
         set_error("bad dense RREF arguments");
         return GBGPU_EINVAL;

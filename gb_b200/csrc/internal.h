@@ -22,6 +22,21 @@ void count_launch(long long n);
 // so a launch in one host thread never sees another thread lower it.
 cudaError_t ensure_smem_limit(const void* kernel, int bytes);
 int device_init(int device, DeviceInfo* info);
+// The C-ABI entry points leave the caller's current device as they found it:
+// the scope notes it on entry (and makes `device` current when >= 0) and
+// restores it on exit.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int device = -1) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (device >= 0) cudaSetDevice(device);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+};
 // GBGPU_EINVAL with a description of the contract violations in `bits`
 // (the error bits of the device-side input checks), GBGPU_OK for none
 int err_to_status(uint32_t bits, std::string* msg);

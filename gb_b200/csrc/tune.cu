@@ -111,6 +111,7 @@ int tc_shape_for(int L, int K) {
 using namespace gbgpu;
 
 extern "C" int gbgpu_autotune(int32_t device, const char* path) {
+    DeviceScope scope;
     DeviceInfo dev;
     int rc = device_init(device, &dev);
     if (rc) return rc;
