@@ -274,6 +274,8 @@ def main():
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
                     help="1: check the timed form's answer against the sparse-row form")
+    ap.add_argument("--other-configs", type=int, default=1,
+                    help="1: add short runs of the other configurations to the line")
     ap.add_argument("--one-thread", type=int, default=0,
                     help="reference arm: also time one full call on one thread")
     args = ap.parse_args()
@@ -419,10 +421,75 @@ def main():
             line["verified_against_reference"] = None
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {e}"}
+    if rank == 0 and ws == 1 and args.scale == 1.0 and args.other_configs:
+        # the other configurations' own figures, measured after (not inside)
+        # this line's timed region; failures are reported, not raised
+        line["other_configs"] = other_configs(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def other_configs(args) -> dict:
+    """Short runs of the other configurations, reported beside the headline:
+    the F4 la calls of the dense systems at the src/f4.c:306 call site
+    (config 1 and its 31-bit stand-in; the golden bases checked), the exact
+    modular GEMM on 8192 x 8192 blocks for the three primes (config 4(i),
+    device time, median of 3) and the RREF of a rank-6144 8192 x 8192 block
+    (config 4(ii)).  Their bit-exact checks at these sizes are the GPU tests."""
+    out = {}
+    try:
+        out["f4_dense_systems"] = f4_systems_timing(3, cpu=not args.no_cpu)
+    except Exception as e:  # noqa: BLE001 - reported in the line
+        out["f4_dense_systems"] = {"error": str(e)}
+    try:
+        import ctypes as Cc
+        import torch
+        from gb_b200 import _lib
+        lib = _lib.load()
+        n = 8192
+        opt = _lib.Options(_lib.FORM_TENSOR, 0, 1, 0, None)
+        gemm, rref = {}, {}
+        for p in (251, 65521, 2147483647):
+            g = torch.Generator(device="cuda")
+            g.manual_seed(p)
+            mk = lambda r, c: torch.randint(0, p, (r, c), device="cuda", dtype=torch.int64,
+                                            generator=g).to(torch.int32)
+            A, B, D = mk(n, n), mk(n, n), mk(n, n)
+            ts = []
+            for rep in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _lib.check(lib.gbgpu_dense_submul(p, n, n, n, A.data_ptr(), n, B.data_ptr(), n,
+                                                  D.data_ptr(), n, Cc.byref(opt)))
+                e1.record()
+                torch.cuda.synchronize()
+                if rep:
+                    ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            gemm[str(p)] = {"ms": ms, "modular_TOPS": 2.0 * n ** 3 / (ms * 1e-3) / 1e12}
+            r = 3 * n // 4
+            Rn = torch.remainder(p - A[:r].to(torch.int64), p).to(torch.int32)
+            L = B[:, :r].contiguous()
+            Dm = torch.zeros(n, n, device="cuda", dtype=torch.int32)
+            _lib.check(lib.gbgpu_dense_submul(p, n, n, r, L.data_ptr(), r, Rn.data_ptr(), n,
+                                              Dm.data_ptr(), n, Cc.byref(opt)))  # L R
+            piv = torch.empty(n, device="cuda", dtype=torch.int32)
+            rank = Cc.c_int32()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(lib.gbgpu_dense_rref(p, n, n, Dm.data_ptr(), n, Cc.byref(rank),
+                                            piv.data_ptr(), Cc.byref(opt)))
+            e1.record()
+            torch.cuda.synchronize()
+            rref[str(p)] = {"ms": e0.elapsed_time(e1), "rank": rank.value}
+            del A, B, D, Dm, L, Rn
+        out["dense_gemm_8192"] = gemm
+        out["dense_rref_8192_rank6144"] = rref
+    except Exception as e:  # noqa: BLE001
+        out["dense_8192"] = {"error": str(e)}
+    return out
 
 
 def _e2e(lib, mat, args, device):
