@@ -1115,7 +1115,9 @@ static int reduce_small(const gbgpu_csr* m, const gbgpu_options* opt, gbgpu_rows
     const int vb = val_bytes_of(m);
     if (!(vb == 1 || vb == 2 || vb == 4) || (vb < 4 && (int64_t)m->p >= ((int64_t)1 << (8 * vb))))
         return GBGPU_OK;
-    if (m->row_ptr[0] != 0 || m->row_ptr[m->nr] < 0) return GBGPU_OK;
+    // 32-bit entry offsets on the small path
+    if (m->row_ptr[0] != 0 || m->row_ptr[m->nr] < 0 || m->row_ptr[m->nr] > INT_MAX / 2)
+        return GBGPU_OK;
     if (!small_eligible(m->nr, m->ncl, m->ncr, o.device)) return GBGPU_OK;
     *handled = true;
     SmallInput in{m->p, m->nr, m->ncl, m->ncr, m->row_ptr[m->nr], o.device, fill_from_csr_vals,

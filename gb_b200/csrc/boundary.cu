@@ -168,10 +168,11 @@ int gbgpu_linear_algebra_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_st
     const int bits = coef_bits(st);
     gbgpu_options o = shim_options();
     int rc;
-    if (st->fc >= 2 && small_eligible(mat->nr, mat->ncl, mat->ncr, o.device)) {
+    int64_t nnz = 0;
+    for (int32_t i = 0; i < mat->nr; ++i) nnz += mat->r[i][2];
+    if (st->fc >= 2 && nnz <= INT32_MAX / 2 &&
+        small_eligible(mat->nr, mat->ncl, mat->ncr, o.device)) {
         // small matrix: rows gathered straight into pinned staging, one pass
-        int64_t nnz = 0;
-        for (int32_t i = 0; i < mat->nr; ++i) nnz += mat->r[i][2];
         GatherCtx g{mat, bs_table(bs, bits), bits, st->fc};
         SmallInput in{st->fc, mat->nr, mat->ncl, mat->ncr, nnz, o.device, fill_from_rows, &g};
         SmallAnswer a;
@@ -254,6 +255,7 @@ static bool batch_small(const gbgpu_csr& m, const gbgpu_options* opt) {
     if (opt && !(opt->form == GBGPU_FORM_AUTO || opt->form == GBGPU_FORM_PLAIN)) return false;
     if (opt && opt->profile) return false;
     if (m.p < 2 || m.nr <= 0 || !m.row_ptr || !m.cols || !m.vals || m.row_ptr[0] != 0) return false;
+    if (m.row_ptr[m.nr] < 0 || m.row_ptr[m.nr] > INT32_MAX / 2) return false;  // 32-bit offsets
     const int vb = m.val_bytes ? m.val_bytes : 4;
     if (!(vb == 1 || vb == 2 || vb == 4) || (vb < 4 && (int64_t)m.p >= ((int64_t)1 << (8 * vb))))
         return false;

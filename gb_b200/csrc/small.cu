@@ -52,7 +52,7 @@ __device__ void small_prep_body(int32_t nr, int32_t ncl, int32_t nc, uint32_t p,
                                 const int64_t* __restrict__ row_ptr,
                                 const int32_t* __restrict__ cols,
                                 const uint32_t* __restrict__ vals, int32_t* piv_row,
-                                int32_t* work, int32_t* n_work, uint32_t* err,
+                                int2* pext, int32_t* work, int32_t* n_work, uint32_t* err,
                                 int32_t* prep_tab /* smem [ncl] */) {
     __shared__ uint32_t s_err;
     __shared__ int s_warp[kPrepThreads / 32];
@@ -86,6 +86,9 @@ __device__ void small_prep_body(int32_t nr, int32_t ncl, int32_t nc, uint32_t p,
         const int32_t r = prep_tab[c];
         if (r == INT_MAX) atomicOr(&s_err, kErrMissingPivot);
         piv_row[c] = r;
+        // the pivot row's applied entries (its lead excluded), as 32-bit offsets
+        pext[c] = r == INT_MAX ? make_int2(0, 0)
+                               : make_int2((int)row_ptr[r] + 1, (int)row_ptr[r + 1]);
     }
     // rows that are not the known pivot of their lead, in row order
     int base = 0;
@@ -122,9 +125,10 @@ __device__ void small_prep_body(int32_t nr, int32_t ncl, int32_t nc, uint32_t p,
 __global__ void __launch_bounds__(kPrepThreads)
 k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __restrict__ row_ptr,
              const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals,
-             int32_t* piv_row, int32_t* work, int32_t* n_work, uint32_t* err) {
+             int32_t* piv_row, int2* pext, int32_t* work, int32_t* n_work, uint32_t* err) {
     extern __shared__ int32_t prep_smem[];  // [ncl]: first row of each lead
-    small_prep_body(nr, ncl, nc, p, row_ptr, cols, vals, piv_row, work, n_work, err, prep_smem);
+    small_prep_body(nr, ncl, nc, p, row_ptr, cols, vals, piv_row, pext, work, n_work, err,
+                    prep_smem);
 }
 
 // One warp per C|D row: the row is scattered into a dense accumulator of nc
@@ -134,19 +138,53 @@ k_small_prep(int32_t nr, int32_t ncl, int32_t nc, uint32_t p, const int64_t* __r
 // row (monic, its lead skipped) is applied by the 32 lanes in coalesced
 // strides (distinct columns, no conflicts).  The right block is written out
 // dense with its lead.  Nothing is read when the checks flagged the input.
-// rows w = first, first + step, ... (< n_rows) by the calling warp, whose
-// accumulator is acc (stride entries, 16-byte aligned)
+// rows w = w0, w0 + step, ... (< n_rows) by the calling warp, whose
+// accumulator is acc (stride entries, 16-byte aligned).  The pivot chain is
+// software-pipelined: before the current pivot row is applied, the warp
+// predicts the next pivot (the next nonzero column of the accumulator as it
+// stands) and loads that pivot row's first 128 entries, so that when the
+// prediction holds (the common case) the next step starts with its data in
+// registers; the pivot rows' extents come from a window of 32 consecutive
+// columns kept one per lane.
 template <class F>
 __device__ void rows_warp_body(int32_t n_rows, int w0, int step,
                                const int32_t* __restrict__ work,
                                const int64_t* __restrict__ row_ptr,
                                const int32_t* __restrict__ cols,
                                const uint32_t* __restrict__ vals,
-                               const int32_t* __restrict__ piv_row, int32_t ncl, int32_t nc,
+                               const int2* __restrict__ pext, int32_t ncl, int32_t nc,
                                int32_t stride, uint32_t* out, int64_t ld, int32_t* out_lead,
                                F f, uint32_t* acc) {
     const int lane = threadIdx.x & 31;
     const int32_t ncr = nc - ncl;
+    // first nonzero left column >= from (-1: none), the same for every lane
+    auto scan = [&](int from) -> int {
+        for (int base = from; base < ncl; base += 32) {
+            const int c = base + lane;
+            const unsigned bal = __ballot_sync(0xffffffffu, c < ncl && acc[c] != 0u);
+            if (bal) return base + __ffs(bal) - 1;
+        }
+        return -1;
+    };
+    int wbase = INT_MIN;  // extents window: lane l holds pext[wbase + l]
+    int2 wext = make_int2(0, 0);
+    auto extent = [&](int c) -> int2 {
+        if (c < wbase || c >= wbase + 32) {
+            wbase = c;
+            wext = c + lane < ncl ? pext[c + lane] : make_int2(0, 0);
+        }
+        const int l = c - wbase;
+        return make_int2(__shfl_sync(0xffffffffu, wext.x, l), __shfl_sync(0xffffffffu, wext.y, l));
+    };
+    // the first 128 entries of a pivot row, four per lane
+    auto fetch = [&](int2 e, int32_t (&c)[4], uint32_t (&v)[4]) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = e.x + lane + 32 * u;
+            c[u] = k < e.y ? cols[k] : -1;
+            v[u] = k < e.y ? vals[k] : 0u;
+        }
+    };
     for (int w = w0; w < n_rows; w += step) {
         const int32_t r = work[w];
         const int64_t rb = row_ptr[r], re = row_ptr[r + 1];
@@ -156,42 +194,51 @@ __device__ void rows_warp_body(int32_t n_rows, int w0, int step,
         __syncwarp();
         for (int64_t k = rb + lane; k < re; k += 32) acc[cols[k]] = vals[k];
         __syncwarp();
-        int last = lead - 1;
-        for (;;) {
-            int found = -1;
-            for (int base = last + 1; base < ncl; base += 32) {
-                const int c = base + lane;
-                const unsigned bal = __ballot_sync(0xffffffffu, c < ncl && acc[c] != 0u);
-                if (bal) {
-                    found = base + __ffs(bal) - 1;
-                    break;
+        int found = scan(lead);
+        if (found >= 0) {
+            int2 e = extent(found);
+            int32_t pc[4];
+            uint32_t pv[4];
+            fetch(e, pc, pv);
+            for (;;) {
+                const uint32_t m = f.prep(acc[found]);
+                // prediction: the next nonzero column before this update
+                const int spec = scan(found + 1);
+                int2 es = make_int2(0, 0);
+                int32_t sc[4];
+                uint32_t sv[4];
+                if (spec >= 0) {
+                    es = extent(spec);
+                    fetch(es, sc, sv);
                 }
-            }
-            if (found < 0) break;
-            const uint32_t m = f.prep(acc[found]);
-            const int32_t pr = piv_row[found];
-            const int64_t pb = row_ptr[pr] + 1, pe = row_ptr[pr + 1];
-            // four entries per lane at a time (distinct columns: loads first)
-            int64_t k = pb + lane;
-            for (; k + 96 < pe; k += 128) {
-                int32_t c[4];
-                uint32_t v[4], y[4];
+                // this pivot row: the first 128 entries from registers (distinct
+                // columns: all loads before the stores), the rest from memory
+                uint32_t y[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    c[u] = cols[k + 32 * u];
-                    v[u] = vals[k + 32 * u];
+                for (int u = 0; u < 4; ++u) y[u] = pc[u] >= 0 ? acc[pc[u]] : 0u;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (pc[u] >= 0) acc[pc[u]] = f.mulsub(y[u], m, pv[u]);
+                for (int k = e.x + 128 + lane; k < e.y; k += 32) {
+                    const int32_t c = cols[k];
+                    acc[c] = f.mulsub(acc[c], m, vals[k]);
                 }
+                __syncwarp();
+                const int nxt = scan(found + 1);
+                if (nxt < 0) break;
+                if (nxt == spec) {
+                    e = es;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) y[u] = acc[c[u]];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) acc[c[u]] = f.mulsub(y[u], m, v[u]);
+                    for (int u = 0; u < 4; ++u) {
+                        pc[u] = sc[u];
+                        pv[u] = sv[u];
+                    }
+                } else {
+                    e = extent(nxt);
+                    fetch(e, pc, pv);
+                }
+                found = nxt;
             }
-            for (; k < pe; k += 32) {
-                const int32_t c = cols[k];
-                acc[c] = f.mulsub(acc[c], m, vals[k]);
-            }
-            last = found;
-            __syncwarp();
         }
         uint32_t* o = out + (size_t)w * ld;
         int first = -1;
@@ -211,14 +258,14 @@ template <class F>
 __global__ void __launch_bounds__(kRowWarpsMax * 32)
 k_reduce_rows_warp(int32_t n_rows, const int32_t* __restrict__ work,
                    const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
-                   const uint32_t* __restrict__ vals, const int32_t* __restrict__ piv_row,
+                   const uint32_t* __restrict__ vals, const int2* __restrict__ pext,
                    int32_t ncl, int32_t nc, int32_t stride, uint32_t* out, int64_t ld,
                    int32_t* out_lead, const uint32_t* err, F f) {
     extern __shared__ __align__(16) uint32_t rw_acc[];
     if (*err) return;  // invalid input: nothing is read (uniform)
     const int warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
     rows_warp_body(n_rows, blockIdx.x * wpc + warp, gridDim.x * wpc, work, row_ptr, cols, vals,
-                   piv_row, ncl, nc, stride, out, ld, out_lead, f,
+                   pext, ncl, nc, stride, out, ld, out_lead, f,
                    rw_acc + (size_t)warp * stride);
 }
 
@@ -239,10 +286,10 @@ struct BatchItem {
     FieldMont fm;
 };
 
-// scratch of one matrix: piv_row [ncl] | work [nr] | n_work, err | D [n_work][ld] |
-// lead [n_work] | piv_of_col [ncr]
+// scratch of one matrix: piv_row [ncl] | pivot extents [ncl] | work [nr] | n_work, err |
+// D [n_work][ld] | lead [n_work] | piv_of_col [ncr]
 struct ScrLayout {
-    int64_t piv, work, cnt, D, lead, poc, bytes, ld;
+    int64_t piv, pext, work, cnt, D, lead, poc, bytes, ld;
 };
 __host__ __device__ inline int64_t rup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 __host__ __device__ inline ScrLayout scr_layout(int32_t nr, int32_t ncl, int32_t ncr) {
@@ -250,7 +297,8 @@ __host__ __device__ inline ScrLayout scr_layout(int32_t nr, int32_t ncl, int32_t
     const int64_t nw = nr - ncl > 0 ? nr - ncl : 1;
     L.ld = rup(ncr > 0 ? ncr : 1, 4);
     L.piv = 0;
-    L.work = rup(4 * (int64_t)(ncl > 0 ? ncl : 1), 256);
+    L.pext = rup(4 * (int64_t)(ncl > 0 ? ncl : 1), 256);
+    L.work = L.pext + rup(8 * (int64_t)(ncl > 0 ? ncl : 1), 256);
     L.cnt = L.work + rup(4 * (int64_t)nr, 256);
     L.D = L.cnt + 256;
     L.lead = L.D + rup(4 * nw * L.ld, 256);
@@ -293,6 +341,7 @@ k_batch_small(int32_t n, const BatchItem* __restrict__ items, const uint8_t* __r
         const ScrLayout S = scr_layout(nr, ncl, ncr);
         uint8_t* sb = scr + it.scr_off;
         int32_t* piv = (int32_t*)(sb + S.piv);
+        int2* pext = (int2*)(sb + S.pext);
         int32_t* work = (int32_t*)(sb + S.work);
         int32_t* nwork = (int32_t*)(sb + S.cnt);
         uint32_t* err = (uint32_t*)(sb + S.cnt + 16);
@@ -302,7 +351,7 @@ k_batch_small(int32_t n, const BatchItem* __restrict__ items, const uint8_t* __r
         const OutLayout O = out_layout(nr, ncl, ncr);
         uint8_t* ob = out + it.out_off;
         int64_t* counts = (int64_t*)ob;
-        small_prep_body(nr, ncl, nc, (uint32_t)it.p, row_ptr, cols, vals, piv, work, nwork, err,
+        small_prep_body(nr, ncl, nc, (uint32_t)it.p, row_ptr, cols, vals, piv, pext, work, nwork, err,
                         (int32_t*)bt_smem);
         __syncthreads();  // prep's global writes are visible to the block
         const uint32_t e = *err;
@@ -315,13 +364,13 @@ k_batch_small(int32_t n, const BatchItem* __restrict__ items, const uint8_t* __r
             uint32_t* acc = (uint32_t*)bt_smem + (size_t)warp * stride;
             if ((uint32_t)it.p < 65536u) {
                 if (warp < wpc)
-                    rows_warp_body(n_work, warp, wpc, work, row_ptr, cols, vals, piv, ncl, nc,
+                    rows_warp_body(n_work, warp, wpc, work, row_ptr, cols, vals, pext, ncl, nc,
                                    stride, D, S.ld, lead, it.fs, acc);
                 __syncthreads();
                 tiny_rref_body(n_work, ncr, D, S.ld, lead, err, to, it.fs, (uint32_t*)bt_smem);
             } else {
                 if (warp < wpc)
-                    rows_warp_body(n_work, warp, wpc, work, row_ptr, cols, vals, piv, ncl, nc,
+                    rows_warp_body(n_work, warp, wpc, work, row_ptr, cols, vals, pext, ncl, nc,
                                    stride, D, S.ld, lead, it.fm, acc);
                 __syncthreads();
                 tiny_rref_body(n_work, ncr, D, S.ld, lead, err, to, it.fm, (uint32_t*)bt_smem);
@@ -487,7 +536,8 @@ int small_reduce(const SmallInput& in, SmallAnswer* ans) {
     in.fill(in.ctx, (int64_t*)S->hin, (int32_t*)(S->hin + o_cols), (uint32_t*)(S->hin + o_vals));
     // device arena
     const size_t o_piv = round_up(in_bytes, 256);
-    const size_t o_work = round_up(o_piv + 4 * (size_t)std::max(ncl, 1), 256);
+    const size_t o_pext = round_up(o_piv + 4 * (size_t)std::max(ncl, 1), 256);
+    const size_t o_work = round_up(o_pext + 8 * (size_t)std::max(ncl, 1), 256);
     const size_t o_cnt = round_up(o_work + 4 * (size_t)nr, 256);  // n_work, err
     const size_t o_D = round_up(o_cnt + 64, 256);
     const size_t o_lead = round_up(o_D + 4 * (size_t)std::max(n_work, 1) * ld, 256);
@@ -499,6 +549,7 @@ int small_reduce(const SmallInput& in, SmallAnswer* ans) {
     const int32_t* d_cols = (const int32_t*)(d + o_cols);
     const uint32_t* d_vals = (const uint32_t*)(d + o_vals);
     int32_t* d_piv = (int32_t*)(d + o_piv);
+    int2* d_pext = (int2*)(d + o_pext);
     int32_t* d_work = (int32_t*)(d + o_work);
     int32_t* d_nwork = (int32_t*)(d + o_cnt);
     uint32_t* d_err = (uint32_t*)(d + o_cnt + 16);
@@ -533,7 +584,8 @@ int small_reduce(const SmallInput& in, SmallAnswer* ans) {
         return GBGPU_ECUDA;
     }
     k_small_prep<<<1, kPrepThreads, prep_bytes, s>>>(nr, ncl, nc, (uint32_t)in.p, d_ptr, d_cols,
-                                                     d_vals, d_piv, d_work, d_nwork, d_err);
+                                                     d_vals, d_piv, d_pext, d_work, d_nwork,
+                                                     d_err);
     ++launches;
     if (n_work > 0) {
         int32_t stride = 0;
@@ -548,7 +600,7 @@ int small_reduce(const SmallInput& in, SmallAnswer* ans) {
                 return GBGPU_ECUDA;
             }
             k_reduce_rows_warp<Fd><<<grid, wpc * 32, bytes, s>>>(
-                n_work, d_work, d_ptr, d_cols, d_vals, d_piv, ncl, nc, stride, d_D, ld, d_lead,
+                n_work, d_work, d_ptr, d_cols, d_vals, d_pext, ncl, nc, stride, d_D, ld, d_lead,
                 d_err, f);
             ++launches;
             cudaError_t e = launch_tiny_rref(n_work, ncr, d_D, ld, d_lead, d_err, ncl,
