@@ -710,8 +710,12 @@ int plan_run(Plan* P) {
                                 cudaMemcpyDeviceToHost, P->stream));
         GB_CUDA(cudaStreamSynchronize(P->stream));
         for (size_t i = 0; i < prof.events.size(); ++i) {
-            float ms = 0;
+            float ms = 0, split_ms = 0;
             cudaEventElapsedTime(&ms, prof.events[i].first, prof.events[i].second);
+            if (i < prof.split_events.size()) {
+                cudaEventElapsedTime(&split_ms, prof.split_events[i], prof.events[i].first);
+                cudaEventDestroy(prof.split_events[i]);
+            }
             cudaEventDestroy(prof.events[i].first);
             cudaEventDestroy(prof.events[i].second);
             const double ops =
@@ -719,9 +723,12 @@ int plan_run(Plan* P) {
             P->stats.gemm_ms += ms;
             P->stats.gemm_int8_ops += ops;
             if (debug_trace())
-                fprintf(stderr, "gbgpu gemm %3zu: M %6d N %6d K %6d batch %5d  %8.3f ms  %8.1f TOPS\n",
+                fprintf(stderr,
+                        "gbgpu gemm %3zu: M %6d N %6d K %6d batch %5d  %8.3f ms  %8.1f TOPS"
+                        "  splits %8.3f ms\n",
                         i, prof.shape[4 * i], prof.shape[4 * i + 1], prof.shape[4 * i + 2],
-                        prof.shape[4 * i + 3], ms, ms > 0 ? ops / (ms * 1e-3) / 1e12 : 0.0);
+                        prof.shape[4 * i + 3], ms, ms > 0 ? ops / (ms * 1e-3) / 1e12 : 0.0,
+                        split_ms);
         }
     }
     if (rc) return rc;

@@ -854,6 +854,13 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     uint8_t* fa = Bp + (size_t)nb * L * Np * Kp;             // [nb][Mp/128][nkbp]
     uint8_t* fb = fa + (size_t)nb * (Mp / Cfg::BM) * nkbp;   // [nb][Np/BN][nkbp]
     const size_t flag_bytes = (size_t)nb * (Mp / Cfg::BM + Np / Cfg::BN) * nkbp;
+    GemmProfile* prof = gemm_profile();
+    if (prof) {
+        cudaEvent_t es = nullptr;
+        cudaEventCreate(&es);
+        cudaEventRecord(es, s);
+        prof->split_events.push_back(es);
+    }
     if (cudaMemsetAsync(fa, 0, flag_bytes, s) != cudaSuccess) {
         set_error("tile flag clear failed");
         return GBGPU_ECUDA;
@@ -909,7 +916,6 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     const int64_t tiles = (int64_t)(Np / Cfg::BN) * (Mp / Cfg::BM) * nb;
     const dim3 grid((unsigned)std::max<int64_t>(
         1, std::min<int64_t>(tiles, (int64_t)num_sms() * Cfg::MIN_CTAS)));
-    GemmProfile* prof = gemm_profile();
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof) {
         const int slot = (int)prof->events.size();

@@ -38,6 +38,7 @@ struct GemmProfile {
     unsigned long long* d_steps = nullptr;  // device counters, one per launch
     int capacity = 0;                       // counters in d_steps
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<cudaEvent_t> split_events;  // per launch: before its limb splits
     std::vector<double> macs_per_step;      // per launch
     std::vector<int> shape;                 // per launch: M, N, K, batch
 };
