@@ -641,7 +641,7 @@ static int run_form(Plan* P, const F& f) {
         }
         GB_LAUNCH(k_row_write<<<grid_for((int64_t)P->np * 32, T), T, 0, s>>>(
             P->np, P->pivcol, P->piv_of_col, final_rows, rows_ld, width, P->offs, shift,
-            P->out_cols, P->out_vals));
+            P->out_cols, P->out_vals, 4));
     }
     GB_CUDA(cudaEventRecord(P->ev[5], s));
     if (P->blocked) {

@@ -88,11 +88,25 @@ __global__ void k_densify(int32_t n, const int32_t* __restrict__ rows,
 // stride is 0); columns left of from_i are not written.  Each CTA assembles
 // DS_COLS-column segments of a row in shared memory and writes them whole
 // with 16-byte stores (ld a multiple of 4, out 16-byte aligned).
+//
+// With split > 0 (the known pivots P = [A | B] of the tensor form, whose
+// readers need less) only two column intervals of row i are written:
+//   [from_i, e1), e1 = min(split, max(from_i + stride, span[i / stride] + 1)):
+//       the diagonal block and the left columns the block's rows reach;
+//   [split + lo, split + hi): the right columns of row group i / 128, from
+//       brange[i / 128] = (first, last) nonzero right column of the group,
+//       widened to 64-column boundaries (the limb split reads whole
+//       64-column blocks); nothing when the group's right part is zero.
+// Everything else in the row is left as it was: its readers (the block
+// inverses, the block solves and the limb split of the Schur product's B)
+// never look there.
 constexpr int DS_COLS = 16384;
 __global__ void __launch_bounds__(512)
 k_densify_seg(int32_t n, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_ptr,
               const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals, int32_t nc,
-              int32_t stride, uint32_t* out, int64_t ld) {
+              int32_t stride, uint32_t* out, int64_t ld, int32_t split = 0,
+              const int32_t* __restrict__ span = nullptr,
+              const int2* __restrict__ brange = nullptr) {
     extern __shared__ uint4 ds_smem[];
     uint32_t* seg = (uint32_t*)ds_smem;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
@@ -100,20 +114,44 @@ k_densify_seg(int32_t n, const int32_t* __restrict__ rows, const int64_t* __rest
         const int64_t b = row_ptr[r], e = row_ptr[r + 1];
         const int32_t from = stride ? (i / stride) * stride : 0;
         uint32_t* o = out + (size_t)i * ld;
-        for (int32_t s0 = from; s0 < nc; s0 += DS_COLS) {
-            const int32_t w = min(DS_COLS, nc - s0);
-            for (int j = threadIdx.x; j < (w + 3) / 4; j += blockDim.x)
-                ds_smem[j] = make_uint4(0u, 0u, 0u, 0u);
-            __syncthreads();
-            for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
-                const int32_t c = cols[k] - s0;
-                if (c >= 0 && c < w) seg[c] = vals[k];
+        // the (one or two) intervals of this row
+        int32_t iv[2][2] = {{from, nc}, {0, 0}};
+        int n_iv = 1;
+        if (split > 0) {
+            int32_t e1 = split;
+            if (span && stride) e1 = min(split, max(from + stride, span[i / stride] + 1));
+            iv[0][1] = e1;
+            const int2 br = brange[i / 128];
+            if (br.y >= br.x) {
+                const int32_t lo = split + (br.x / 64) * 64;
+                const int32_t hi = min(nc, split + (br.y / 64 + 1) * 64);
+                const int32_t s = lo & ~3;
+                if (s <= e1) {
+                    iv[0][1] = max(e1, hi);
+                } else {
+                    iv[1][0] = s;
+                    iv[1][1] = hi;
+                    n_iv = 2;
+                }
             }
-            __syncthreads();
-            uint4* o4 = (uint4*)(o + s0);
-            for (int j = threadIdx.x; j < w / 4; j += blockDim.x) o4[j] = ds_smem[j];
-            for (int j = (w / 4) * 4 + threadIdx.x; j < w; j += blockDim.x) o[s0 + j] = seg[j];
-            __syncthreads();
+        }
+        for (int q = 0; q < n_iv; ++q) {
+            const int32_t a0 = iv[q][0], a1 = iv[q][1];
+            for (int32_t s0 = a0; s0 < a1; s0 += DS_COLS) {
+                const int32_t w = min(DS_COLS, a1 - s0);
+                for (int j = threadIdx.x; j < (w + 3) / 4; j += blockDim.x)
+                    ds_smem[j] = make_uint4(0u, 0u, 0u, 0u);
+                __syncthreads();
+                for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
+                    const int32_t c = cols[k] - s0;
+                    if (c >= 0 && c < w) seg[c] = vals[k];
+                }
+                __syncthreads();
+                uint4* o4 = (uint4*)(o + s0);
+                for (int j = threadIdx.x; j < w / 4; j += blockDim.x) o4[j] = ds_smem[j];
+                for (int j = (w / 4) * 4 + threadIdx.x; j < w; j += blockDim.x) o[s0 + j] = seg[j];
+                __syncthreads();
+            }
         }
     }
 }
@@ -133,23 +171,44 @@ __global__ void k_densify_pivots(int32_t ncl, const int32_t* __restrict__ piv_ro
     }
 }
 
-// span[b] = largest column < limit of the known pivots of rows [bs b, bs b + bs)
+// span[b] = largest column < limit of the known pivots of rows [bs b, bs b + bs);
+// with brange, also the first and last column >= limit (as column - limit)
+// of every group of 128 rows, (INT_MAX, -1) filled in before
 __global__ void k_block_span(int32_t ncl, const int32_t* __restrict__ piv_row,
                              const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
-                             int32_t limit, int32_t bs, int32_t* span) {
+                             int32_t limit, int32_t bs, int32_t* span, int2* brange = nullptr) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int c = warp; c < ncl; c += nwarps) {
         const int32_t r = piv_row[c];
-        int32_t mx = -1;
+        int32_t mx = -1, blo = INT_MAX, bhi = -1;
         for (int64_t k = row_ptr[r] + lane; k < row_ptr[r + 1]; k += 32) {
             const int32_t col = cols[k];
-            if (col < limit && col > mx) mx = col;
+            if (col < limit) {
+                mx = max(mx, col);
+            } else {
+                blo = min(blo, col - limit);
+                bhi = max(bhi, col - limit);
+            }
         }
-        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        for (int o = 16; o > 0; o >>= 1) {
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            blo = min(blo, __shfl_xor_sync(0xffffffffu, blo, o));
+            bhi = max(bhi, __shfl_xor_sync(0xffffffffu, bhi, o));
+        }
         if (lane == 0 && mx >= 0) atomicMax(&span[c / bs], mx);
+        if (lane == 0 && brange && bhi >= 0) {
+            atomicMin(&brange[c / 128].x, blo);
+            atomicMax(&brange[c / 128].y, bhi);
+        }
     }
+}
+
+// every range empty: (INT_MAX, -1)
+__global__ void k_clear_ranges(int32_t n, int2* r) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        r[i] = make_int2(INT_MAX, -1);
 }
 
 // lead (first column) of each listed CSR row
@@ -333,7 +392,9 @@ __global__ void k_scatter_rows_dense(int32_t nrows, const int32_t* __restrict__ 
 
 // first nonzero column of every row (-1 for zero rows), one warp per row;
 // with from_prev the scan starts at the row's current lead (leads only move
-// right under elimination)
+// right under elimination).  A pass covers LEAD_U chunks of 32 columns whose
+// loads are in flight together.
+constexpr int LEAD_U = 8;
 __global__ void k_row_leads(int32_t rows, const int32_t* __restrict__ list, int32_t ncols,
                             const uint32_t* __restrict__ M, int64_t ld, int32_t* lead,
                             int32_t from_prev = 0) {
@@ -345,21 +406,22 @@ __global__ void k_row_leads(int32_t rows, const int32_t* __restrict__ list, int3
         const uint32_t* row = M + (size_t)r * ld;
         int found = -1;
         const int start = from_prev && lead[r] > 0 ? lead[r] : 0;
-        for (int base = start; base < ncols; base += 32) {
-            const int c = base + lane;
-            const unsigned bal = __ballot_sync(0xffffffffu, c < ncols && row[c] != 0u);
-            if (bal) {
-                found = base + __ffs(bal) - 1;
-                break;
+        for (int base = start; base < ncols && found < 0; base += 32 * LEAD_U) {
+            uint32_t v[LEAD_U];
+#pragma unroll
+            for (int u = 0; u < LEAD_U; ++u) {
+                const int c = base + 32 * u + lane;
+                v[u] = c < ncols ? row[c] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < LEAD_U; ++u) {
+                const unsigned bal = __ballot_sync(0xffffffffu, v[u] != 0u);
+                if (bal && found < 0) found = base + 32 * u + __ffs(bal) - 1;
             }
         }
         if (lane == 0) lead[r] = found;
     }
 }
-
-
-
-
 
 // columns with flag set, ascending, via a precomputed exclusive scan
 __global__ void k_compact_cols(int32_t n, const int32_t* __restrict__ flag,
@@ -514,7 +576,8 @@ __global__ void k_register_chunks(const int32_t* __restrict__ n_piv,
 }
 
 // scale row rows[i] by the inverse of its entry at column cols[i] (one CTA
-// per row)
+// per row; NORM_U independent loads per thread and pass)
+constexpr int NORM_U = 8;
 template <class F>
 __global__ void k_normalize_at(const int32_t* __restrict__ n_dev, const int32_t* __restrict__ rows,
                                const int32_t* __restrict__ cols, int32_t ncols, uint32_t* M,
@@ -526,14 +589,23 @@ __global__ void k_normalize_at(const int32_t* __restrict__ n_dev, const int32_t*
         const int32_t c0 = cols[i];
         const uint32_t lv = row[c0];
         if (lv == 1u) continue;  // uniform over the CTA
-        if (threadIdx.x == 0) s_inv = inverse_mod(lv, f.p);
+        __syncthreads();  // the previous row's readers of s_inv are done
+        if (threadIdx.x == 0) s_inv = f.prep(inverse_mod(lv, f.p));
         __syncthreads();
         const uint32_t inv = s_inv;
-        for (int c = c0 + 1 + threadIdx.x; c < ncols; c += blockDim.x) {
-            const uint32_t v = row[c];
-            if (v) row[c] = f.mulmod(v, inv);
+        for (int c = c0 + 1 + threadIdx.x; c < ncols; c += blockDim.x * NORM_U) {
+            uint32_t v[NORM_U];
+#pragma unroll
+            for (int u = 0; u < NORM_U; ++u) {
+                const int cc = c + u * (int)blockDim.x;
+                v[u] = cc < ncols ? row[cc] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < NORM_U; ++u) {
+                const int cc = c + u * (int)blockDim.x;
+                if (v[u]) row[cc] = f.mulp(v[u], inv);
+            }
         }
-        __syncthreads();
         if (threadIdx.x == 0) row[c0] = 1u;
     }
 }
@@ -553,7 +625,10 @@ __global__ void k_normalize_at(const int32_t* __restrict__ n_dev, const int32_t*
 // lead, fraction-free: row_r <- P[i][c] row_r - P[r][c] row_i on the columns
 // after c and on E (a nonzero multiple of the usual update: the same zero
 // pattern, hence the same leads and pivots, and no inverse on the sequential
-// path).  Pivot rows are not scaled (they are normalised after the round).
+// path; each entry takes one reduction, f.ffsub).  On E only the columns in
+// the union of the two rows' supports are touched: every E row keeps its
+// support as a 128-bit mask (the chunk rows combined into it so far).
+// Pivot rows are not scaled (they are normalised after the round).
 // Column c is never read again, so it is not written; the pivot row is not
 // written in the step that chooses it, so the updates need no barrier of their
 // own.  The updated rows recompute their leads from the values they wrote and
@@ -575,10 +650,11 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     int32_t* piv_pos = piv_pos_b + d * KB;
     int32_t* piv_col = piv_col_b + d * KB;
     int32_t* n_piv = n_piv_b + d;
-    extern __shared__ uint32_t pf_smem[];
+    extern __shared__ __align__(16) uint32_t pf_smem[];
     uint32_t(*P)[PF_LD] = (uint32_t(*)[PF_LD])pf_smem;
     uint32_t(*E)[PF_LD] = (uint32_t(*)[PF_LD])(pf_smem + KB * PF_LD);
     __shared__ int s_min[2][KB * PF_GROUPS / 32];  // double-buffered block minimum
+    __shared__ uint32_t s_emask[KB][4];             // support of every E row
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int r = tid / PF_GROUPS, g = tid % PF_GROUPS;  // row and column group of this thread
@@ -587,6 +663,10 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
         const int i = t / KB, c = t % KB;
         P[i][c] = (i < n && c < bw) ? Dp[(size_t)rows[i] * ld + pj + c] : 0u;
         E[i][c] = i == c ? 1u : 0u;
+    }
+    for (int t = tid; t < KB * 4; t += nt) {
+        const int i = t / 4, w = t % 4;
+        s_emask[i][w] = (i / 32 == w) ? 1u << (i % 32) : 0u;
     }
     __syncthreads();
     int my_lead = INT_MAX;  // this row's lead (INT_MAX: zero in the panel or not a row)
@@ -619,46 +699,50 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
         }
         if (r == i) my_piv = true;
         if (!my_piv && my_lead == c) {
-            const uint32_t ap = f.prep(P[i][c]);  // the pivot's lead value
-            const uint32_t mp = f.prep(P[r][c]);  // this row's value in column c
+            // row_r <- a row_r - m row_i, a = P[i][c], m = P[r][c], one
+            // reduction per entry (f.ffsub).  Lane g takes the 4-column groups
+            // 4 g + 32 t (16-byte shared-memory accesses).  Left of c both rows
+            // are zero and at c the result is zero, so whole groups are
+            // computed; groups entirely left of c are skipped.
+            const uint32_t ap = f.prep(P[i][c]);
+            const uint32_t mn = f.prep(f.p - P[r][c]);
             int nl = INT_MAX;
-            // four independent columns per pass (loads first, then stores)
-            for (int cc = c + 1 + g; cc < bw; cc += 4 * PF_GROUPS) {
-                uint32_t x[4], v[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int col = cc + u * PF_GROUPS;
-                    v[u] = col < bw ? P[i][col] : 0u;
-                    x[u] = col < bw ? P[r][col] : 0u;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int col = cc + u * PF_GROUPS;
-                    if (col < bw && (x[u] | v[u])) {
-                        const uint32_t ax = x[u] ? f.mulp(x[u], ap) : 0u;
-                        const uint32_t y = v[u] ? f.mulsub(ax, mp, v[u]) : ax;
-                        P[r][col] = y;
-                        if (y != 0u && col < nl) nl = col;
-                    }
-                }
+            for (int t4 = 0; t4 < 4; ++t4) {
+                const int base = 32 * t4 + 4 * g;
+                if (base + 3 <= c || base >= bw) continue;
+                const uint4 x4 = *(const uint4*)&P[r][base];
+                const uint4 v4 = *(const uint4*)&P[i][base];
+                uint4 y;
+                y.x = f.ffsub(x4.x, ap, v4.x, mn);
+                y.y = f.ffsub(x4.y, ap, v4.y, mn);
+                y.z = f.ffsub(x4.z, ap, v4.z, mn);
+                y.w = f.ffsub(x4.w, ap, v4.w, mn);
+                *(uint4*)&P[r][base] = y;
+                const int first = y.x ? 0 : y.y ? 1 : y.z ? 2 : y.w ? 3 : 4;
+                if (first < 4) nl = min(nl, base + first);
             }
-            for (int cc = g; cc < n; cc += 4 * PF_GROUPS) {
-                uint32_t x[4], v[4];
+            // E: only the 4-column groups that meet the union of the two
+            // rows' supports (every E row keeps its support as a mask of the
+            // chunk rows combined into it so far)
+            uint32_t U[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int col = cc + u * PF_GROUPS;
-                    v[u] = col < n ? E[i][col] : 0u;
-                    x[u] = col < n ? E[r][col] : 0u;
-                }
+            for (int w = 0; w < 4; ++w) U[w] = s_emask[r][w] | s_emask[i][w];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int col = cc + u * PF_GROUPS;
-                    if (col < n && (x[u] | v[u])) {
-                        const uint32_t ax = x[u] ? f.mulp(x[u], ap) : 0u;
-                        E[r][col] = v[u] ? f.mulsub(ax, mp, v[u]) : ax;
-                    }
-                }
+            for (int t4 = 0; t4 < 4; ++t4) {
+                const int base = 32 * t4 + 4 * g;
+                if (base >= n || ((U[t4] >> (4 * g)) & 0xFu) == 0u) continue;
+                const uint4 x4 = *(const uint4*)&E[r][base];
+                const uint4 v4 = *(const uint4*)&E[i][base];
+                uint4 y;
+                y.x = f.ffsub(x4.x, ap, v4.x, mn);
+                y.y = f.ffsub(x4.y, ap, v4.y, mn);
+                y.z = f.ffsub(x4.z, ap, v4.z, mn);
+                y.w = f.ffsub(x4.w, ap, v4.w, mn);
+                *(uint4*)&E[r][base] = y;
             }
+            __syncwarp(grp);  // the row's lanes have read its old support
+            if (g < 4) s_emask[r][g] = g == 0 ? U[0] : g == 1 ? U[1] : g == 2 ? U[2] : U[3];
             nl = min(nl, __shfl_xor_sync(grp, nl, 1));
             nl = min(nl, __shfl_xor_sync(grp, nl, 2));
             nl = min(nl, __shfl_xor_sync(grp, nl, 4));
@@ -686,109 +770,244 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
 // rows of chunk d become E_d old over the columns from the first dirty panel
 // on, as  D[row of pivot k] = old[pos_k] - sum_j (I - E_d)[pos_k][j] old[j]
 // (ime = I - E_d from k_panel_factor; pos_k = the pivot's chunk position).
-// A block walks PA_TILES tiles of 64 columns of one chunk: it stages the old
-// values of the chunk's n rows for a tile in shared memory, then every thread
-// forms the new values of four pivots in one column, reading the (I - E) rows
-// through the L1 cache (all lanes of a warp read the same entry): 64-bit sums
-// without reduction (p < 2^16: each product < 2^32, at most 128 of them;
-// otherwise the column value in 16-bit halves), one reduction per result.
-// Reads happen before any write of the same columns (a block owns its columns
-// of the chunk), so the update is in place.  Only pivot rows are written.
+// It is a small GEMM per chunk (np x n times n x width), done with register
+// tiles: a block owns tiles of 64 columns of one chunk; it stages the (I - E)
+// rows of its pivots transposed (A^T, n x 16 QC) once and, per tile, the old
+// values of the chunk's n rows (T, n x 64).  Every thread forms 4 pivots x QC
+// columns, one 16-byte read of A^T and QC reads of T per step of the sum; QC
+// (1, 2 or 4) is the smallest that covers the chunk's pivots in one pass
+// (16 QC pivots), so that every thread has work; chunks of more than 64
+// pivots take several passes.  64-bit sums without reduction (p < 2^16: each
+// product < 2^32, at most 128 of them; otherwise the column value in 16-bit
+// halves), one reduction per result.  A block reads all of a tile's columns
+// before it writes any (it owns them), so the update is in place.  Only pivot
+// rows are written.
 constexpr int PA_COLS = 64;
 constexpr int PA_THREADS = 256;
-constexpr int PA_PIV = 4;
-constexpr int PA_TILES = 4;
-constexpr int PA_AST = 3072;  // (I - E) entries kept in shared memory
+constexpr int PA_PB = 64;            // most pivots per pass (QC = 4)
+constexpr int PA_SMALL_ROWS = 32;    // chunks up to this many rows: k_panel_apply_small
+constexpr int PA_ALD = PA_PB + 4;    // row stride of A^T (16-byte aligned rows)
+constexpr int PA_SMEM = (KB * PA_COLS + KB * PA_ALD) * (int)sizeof(uint32_t);
+
+// the sums of one pass: pivots kp + 4 pg + q (q < 4, below kp + kn) times
+// columns cg + (64 / QC) u (u < QC) of the tile at c0, written to the pivots'
+// rows
+template <bool WIDE, int QC>
+__device__ __forceinline__ void pa_pass(uint32_t* Dp, int64_t ld, int32_t ncr, int c0, int n,
+                                        int kp, int kn, const uint32_t (*T)[PA_COLS],
+                                        const uint32_t (*At)[PA_ALD], const int32_t* s_pos,
+                                        const int32_t* s_drow, uint32_t p, uint64_t m) {
+    constexpr int CG = PA_COLS / QC;  // column groups
+    const int cg = threadIdx.x % CG, pg = threadIdx.x / CG;
+    if (4 * pg >= kn) return;
+    uint64_t lo[4][QC], hi[4][QC];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int u = 0; u < QC; ++u) lo[q][u] = hi[q][u] = 0;
+    const bool full = 4 * pg + 4 <= kn;
+#pragma unroll 2
+    for (int j = 0; j < n; ++j) {
+        uint4 a4 = *(const uint4*)&At[j][4 * pg];
+        if (!full) {  // entries past kn are not this pass's pivots
+            const int r = kn - 4 * pg;
+            if (r < 4) a4.w = 0u;
+            if (r < 3) a4.z = 0u;
+            if (r < 2) a4.y = 0u;
+        }
+        const uint32_t a[4] = {a4.x, a4.y, a4.z, a4.w};
+        uint32_t v[QC];
+#pragma unroll
+        for (int u = 0; u < QC; ++u) v[u] = T[j][cg + CG * u];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int u = 0; u < QC; ++u) {
+                if (WIDE) {
+                    lo[q][u] += (uint64_t)a[q] * (v[u] & 0xFFFFu);
+                    hi[q][u] += (uint64_t)a[q] * (v[u] >> 16);
+                } else {
+                    lo[q][u] += (uint64_t)a[q] * v[u];
+                }
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = kp + 4 * pg + q;
+        if (k >= kp + kn) break;
+        const int pos = s_pos[k];
+        uint32_t* out = Dp + (size_t)s_drow[k] * ld;
+#pragma unroll
+        for (int u = 0; u < QC; ++u) {
+            const int cc = cg + CG * u, col = c0 + cc;
+            if (col < ncr) {
+                const uint32_t s = WIDE ? fold_lohi(lo[q][u], hi[q][u], p, m) : mod64(lo[q][u], p, m);
+                const uint32_t old = T[pos][cc];
+                out[col] = old >= s ? old - s : old + (p - s);
+            }
+        }
+    }
+}
+
+// Chunks of at most 32 rows: a warp per 32-column strip, the strip's old
+// values of the chunk's n rows in registers (one independent load each), the
+// chunk's transformation rows E (np x n, E = I - (I - E), so the pivot's own
+// old value is part of the sum) broadcast from shared memory.  No barrier
+// after the staging.  NJ >= n is the unrolled row count.
+template <bool WIDE, int NJ>
+__device__ __forceinline__ void pa_small(uint32_t* Dp, int64_t ld, int32_t ncr, int c_lo,
+                                         int c_hi, int n, int np, const uint32_t* Es,
+                                         const int32_t* s_rows, const int32_t* s_drow,
+                                         uint32_t p, uint64_t m) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int s0 = c_lo + 32 * warp; s0 < c_hi; s0 += 32 * (PA_THREADS / 32)) {
+        const int col = s0 + lane;
+        const bool ok = col < c_hi && col < ncr;
+        uint32_t v[NJ];
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) v[j] = (ok && j < n) ? Dp[(size_t)s_rows[j] * ld + col] : 0u;
+        for (int k = 0; k < np; ++k) {
+            const uint32_t* e = Es + k * 32;
+            uint64_t lo = 0, hi = 0;
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                const uint32_t a = e[j];  // zero for j >= n
+                if (WIDE) {
+                    lo += (uint64_t)a * (v[j] & 0xFFFFu);
+                    hi += (uint64_t)a * (v[j] >> 16);
+                } else {
+                    lo += (uint64_t)a * v[j];
+                }
+            }
+            if (ok) Dp[(size_t)s_drow[k] * ld + col] = WIDE ? fold_lohi(lo, hi, p, m) : mod64(lo, p, m);
+        }
+    }
+}
 
 template <bool WIDE>
 __global__ void __launch_bounds__(PA_THREADS)
-k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0,
+k_panel_apply(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0, int32_t tiles_per_block,
               const int32_t* __restrict__ chunk_rows, const int32_t* __restrict__ dpanel,
               const int32_t* __restrict__ cursor, const uint32_t* __restrict__ ime_b,
               const int32_t* __restrict__ n_piv_b, const int32_t* __restrict__ arows_b,
               const int32_t* __restrict__ drows_b, uint32_t p) {
-    __shared__ uint32_t T[KB][PA_COLS];
-    __shared__ uint32_t s_a[PA_AST];
+    extern __shared__ __align__(16) uint32_t pa_smem[];
+    uint32_t(*T)[PA_COLS] = (uint32_t(*)[PA_COLS])pa_smem;
+    uint32_t(*At)[PA_ALD] = (uint32_t(*)[PA_ALD])(pa_smem + KB * PA_COLS);
     __shared__ int32_t s_rows[KB], s_pos[KB], s_drow[KB];
     const int d = blockIdx.y;
     const int n = min(cursor[d], KB), np = n_piv_b[d];
     const int pj = dpanel[d] * KB;
-    if (np == 0) return;  // uniform
+    // the block's tiles: [tile0, tile1), the first one right of the chunk's
+    // panel start (the chunk rows are zero left of it)
+    const int ntiles = (ncr - j0 + PA_COLS - 1) / PA_COLS;
+    int tile0 = blockIdx.x * tiles_per_block;
+    const int tile1 = min(ntiles, tile0 + tiles_per_block);
+    tile0 = max(tile0, pj > j0 ? (pj - j0) / PA_COLS : 0);
+    // uniform: nothing to do, or a chunk for k_panel_apply_small
+    if (np == 0 || tile0 >= tile1 || n <= PA_SMALL_ROWS) return;
     for (int t = threadIdx.x; t < KB; t += PA_THREADS) {
         s_rows[t] = t < n ? chunk_rows[(size_t)d * KB + t] : 0;
         s_pos[t] = t < np ? arows_b[(size_t)d * KB + t] : 0;
         s_drow[t] = t < np ? drows_b[(size_t)d * KB + t] : 0;
     }
+    __syncthreads();
     const uint32_t* ime = ime_b + (size_t)d * KB * KB;
-    // the (I - E) rows of the block's pivots, n entries each, in shared memory
-    // when they fit (else read through L1)
-    const bool in_smem = np * n <= PA_AST;
-    if (in_smem)
-        for (int t = threadIdx.x; t < np * n; t += PA_THREADS) {
-            const int k = t / n, j = t % n;
-            s_a[t] = ime[(size_t)arows_b[(size_t)d * KB + k] * KB + j];
-        }
     const uint64_t m = ~0ull / p;
-    const int c = threadIdx.x % PA_COLS, g = threadIdx.x / PA_COLS;
-    for (int tile = 0; tile < PA_TILES; ++tile) {
-        const int c0 = j0 + (blockIdx.x * PA_TILES + tile) * PA_COLS;
-        if (c0 >= ncr) break;                // uniform
-        if (c0 + PA_COLS <= pj) continue;    // uniform: the chunk rows are zero here
-        __syncthreads();  // the row lists are in place / the last tile's readers are done
-        for (int t = threadIdx.x; t < n * PA_COLS; t += PA_THREADS) {
-            const int j = t / PA_COLS, cc = t % PA_COLS, col = c0 + cc;
-            T[j][cc] = col < ncr ? Dp[(size_t)s_rows[j] * ld + col] : 0u;
+    // columns per thread and pivots per pass (uniform over the block)
+    const int qc = np <= 16 ? 1 : (np <= 32 ? 2 : 4);
+    const int pb = 16 * qc;
+    // A^T of pivots [kp, kp + kn)
+    auto stage_a = [&](int kp, int kn) {
+        for (int t = threadIdx.x; t < kn * n; t += PA_THREADS) {
+            const int k = t / n, j = t % n;
+            At[j][k] = ime[(size_t)s_pos[kp + k] * KB + j];
         }
-        __syncthreads();
-        const int col = c0 + c;
-        for (int k0 = g * PA_PIV; k0 < np; k0 += (PA_THREADS / PA_COLS) * PA_PIV) {
-            uint64_t lo[PA_PIV], hi[PA_PIV];
+    };
+    const bool one_pass = np <= pb;
+    if (one_pass) stage_a(0, np);  // once for all tiles
+    for (int tile = tile0; tile < tile1; ++tile) {
+        const int c0 = j0 + tile * PA_COLS;
+        __syncthreads();  // the last tile's readers of T are done
+        {
+            // n x 64 old values, eight independent loads per thread at a time
+            const int total = n * PA_COLS;
+            for (int t0 = threadIdx.x; t0 < total; t0 += 8 * PA_THREADS) {
+                uint32_t v[8];
 #pragma unroll
-            for (int q = 0; q < PA_PIV; ++q) lo[q] = hi[q] = 0;
-            if (in_smem) {
-                const uint32_t* ar = s_a + (size_t)k0 * n;
-                const int kq = min(PA_PIV, np - k0);
-#pragma unroll 4
-                for (int j = 0; j < n; ++j) {
-                    const uint32_t v = T[j][c];
-                    const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
-#pragma unroll
-                    for (int q = 0; q < PA_PIV; ++q) {
-                        const uint32_t a = q < kq ? ar[q * n + j] : 0u;
-                        lo[q] += (uint64_t)a * vl;
-                        if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
-                    }
+                for (int q = 0; q < 8; ++q) {
+                    const int t = t0 + q * PA_THREADS;
+                    const int j = t / PA_COLS, col = c0 + t % PA_COLS;
+                    v[q] = (t < total && col < ncr) ? Dp[(size_t)s_rows[j] * ld + col] : 0u;
                 }
-            } else {
-                const uint32_t* ar[PA_PIV];
 #pragma unroll
-                for (int q = 0; q < PA_PIV; ++q)
-                    ar[q] = ime + (size_t)s_pos[min(k0 + q, np - 1)] * KB;
-                for (int j = 0; j < n; ++j) {
-                    const uint32_t v = T[j][c];
-                    const uint32_t vl = WIDE ? (v & 0xFFFFu) : v;
-#pragma unroll
-                    for (int q = 0; q < PA_PIV; ++q) {
-                        const uint32_t a = __ldg(ar[q] + j);
-                        lo[q] += (uint64_t)a * vl;
-                        if (WIDE) hi[q] += (uint64_t)a * (v >> 16);
-                    }
+                for (int q = 0; q < 8; ++q) {
+                    const int t = t0 + q * PA_THREADS;
+                    if (t < total) T[t / PA_COLS][t % PA_COLS] = v[q];
                 }
             }
-            if (col < ncr) {
-#pragma unroll
-                for (int q = 0; q < PA_PIV; ++q) {
-                    const int k = k0 + q;
-                    if (k < np) {
-                        const uint32_t s =
-                            WIDE ? fold_lohi(lo[q], hi[q], p, m) : mod64(lo[q], p, m);
-                        const uint32_t old = T[s_pos[k]][c];
-                        Dp[(size_t)s_drow[k] * ld + col] = old >= s ? old - s : old + (p - s);
-                    }
-                }
+        }
+        for (int kp = 0; kp < np; kp += pb) {
+            const int kn = min(pb, np - kp);
+            if (!one_pass) {
+                __syncthreads();  // the last pass's readers of A^T are done
+                stage_a(kp, kn);
             }
+            __syncthreads();  // T and A^T are in place
+            if (qc == 1)
+                pa_pass<WIDE, 1>(Dp, ld, ncr, c0, n, kp, kn, T, At, s_pos, s_drow, p, m);
+            else if (qc == 2)
+                pa_pass<WIDE, 2>(Dp, ld, ncr, c0, n, kp, kn, T, At, s_pos, s_drow, p, m);
+            else
+                pa_pass<WIDE, 4>(Dp, ld, ncr, c0, n, kp, kn, T, At, s_pos, s_drow, p, m);
         }
     }
+}
+
+// the chunks of k_panel_apply with at most PA_SMALL_ROWS rows (same grid)
+template <bool WIDE>
+__global__ void __launch_bounds__(PA_THREADS)
+k_panel_apply_small(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0, int32_t tiles_per_block,
+                    const int32_t* __restrict__ chunk_rows, const int32_t* __restrict__ dpanel,
+                    const int32_t* __restrict__ cursor, const uint32_t* __restrict__ ime_b,
+                    const int32_t* __restrict__ n_piv_b, const int32_t* __restrict__ arows_b,
+                    const int32_t* __restrict__ drows_b, uint32_t p) {
+    __shared__ uint32_t Es[PA_SMALL_ROWS * 32];
+    __shared__ int32_t s_rows[PA_SMALL_ROWS], s_drow[PA_SMALL_ROWS];
+    const int d = blockIdx.y;
+    const int n = min(cursor[d], KB), np = n_piv_b[d];
+    const int pj = dpanel[d] * KB;
+    const int ntiles = (ncr - j0 + PA_COLS - 1) / PA_COLS;
+    int tile0 = blockIdx.x * tiles_per_block;
+    const int tile1 = min(ntiles, tile0 + tiles_per_block);
+    tile0 = max(tile0, pj > j0 ? (pj - j0) / PA_COLS : 0);
+    if (np == 0 || tile0 >= tile1 || n > PA_SMALL_ROWS) return;  // uniform
+    for (int t = threadIdx.x; t < PA_SMALL_ROWS; t += PA_THREADS) {
+        s_rows[t] = t < n ? chunk_rows[(size_t)d * KB + t] : 0;
+        s_drow[t] = t < np ? drows_b[(size_t)d * KB + t] : 0;
+    }
+    // E rows of the pivots, 32 entries each (zero past n):
+    // E[k][j] = [j = pos_k] - (I - E)[pos_k][j] mod p
+    const uint32_t* ime = ime_b + (size_t)d * KB * KB;
+    for (int t = threadIdx.x; t < np * 32; t += PA_THREADS) {
+        const int k = t / 32, j = t % 32;
+        uint32_t e = 0u;
+        if (j < n) {
+            const int pos = arows_b[(size_t)d * KB + k];
+            const uint32_t a = ime[(size_t)pos * KB + j];
+            e = (j == pos) ? (a == 0u ? 1u : (1u + p - a) % p) : (a ? p - a : 0u);
+        }
+        Es[t] = e;
+    }
+    __syncthreads();
+    const uint64_t m = ~0ull / p;
+    const int c_lo = j0 + tile0 * PA_COLS, c_hi = min(ncr, j0 + tile1 * PA_COLS);
+    if (n <= 8)
+        pa_small<WIDE, 8>(Dp, ld, ncr, c_lo, c_hi, n, np, Es, s_rows, s_drow, p, m);
+    else if (n <= 16)
+        pa_small<WIDE, 16>(Dp, ld, ncr, c_lo, c_hi, n, np, Es, s_rows, s_drow, p, m);
+    else
+        pa_small<WIDE, 32>(Dp, ld, ncr, c_lo, c_hi, n, np, Es, s_rows, s_drow, p, m);
 }
 
 // dst block b (NB x NB, leading dimension NB, block stride NB (NB + 1)) =
@@ -963,15 +1182,6 @@ __global__ void k_offs_write(int32_t n, const int64_t* __restrict__ loc, int64_t
         offs[k] = base + loc[k];
 }
 
-// values narrowed to vb (1 or 2) bytes
-__global__ void k_narrow_vals(int64_t n, const int32_t* __restrict__ in, int32_t vb, uint8_t* out) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (vb == 1) out[i] = (uint8_t)in[i];
-        else ((uint16_t*)out)[i] = (uint16_t)in[i];
-    }
-}
-
 // Rows t_rows[0 .. rows) of M (leading dimension ld, ncols columns) are
 // reduced by the pivot rows u_rows[0 .. n_p) of M (sorted by lead, monic,
 // zero left of their leads, pivot columns pc ascending):
@@ -1056,20 +1266,29 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         uint32_t* X = c.alloc<uint32_t>((size_t)t * NB);
         int32_t* act = c.alloc<int32_t>(nbk);
         int32_t* span = c.alloc<int32_t>(nbk);
-        if (!P || !Ninv || !X || !act || !span) return GBGPU_ENOMEM;
-        // pivot row of lead c into row c of P, from its diagonal block on (the
-        // only part any later step reads)
+        const int32_t ngrp = (ncl + 127) / 128;
+        int2* brange = c.alloc<int2>(ngrp);
+        if (!P || !Ninv || !X || !act || !span || !brange) return GBGPU_ENOMEM;
+        // active rows of each block (rows sorted by lead), the last left
+        // column the known pivots of each block touch, and the right columns
+        // every 128 known pivots reach
+        BL_LAUNCH(k_count_below<<<grid_of(nbk), 256, 0, s>>>(t, lead_sorted, nbk, NB, act));
+        BL_LAUNCH(k_fill_i32<<<grid_of(nbk), 256, 0, s>>>(span, nbk, -1));
+        BL_LAUNCH(k_clear_ranges<<<grid_of(ngrp), 256, 0, s>>>(ngrp, brange));
+        BL_LAUNCH(k_block_span<<<grid_of((int64_t)ncl * 32), 256, 0, s>>>(
+            ncl, in.piv_row, in.row_ptr, in.cols, ncl, NB, span, brange));
+        // pivot row of lead c into row c of P: on the tensor cores only the
+        // parts a later step reads (its diagonal block, the left columns its
+        // block reaches, the right columns its group of 128 reaches); the
+        // CUDA-core GEMM reads B whole, so there P gets everything from the
+        // diagonal block on
+        const bool banded = c.form != GBGPU_FORM_PLAIN;
         BL_LAUNCH(k_densify_seg<<<std::min(ncl, 148 * 3), 512, DS_COLS * 4, s>>>(
-            ncl, in.piv_row, in.row_ptr, in.cols, in.vals, nc, NB, P, ld));
+            ncl, in.piv_row, in.row_ptr, in.cols, in.vals, nc, NB, P, ld, banded ? ncl : 0, span,
+            brange));
         // -A_kk^-1 of every NB x NB diagonal block of A (read in place from P)
         BL_CHECK(neg_inverse_big(c, f, P, ld, (int64_t)NB * ld + NB, nbk, ncl - (nbk - 1) * NB, NB,
                                  Ninv));
-        // active rows of each block (rows sorted by lead) and the last left
-        // column the known pivots of each block touch
-        BL_LAUNCH(k_count_below<<<grid_of(nbk), 256, 0, s>>>(t, lead_sorted, nbk, NB, act));
-        BL_LAUNCH(k_fill_i32<<<grid_of(nbk), 256, 0, s>>>(span, nbk, -1));
-        BL_LAUNCH(k_block_span<<<grid_of((int64_t)ncl * 32), 256, 0, s>>>(
-            ncl, in.piv_row, in.row_ptr, in.cols, ncl, NB, span));
         std::vector<int32_t> h_act(nbk), h_span(nbk);
         BL_CUDA(cudaMemcpyAsync(h_act.data(), act, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
         BL_CUDA(cudaMemcpyAsync(h_span.data(), span, sizeof(int32_t) * nbk, cudaMemcpyDeviceToHost, s));
@@ -1092,7 +1311,11 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         }
         // (b) D' = D - X B: one GEMM over the whole left block; the tile flags of
         //     the GEMM skip the zero tiles of the staircase X and of B
-        BL_CHECK(gemm(c, W + ncl, ld, W, ld, P + ncl, ld, t, ncr, ncl));
+        {
+            TcGemmArgs g{c.p, t, ncr, ncl, W, ld, P + ncl, ld, W + ncl, ld};
+            if (banded) g.b_nrange = brange;  // B is zero outside these columns
+            BL_CHECK(gemm_args(c, g));
+        }
     }
     if (out->ms_event_schur) BL_CUDA(cudaEventRecord(out->ms_event_schur, s));
     BL_CHECK(echelon_rref(c, f, W + ncl, ld, t, ncr, out));
@@ -1255,16 +1478,31 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             {
                 // pivot rows of every chunk <- E_d old (CUDA cores, in place)
                 const bool wide = c.p >= 65536u;
+                // tiles per block: enough blocks for about six per SM, at most 8
+                // tiles each (a block stages the (I - E) rows once for its tiles)
                 const int tiles = (width + PA_COLS - 1) / PA_COLS;
-                const dim3 grid((unsigned)((tiles + PA_TILES - 1) / PA_TILES), (unsigned)n_dirty);
-                if (wide)
-                    BL_LAUNCH(k_panel_apply<true><<<grid, PA_THREADS, 0, s>>>(
-                        Dp, ld, ncr, j0, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
+                const int tpb = (int)std::max<int64_t>(
+                    1, std::min<int64_t>(8, (int64_t)tiles * n_dirty / (148 * 6)));
+                const dim3 grid((unsigned)((tiles + tpb - 1) / tpb), (unsigned)n_dirty);
+                // the chunks of more than 32 rows are few and long: one tile per block
+                const dim3 grid1((unsigned)tiles, (unsigned)n_dirty);
+                if (wide) {
+                    BL_CUDA(ensure_smem_limit((const void*)k_panel_apply<true>, PA_SMEM));
+                    BL_LAUNCH(k_panel_apply_small<true><<<grid, PA_THREADS, 0, s>>>(
+                        Dp, ld, ncr, j0, tpb, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
                         piv_rows, c.p));
-                else
-                    BL_LAUNCH(k_panel_apply<false><<<grid, PA_THREADS, 0, s>>>(
-                        Dp, ld, ncr, j0, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
+                    BL_LAUNCH(k_panel_apply<true><<<grid1, PA_THREADS, PA_SMEM, s>>>(
+                        Dp, ld, ncr, j0, 1, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
                         piv_rows, c.p));
+                } else {
+                    BL_CUDA(ensure_smem_limit((const void*)k_panel_apply<false>, PA_SMEM));
+                    BL_LAUNCH(k_panel_apply_small<false><<<grid, PA_THREADS, 0, s>>>(
+                        Dp, ld, ncr, j0, tpb, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
+                        piv_rows, c.p));
+                    BL_LAUNCH(k_panel_apply<false><<<grid1, PA_THREADS, PA_SMEM, s>>>(
+                        Dp, ld, ncr, j0, 1, chunk_rows, dpanel, cursor, imeB, n_piv, piv_arows,
+                        piv_rows, c.p));
+                }
             }
             BL_LAUNCH(k_register_chunks<<<n_dirty, KB, 0, s>>>(n_piv, piv_pos, piv_colb, chunk_rows,
                                                                 piv_of_col, is_piv, wflag));
@@ -1369,35 +1607,30 @@ static int echelon_rref(Ctx& c, const F& f, uint32_t* Dp, int64_t ld, int32_t t,
             BL_LAUNCH(k_offs_write<<<grid_of(kb + 1), 256, 0, s>>>(kb + 1, loc, so->nnz,
                                                                    so->offs + out0));
             if (blk > 0) {
-                int32_t *bc = nullptr, *bv = nullptr;
+                int32_t* bc = nullptr;
                 uint8_t* bw = nullptr;
                 const int vb = so->val_bytes;
                 if (cudaMallocAsync((void**)&bc, sizeof(int32_t) * blk, s) != cudaSuccess ||
-                    cudaMallocAsync((void**)&bv, sizeof(int32_t) * blk, s) != cudaSuccess ||
-                    (vb < 4 && cudaMallocAsync((void**)&bw, (size_t)vb * blk, s) != cudaSuccess)) {
+                    cudaMallocAsync((void**)&bw, (size_t)vb * blk, s) != cudaSuccess) {
                     set_error("answer block allocation failed");
                     return GBGPU_ENOMEM;
                 }
                 BL_LAUNCH(k_row_write<<<grid_of((int64_t)kb * 32), 256, 0, s>>>(
-                    kb, pcd + out0, piv_of_col, Dp, ld, ncr, loc, so->col_shift, bc, bv));
-                if (vb < 4)
-                    BL_LAUNCH(k_narrow_vals<<<grid_of(blk), 256, 0, s>>>(blk, bv, vb, bw));
+                    kb, pcd + out0, piv_of_col, Dp, ld, ncr, loc, so->col_shift, bc, bw, vb));
                 cudaStream_t fs = s;
                 if (!so->overflow && so->nnz + blk <= so->cap_nnz) {
                     BL_CUDA(cudaEventRecord(blk_ev, s));
                     BL_CUDA(cudaStreamWaitEvent(so->s_out, blk_ev, 0));
                     BL_CUDA(cudaMemcpyAsync(so->h_cols + so->nnz, bc, sizeof(int32_t) * blk,
                                             cudaMemcpyDeviceToHost, so->s_out));
-                    BL_CUDA(cudaMemcpyAsync((uint8_t*)so->h_vals + (size_t)so->nnz * vb,
-                                            vb < 4 ? (void*)bw : (void*)bv, (size_t)vb * blk,
-                                            cudaMemcpyDeviceToHost, so->s_out));
+                    BL_CUDA(cudaMemcpyAsync((uint8_t*)so->h_vals + (size_t)so->nnz * vb, bw,
+                                            (size_t)vb * blk, cudaMemcpyDeviceToHost, so->s_out));
                     fs = so->s_out;  // freed once copied
                 } else {
                     so->overflow = true;
                 }
                 cudaFreeAsync(bc, fs);
-                cudaFreeAsync(bv, fs);
-                if (bw) cudaFreeAsync(bw, fs);
+                cudaFreeAsync(bw, fs);
             }
             so->nnz += blk;
             return GBGPU_OK;

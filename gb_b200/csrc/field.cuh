@@ -46,6 +46,17 @@ struct FieldSmall {
     __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) const { return mul(a, b); }
     // x * a mod p with ap = prep(a)
     __device__ __forceinline__ uint32_t mulp(uint32_t x, uint32_t ap) const { return mul(ap, x); }
+    // a x - m v mod p with one final reduction, ap = prep(a), mn = prep(p - m)
+    // (a, p - m in [1, p), x, v in [0, p)): a x reduced to [0, 2p) by one
+    // Barrett step, plus (p - m) v, stays below 2p - 1 + (p - 1)^2 = p^2 < 2^32
+    __device__ __forceinline__ uint32_t ffsub(uint32_t x, uint32_t ap, uint32_t v,
+                                              uint32_t mn) const {
+        const uint32_t t = ap * x;
+        const uint32_t s = t - __umulhi(t, mu) * p + mn * v;
+        const uint32_t q = __umulhi(s, mu);
+        const uint32_t r = s - q * p;
+        return r >= p ? r - p : r;
+    }
     // a^-1 = a^(p-2) mod p (0 < a < p), square and multiply
     __device__ __forceinline__ uint32_t inv(uint32_t a) const {
         uint32_t r = 1u, b = a;
@@ -92,6 +103,15 @@ struct FieldMont {
     // x * a mod p with ap = prep(a)
     __device__ __forceinline__ uint32_t mulp(uint32_t x, uint32_t ap) const {
         return redc((uint64_t)ap * x);
+    }
+    // a x - m v mod p with one reduction, ap = prep(a), mn = prep(p - m):
+    // T = ap x + mn v < 2 p^2 and REDC(T) = (T + q p) / 2^32 < 2p (p < 2^31)
+    __device__ __forceinline__ uint32_t ffsub(uint32_t x, uint32_t ap, uint32_t v,
+                                              uint32_t mn) const {
+        const uint64_t T = (uint64_t)ap * x + (uint64_t)mn * v;
+        const uint32_t q = (uint32_t)T * pneg_inv;
+        const uint32_t r = (uint32_t)((T + (uint64_t)q * p) >> 32);
+        return r >= p ? r - p : r;
     }
     // a^-1 = a^(p-2) mod p (0 < a < p), square and multiply in Montgomery form
     __device__ __forceinline__ uint32_t inv(uint32_t a) const {

@@ -104,6 +104,6 @@ __global__ void k_row_nnz(int32_t np, const int32_t* pivcol, const int32_t* piv_
                           const uint32_t* rows, int64_t ld, int32_t ncr, int64_t* counts);
 __global__ void k_row_write(int32_t np, const int32_t* pivcol, const int32_t* piv_of_col,
                             const uint32_t* rows, int64_t ld, int32_t ncr, const int64_t* offs,
-                            int32_t col_shift, int32_t* out_cols, int32_t* out_vals);
+                            int32_t col_shift, int32_t* out_cols, void* out_vals, int32_t vb);
 
 }  // namespace gbgpu

@@ -558,6 +558,12 @@ __global__ void k_pivot_list(int32_t ncr, const int32_t* __restrict__ flag,
         if (flag[i]) pivcol[pos[i]] = desc ? ncr - 1 - i : i;
 }
 
+// Both compaction kernels walk a row with one warp, ROW_U chunks of 32
+// columns per pass: the ROW_U loads of a lane are independent and in flight
+// together (a pass covers 256 columns), so a row costs a few load latencies
+// instead of one per 32 columns.
+constexpr int ROW_U = 8;
+
 // nnz of each reduced pivot row (one warp per row)
 __global__ void k_row_nnz(int32_t np, const int32_t* __restrict__ pivcol,
                           const int32_t* __restrict__ piv_of_col, const uint32_t* __restrict__ rows,
@@ -568,20 +574,30 @@ __global__ void k_row_nnz(int32_t np, const int32_t* __restrict__ pivcol,
     for (int i = warp; i < np; i += nwarps) {
         const int32_t c0 = pivcol[i];
         const uint32_t* row = rows + (size_t)piv_of_col[c0] * ld;
-        int64_t cnt = 0;
-        for (int j = c0 + lane; j < ncr; j += 32) cnt += row[j] != 0u;
+        int cnt = 0;
+        for (int base = c0; base < ncr; base += 32 * ROW_U) {
+            uint32_t v[ROW_U];
+#pragma unroll
+            for (int u = 0; u < ROW_U; ++u) {
+                const int j = base + 32 * u + lane;
+                v[u] = j < ncr ? row[j] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < ROW_U; ++u) cnt += v[u] != 0u;
+        }
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         if (lane == 0) counts[i] = cnt;
     }
 }
 
-// write CSR rows: columns shifted by col_shift, order preserved by a warp
+// write CSR rows: columns shifted by col_shift, values at vb bytes (1, 2 or
+// 4: the reference's cf_8 / cf_16 / cf_32 widths), order preserved by a warp
 // ballot prefix over each 32-column chunk
 __global__ void k_row_write(int32_t np, const int32_t* __restrict__ pivcol,
                             const int32_t* __restrict__ piv_of_col,
                             const uint32_t* __restrict__ rows, int64_t ld, int32_t ncr,
                             const int64_t* __restrict__ offs, int32_t col_shift,
-                            int32_t* out_cols, int32_t* out_vals) {
+                            int32_t* out_cols, void* out_vals, int32_t vb) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -589,16 +605,25 @@ __global__ void k_row_write(int32_t np, const int32_t* __restrict__ pivcol,
         const int32_t c0 = pivcol[i];
         const uint32_t* row = rows + (size_t)piv_of_col[c0] * ld;
         int64_t o = offs[i];
-        for (int base = c0; base < ncr; base += 32) {
-            const int j = base + lane;
-            const uint32_t v = j < ncr ? row[j] : 0u;
-            const unsigned bal = __ballot_sync(0xffffffffu, v != 0u);
-            if (v != 0u) {
-                const int64_t at = o + __popc(bal & ((1u << lane) - 1u));
-                out_cols[at] = j + col_shift;
-                out_vals[at] = (int32_t)v;
+        for (int base = c0; base < ncr; base += 32 * ROW_U) {
+            uint32_t v[ROW_U];
+#pragma unroll
+            for (int u = 0; u < ROW_U; ++u) {
+                const int j = base + 32 * u + lane;
+                v[u] = j < ncr ? __ldcs(row + j) : 0u;
             }
-            o += __popc(bal);
+#pragma unroll
+            for (int u = 0; u < ROW_U; ++u) {
+                const unsigned bal = __ballot_sync(0xffffffffu, v[u] != 0u);
+                if (v[u] != 0u) {
+                    const int64_t at = o + __popc(bal & ((1u << lane) - 1u));
+                    out_cols[at] = base + 32 * u + lane + col_shift;
+                    if (vb == 4) ((uint32_t*)out_vals)[at] = v[u];
+                    else if (vb == 2) ((uint16_t*)out_vals)[at] = (uint16_t)v[u];
+                    else ((uint8_t*)out_vals)[at] = (uint8_t)v[u];
+                }
+                o += __popc(bal);
+            }
         }
     }
 }

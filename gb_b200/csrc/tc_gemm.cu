@@ -628,12 +628,16 @@ k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
 // per pair of warps; the bytes go to shared memory as [l][n][k] (rows padded
 // to 132 bytes: conflict-free in both phases) and leave as whole 128-byte
 // k-rows of every n, four threads per row.
+// With nrange (see TcGemmArgs::b_nrange) a tile outside its rows' column
+// range is not read: it is written as zeros when another part of its
+// bn-wide flag tile is live, and not at all otherwise (its flag stays 0, so
+// the GEMM never loads it).
 constexpr int SPLIT_ROW = 132;
 __global__ void __launch_bounds__(256)
 k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
              const int32_t* __restrict__ b_rows, int64_t sBr, int32_t K, int32_t N, int32_t Np,
              int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t bn,
-             int32_t fstride) {
+             int32_t fstride, const int2* __restrict__ nrange) {
     extern __shared__ uint8_t split_smem[];  // [L][64][SPLIT_ROW] bytes
     __shared__ const uint32_t* rowp[128];
     // batch item blockIdx.z
@@ -642,6 +646,21 @@ k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
     out += (size_t)blockIdx.z * L * Np * Kp;
     if (flags) flags += (size_t)blockIdx.z * (Np / bn) * fstride;
     const int k0 = blockIdx.y * 128, n0 = blockIdx.x * 64;
+    if (nrange) {  // uniform over the block
+        const int2 rg = k0 < K ? nrange[blockIdx.y] : make_int2(1, 0);
+        const int t0 = (n0 / bn) * bn;
+        if (rg.y < rg.x || t0 + bn <= rg.x || t0 > rg.y) return;
+        if (n0 + 64 <= rg.x || n0 > rg.y) {
+            // zeros: 64 k-rows of 128 bytes per limb, four threads per row
+            const int nn = threadIdx.x >> 2, part = threadIdx.x & 3;
+            for (int l = 0; l < L; ++l) {
+                uint4* dst = (uint4*)(out + ((size_t)l * Np + n0 + nn) * Kp + k0 + 32 * part);
+                dst[0] = make_uint4(0u, 0u, 0u, 0u);
+                dst[1] = make_uint4(0u, 0u, 0u, 0u);
+            }
+            return;
+        }
+    }
     if (threadIdx.x < 128) {
         const int k = k0 + threadIdx.x;
         int64_t src = -1;
@@ -874,7 +893,9 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
                                                     Mp, Kp, L, Ap, fa, nkbp, vec);
         dim3 gb(Np / 64, Kp / 128, nb);
         k_split_cols<<<gb, 256, L * 64 * SPLIT_ROW, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K,
-                                                          g.N, Np, Kp, L, Bp, fb, Cfg::BN, nkbp);
+                                                          g.N, Np, Kp, L, Bp, fb, Cfg::BN, nkbp,
+                                                          nb == 1 && !g.b_rows ? g.b_nrange
+                                                                               : nullptr);
         *launches += 2;
     }
     CUtensorMap ma, mb;

@@ -30,6 +30,12 @@ struct TcGemmArgs {
     const int32_t* b_rows = nullptr;
     const int32_t* d_rows = nullptr;
     int64_t sAr = 0, sBr = 0, sDr = 0;
+    // optional (unbatched, no b_rows): for every group of 128 rows of B
+    // (rows [128 g, 128 g + 128)) the first and last column that may be
+    // nonzero (.x > .y: the group is zero).  B is zero outside, and its
+    // memory there is never read; between the two columns widened to
+    // 64-column boundaries every entry must be valid.
+    const int2* b_nrange = nullptr;
 };
 
 // Optional per-thread profiling of the tensor-core GEMM launches: CUDA events
