@@ -244,7 +244,7 @@ __device__ __forceinline__ uint32_t mod64(uint64_t x, uint32_t p, uint64_t m) {
     return (uint32_t)r;
 }
 
-constexpr int INV_THREADS = 512;  // threads of k_neg_inverse
+constexpr int INV_THREADS = 1024;  // threads of k_neg_inverse
 
 // sum of u_k v_k mod p for u_k, v_k < p < 2^31, from 16-bit halves of v
 // accumulated without reduction (each product < 2^47, at most 128 terms)
@@ -349,17 +349,39 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
     }
 }
 
+// The row copies below give every piece of GB_PIECE columns of a row to one
+// warp (32-bit index arithmetic, four independent loads per lane in flight);
+// the loop body sees the row i and its columns [jb, je).
+constexpr int GB_PIECE = 512;
+#define GB_WARP_ROWS(rows, ncols)                                                    \
+    const int lane = threadIdx.x & 31;                                               \
+    const int warp_ = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;                  \
+    const int nwarps_ = (gridDim.x * blockDim.x) >> 5;                               \
+    const int npc_ = ((ncols) + GB_PIECE - 1) / GB_PIECE;                            \
+    for (int it_ = warp_, i = it_ / max(npc_, 1), jb = (it_ % max(npc_, 1)) * GB_PIECE, \
+             je = min((int)(ncols), jb + GB_PIECE);                                  \
+         it_ < (rows) * npc_;                                                        \
+         it_ += nwarps_, i = it_ / max(npc_, 1), jb = (it_ % max(npc_, 1)) * GB_PIECE, \
+             je = min((int)(ncols), jb + GB_PIECE))
+
 // dst[i][j] = src[r_i][cols[j]], r_i = rlist[i] (i without a list)
 __global__ void k_gather_cols(int32_t rows, int32_t n, const uint32_t* __restrict__ src,
                               int64_t lds, const int32_t* __restrict__ cols, uint32_t* dst,
                               int64_t ldd, const int32_t* __restrict__ rlist = nullptr) {
-    const int64_t total = (int64_t)rows * n;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = t / n;
-        const int j = (int)(t % n);
-        const int64_t r = rlist ? (int64_t)rlist[i] : i;
-        dst[i * ldd + j] = src[r * lds + cols[j]];
+    GB_WARP_ROWS(rows, n) {
+        const uint32_t* s = src + (size_t)(rlist ? rlist[i] : i) * lds;
+        uint32_t* o = dst + (size_t)i * ldd;
+        for (int j0 = jb + lane; j0 < je; j0 += 128) {
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int jj = j0 + 32 * u;
+                v[u] = jj < je ? s[cols[jj]] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j0 + 32 * u < je) o[j0 + 32 * u] = v[u];
+        }
     }
 }
 
@@ -367,13 +389,21 @@ __global__ void k_gather_cols(int32_t rows, int32_t n, const uint32_t* __restric
 __global__ void k_gather_rows_dense(int32_t nrows, const int32_t* __restrict__ rows, int32_t n,
                                     const uint32_t* __restrict__ src, int64_t lds, uint32_t* dst,
                                     int64_t ldd) {
-    const int64_t total = (int64_t)nrows * n;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = t / n;
-        const int j = (int)(t % n);
+    GB_WARP_ROWS(nrows, n) {
         const int32_t r = rows[i];
-        dst[i * ldd + j] = r >= 0 ? src[(int64_t)r * lds + j] : 0u;
+        const uint32_t* s = r >= 0 ? src + (size_t)r * lds : nullptr;
+        uint32_t* o = dst + (size_t)i * ldd;
+        for (int j0 = jb + lane; j0 < je; j0 += 128) {
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int jj = j0 + 32 * u;
+                v[u] = (s && jj < je) ? s[jj] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j0 + 32 * u < je) o[j0 + 32 * u] = v[u];
+        }
     }
 }
 
@@ -381,12 +411,20 @@ __global__ void k_gather_rows_dense(int32_t nrows, const int32_t* __restrict__ r
 __global__ void k_scatter_rows_dense(int32_t nrows, const int32_t* __restrict__ rows, int32_t n,
                                      const uint32_t* __restrict__ src, int64_t lds,
                                      uint32_t* dst, int64_t ldd) {
-    const int64_t total = (int64_t)nrows * n;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = t / n;
-        const int j = (int)(t % n);
-        dst[(int64_t)rows[i] * ldd + j] = src[i * lds + j];
+    GB_WARP_ROWS(nrows, n) {
+        const uint32_t* s = src + (size_t)i * lds;
+        uint32_t* o = dst + (size_t)rows[i] * ldd;
+        for (int j0 = jb + lane; j0 < je; j0 += 128) {
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int jj = j0 + 32 * u;
+                v[u] = jj < je ? s[jj] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j0 + 32 * u < je) o[j0 + 32 * u] = v[u];
+        }
     }
 }
 
@@ -1015,17 +1053,22 @@ k_panel_apply_small(uint32_t* Dp, int64_t ld, int32_t ncr, int32_t j0, int32_t t
 // identity-padded; nb_b = NB except for the last block
 __global__ void k_copy_blocks(const uint32_t* __restrict__ src, int64_t lds, int64_t stride_src,
                               int32_t n_blocks, int32_t last_nb, int32_t NB, uint32_t* dst) {
-    const int64_t per = (int64_t)NB * NB;
-    const int64_t total = per * n_blocks;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t b = (int32_t)(t / per);
-        const int32_t i = (int32_t)((t % per) / NB), j = (int32_t)(t % NB);
+    GB_WARP_ROWS(n_blocks * NB, NB) {
+        const int32_t b = i / NB, r = i % NB;
         const int32_t nb = b == n_blocks - 1 ? last_nb : NB;
-        uint32_t v;
-        if (i < nb && j < nb) v = src[(size_t)b * stride_src + (size_t)i * lds + j];
-        else v = i == j ? 1u : 0u;
-        dst[(size_t)b * NB * (NB + 1) + (size_t)i * NB + j] = v;
+        const uint32_t* s = src + (size_t)b * stride_src + (size_t)r * lds;
+        uint32_t* o = dst + (size_t)b * NB * (NB + 1) + (size_t)r * NB;
+        for (int j0 = jb + lane; j0 < je; j0 += 128) {
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int jj = j0 + 32 * u;
+                v[u] = (r < nb && jj < nb) ? s[jj] : (r == jj ? 1u : 0u);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j0 + 32 * u < je) o[j0 + 32 * u] = v[u];
+        }
     }
 }
 
