@@ -254,10 +254,13 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     const int nkbp = prm.nkbp;
     auto flag_ptrs = [&](int z, int mt, int nt, const uint8_t*& fa, const uint8_t*& fb) {
         fa = prm.fa ? prm.fa + ((size_t)z * tiles_m + mt) * nkbp : nullptr;
-        fb = prm.fb ? prm.fb + ((size_t)z * tiles_n + nt) * nkbp : nullptr;
+        // B flags are kept per 64 rows of B's planes: the tile's BN / 64 rows
+        fb = prm.fb ? prm.fb + ((size_t)z * (prm.Np / 64) + (size_t)nt * (C::BN / 64)) * nkbp
+                    : nullptr;
     };
     // live K steps [64 ch, 64 ch + 64) of a tile as a bit mask, from 16-byte
-    // loads of both flag rows (flags are 0 or 1 bytes)
+    // loads of the A flag row and of the OR of the tile's B flag rows (flags
+    // are 0 or 1 bytes)
     auto live_mask = [&](const uint8_t* fa, const uint8_t* fb, int ch) -> uint64_t {
         uint64_t msk = 0;
 #pragma unroll
@@ -267,7 +270,17 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             uint4 a = make_uint4(0x01010101u, 0x01010101u, 0x01010101u, 0x01010101u);
             uint4 b = a;
             if (fa) a = *(const uint4*)(fa + kb0);
-            if (fb) b = *(const uint4*)(fb + kb0);
+            if (fb) {
+                b = *(const uint4*)(fb + kb0);
+#pragma unroll
+                for (int r = 1; r < C::BN / 64; ++r) {
+                    const uint4 o = *(const uint4*)(fb + (size_t)r * nkbp + kb0);
+                    b.x |= o.x;
+                    b.y |= o.y;
+                    b.z |= o.z;
+                    b.w |= o.w;
+                }
+            }
             const uint32_t w[4] = {a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w};
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -567,94 +580,122 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 }
 
 // ---------------------------------------------------------------------------
-// limb planes: out[l][r][k] = byte l of src (rows x cols), zero padded; row m
-// of A is A + a_rows[m] lda when a_rows is given (negative: a zero row).
-// Every thread splits 16 consecutive k of one row (one 16-byte store per limb);
-// with `vec` (A and its row and batch strides 16-byte aligned) a full group is
-// read as four 16-byte loads.
-__global__ void __launch_bounds__(256)
-k_split_rows(const uint32_t* __restrict__ A, int64_t lda, int64_t sA,
-             const int32_t* __restrict__ a_rows, int64_t sAr, int32_t M, int32_t K, int32_t Mp,
-             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t fstride,
-             int32_t vec) {
-    // batch item blockIdx.y
-    A += (size_t)blockIdx.y * sA;
-    if (a_rows) a_rows += (size_t)blockIdx.y * sAr;
-    out += (size_t)blockIdx.y * L * Mp * Kp;
-    if (flags) flags += (size_t)blockIdx.y * (Mp / 128) * fstride;
-    const int32_t kq = Kp / 16;  // 16-column groups per row
-    const int64_t total = (int64_t)Mp * kq;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t m = (int32_t)(t / kq);
-        const int32_t k = (int32_t)(t % kq) * 16;
-        int64_t src = -1;
-        if (m < M) src = a_rows ? (int64_t)a_rows[m] : (int64_t)m;
-        const uint32_t* row = src >= 0 ? A + (size_t)src * lda : nullptr;
-        uint32_t v[16];
-        uint32_t any = 0;
-        if (vec && row && k + 16 <= K) {
-            const uint4* r4 = (const uint4*)(row + k);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint4 w = r4[q];
-                v[4 * q] = w.x;
-                v[4 * q + 1] = w.y;
-                v[4 * q + 2] = w.z;
-                v[4 * q + 3] = w.w;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = (row && k + i < K) ? row[k + i] : 0u;
-        }
-#pragma unroll
-        for (int i = 0; i < 16; ++i) any |= v[i];
-        if (flags && any) flags[(size_t)(m / 128) * fstride + k / 128] = 1;
-        for (int l = 0; l < L; ++l) {
-            uint32_t w[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                w[j] = ((v[4 * j] >> (8 * l)) & 255u) | (((v[4 * j + 1] >> (8 * l)) & 255u) << 8) |
-                       (((v[4 * j + 2] >> (8 * l)) & 255u) << 16) |
-                       (((v[4 * j + 3] >> (8 * l)) & 255u) << 24);
-            *(uint4*)(out + ((size_t)l * Mp + m) * Kp + k) = make_uint4(w[0], w[1], w[2], w[3]);
-        }
-    }
-}
-
-// transposing split: out[l][n][k] = byte l of B[k][n]; row k of B is
-// B + b_rows[k] ldb when b_rows is given (negative: a zero row).
-// One 128 (k) x 64 (n) tile per 256 threads.  Rows of B are read 256 bytes
-// per pair of warps; the bytes go to shared memory as [l][n][k] (rows padded
-// to 132 bytes: conflict-free in both phases) and leave as whole 128-byte
-// k-rows of every n, four threads per row.
-// With nrange (see TcGemmArgs::b_nrange) a tile outside its rows' column
-// range is not read: it is written as zeros when another part of its
-// bn-wide flag tile is live, and not at all otherwise (its flag stays 0, so
-// the GEMM never loads it).
+// Limb planes of both operands and their tile flags, one launch per GEMM.
+//
+// A part (blocks [0, a_blocks)): one 128-row x 128-column tile of A per
+// block; out[l][m][k] = byte l of A[m][k], zero padded; row m of A is
+// A + a_rows[m] lda when a_rows is given (negative: a zero row).  Every item
+// is 16 consecutive k of one row (one 16-byte store per limb); with `vec` (A
+// and its row and batch strides 16-byte aligned) a full item is read as four
+// 16-byte loads.  The block writes its tile flag fa[mt][kb] (0 or 1).
+//
+// B part (the other blocks): transposing split, out[l][n][k] = byte l of
+// B[k][n]; row k of B is B + b_rows[k] ldb when b_rows is given (negative: a
+// zero row).  One 128 (k) x 64 (n) tile per block: rows of B are read 256
+// bytes per pair of warps; the bytes go to shared memory as [l][n][k] (rows
+// padded to 132 bytes: conflict-free in both phases) and leave as whole
+// 128-byte k-rows of every n, four threads per row.  The block writes its flag
+// fb[n / 64][kb]; the GEMM ORs the flags of the 64-row groups of its tile.
+// With nrange (see TcGemmArgs::b_nrange) a tile outside its rows' column range
+// is not read: it is written as zeros when another part of its bn-wide GEMM
+// tile is live, and not at all otherwise (the GEMM never loads it).
+//
+// Every flag of the GEMM is written here, so nothing clears them first.
 constexpr int SPLIT_ROW = 132;
-__global__ void __launch_bounds__(256)
-k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
-             const int32_t* __restrict__ b_rows, int64_t sBr, int32_t K, int32_t N, int32_t Np,
-             int32_t Kp, int32_t L, uint8_t* __restrict__ out, uint8_t* flags, int32_t bn,
-             int32_t fstride, const int2* __restrict__ nrange) {
-    extern __shared__ uint8_t split_smem[];  // [L][64][SPLIT_ROW] bytes
+struct SplitArgs {
+    const uint32_t* A;
+    int64_t lda, sA;
+    const int32_t* a_rows;
+    int64_t sAr;
+    int32_t M, K, Mp, Kp, L;
+    uint8_t* Ap;
+    uint8_t* fa;
+    int32_t nkbp, vec;
+    const uint32_t* B;
+    int64_t ldb, sB;
+    const int32_t* b_rows;
+    int64_t sBr;
+    int32_t N, Np, bn;
+    uint8_t* Bp;
+    uint8_t* fb;
+    const int2* nrange;
+    int32_t a_blocks;  // (Mp / 128) (Kp / 128)
+};
+
+__global__ void __launch_bounds__(256) k_split_ab(const SplitArgs a) {
+    extern __shared__ uint8_t split_smem[];  // [L][64][SPLIT_ROW] bytes (B part)
     __shared__ const uint32_t* rowp[128];
-    // batch item blockIdx.z
-    B += (size_t)blockIdx.z * sB;
-    if (b_rows) b_rows += (size_t)blockIdx.z * sBr;
-    out += (size_t)blockIdx.z * L * Np * Kp;
-    if (flags) flags += (size_t)blockIdx.z * (Np / bn) * fstride;
-    const int k0 = blockIdx.y * 128, n0 = blockIdx.x * 64;
-    if (nrange) {  // uniform over the block
-        const int2 rg = k0 < K ? nrange[blockIdx.y] : make_int2(1, 0);
-        const int t0 = (n0 / bn) * bn;
-        if (rg.y < rg.x || t0 + bn <= rg.x || t0 > rg.y) return;
-        if (n0 + 64 <= rg.x || n0 > rg.y) {
+    const int z = blockIdx.z;  // batch item
+    const int nkb = a.Kp / 128;
+    const int L = a.L;
+    if ((int)blockIdx.x < a.a_blocks) {
+        // ---- A part ----
+        const int mt = blockIdx.x / nkb, kbi = blockIdx.x % nkb;
+        const uint32_t* A = a.A + (size_t)z * a.sA;
+        const int32_t* a_rows = a.a_rows ? a.a_rows + (size_t)z * a.sAr : nullptr;
+        uint8_t* out = a.Ap + (size_t)z * L * a.Mp * a.Kp;
+        uint32_t any = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int item = threadIdx.x + 256 * q;
+            const int m = mt * 128 + (item >> 3);
+            const int k = kbi * 128 + (item & 7) * 16;
+            int64_t src = -1;
+            if (m < a.M) src = a_rows ? (int64_t)a_rows[m] : (int64_t)m;
+            const uint32_t* row = src >= 0 ? A + (size_t)src * a.lda : nullptr;
+            uint32_t v[16];
+            if (a.vec && row && k + 16 <= a.K) {
+                const uint4* r4 = (const uint4*)(row + k);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint4 w = r4[u];
+                    v[4 * u] = w.x;
+                    v[4 * u + 1] = w.y;
+                    v[4 * u + 2] = w.z;
+                    v[4 * u + 3] = w.w;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 16; ++e) v[e] = (row && k + e < a.K) ? row[k + e] : 0u;
+            }
+#pragma unroll
+            for (int e = 0; e < 16; ++e) any |= v[e];
+            for (int l = 0; l < L; ++l) {
+                uint32_t w[4];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj)
+                    w[jj] = ((v[4 * jj] >> (8 * l)) & 255u) |
+                            (((v[4 * jj + 1] >> (8 * l)) & 255u) << 8) |
+                            (((v[4 * jj + 2] >> (8 * l)) & 255u) << 16) |
+                            (((v[4 * jj + 3] >> (8 * l)) & 255u) << 24);
+                *(uint4*)(out + ((size_t)l * a.Mp + m) * a.Kp + k) =
+                    make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+        any = __syncthreads_or(any != 0);
+        if (threadIdx.x == 0)
+            a.fa[((size_t)z * (a.Mp / 128) + mt) * a.nkbp + kbi] = any ? 1 : 0;
+        return;
+    }
+    // ---- B part ----
+    const int bq = blockIdx.x - a.a_blocks;
+    const int nx = bq % (a.Np / 64), kbi = bq / (a.Np / 64);
+    const int k0 = kbi * 128, n0 = nx * 64;
+    const uint32_t* B = a.B + (size_t)z * a.sB;
+    const int32_t* b_rows = a.b_rows ? a.b_rows + (size_t)z * a.sBr : nullptr;
+    uint8_t* out = a.Bp + (size_t)z * L * a.Np * a.Kp;
+    uint8_t* flag = a.fb + ((size_t)z * (a.Np / 64) + nx) * a.nkbp + kbi;
+    if (a.nrange) {  // uniform over the block
+        const int2 rg = k0 < a.K ? a.nrange[kbi] : make_int2(1, 0);
+        const int t0 = (n0 / a.bn) * a.bn;
+        const bool tile_live = !(rg.y < rg.x || t0 + a.bn <= rg.x || t0 > rg.y);
+        if (!tile_live || n0 + 64 <= rg.x || n0 > rg.y) {
+            if (threadIdx.x == 0) *flag = 0;
+            if (!tile_live) return;
             // zeros: 64 k-rows of 128 bytes per limb, four threads per row
             const int nn = threadIdx.x >> 2, part = threadIdx.x & 3;
             for (int l = 0; l < L; ++l) {
-                uint4* dst = (uint4*)(out + ((size_t)l * Np + n0 + nn) * Kp + k0 + 32 * part);
+                uint4* dst = (uint4*)(out + ((size_t)l * a.Np + n0 + nn) * a.Kp + k0 + 32 * part);
                 dst[0] = make_uint4(0u, 0u, 0u, 0u);
                 dst[1] = make_uint4(0u, 0u, 0u, 0u);
             }
@@ -664,8 +705,8 @@ k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
     if (threadIdx.x < 128) {
         const int k = k0 + threadIdx.x;
         int64_t src = -1;
-        if (k < K) src = b_rows ? (int64_t)b_rows[k] : (int64_t)k;
-        rowp[threadIdx.x] = src >= 0 ? B + (size_t)src * ldb : nullptr;
+        if (k < a.K) src = b_rows ? (int64_t)b_rows[k] : (int64_t)k;
+        rowp[threadIdx.x] = src >= 0 ? B + (size_t)src * a.ldb : nullptr;
     }
     __syncthreads();
     uint32_t any = 0;
@@ -677,7 +718,7 @@ k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
             const uint32_t* rp = rowp[r0 + 4 * i];
-            v[i] = (rp && n < N) ? rp[n] : 0u;
+            v[i] = (rp && n < a.N) ? rp[n] : 0u;
         }
         for (int l = 0; l < L; ++l) {
             uint8_t* dst = split_smem + ((size_t)l * 64 + c) * SPLIT_ROW + r0;
@@ -696,15 +737,12 @@ k_split_cols(const uint32_t* __restrict__ B, int64_t ldb, int64_t sB,
             (const uint32_t*)(split_smem + ((size_t)l * 64 + nn) * SPLIT_ROW + 32 * part);
         uint32_t w[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) w[j] = src[j];
-        uint4* dst = (uint4*)(out + ((size_t)l * Np + n) * Kp + k0 + 32 * part);
+        for (int jj = 0; jj < 8; ++jj) w[jj] = src[jj];
+        uint4* dst = (uint4*)(out + ((size_t)l * a.Np + n) * a.Kp + k0 + 32 * part);
         dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
         dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
     }
-    if (flags && any && threadIdx.x == 0) {
-        // the 64 columns lie inside one bn-wide tile (bn is a multiple of 64)
-        flags[(size_t)(n0 / bn) * fstride + k0 / 128] = 1;
-    }
+    if (threadIdx.x == 0) *flag = any ? 1 : 0;
 }
 
 // row index lists of the plain GEMM (see TcGemmArgs)
@@ -871,8 +909,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     const int32_t nkb = Kp / Cfg::BK;
     const int32_t nkbp = (nkb + 63) / 64 * 64;
     uint8_t* fa = Bp + (size_t)nb * L * Np * Kp;             // [nb][Mp/128][nkbp]
-    uint8_t* fb = fa + (size_t)nb * (Mp / Cfg::BM) * nkbp;   // [nb][Np/BN][nkbp]
-    const size_t flag_bytes = (size_t)nb * (Mp / Cfg::BM + Np / Cfg::BN) * nkbp;
+    uint8_t* fb = fa + (size_t)nb * (Mp / Cfg::BM) * nkbp;   // [nb][Np/64][nkbp]
     GemmProfile* prof = gemm_profile();
     if (prof) {
         cudaEvent_t es = nullptr;
@@ -880,23 +917,37 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
         cudaEventRecord(es, s);
         prof->split_events.push_back(es);
     }
-    if (cudaMemsetAsync(fa, 0, flag_bytes, s) != cudaSuccess) {
-        set_error("tile flag clear failed");
-        return GBGPU_ECUDA;
-    }
     {
-        const int64_t total = (int64_t)Mp * (Kp / 16);
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256,
-                                                                       148 * 32 / nb + 1));
-        const int32_t vec = ((uintptr_t)g.A % 16 == 0) && g.lda % 4 == 0 && g.sA % 4 == 0;
-        k_split_rows<<<dim3(grid, nb), 256, 0, s>>>(g.A, g.lda, g.sA, g.a_rows, g.sAr, g.M, g.K,
-                                                    Mp, Kp, L, Ap, fa, nkbp, vec);
-        dim3 gb(Np / 64, Kp / 128, nb);
-        k_split_cols<<<gb, 256, L * 64 * SPLIT_ROW, s>>>(g.B, g.ldb, g.sB, g.b_rows, g.sBr, g.K,
-                                                          g.N, Np, Kp, L, Bp, fb, Cfg::BN, nkbp,
-                                                          nb == 1 && !g.b_rows ? g.b_nrange
-                                                                               : nullptr);
-        *launches += 2;
+        SplitArgs sa{};
+        sa.A = g.A;
+        sa.lda = g.lda;
+        sa.sA = g.sA;
+        sa.a_rows = g.a_rows;
+        sa.sAr = g.sAr;
+        sa.M = g.M;
+        sa.K = g.K;
+        sa.Mp = Mp;
+        sa.Kp = Kp;
+        sa.L = L;
+        sa.Ap = Ap;
+        sa.fa = fa;
+        sa.nkbp = nkbp;
+        sa.vec = ((uintptr_t)g.A % 16 == 0) && g.lda % 4 == 0 && g.sA % 4 == 0;
+        sa.B = g.B;
+        sa.ldb = g.ldb;
+        sa.sB = g.sB;
+        sa.b_rows = g.b_rows;
+        sa.sBr = g.sBr;
+        sa.N = g.N;
+        sa.Np = Np;
+        sa.bn = Cfg::BN;
+        sa.Bp = Bp;
+        sa.fb = fb;
+        sa.nrange = nb == 1 && !g.b_rows ? g.b_nrange : nullptr;
+        sa.a_blocks = (Mp / 128) * (Kp / 128);
+        const int64_t blocks = (int64_t)sa.a_blocks + (int64_t)(Np / 64) * (Kp / 128);
+        k_split_ab<<<dim3((unsigned)blocks, 1, nb), 256, L * 64 * SPLIT_ROW, s>>>(sa);
+        *launches += 1;
     }
     CUtensorMap ma, mb;
     int rc = make_map(&ma, Ap, Kp, (int64_t)nb * L * Mp, Cfg::BK, Cfg::BM);
@@ -971,7 +1022,7 @@ size_t tc_workspace_bytes(uint32_t p, int32_t M, int32_t N, int32_t K, int32_t b
     const size_t Kp = (size_t)(K + 127) / 128 * 128;
     const size_t nkbp = (Kp / 128 + 63) / 64 * 64;
     const size_t nb = (size_t)(batch > 0 ? batch : 1);
-    const size_t flags = nb * (Mp / 128 + (size_t)(N + 63) / 64) * nkbp;
+    const size_t flags = nb * (Mp / 128 + Np / 64) * nkbp;
     return nb * L * (Mp + Np) * Kp + ((flags + 255) & ~(size_t)255);
 }
 
