@@ -71,7 +71,10 @@ EXPORTS = [
     "gbgpu_dense_submul_noalloc", "gbgpu_plan_result_into", "gbgpu_dense_rref",
     "gbgpu_plan_result_into_v", "gbgpu_plan_run_into_v", "gbgpu_autotune",
     "gbgpu_convert_hashes_to_columns_flat", "gbgpu_convert_hashes_to_columns",
-    "gbgpu_sort_matrix_rows",
+    "gbgpu_sort_matrix_rows", "gbgpu_linear_algebra_keep", "gbgpu_linear_algebra_keep_status",
+    "gbgpu_kept_answer", "gbgpu_convert_sparse_matrix_rows_to_basis_elements",
+    "gbgpu_convert_sparse_matrix_rows_to_basis_elements_status", "gbgpu_plan_first_entry",
+    "gbgpu_plan_map_columns",
 ]
 
 _lib = None
@@ -101,6 +104,8 @@ def load(path: str = LIB_PATH):
                                              C.c_int32, C.c_int64, C.c_int64, _PI32, _PI64]
     lib.gbgpu_plan_run_into_v.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_int32, C.c_int64, C.c_int64, _PI32, _PI64]
+    lib.gbgpu_plan_first_entry.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.gbgpu_plan_map_columns.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
     lib.gbgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.gbgpu_plan_destroy.restype = None
     lib.gbgpu_reduce_batch.argtypes = [C.c_int32, C.POINTER(Csr), C.POINTER(Options),

@@ -785,6 +785,86 @@ __global__ void k_narrow(const uint32_t* __restrict__ in, int32_t vb, int64_t n,
 
 static int val_bytes_of(const gbgpu_csr* m) { return m->val_bytes ? m->val_bytes : 4; }
 
+// ---------------------------------------------------------------------------
+// The step after the linear algebra (src/convert.c:137-280): the answer's
+// columns become indices of the basis hash table.  The reference looks every
+// entry up in that table (insert_in_basis_hash_table_pivots, src/hash.c:604),
+// visiting the rows in answer order; a monomial that is not in the table yet
+// is inserted when its first entry is met.  Here the answer stays on the
+// device: k_first_entry gives every right column the position of its first
+// entry in the answer (the order in which the reference inserts), the caller
+// looks up or inserts each column's monomial once, and k_map_columns
+// rewrites every entry through the resulting column -> index map.
+
+// first[j] = smallest e with cols[e] = shift + j (INT64_MAX: no entry)
+__global__ void k_first_entry(int64_t nnz, const int32_t* __restrict__ cols, int32_t shift,
+                              unsigned long long* first) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t j = cols[e] - shift;
+        // rows are visited roughly in order, so most later entries see a
+        // smaller position already and skip the atomic
+        if (first[j] > (unsigned long long)e) atomicMin(first + j, (unsigned long long)e);
+    }
+}
+
+__global__ void k_fill_u64(int64_t n, unsigned long long v, unsigned long long* out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = v;
+}
+
+// cols[e] = map[cols[e] - shift]
+__global__ void k_map_columns(int64_t nnz, int32_t* cols, int32_t shift,
+                              const int32_t* __restrict__ map) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x)
+        cols[e] = map[cols[e] - shift];
+}
+
+int plan_first_entry(Plan* P, int64_t* first, int32_t n) {
+    if (int rc = settle(P)) return rc;
+    if (P->mode != 0 || P->streamed || n != P->ncr) {
+        set_error("first entries: a linear_algebra plan whose answer is on the device, "
+                  "n = ncr");
+        return GBGPU_EINVAL;
+    }
+    if (n == 0) return GBGPU_OK;
+    unsigned long long* d = nullptr;
+    if (int rc = P->alloc(&d, (size_t)n)) return rc;
+    cudaStream_t s = P->stream;
+    k_fill_u64<<<grid_for(n, 256), 256, 0, s>>>(n, ~0ull >> 1, d);
+    if (P->onnz > 0)
+        k_first_entry<<<grid_for(P->onnz, 256), 256, 0, s>>>(P->onnz, P->out_cols, P->ncl, d);
+    GB_CUDA(cudaGetLastError());
+    count_launch(P->onnz > 0 ? 2 : 1);
+    GB_CUDA(cudaMemcpyAsync(first, d, sizeof(int64_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    for (int32_t j = 0; j < n; ++j)
+        if (first[j] == (int64_t)(~0ull >> 1)) first[j] = -1;
+    return GBGPU_OK;
+}
+
+int plan_map_columns(Plan* P, const int32_t* map, int32_t n) {
+    if (int rc = settle(P)) return rc;
+    if (P->mode != 0 || P->streamed || n != P->ncr) {
+        set_error("column map: a linear_algebra plan whose answer is on the device, n = ncr");
+        return GBGPU_EINVAL;
+    }
+    if (P->onnz == 0) return GBGPU_OK;
+    int32_t* d = nullptr;
+    if (int rc = P->alloc(&d, (size_t)n)) return rc;
+    cudaStream_t s = P->stream;
+    GB_CUDA(cudaMemcpyAsync(d, map, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s));
+    k_map_columns<<<grid_for(P->onnz, 256), 256, 0, s>>>(P->onnz, P->out_cols, P->ncl, d);
+    GB_CUDA(cudaGetLastError());
+    count_launch(1);
+    // the answer's columns are indices of the caller's table from now on:
+    // they no longer count from ncl
+    GB_CUDA(cudaStreamSynchronize(s));
+    return GBGPU_OK;
+}
+
 int plan_create(const gbgpu_csr* m, const gbgpu_options* opt, int mode, Plan** out) {
     *out = nullptr;
     if (!m || m->p < 2 || m->nr < 0 || m->ncl < 0 || m->ncr < 0 ||
@@ -1056,6 +1136,18 @@ int gbgpu_plan_run(gbgpu_plan* plan) {
     DeviceScope scope(plan ? plan->impl_device() : -1);
     if (!plan) return GBGPU_EINVAL;
     return plan_run(plan->impl);
+}
+
+int gbgpu_plan_first_entry(gbgpu_plan* plan, int64_t* first, int32_t n) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
+    if (!plan || (!first && n > 0)) return GBGPU_EINVAL;
+    return plan_first_entry(plan->impl, first, n);
+}
+
+int gbgpu_plan_map_columns(gbgpu_plan* plan, const int32_t* map, int32_t n) {
+    DeviceScope scope(plan ? plan->impl_device() : -1);
+    if (!plan || (!map && n > 0)) return GBGPU_EINVAL;
+    return plan_map_columns(plan->impl, map, n);
 }
 
 int gbgpu_plan_result(gbgpu_plan* plan, gbgpu_rows* out) {

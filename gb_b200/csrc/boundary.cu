@@ -250,6 +250,291 @@ void gbgpu_interreduce_matrix_rows(gbgpu_mat_t* mat, gbgpu_bs_t* bs, const gbgpu
     }
 }
 
+// ---------------------------------------------------------------------------
+// The linear algebra and the step after it (src/f4.c:306-311) with the answer
+// kept on the device in between: gbgpu_linear_algebra_keep leaves the answer
+// of the round in the calling thread's slot, and
+// gbgpu_convert_sparse_matrix_rows_to_basis_elements turns it into basis
+// elements, their columns already mapped to the basis hash table on the
+// device (api.cu: gbgpu_plan_first_entry, gbgpu_plan_map_columns).
+
+}  // extern "C"
+
+namespace {
+
+struct KeptAnswer {
+    gbgpu_plan* plan = nullptr;
+    const gbgpu_mat_t* mat = nullptr;
+    int32_t np = 0, ncl = 0, ncr = 0;
+    int64_t nnz = 0;
+    int bits = 32;
+};
+thread_local KeptAnswer g_kept;
+
+void drop_kept() {
+    if (g_kept.plan) gbgpu_plan_destroy(g_kept.plan);
+    g_kept = KeptAnswer{};
+}
+
+// check_enlarge_basis_ff_{8,16,32} (src/basis.c:149-165 and twins): room
+// for `added` more elements, the new reducibility flags cleared
+int grow_basis(gbgpu_bs_t* bs, int32_t added, int bits) {
+    if (bs->ld + added < bs->sz) return GBGPU_OK;
+    const int32_t sz = bs->sz * 2 > bs->ld + added ? bs->sz * 2 : bs->ld + added;
+    const size_t esz = bits == 8 ? sizeof(int8_t*) : bits == 16 ? sizeof(int16_t*) : sizeof(int32_t*);
+    void** cf = bits == 8 ? (void**)&bs->cf_8 : bits == 16 ? (void**)&bs->cf_16 : (void**)&bs->cf_32;
+    void* ncf = realloc(*cf, esz * (size_t)sz);
+    void* nhm = realloc(bs->hm, sizeof(gbgpu_hm_t*) * (size_t)sz);
+    void* nlm = realloc(bs->lm, sizeof(int32_t) * (size_t)sz);
+    void* nlmps = realloc(bs->lmps, sizeof(int32_t) * (size_t)sz);
+    void* nred = realloc(bs->red, sizeof(int8_t) * (size_t)sz);
+    if (ncf) *cf = ncf;
+    if (nhm) bs->hm = (gbgpu_hm_t**)nhm;
+    if (nlm) bs->lm = (int32_t*)nlm;
+    if (nlmps) bs->lmps = (int32_t*)nlmps;
+    if (nred) bs->red = (int8_t*)nred;
+    if (!ncf || !nhm || !nlm || !nlmps || !nred) return GBGPU_ENOMEM;
+    bs->sz = sz;
+    memset(bs->red + bs->ld, 0, (size_t)(sz - bs->ld));
+    return GBGPU_OK;
+}
+
+// enlarge_hash_table (src/hash.c:185-240): twice the exponent storage and
+// twice the hash map, every element reinserted in index order with the
+// table's probe sequence k <- (k + i) mod hsz.  The same layout as the
+// reference's: later lookups by the reference's own code probe it.
+int grow_hash_table(gbgpu_ht_t* ht) {
+    const int32_t nv = ht->nv, eld = ht->eld, esz = 2 * ht->esz;
+    gbgpu_hd_t* hd = (gbgpu_hd_t*)realloc(ht->hd, sizeof(gbgpu_hd_t) * (size_t)esz);
+    if (!hd) return GBGPU_ENOMEM;
+    ht->hd = hd;
+    memset(hd + eld, 0, sizeof(gbgpu_hd_t) * (size_t)(esz - eld));
+    int16_t** ev = (int16_t**)realloc(ht->ev, sizeof(int16_t*) * (size_t)esz);
+    if (!ev) return GBGPU_ENOMEM;
+    ht->ev = ev;
+    int16_t* blk = (int16_t*)realloc(ev[0], sizeof(int16_t) * (size_t)esz * (size_t)nv);
+    if (!blk) return GBGPU_ENOMEM;
+    for (int32_t i = 0; i < esz; ++i) ev[i] = blk + (size_t)i * (size_t)nv;
+    ht->esz = esz;
+    const int32_t hsz = 2 * ht->hsz;
+    int32_t* hmap = (int32_t*)realloc(ht->hmap, sizeof(int32_t) * (size_t)hsz);
+    if (!hmap) return GBGPU_ENOMEM;
+    ht->hmap = hmap;
+    ht->hsz = hsz;
+    memset(hmap, 0, sizeof(int32_t) * (size_t)hsz);
+    const uint32_t mask = (uint32_t)hsz - 1u;
+    for (int32_t i = 1; i < eld; ++i) {
+        uint32_t k = (uint32_t)hd[i].val;
+        for (int32_t j = 0; j < hsz; ++j) {
+            k = (k + (uint32_t)j) & mask;
+            if (hmap[k]) continue;
+            hmap[k] = i;
+            break;
+        }
+    }
+    return GBGPU_OK;
+}
+
+// the index of monomial e (hash value h) in the table, inserted at the first
+// free slot of its probe sequence when absent, as insert_in_basis_hash_table_
+// pivots does it (src/hash.c:604-669): a new element takes the next free
+// index with the degree and divisor mask of its secondary-table entry
+int32_t table_index(gbgpu_ht_t* ht, const int16_t* e, int32_t h, int32_t deg, int32_t sdm) {
+    const int32_t nv = ht->nv, hsz = ht->hsz;
+    const uint32_t mask = (uint32_t)hsz - 1u;
+    uint32_t k = (uint32_t)h;
+    for (int32_t i = 0; i < hsz; ++i) {
+        k = (k + (uint32_t)i) & mask;
+        const int32_t hm = ht->hmap[k];
+        if (!hm) break;
+        if (ht->hd[hm].val != h) continue;
+        if (memcmp(ht->ev[hm], e, sizeof(int16_t) * (size_t)nv) == 0) return hm;
+    }
+    const int32_t pos = ht->eld;
+    memcpy(ht->ev[pos], e, sizeof(int16_t) * (size_t)nv);
+    ht->hmap[k] = pos;
+    ht->hd[pos].deg = deg;
+    ht->hd[pos].sdm = sdm;
+    ht->hd[pos].val = h;
+    ht->eld = pos + 1;
+    return pos;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gbgpu_linear_algebra_keep_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_stat_t* st) {
+    DeviceScope scope;
+    drop_kept();
+    if (!mat || !bs || !st) return GBGPU_EINVAL;
+    const double ct0 = cpu_seconds(), rt0 = wall_seconds();
+    const int bits = coef_bits(st);
+    gbgpu_options o = shim_options();
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> cols, vals;
+    gather_rows(mat->r, mat->nr, bs_table(bs, bits), bits, st->fc, ptr, cols, vals);
+    gbgpu_csr m{st->fc, st->laopt, mat->nr, mat->ncl, mat->ncr, ptr.data(), cols.data(),
+                vals.data()};
+    gbgpu_plan* plan = nullptr;
+    int rc = gbgpu_plan_create(&m, &o, &plan);
+    if (!rc) rc = gbgpu_plan_run(plan);
+    int32_t np = 0;
+    int64_t nnz = 0;
+    if (!rc) {
+        // a size query: NULL buffers of zero capacity
+        rc = gbgpu_plan_result_into(plan, nullptr, nullptr, nullptr, 0, 0, &np, &nnz);
+        if (rc == GBGPU_ERANGE) rc = GBGPU_OK;
+    }
+    if (rc) {
+        if (plan) gbgpu_plan_destroy(plan);
+        return rc;
+    }
+    // the la functions free their input rows (src/la_ff_16.c:665, :688-691, :804)
+    for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
+    mat->np = np;
+    const int32_t lo = st->laopt;
+    if (!(lo == 1 || lo == 42 || lo == 43)) mat->nr = mat->sz = mat->np;
+    if (np > 0) {
+        g_kept.plan = plan;
+        g_kept.mat = mat;
+        g_kept.np = np;
+        g_kept.nnz = nnz;
+        g_kept.ncl = mat->ncl;
+        g_kept.ncr = mat->ncr;
+        g_kept.bits = bits;
+    } else {
+        gbgpu_plan_destroy(plan);
+    }
+    st->la_ctime += cpu_seconds() - ct0;
+    st->la_rtime += wall_seconds() - rt0;
+    st->num_zerored += (mat->nrl - mat->np);
+    if (st->info_level > 1) {
+        printf("%7d new %7d zero", mat->np, mat->nrl - mat->np);
+        fflush(stdout);
+    }
+    return GBGPU_OK;
+}
+
+void gbgpu_linear_algebra_keep(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_stat_t* st) {
+    const int rc = gbgpu_linear_algebra_keep_status(mat, bs, st);
+    if (rc) {
+        fprintf(stderr, "gbgpu_linear_algebra_keep failed (%d): %s\n", rc, gbgpu_last_error());
+        exit(1);
+    }
+}
+
+int gbgpu_kept_answer(const gbgpu_mat_t* mat) {
+    return g_kept.plan && g_kept.mat == mat && mat && g_kept.np == mat->np ? 1 : 0;
+}
+
+int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
+    gbgpu_mat_t* mat, gbgpu_bs_t* bs, gbgpu_ht_t* bht, const gbgpu_ht_t* sht,
+    const int32_t* hcm, gbgpu_stat_t* st) {
+    if (!mat || !bs || !bht || !sht || !hcm || !st) return GBGPU_EINVAL;
+    if (!gbgpu_kept_answer(mat)) {
+        set_error("no answer of gbgpu_linear_algebra_keep for this matrix");
+        return GBGPU_EINVAL;
+    }
+    if (bht->hsz <= 0 || (bht->hsz & (bht->hsz - 1)) != 0 || bht->nv != sht->nv) {
+        set_error("basis hash table: size not a power of two, or variables differ");
+        return GBGPU_EINVAL;
+    }
+    const double ct0 = cpu_seconds(), rt0 = wall_seconds();
+    const KeptAnswer ka = g_kept;
+    const int bits = ka.bits;
+    int rc;
+    // room for the new elements and for every entry's monomial
+    // (src/convert.c:157-168)
+    if ((rc = grow_basis(bs, ka.np, bits))) return rc;
+    while ((int64_t)bht->esz - bht->eld < ka.nnz)
+        if ((rc = grow_hash_table(bht))) return rc;
+    // the right columns by their first entry in the answer: the order in
+    // which the reference meets (and inserts) their monomials
+    std::vector<int64_t> first((size_t)std::max(ka.ncr, 1));
+    if ((rc = gbgpu_plan_first_entry(ka.plan, first.data(), ka.ncr))) return rc;
+    std::vector<int32_t> order;
+    order.reserve((size_t)ka.ncr);
+    for (int32_t j = 0; j < ka.ncr; ++j)
+        if (first[j] >= 0) order.push_back(j);
+    std::sort(order.begin(), order.end(),
+              [&](int32_t a, int32_t b) { return first[a] < first[b]; });
+    std::vector<int32_t> map((size_t)std::max(ka.ncr, 1), 0);
+    for (int32_t j : order) {
+        const int32_t h = hcm[ka.ncl + j];  // the column's monomial in the secondary table
+        map[j] = table_index(bht, sht->ev[h], sht->hd[h].val, sht->hd[h].deg, sht->hd[h].sdm);
+    }
+    if ((rc = gbgpu_plan_map_columns(ka.plan, map.data(), ka.ncr))) return rc;
+    gbgpu_rows out{};
+    if ((rc = gbgpu_plan_result(ka.plan, &out))) return rc;
+    // the rows join the basis at bs->ld + i (src/convert.c:225-236); mat keeps
+    // the pointer arrays the la would have left
+    const int32_t bl = bs->ld, np = out.np;
+    const size_t esz = bits == 8 ? 1 : bits == 16 ? 2 : 4;
+    void** cf = (void**)malloc(sizeof(void*) * (size_t)std::max(np, 1));
+    gbgpu_hm_t** r = (gbgpu_hm_t**)malloc(sizeof(gbgpu_hm_t*) * (size_t)std::max(np, 1));
+    if (!cf || !r) {
+        free(cf);
+        free(r);
+        gbgpu_rows_free(&out);
+        return GBGPU_ENOMEM;
+    }
+    for (int32_t i = 0; i < np; ++i) {
+        const int64_t b0 = out.row_ptr[i], len = out.row_ptr[i + 1] - b0;
+        gbgpu_hm_t* row = (gbgpu_hm_t*)malloc(sizeof(gbgpu_hm_t) * (size_t)(len + 3));
+        void* c = malloc(esz * (size_t)std::max<int64_t>(len, 1));
+        if (!row || !c) {
+            gbgpu_rows_free(&out);
+            return GBGPU_ENOMEM;
+        }
+        row[0] = bl + i;
+        row[1] = (gbgpu_hm_t)(len % 4);
+        row[2] = (gbgpu_hm_t)len;
+        memcpy(row + 3, out.cols + b0, sizeof(int32_t) * (size_t)len);
+        for (int64_t j = 0; j < len; ++j) {
+            const int32_t v = out.vals[b0 + j];
+            if (bits == 8) ((int8_t*)c)[j] = (int8_t)v;
+            else if (bits == 16) ((int16_t*)c)[j] = (int16_t)v;
+            else ((int32_t*)c)[j] = v;
+        }
+        r[i] = row;
+        cf[i] = c;
+        bs->hm[bl + i] = row;
+        if (bits == 8) bs->cf_8[bl + i] = (int8_t*)c;
+        else if (bits == 16) bs->cf_16[bl + i] = (int16_t*)c;
+        else bs->cf_32[bl + i] = (int32_t*)c;
+    }
+    gbgpu_rows_free(&out);
+    free(mat->r);
+    mat->r = r;
+    if (bits == 8) {
+        free(mat->cf_8);
+        mat->cf_8 = (int8_t**)cf;
+    } else if (bits == 16) {
+        free(mat->cf_16);
+        mat->cf_16 = (int16_t**)cf;
+    } else {
+        free(mat->cf_32);
+        mat->cf_32 = (int32_t**)cf;
+    }
+    drop_kept();
+    st->convert_ctime += cpu_seconds() - ct0;
+    st->convert_rtime += wall_seconds() - rt0;
+    return GBGPU_OK;
+}
+
+void gbgpu_convert_sparse_matrix_rows_to_basis_elements(gbgpu_mat_t* mat, gbgpu_bs_t* bs,
+                                                        gbgpu_ht_t* bht, const gbgpu_ht_t* sht,
+                                                        const int32_t* hcm, gbgpu_stat_t* st) {
+    const int rc =
+        gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(mat, bs, bht, sht, hcm, st);
+    if (rc) {
+        fprintf(stderr, "gbgpu_convert_sparse_matrix_rows_to_basis_elements failed (%d): %s\n",
+                rc, gbgpu_last_error());
+        exit(1);
+    }
+}
+
 // a batch matrix the one-launch small-matrix kernel takes
 static bool batch_small(const gbgpu_csr& m, const gbgpu_options* opt) {
     if (opt && !(opt->form == GBGPU_FORM_AUTO || opt->form == GBGPU_FORM_PLAIN)) return false;

@@ -98,6 +98,22 @@ class Plan:
         _lib.check(self._lib.gbgpu_plan_result(self._h, C.byref(out)))
         return _take(self._lib, out)
 
+    def first_entry(self) -> np.ndarray:
+        """Per right column j: the position of its first entry in the answer's
+        entry array (-1: none) -- the order in which src/hash.c:604-669
+        inserts the answer's monomials into the basis hash table."""
+        n = int(self._mat.ncr)
+        out = np.empty(max(n, 1), dtype=np.int64)
+        _lib.check(self._lib.gbgpu_plan_first_entry(self._h, out.ctypes.data, n))
+        return out[:n]
+
+    def map_columns(self, mapping: np.ndarray) -> None:
+        """Rewrite the answer on the device: column ncl + j becomes mapping[j]."""
+        m = np.ascontiguousarray(mapping, dtype=np.int32)
+        if m.shape[0] != self._mat.ncr:
+            raise ValueError("mapping needs ncr entries")
+        _lib.check(self._lib.gbgpu_plan_map_columns(self._h, m.ctypes.data, int(m.shape[0])))
+
     def stats(self) -> dict:
         st = _lib.Stats()
         _lib.check(self._lib.gbgpu_plan_stats(self._h, C.byref(st)))

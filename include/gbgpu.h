@@ -136,6 +136,44 @@ void gbgpu_convert_hashes_to_columns(int32_t **hcmp, gbgpu_mat_t *mat, gbgpu_sta
  * order. */
 void gbgpu_sort_matrix_rows(gbgpu_mat_t *mat);
 
+/* The linear algebra and the step after it with the answer kept on the
+ * device in between (src/f4.c:306-311).
+ *
+ * gbgpu_linear_algebra_keep replaces `linear_algebra(mat, bs, st)` at
+ * src/f4.c:306 like gbgpu_linear_algebra (input rows freed, mat->np and, for
+ * the sparse options, mat->nr / mat->sz set, statistics updated), but keeps
+ * the answer on the device, in a slot of the calling thread, instead of
+ * building mat->r; the next call of either function below on this thread
+ * takes it (a new gbgpu_linear_algebra_keep drops an answer nobody took).
+ *
+ * gbgpu_convert_sparse_matrix_rows_to_basis_elements replaces
+ * `convert_sparse_matrix_rows_to_basis_elements(mat, bs, bht, sht, hcm, st)`
+ * at src/f4.c:309 (src/convert.c:137-280): the kept answer becomes basis
+ * elements bs->hm[bs->ld + i] / bs->cf_X[bs->ld + i] (mat->r and mat->cf_X
+ * point to the same rows, as after the reference), every entry holding the
+ * index of its monomial in the basis hash table bht.  The reference looks up
+ * every entry in bht and inserts the monomials it does not find
+ * (src/hash.c:604-669); here each right column is looked up once, in the
+ * order of its first entry in the answer (found on the device), which gives
+ * bht exactly the indices and the layout the reference gives it, and the
+ * entries are rewritten on the device through the column -> index map.
+ * Grows bs (src/basis.c:149-165) and bht (src/hash.c:185-240) as the
+ * reference does.  GBGPU_EINVAL without a kept answer for mat.  The call at
+ * src/f4.c:140 (after the final interreduction) has no kept answer and stays
+ * the reference's. */
+void gbgpu_linear_algebra_keep(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
+                               gbgpu_stat_t *st);
+int gbgpu_linear_algebra_keep_status(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
+                                     gbgpu_stat_t *st);
+/* 1 when the calling thread holds the kept answer of mat, else 0 */
+int gbgpu_kept_answer(const gbgpu_mat_t *mat);
+void gbgpu_convert_sparse_matrix_rows_to_basis_elements(gbgpu_mat_t *mat, gbgpu_bs_t *bs,
+                                                        gbgpu_ht_t *bht, const gbgpu_ht_t *sht,
+                                                        const int32_t *hcm, gbgpu_stat_t *st);
+int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
+    gbgpu_mat_t *mat, gbgpu_bs_t *bs, gbgpu_ht_t *bht, const gbgpu_ht_t *sht,
+    const int32_t *hcm, gbgpu_stat_t *st);
+
 /* Same as the two above but returning a status instead of exiting. */
 int gbgpu_linear_algebra_status(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
                                 gbgpu_stat_t *st);
@@ -255,6 +293,16 @@ int gbgpu_plan_run_into_v(gbgpu_plan *plan, int64_t *row_ptr, int32_t *cols,
                           void *vals, int32_t val_bytes, int64_t cap_rows,
                           int64_t cap_nnz, int32_t *np, int64_t *nnz);
 int gbgpu_plan_stats(const gbgpu_plan *plan, gbgpu_stats *stats);
+/* After gbgpu_plan_run of a linear_algebra plan (not streamed): first[j]
+ * (n = ncr entries) = the position, in the answer's entry array, of the
+ * first entry in right column j (column ncl + j), -1 when no row has one.
+ * The basis conversion's insertion order (src/hash.c:604-669). */
+int gbgpu_plan_first_entry(gbgpu_plan *plan, int64_t *first, int32_t n);
+/* Rewrites every entry of the plan's answer on the device: column ncl + j
+ * becomes map[j] (n = ncr entries; the basis hash table's indices for the
+ * conversion of src/convert.c:137-280).  The gbgpu_plan_result* calls then
+ * return the mapped entries. */
+int gbgpu_plan_map_columns(gbgpu_plan *plan, const int32_t *map, int32_t n);
 void gbgpu_plan_destroy(gbgpu_plan *plan);
 
 /* Batched reduction of n independent matrices (different sizes and primes)

@@ -6,3 +6,8 @@ void gbgpu_linear_algebra(void *mat, const void *bs, void *st);
 void gbgpu_interreduce_matrix_rows(void *mat, void *bs, const void *st);
 void gbgpu_convert_hashes_to_columns(void *hcmp, void *mat, void *st, void *sht);
 void gbgpu_sort_matrix_rows(void *mat);
+void gbgpu_linear_algebra_keep(void *mat, const void *bs, void *st);
+int gbgpu_kept_answer(const void *mat);
+void gbgpu_convert_sparse_matrix_rows_to_basis_elements(void *mat, void *bs, void *bht,
+                                                        const void *sht, const void *hcm,
+                                                        void *st);

@@ -77,3 +77,39 @@ def test_f4_with_conversion_on_gpu_matches_golden(case):
     assert lens.tolist() == exp["tlen"]
     assert cfs.tolist() == exp["tcf"]
     assert exps.tolist() == exp["texp"]
+
+
+def _first_entries_host(rr, ncl, ncr):
+    first = np.full(ncr, -1, dtype=np.int64)
+    cols = np.asarray(rr.cols, dtype=np.int64) - ncl
+    seen = np.zeros(ncr, dtype=bool)
+    for e, j in enumerate(cols.tolist()):
+        if not seen[j]:
+            seen[j] = True
+            first[j] = e
+    return first
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,form", [(65521, _lib.FORM_TENSOR), (2147483647, _lib.FORM_AUTO),
+                                    (32003, _lib.FORM_PLAIN)])
+def test_plan_first_entry_and_column_map(p, form):
+    """The device side of src/convert.c:137-280: the first entry of every
+    right column in the answer and the rewrite of every entry through a
+    column map, against the host answer."""
+    from gb_b200 import la
+    m = synth.staircase(900, 300, 700, p, seed=11)
+    plan = la.Plan(m, form=form)
+    plan.run()
+    rr = plan.result()
+    first = plan.first_entry()
+    assert first.tolist() == _first_entries_host(rr, m.ncl, m.ncr).tolist()
+    rng = np.random.default_rng(5)
+    mapping = rng.permutation(m.ncr).astype(np.int32) + 7
+    plan.map_columns(mapping)
+    mapped = plan.result()
+    assert np.array_equal(mapped.row_ptr, rr.row_ptr)
+    assert np.array_equal(mapped.vals, rr.vals)
+    want = mapping[np.asarray(rr.cols, dtype=np.int64) - m.ncl]
+    assert np.array_equal(np.asarray(mapped.cols), want)
+    plan.close()
