@@ -263,13 +263,14 @@ def main():
                     help="shrink the workload (profiling captures only)")
     ap.add_argument("--workload", default="staircase",
                     choices=["staircase", "dense", "rref", "batch", "f4", "f4cubic10",
-                             "multimod"],
+                             "multimod", "basis"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
                          "rref: RREF of a rank-3n/4 n x n block; batch: 2 x 128 independent "
                          "matrices through the batch entry point; f4: the captured la calls "
                          "of the dense F4 systems; multimod: an integer matrix reduced over Q "
-                         "from its GF(p) images")
+                         "from its GF(p) images; basis: the step after the la "
+                         "(src/convert.c:137-280) on the staircase's answer")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
@@ -296,6 +297,9 @@ def main():
         return
     if args.workload == "multimod":
         run_multimod(args)
+        return
+    if args.workload == "basis":
+        run_basis(args)
         return
 
     import torch
@@ -894,6 +898,48 @@ def run_f4_captures(args):
             "data": "dense systems of tests/golden/f4 (seeded coefficients)",
             "config": {"workload": "f4: dense_quadratic_7 (p=32003, la 2) + "
                                    "dense_cubic_5_p31 (p=2^31-1, la 1)", "systems": systems}}
+    print(json.dumps(line), flush=True)
+
+
+def run_basis(args):
+    """The step after the linear algebra (src/f4.c:309, src/convert.c:137-280)
+    on the answer of the staircase (5000 rows, about 77 million entries):
+    the answer turned into basis elements of a fresh basis hash table (40000
+    column monomials of 8 variables).  The GPU arm keeps the la's answer on
+    the device and maps its columns there (gbgpu_linear_algebra_keep +
+    gbgpu_convert_sparse_matrix_rows_to_basis_elements, the answer's trip to
+    host memory included); the reference arm runs the reference's own
+    conversion on its own la's answer.  Both must leave the same basis
+    elements and the same table layout.  Timed: the conversion call only."""
+    import oracle
+    from gb_b200 import la, synth
+    c = CONFIG
+    mat = synth.staircase(c["nru"], c["nrl"], c["ncr"], c["p"], c["dmin"], c["dmax"],
+                          seed=c["seed"])
+    exps = synth.distinct_monomials(mat.ncl + mat.ncr, 8, seed=5)
+    keep = la.function_address("gbgpu_linear_algebra_keep")
+    conv = la.function_address("gbgpu_convert_sparse_matrix_rows_to_basis_elements")
+    gpu = [oracle.basis_bench(mat, exps, keep, conv) for _ in range(max(1, args.steps))]
+    secs = sorted(g["seconds"] for g in gpu)
+    threads = os.cpu_count() or 1
+    ref = None if args.no_cpu else oracle.basis_bench(mat, exps, nthreads=threads)
+    same = None if ref is None else all(
+        g[k] == ref[k] for g in gpu for k in ("np", "eld", "digest", "map_digest"))
+    med = secs[len(secs) // 2]
+    line = {"metric": "basis conversions/s (the staircase answer into basis elements, "
+                      "src/convert.c:137-280)",
+            "value": 1.0 / med, "unit": "conversions/s", "n_gpus": 1, "steps": len(secs),
+            "warmup": 0, "ms_per_step": med * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 indices",
+            "data": "synthetic (seeded staircase; distinct random monomials)",
+            "config": {"workload": "basis conversion of the 20000x5000 staircase answer "
+                                   "(np 5000, 40000 columns, 8 variables, fresh table)"},
+            "gpu_seconds": secs,
+            "cpu_baseline": None if ref is None else {
+                "value": 1.0 / ref["seconds"], "unit": "conversions/s", "cores": 1,
+                "kind": "reference", "sample": "one whole conversion (the reference's "
+                "conversion is single-threaded)", "seconds": ref["seconds"]},
+            "same_basis_as_reference": same}
     print(json.dumps(line), flush=True)
 
 

@@ -276,6 +276,22 @@ void drop_kept() {
     g_kept = KeptAnswer{};
 }
 
+// f(begin, end) over [0, n) split among the host's threads (at most 16, at
+// least `grain` items each)
+template <class Fn>
+void host_parallel(int64_t n, int64_t grain, Fn f) {
+    const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(16, std::thread::hardware_concurrency()));
+    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, n / grain));
+    if (nt <= 1) {
+        f((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int64_t q = 0; q < nt; ++q)
+        th.emplace_back([&, q] { f(n * q / nt, n * (q + 1) / nt); });
+    for (auto& x : th) x.join();
+}
+
 // check_enlarge_basis_ff_{8,16,32} (src/basis.c:149-165 and twins): room
 // for `added` more elements, the new reducibility flags cleared
 int grow_basis(gbgpu_bs_t* bs, int32_t added, int bits) {
@@ -299,33 +315,55 @@ int grow_basis(gbgpu_bs_t* bs, int32_t added, int bits) {
     return GBGPU_OK;
 }
 
-// enlarge_hash_table (src/hash.c:185-240): twice the exponent storage and
-// twice the hash map, every element reinserted in index order with the
-// table's probe sequence k <- (k + i) mod hsz.  The same layout as the
-// reference's: later lookups by the reference's own code probe it.
-int grow_hash_table(gbgpu_ht_t* ht) {
-    const int32_t nv = ht->nv, eld = ht->eld, esz = 2 * ht->esz;
-    gbgpu_hd_t* hd = (gbgpu_hd_t*)realloc(ht->hd, sizeof(gbgpu_hd_t) * (size_t)esz);
-    if (!hd) return GBGPU_ENOMEM;
+// enlarge_hash_table (src/hash.c:185-240), called until at least `need` free
+// entries remain (src/convert.c:166-168): every call doubles the exponent
+// storage and the hash map and reinserts every element, in index order, into
+// the cleared map with the table's probe sequence k <- (k + i) mod hsz.  Only
+// the last reinsertion decides the map, so one growth to the final size with
+// one reinsertion leaves the same table (the same sizes, indices and map
+// layout, which the reference's own code probes later), without the
+// intermediate copies: fresh zeroed blocks for the map and the hash data.
+int grow_hash_table(gbgpu_ht_t* ht, int64_t need) {
+    int64_t esz = ht->esz, hsz = ht->hsz;
+    const int32_t eld = ht->eld, nv = ht->nv;
+    if (esz - eld >= need) return GBGPU_OK;
+    while (esz - eld < need) {
+        esz *= 2;
+        hsz *= 2;
+    }
+    if (esz > INT32_MAX || hsz > INT32_MAX) {
+        set_error("basis hash table would exceed 2^31 entries");
+        return GBGPU_ERANGE;
+    }
+    gbgpu_hd_t* hd = (gbgpu_hd_t*)calloc((size_t)esz, sizeof(gbgpu_hd_t));
+    int16_t* blk = (int16_t*)malloc(sizeof(int16_t) * (size_t)esz * (size_t)nv);
+    int16_t** ev = (int16_t**)malloc(sizeof(int16_t*) * (size_t)esz);
+    int32_t* hmap = (int32_t*)calloc((size_t)hsz, sizeof(int32_t));
+    if (!hd || !blk || !ev || !hmap) {
+        free(hd);
+        free(blk);
+        free(ev);
+        free(hmap);
+        return GBGPU_ENOMEM;
+    }
+    memcpy(hd, ht->hd, sizeof(gbgpu_hd_t) * (size_t)eld);
+    memcpy(blk, ht->ev[0], sizeof(int16_t) * (size_t)eld * (size_t)nv);
+    host_parallel(esz, 1 << 16, [&](int64_t a, int64_t b) {
+        for (int64_t i = a; i < b; ++i) ev[i] = blk + (size_t)i * (size_t)nv;
+    });
+    free(ht->hd);
+    free(ht->ev[0]);
+    free(ht->ev);
+    free(ht->hmap);
     ht->hd = hd;
-    memset(hd + eld, 0, sizeof(gbgpu_hd_t) * (size_t)(esz - eld));
-    int16_t** ev = (int16_t**)realloc(ht->ev, sizeof(int16_t*) * (size_t)esz);
-    if (!ev) return GBGPU_ENOMEM;
     ht->ev = ev;
-    int16_t* blk = (int16_t*)realloc(ev[0], sizeof(int16_t) * (size_t)esz * (size_t)nv);
-    if (!blk) return GBGPU_ENOMEM;
-    for (int32_t i = 0; i < esz; ++i) ev[i] = blk + (size_t)i * (size_t)nv;
-    ht->esz = esz;
-    const int32_t hsz = 2 * ht->hsz;
-    int32_t* hmap = (int32_t*)realloc(ht->hmap, sizeof(int32_t) * (size_t)hsz);
-    if (!hmap) return GBGPU_ENOMEM;
     ht->hmap = hmap;
-    ht->hsz = hsz;
-    memset(hmap, 0, sizeof(int32_t) * (size_t)hsz);
+    ht->esz = (int32_t)esz;
+    ht->hsz = (int32_t)hsz;
     const uint32_t mask = (uint32_t)hsz - 1u;
     for (int32_t i = 1; i < eld; ++i) {
         uint32_t k = (uint32_t)hd[i].val;
-        for (int32_t j = 0; j < hsz; ++j) {
+        for (int64_t j = 0; j < hsz; ++j) {
             k = (k + (uint32_t)j) & mask;
             if (hmap[k]) continue;
             hmap[k] = i;
@@ -447,8 +485,7 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
     // room for the new elements and for every entry's monomial
     // (src/convert.c:157-168)
     if ((rc = grow_basis(bs, ka.np, bits))) return rc;
-    while ((int64_t)bht->esz - bht->eld < ka.nnz)
-        if ((rc = grow_hash_table(bht))) return rc;
+    if ((rc = grow_hash_table(bht, ka.nnz))) return rc;
     // the right columns by their first entry in the answer: the order in
     // which the reference meets (and inserts) their monomials
     std::vector<int64_t> first((size_t)std::max(ka.ncr, 1));
@@ -479,13 +516,17 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
         gbgpu_rows_free(&out);
         return GBGPU_ENOMEM;
     }
-    for (int32_t i = 0; i < np; ++i) {
+    std::atomic<bool> oom{false};
+    host_parallel(np, 8, [&](int64_t ia, int64_t ib) {
+      for (int32_t i = (int32_t)ia; i < (int32_t)ib; ++i) {
         const int64_t b0 = out.row_ptr[i], len = out.row_ptr[i + 1] - b0;
         gbgpu_hm_t* row = (gbgpu_hm_t*)malloc(sizeof(gbgpu_hm_t) * (size_t)(len + 3));
         void* c = malloc(esz * (size_t)std::max<int64_t>(len, 1));
         if (!row || !c) {
-            gbgpu_rows_free(&out);
-            return GBGPU_ENOMEM;
+            free(row);
+            free(c);
+            oom = true;
+            return;
         }
         row[0] = bl + i;
         row[1] = (gbgpu_hm_t)(len % 4);
@@ -503,8 +544,10 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
         if (bits == 8) bs->cf_8[bl + i] = (int8_t*)c;
         else if (bits == 16) bs->cf_16[bl + i] = (int16_t*)c;
         else bs->cf_32[bl + i] = (int32_t*)c;
-    }
+      }
+    });
     gbgpu_rows_free(&out);
+    if (oom) return GBGPU_ENOMEM;
     free(mat->r);
     mat->r = r;
     if (bits == 8) {

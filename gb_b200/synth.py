@@ -348,3 +348,17 @@ def column_order_key(exps: np.ndarray, deg: np.ndarray, idx: np.ndarray, mo: int
         else:
             keys.append((-i, -d) + tuple(reversed(e)))
     return keys
+
+
+def distinct_monomials(n: int, nv: int, max_exp: int = 31, seed: int = 1) -> np.ndarray:
+    """``n`` distinct exponent vectors of ``nv`` variables (int16, entries in
+    [0, max_exp]): the monomials of a matrix's columns for the basis-
+    conversion workloads."""
+    rng = np.random.default_rng(seed)
+    if (max_exp + 1) ** nv < 2 * n:
+        raise ValueError("too few monomials of this shape")
+    out = np.empty((0, nv), dtype=np.int16)
+    while out.shape[0] < n:
+        cand = rng.integers(0, max_exp + 1, size=(2 * n, nv)).astype(np.int16)
+        out = np.unique(np.concatenate([out, cand]), axis=0)
+    return rng.permutation(out)[:n]

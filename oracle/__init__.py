@@ -89,6 +89,9 @@ def _load_ref():
         lib.gbref_layout.restype = C.c_int
         lib.gbref_hook_calls.restype = C.c_int64
         lib.gbref_hook_seconds.restype = C.c_double
+        lib.gbref_basis_bench.argtypes = [C.c_int32] * 8 + [
+            _i64p, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+            _PI32, _PI32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         lib.f4_julia.restype = C.c_int64
         lib.f4_julia.argtypes = [_PI32, C.POINTER(_PI32), C.POINTER(_PI32), C.POINTER(C.c_void_p),
                                  _i32p, _i32p, _i32p] + [C.c_int32] * 12
@@ -172,6 +175,31 @@ def ref_interreduce(p: int, nc: int, rows: ReducedRows) -> Tuple[ReducedRows, fl
     if rc != 0:
         raise RuntimeError(f"reference interreduce failed (rc={rc})")
     return _take(lib.gbref_free, rows.np, ptr, cols, vals), secs.value
+
+
+def basis_bench(mat: MacaulayMatrix, exps: np.ndarray, keep_fn: Optional[int] = None,
+                convert_fn: Optional[int] = None, nthreads: int = 1) -> dict:
+    """One matrix through the la and then src/convert.c:137-280 (the answer
+    turned into basis elements of a fresh basis and basis hash table), with
+    the reference's own functions or, when given, the raw addresses of
+    gbgpu_linear_algebra_keep / gbgpu_convert_sparse_matrix_rows_to_basis_
+    elements.  ``exps`` (nc x nv int16, distinct rows) are the column
+    monomials.  Returns the conversion's seconds, np, bht->eld and digests of
+    the new basis elements and of the table's hash map."""
+    lib = _load_ref()
+    nru, nrl = mat.split_counts()
+    exps = np.ascontiguousarray(exps, dtype=np.int16)
+    secs = C.c_double()
+    npv, eld = C.c_int32(), C.c_int32()
+    dig, mdig = C.c_uint64(), C.c_uint64()
+    rc = lib.gbref_basis_bench(mat.p, int(exps.shape[1]), nthreads, mat.nr, nru, nrl, mat.ncl,
+                               mat.ncr, mat.row_ptr, mat.cols, mat.vals, exps.ctypes.data,
+                               keep_fn, convert_fn, C.byref(secs), C.byref(npv), C.byref(eld),
+                               C.byref(dig), C.byref(mdig))
+    if rc != 0:
+        raise RuntimeError(f"basis bench failed (rc={rc})")
+    return {"seconds": secs.value, "np": npv.value, "eld": eld.value, "digest": dig.value,
+            "map_digest": mdig.value}
 
 
 def ref_layout() -> np.ndarray:

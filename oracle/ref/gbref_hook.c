@@ -613,3 +613,150 @@ int gbref_convert_csr(int32_t nv, int32_t n, const int16_t *exps, const int32_t 
     free(st);
     return 0;
 }
+
+/* ---- the step after the linear algebra, timed and digested --------------
+ * One matrix through the la and then convert_sparse_matrix_rows_to_basis_
+ * elements (src/f4.c:306-311, src/convert.c:137-280) with a fresh basis and a
+ * fresh basis hash table: the reference's own functions, or ext_keep /
+ * ext_convert (gbgpu_linear_algebra_keep and
+ * gbgpu_convert_sparse_matrix_rows_to_basis_elements) when given.  The nc
+ * column monomials (exps, nc x nv, distinct) go into a secondary table in
+ * column order; hcm maps columns to them.  Returns the conversion's seconds,
+ * the new elements' count, bht->eld, a digest of the new basis elements
+ * (every entry's table index, its monomial's exponents and its coefficient,
+ * FNV-1a) and a digest of the table's hash map (every occupied slot). */
+typedef void (*gbref_conv_fn)(mat_t *, bs_t *, ht_t *, const ht_t *, const hl_t *, stat_t *);
+
+static uint64_t gbref_fnv(uint64_t h, uint64_t v)
+{
+    for (int b = 0; b < 8; ++b) {
+        h ^= (v >> (8 * b)) & 0xFFu;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+int gbref_basis_bench(int32_t p, int32_t nv, int32_t nthreads, int32_t nr, int32_t nru,
+                      int32_t nrl, int32_t ncl, int32_t ncr, const int64_t *row_ptr,
+                      const int32_t *cols, const int32_t *vals, const int16_t *exps,
+                      void *ext_keep, void *ext_convert, double *seconds, int32_t *out_np,
+                      int32_t *out_eld, uint64_t *digest, uint64_t *map_digest)
+{
+    int32_t i;
+    const int32_t nc = ncl + ncr;
+    const int ff_bits = gbref_ff_bits(p);
+    stat_t *st = (stat_t *)calloc(1, sizeof(stat_t));
+    bs_t *bs = (bs_t *)calloc(1, sizeof(bs_t));
+    mat_t *mat = (mat_t *)calloc(1, sizeof(mat_t));
+    void **tab = (void **)calloc((size_t)(nr > 0 ? nr : 1), sizeof(void *));
+    void **inputs = (void **)calloc((size_t)(nr > 0 ? nr : 1), sizeof(void *));
+    int hts = 17;
+    while ((1 << (hts - 6)) < nc + 2) ++hts;
+
+    st->fc = p;
+    st->ff_bits = ff_bits;
+    st->laopt = 1;
+    st->nthrds = nthreads > 0 ? nthreads : 1;
+    st->info_level = 0;
+    st->mo = 0;
+    st->nvars = nv;
+    st->init_hts = hts;
+    set_function_pointers(st);
+
+    ht_t *bht = initialize_basis_hash_table(st);
+    ht_t *sht = initialize_secondary_hash_table(bht, st);
+    hl_t *hcm = (hl_t *)malloc((size_t)(nc > 0 ? nc : 1) * sizeof(hl_t));
+    for (i = 0; i < nc; ++i) hcm[i] = insert_in_hash_table(exps + (size_t)i * nv, sht);
+
+    if (ff_bits == 8) bs->cf_8 = (cf8_t **)tab;
+    else if (ff_bits == 16) bs->cf_16 = (cf16_t **)tab;
+    else bs->cf_32 = (cf32_t **)tab;
+    mat->r = (hm_t **)malloc((size_t)(nr > 0 ? nr : 1) * sizeof(hm_t *));
+    for (i = 0; i < nr; ++i) {
+        const int64_t len = row_ptr[i + 1] - row_ptr[i];
+        hm_t *row = (hm_t *)malloc((size_t)(len + 3) * sizeof(hm_t));
+        row[0] = i;
+        row[1] = (hm_t)(len % UNROLL);
+        row[2] = (hm_t)len;
+        memcpy(row + 3, cols + row_ptr[i], (size_t)len * sizeof(int32_t));
+        mat->r[i] = row;
+        tab[i] = gbref_alloc_cf(ff_bits, vals + row_ptr[i], len);
+        inputs[i] = tab[i];
+    }
+    mat->nr = nr;
+    mat->sz = nr;
+    mat->nru = nru;
+    mat->nrl = nrl;
+    mat->ncl = ncl;
+    mat->ncr = ncr;
+    mat->nc = nc;
+
+    if (ext_keep) ((gbref_la_fn)ext_keep)(mat, bs, st);
+    else (linear_algebra)(mat, bs, st);
+    /* the basis' coefficient table is the input table until it grows */
+    const int32_t np = mat->np;
+    double t0 = realtime();
+    if (np > 0) {
+        if (ext_convert) ((gbref_conv_fn)ext_convert)(mat, bs, bht, sht, hcm, st);
+        else convert_sparse_matrix_rows_to_basis_elements(mat, bs, bht, sht, hcm, st);
+    }
+    double t1 = realtime();
+    if (seconds) *seconds = t1 - t0;
+
+    uint64_t h = 1469598103934665603ull;
+    void *const *btab = gbref_bs_table(bs, ff_bits);
+    for (i = 0; i < np; ++i) {
+        const hm_t *row = bs->hm[bs->ld + i];
+        h = gbref_fnv(h, (uint64_t)row[2]);
+        for (int32_t l = 0; l < row[2]; ++l) {
+            const hl_t ix = row[3 + l];
+            h = gbref_fnv(h, (uint64_t)(uint32_t)ix);
+            for (int32_t v = 0; v < nv; ++v) h = gbref_fnv(h, (uint64_t)(uint16_t)bht->ev[ix][v]);
+            h = gbref_fnv(h, (uint64_t)(uint32_t)gbref_cf(btab, ff_bits, row[0], l));
+        }
+    }
+    uint64_t hm = 1469598103934665603ull;
+    for (hl_t k = 0; k < bht->hsz; ++k)
+        if (bht->hmap[k]) {
+            hm = gbref_fnv(hm, (uint64_t)(uint32_t)k);
+            hm = gbref_fnv(hm, (uint64_t)(uint32_t)bht->hmap[k]);
+        }
+    *out_np = np;
+    *out_eld = bht->eld;
+    *digest = h;
+    *map_digest = hm;
+
+    for (i = 0; i < np; ++i) {
+        free(bs->hm[bs->ld + i]);
+        free(((void **)btab)[bs->ld + i]);
+    }
+    for (i = 0; i < nr; ++i)
+        if (i >= np || inputs[i] != ((void **)btab)[i]) free(inputs[i]);
+    free(inputs);
+    free((void *)btab);
+    free(bs->hm);
+    free(bs->lm);
+    free(bs->lmps);
+    free(bs->red);
+    free(bs);
+    free(mat->r);
+    free(mat->cf_8);
+    free(mat->cf_16);
+    free(mat->cf_32);
+    free(mat);
+    free(hcm);
+    free(sht->ev[0]);
+    free(sht->ev);
+    free(sht->hd);
+    free(sht->hmap);
+    free(sht);
+    free(bht->ev[0]);
+    free(bht->ev);
+    free(bht->hd);
+    free(bht->hmap);
+    free(bht->dm);
+    free(bht->rn);
+    free(bht);
+    free(st);
+    return 0;
+}

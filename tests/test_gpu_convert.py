@@ -113,3 +113,25 @@ def test_plan_first_entry_and_column_map(p, form):
     want = mapping[np.asarray(rr.cols, dtype=np.int64) - m.ncl]
     assert np.array_equal(np.asarray(mapped.cols), want)
     plan.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("p", [251, 32003, 65521, 2147483647])
+def test_basis_conversion_matches_reference(p):
+    """src/f4.c:306-311 on one matrix with a fresh basis: the reference's la
+    and convert_sparse_matrix_rows_to_basis_elements against
+    gbgpu_linear_algebra_keep + gbgpu_convert_sparse_matrix_rows_to_basis_
+    elements -- the same new basis elements (table indices, monomials,
+    coefficients), the same table size and the same hash-map layout."""
+    from gb_b200 import la
+    m = synth.staircase(1500, 500, 1200, p, seed=21)
+    exps = synth.distinct_monomials(m.ncl + m.ncr, 7, seed=3)
+    want = oracle.basis_bench(m, exps)
+    got = oracle.basis_bench(
+        m, exps, keep_fn=la.function_address("gbgpu_linear_algebra_keep"),
+        convert_fn=la.function_address("gbgpu_convert_sparse_matrix_rows_to_basis_elements"))
+    assert got["np"] == want["np"] > 0
+    assert got["eld"] == want["eld"]
+    assert got["digest"] == want["digest"]
+    assert got["map_digest"] == want["map_digest"]

@@ -11,7 +11,10 @@ exact CPU evaluation, as the checker):
   three primes, against the reference's dense echelon and interreduction
   (exact_dense_linear_algebra + interreduce_dense_matrix, src/la_ff_32.c:1217
   and :1181, src/la_ff_16.c:873-989 and :837-871 for p = 251) run on the
-  same block through a Macaulay matrix whose Schur complement is the block.
+  same block through a Macaulay matrix whose Schur complement is the block;
+* the step after the linear algebra (src/convert.c:137-280) on the answer of
+  the 20000 x 5000 staircase: the same new basis elements, basis hash table
+  size and hash-map layout as the reference's own conversion.
 """
 import ctypes as C
 import os
@@ -36,6 +39,20 @@ def test_staircase_20000x5000_matches_reference_whole():
     want, _ = oracle.ref_la(mat, 1, nthreads=THREADS)
     assert got.np == want.np and got.nnz == want.nnz
     assert got.equals(want), got.first_difference(want)
+
+
+@needs_ref
+def test_basis_conversion_of_the_staircase_answer_matches_reference():
+    mat = synth.staircase(20000, 5000, 20000, 65521, 0.02, 0.05, seed=1)
+    exps = synth.distinct_monomials(mat.ncl + mat.ncr, 8, seed=5)
+    want = oracle.basis_bench(mat, exps, nthreads=THREADS)
+    got = oracle.basis_bench(
+        mat, exps, keep_fn=la.function_address("gbgpu_linear_algebra_keep"),
+        convert_fn=la.function_address("gbgpu_convert_sparse_matrix_rows_to_basis_elements"))
+    assert got["np"] == want["np"] == 5000
+    assert got["eld"] == want["eld"]
+    assert got["digest"] == want["digest"]
+    assert got["map_digest"] == want["map_digest"]
 
 
 def _uniform(torch, p, shape, seed):

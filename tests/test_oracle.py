@@ -229,3 +229,20 @@ def test_reference_conversion_matches_restated_order(mo):
         seg = r["hashes"][ptr[i]:ptr[i + 1]]
         assert cols[off:off + seg.shape[0]].tolist() == col_of[seg].tolist()
         off += seg.shape[0]
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build absent")
+def test_basis_bench_harness_inserts_each_answer_column_once():
+    """The basis-conversion harness (reference functions only): the fresh
+    basis hash table ends with one element per distinct column of the answer
+    (src/hash.c:604-669 inserts a monomial at its first entry and finds it
+    afterwards), and two runs give the same digests."""
+    from gb_b200 import synth
+    m = synth.staircase(300, 100, 250, 65521, seed=4)
+    exps = synth.distinct_monomials(m.ncl + m.ncr, 6, seed=2)
+    a = oracle.basis_bench(m, exps)
+    b = oracle.basis_bench(m, exps)
+    want, _ = oracle.ref_la(m)
+    assert a["np"] == want.np
+    assert a["eld"] == 1 + len(np.unique(want.cols))
+    assert a == {**b, "seconds": a["seconds"]}
