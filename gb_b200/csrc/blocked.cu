@@ -156,6 +156,73 @@ k_densify_seg(int32_t n, const int32_t* __restrict__ rows, const int64_t* __rest
     }
 }
 
+// The same rows without shared memory, for the known pivots (whose written
+// intervals are short): a CTA takes a row:
+// it fills each interval with zeros (16-byte stores; ld a multiple of 4, out
+// 16-byte aligned), waits at a barrier (the zeros are then ordered before any
+// later store of the CTA) and scatters the row's entries of the interval
+// straight into place.  Every entry is read once per interval.
+//
+// With split > 0 (the known pivots P = [A | B] of the tensor form, whose
+// readers need less) only two column intervals of row i are written:
+//   [from_i, e1), e1 = min(split, max(from_i + stride, span[i / stride] + 1)):
+//       the diagonal block and the left columns the block's rows reach;
+//   [split + lo, split + hi): the right columns of row group i / 128, from
+//       brange[i / 128] = (first, last) nonzero right column of the group,
+//       widened to 64-column boundaries (the limb split reads whole
+//       64-column blocks); nothing when the group's right part is zero.
+// Everything else in the row is left as it was: its readers (the block
+// inverses, the block solves and the limb split of the Schur product's B)
+// never look there.
+constexpr int DS_THREADS = 256;
+__global__ void __launch_bounds__(DS_THREADS)
+k_densify_direct(int32_t n, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_ptr,
+              const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals, int32_t nc,
+              int32_t stride, uint32_t* out, int64_t ld, int32_t split = 0,
+              const int32_t* __restrict__ span = nullptr,
+              const int2* __restrict__ brange = nullptr) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int32_t r = rows ? rows[i] : i;
+        const int64_t b = row_ptr[r], e = row_ptr[r + 1];
+        const int32_t from = stride ? (i / stride) * stride : 0;
+        uint32_t* o = out + (size_t)i * ld;
+        // the (one or two) intervals of this row
+        int32_t iv[2][2] = {{from, nc}, {0, 0}};
+        int n_iv = 1;
+        if (split > 0) {
+            int32_t e1 = split;
+            if (span && stride) e1 = min(split, max(from + stride, span[i / stride] + 1));
+            iv[0][1] = e1;
+            const int2 br = brange[i / 128];
+            if (br.y >= br.x) {
+                const int32_t lo = split + (br.x / 64) * 64;
+                const int32_t hi = min(nc, split + (br.y / 64 + 1) * 64);
+                const int32_t s = lo & ~3;
+                if (s <= e1) {
+                    iv[0][1] = max(e1, hi);
+                } else {
+                    iv[1][0] = s;
+                    iv[1][1] = hi;
+                    n_iv = 2;
+                }
+            }
+        }
+        for (int q = 0; q < n_iv; ++q) {
+            const int32_t a0 = iv[q][0], a1 = iv[q][1];  // a0 is a multiple of 4
+            const int32_t w4 = (a1 - a0) / 4;
+            uint4* o4 = (uint4*)(o + a0);
+            for (int j = threadIdx.x; j < w4; j += blockDim.x) o4[j] = make_uint4(0u, 0u, 0u, 0u);
+            for (int32_t j = a0 + 4 * w4 + threadIdx.x; j < a1; j += blockDim.x) o[j] = 0u;
+            __syncthreads();
+            for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
+                const int32_t c = cols[k];
+                if (c >= a0 && c < a1) o[c] = vals[k];
+            }
+        }
+        __syncthreads();  // this row's stores are done before the CTA's next row
+    }
+}
+
 // dense known-pivot matrix: row c of out = the pivot row of lead c
 __global__ void k_densify_pivots(int32_t ncl, const int32_t* __restrict__ piv_row,
                                  const int64_t* __restrict__ row_ptr,
@@ -294,13 +361,23 @@ k_neg_inverse(const uint32_t* __restrict__ src, int64_t ld, int64_t stride_b, in
     const int kb = b == n_blocks - 1 ? last_kb : KB;
     const uint32_t* s = src + (size_t)b * stride_b;
     const int tid = threadIdx.x;
-    for (int t = tid; t < KB * KB; t += blockDim.x) {
-        const int i = t / KB, j = t % KB;
-        uint32_t v;
-        if (i < kb && j < kb) v = s[(size_t)i * ld + j];
-        else v = i == j ? 1u : 0u;
-        U[i][j] = v;
-        V[i][j] = i == j ? 1u : 0u;
+    // the block: KB * KB / blockDim.x entries per thread, all loads in flight
+    constexpr int PER = KB * KB / INV_THREADS;
+    {
+        uint32_t v[PER];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int t = tid + q * INV_THREADS;
+            const int i = t / KB, j = t % KB;
+            v[q] = (i < kb && j < kb) ? s[(size_t)i * ld + j] : (i == j ? 1u : 0u);
+        }
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int t = tid + q * INV_THREADS;
+            const int i = t / KB, j = t % KB;
+            U[i][j] = v[q];
+            V[i][j] = i == j ? 1u : 0u;
+        }
     }
     __syncthreads();
     const uint32_t p = f.p;
@@ -1326,7 +1403,7 @@ static int blocked_run(const BlockedInput& in, BlockedOutput* out, Ctx& c, const
         // CUDA-core GEMM reads B whole, so there P gets everything from the
         // diagonal block on
         const bool banded = c.form != GBGPU_FORM_PLAIN;
-        BL_LAUNCH(k_densify_seg<<<std::min(ncl, 148 * 3), 512, DS_COLS * 4, s>>>(
+        BL_LAUNCH(k_densify_direct<<<std::min(ncl, 148 * 8), DS_THREADS, 0, s>>>(
             ncl, in.piv_row, in.row_ptr, in.cols, in.vals, nc, NB, P, ld, banded ? ncl : 0, span,
             brange));
         // -A_kk^-1 of every NB x NB diagonal block of A (read in place from P)
