@@ -74,7 +74,8 @@ EXPORTS = [
     "gbgpu_sort_matrix_rows", "gbgpu_linear_algebra_keep", "gbgpu_linear_algebra_keep_status",
     "gbgpu_kept_answer", "gbgpu_convert_sparse_matrix_rows_to_basis_elements",
     "gbgpu_convert_sparse_matrix_rows_to_basis_elements_status", "gbgpu_plan_first_entry",
-    "gbgpu_plan_map_columns",
+    "gbgpu_plan_map_columns", "gbgpu_symbolic_preprocessing",
+    "gbgpu_symbolic_preprocessing_status",
 ]
 
 _lib = None

@@ -315,6 +315,10 @@ int grow_basis(gbgpu_bs_t* bs, int32_t added, int bits) {
     return GBGPU_OK;
 }
 
+}  // namespace
+
+namespace gbgpu {
+
 // enlarge_hash_table (src/hash.c:185-240), called until at least `need` free
 // entries remain (src/convert.c:166-168): every call doubles the exponent
 // storage and the hash map and reinserts every element, in index order, into
@@ -372,6 +376,10 @@ int grow_hash_table(gbgpu_ht_t* ht, int64_t need) {
     }
     return GBGPU_OK;
 }
+
+}  // namespace gbgpu
+
+namespace {
 
 // the index of monomial e (hash value h) in the table, inserted at the first
 // free slot of its probe sequence when absent, as insert_in_basis_hash_table_

@@ -53,5 +53,8 @@ void plan_destroy(Plan* P);
 const gbgpu_stats& plan_stats(const Plan* P);
 // waits for a pending small-matrix run and reads its checks and sizes
 int settle(Plan* P);
+// gb's enlarge_hash_table (src/hash.c:185-240) applied until at least `need`
+// entries are free, done as one growth to the final size (boundary.cu)
+int grow_hash_table(gbgpu_ht_t* ht, int64_t need);
 
 }  // namespace gbgpu

@@ -136,6 +136,22 @@ void gbgpu_convert_hashes_to_columns(int32_t **hcmp, gbgpu_mat_t *mat, gbgpu_sta
  * order. */
 void gbgpu_sort_matrix_rows(gbgpu_mat_t *mat);
 
+/* Replaces `symbolic_preprocessing(mat, bs, st, sht, bht)` at src/f4.c:298
+ * and :121 (src/symbol.c:202-272): walks the secondary table's monomials in
+ * index order, marks every one as a column, and for each the first basis
+ * element of the lead-monomial list whose lead divides it becomes a matrix
+ * row (multiplied by the quotient, its terms inserted into sht as
+ * src/hash.c:672-746 inserts them).  The reducer search runs on the device
+ * for a wave of monomials at a time; the walk itself, the rows and the
+ * insertions follow the reference step by step, so sht and mat end as the
+ * reference leaves them.  Grows sht and mat->r as the reference does.
+ * Prints the status and exits on error. */
+void gbgpu_symbolic_preprocessing(gbgpu_mat_t *mat, const gbgpu_bs_t *bs, gbgpu_stat_t *st,
+                                  gbgpu_ht_t *sht, const gbgpu_ht_t *bht);
+int gbgpu_symbolic_preprocessing_status(gbgpu_mat_t *mat, const gbgpu_bs_t *bs,
+                                        gbgpu_stat_t *st, gbgpu_ht_t *sht,
+                                        const gbgpu_ht_t *bht);
+
 /* The linear algebra and the step after it with the answer kept on the
  * device in between (src/f4.c:306-311).
  *

@@ -1,11 +1,11 @@
 /* gb_gpu_full.c -- TEST INFRASTRUCTURE ONLY (and the recipe a user follows).
  *
- * gb (ederc/gb v0.16) with the step before the linear algebra on the GPU as
- * well: its unity build (the include list of src/gb.c) with two function-like
+ * gb (ederc/gb v0.16) with the steps before the linear algebra on the GPU as
+ * well: its unity build (the include list of src/gb.c) with function-like
  * macros defined just before f4.c, so that only f4.c's calls of
- * convert_hashes_to_columns and sort_matrix_rows (src/f4.c:132-135 and
- * :299-300) go to libgbgpu.so; their definitions in convert.c and order.c,
- * compiled earlier, keep their names.  The Makefile adds the two -D macros
+ * symbolic_preprocessing, convert_hashes_to_columns and sort_matrix_rows
+ * (src/f4.c:121, :132-135, :298-300) go to libgbgpu.so; their definitions in
+ * symbol.c, convert.c and order.c, compiled earlier, keep their names.  The Makefile adds the two -D macros
  * that reroute the linear algebra (src/f4.c:137, :306), as for libgb_gpu.so;
  * below, the round's linear algebra and the conversion of its answer into
  * basis elements (src/f4.c:306-311) are rerouted together. */
@@ -32,6 +32,9 @@
 #define convert_hashes_to_columns(a, b, c, d) \
     gbgpu_convert_hashes_to_columns((void *)(a), (void *)(b), (void *)(c), (void *)(d))
 #define sort_matrix_rows(m) gbgpu_sort_matrix_rows((void *)(m))
+#define symbolic_preprocessing(m, b, s, sh, bh) \
+    gbgpu_symbolic_preprocessing((void *)(m), (const void *)(b), (void *)(s), (void *)(sh), \
+                                 (const void *)(bh))
 
 /* The linear algebra of every round keeps its answer on the device, and the
  * step after it (src/f4.c:309) turns that answer into basis elements there.

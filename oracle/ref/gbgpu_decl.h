@@ -11,3 +11,5 @@ int gbgpu_kept_answer(const void *mat);
 void gbgpu_convert_sparse_matrix_rows_to_basis_elements(void *mat, void *bs, void *bht,
                                                         const void *sht, const void *hcm,
                                                         void *st);
+void gbgpu_symbolic_preprocessing(void *mat, const void *bs, void *st, void *sht,
+                                  const void *bht);
