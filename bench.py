@@ -263,14 +263,15 @@ def main():
                     help="shrink the workload (profiling captures only)")
     ap.add_argument("--workload", default="staircase",
                     choices=["staircase", "dense", "rref", "batch", "f4", "f4cubic10",
-                             "multimod", "basis"],
+                             "multimod", "basis", "f4full"],
                     help="staircase: the metric's workload; dense: exact modular GEMM "
                          "D - A B mod p on n x n residue blocks (tensor vs CUDA-core form); "
                          "rref: RREF of a rank-3n/4 n x n block; batch: 2 x 128 independent "
                          "matrices through the batch entry point; f4: the captured la calls "
                          "of the dense F4 systems; multimod: an integer matrix reduced over Q "
                          "from its GF(p) images; basis: the step after the la "
-                         "(src/convert.c:137-280) on the staircase's answer")
+                         "(src/convert.c:137-280) on the staircase's answer; f4full: whole F4 "
+                         "runs of a dense cubic system with more and more steps on the GPU")
     ap.add_argument("--n", type=int, default=16384, help="dense workload size")
     ap.add_argument("--p", type=int, default=65521, help="dense workload prime")
     ap.add_argument("--verify", type=int, default=1,
@@ -300,6 +301,9 @@ def main():
         return
     if args.workload == "basis":
         run_basis(args)
+        return
+    if args.workload == "f4full":
+        run_f4_full(args)
         return
 
     import torch
@@ -940,6 +944,59 @@ def run_basis(args):
                 "kind": "reference", "sample": "one whole conversion (the reference's "
                 "conversion is single-threaded)", "seconds": ref["seconds"]},
             "same_basis_as_reference": same}
+    print(json.dumps(line), flush=True)
+
+
+def run_f4_full(args):
+    """Whole F4 runs (gb's f4_julia) of the dense cubic system in 7 variables
+    over 2^31 - 1 (7 polynomials, every monomial of degree <= 3, seeded
+    coefficients, la option 1): gb as built from its sources (every step on
+    the host, the la with all host threads), gb with its linear algebra on
+    the GPU (libgb_gpu.so), and gb with symbolic preprocessing, the column
+    mapping and row sort, the la and the conversion of the answer into basis
+    elements on the GPU (libgb_gpu_full.so).  The three bases must be equal.
+    Timed: each whole run, median of `steps` runs (the reference once)."""
+    import time
+    import oracle
+    from gb_b200 import synth
+    threads = os.cpu_count() or 1
+    case = synth.f4_case("dense_cubic_7_p31", 7, 7, 3, 2147483647, 1, seed=10,
+                         nr_threads=threads)
+
+    def timed(fn):
+        t0 = time.perf_counter()
+        out = fn(case)
+        return time.perf_counter() - t0, out
+
+    oracle.gb_gpu_full_f4(case)  # first use: library load, device set-up
+    oracle.gb_gpu_f4(case)
+    full = [timed(oracle.gb_gpu_full_f4) for _ in range(max(1, args.steps))]
+    la_only = [timed(oracle.gb_gpu_f4) for _ in range(max(1, args.steps))]
+    ref = None if args.no_cpu else timed(oracle.ref_f4)
+
+    def same(a, b):
+        return all(x.tolist() == y.tolist() for x, y in zip(a, b))
+
+    def med(v):
+        s = sorted(x[0] for x in v)
+        return s[len(s) // 2]
+
+    line = {"metric": "F4 runs/s (dense cubic, 7 variables, p = 2^31-1, whole gb F4)",
+            "value": 1.0 / med(full), "unit": "runs/s", "n_gpus": 1, "steps": len(full),
+            "warmup": 1, "ms_per_step": med(full) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (mod p, exact)",
+            "data": "synthetic (seeded coefficients, gb_b200.synth.f4_case)",
+            "config": {"workload": "gb f4_julia on dense_cubic_7_p31 (la option 1, "
+                                   f"{threads} host threads)"},
+            "gpu_steps_seconds": {"symbolic_preprocessing_conversion_la_basis": med(full),
+                                  "la_only": med(la_only)},
+            "bases_equal": same(full[0][1], la_only[0][1]) and
+                           (ref is None or same(full[0][1], ref[1])),
+            "basis_length": int(len(full[0][1][0])),
+            "cpu_baseline": None if ref is None else {
+                "value": 1.0 / ref[0], "unit": "runs/s", "cores": threads,
+                "kind": "reference", "sample": "one whole F4 run of gb built from its sources",
+                "seconds": ref[0]}}
     print(json.dumps(line), flush=True)
 
 

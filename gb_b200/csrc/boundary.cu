@@ -262,8 +262,14 @@ void gbgpu_interreduce_matrix_rows(gbgpu_mat_t* mat, gbgpu_bs_t* bs, const gbgpu
 
 namespace {
 
+// The kept answer: on the device in a plan, or -- for the matrices the
+// one-pass small path reduces, whose answer lands in host memory anyway -- as
+// host CSR arrays.
 struct KeptAnswer {
     gbgpu_plan* plan = nullptr;
+    bool host = false;
+    std::vector<int64_t> hptr;
+    std::vector<int32_t> hcols, hvals;
     const gbgpu_mat_t* mat = nullptr;
     int32_t np = 0, ncl = 0, ncr = 0;
     int64_t nnz = 0;
@@ -417,6 +423,30 @@ int gbgpu_linear_algebra_keep_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbg
     const double ct0 = cpu_seconds(), rt0 = wall_seconds();
     const int bits = coef_bits(st);
     gbgpu_options o = shim_options();
+    int64_t in_nnz = 0;
+    for (int32_t i = 0; i < mat->nr; ++i) in_nnz += mat->r[i][2];
+    if (st->fc >= 2 && in_nnz <= INT32_MAX / 2 &&
+        small_eligible(mat->nr, mat->ncl, mat->ncr, o.device)) {
+        // one pass; the answer comes back to host memory, where it is kept
+        GatherCtx gc{mat, bs_table(bs, bits), bits, st->fc};
+        SmallInput in{st->fc, mat->nr, mat->ncl, mat->ncr, in_nnz, o.device, fill_from_rows, &gc};
+        SmallAnswer a;
+        if (int rc = small_reduce(in, &a)) return rc;
+        for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
+        mat->np = a.np;
+        if (a.np > 0) {
+            g_kept.host = true;
+            g_kept.hptr.assign(a.offs, a.offs + a.np + 1);
+            g_kept.hcols.assign(a.cols, a.cols + a.nnz);
+            g_kept.hvals.assign(a.vals, a.vals + a.nnz);
+            g_kept.mat = mat;
+            g_kept.np = a.np;
+            g_kept.nnz = a.nnz;
+            g_kept.ncl = mat->ncl;
+            g_kept.ncr = mat->ncr;
+            g_kept.bits = bits;
+        }
+    } else {
     std::vector<int64_t> ptr;
     std::vector<int32_t> cols, vals;
     gather_rows(mat->r, mat->nr, bs_table(bs, bits), bits, st->fc, ptr, cols, vals);
@@ -439,8 +469,6 @@ int gbgpu_linear_algebra_keep_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbg
     // the la functions free their input rows (src/la_ff_16.c:665, :688-691, :804)
     for (int32_t i = 0; i < mat->nr; ++i) free(mat->r[i]);
     mat->np = np;
-    const int32_t lo = st->laopt;
-    if (!(lo == 1 || lo == 42 || lo == 43)) mat->nr = mat->sz = mat->np;
     if (np > 0) {
         g_kept.plan = plan;
         g_kept.mat = mat;
@@ -452,6 +480,9 @@ int gbgpu_linear_algebra_keep_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbg
     } else {
         gbgpu_plan_destroy(plan);
     }
+    }  // plan path
+    const int32_t lo = st->laopt;
+    if (!(lo == 1 || lo == 42 || lo == 43)) mat->nr = mat->sz = mat->np;
     st->la_ctime += cpu_seconds() - ct0;
     st->la_rtime += wall_seconds() - rt0;
     st->num_zerored += (mat->nrl - mat->np);
@@ -471,7 +502,8 @@ void gbgpu_linear_algebra_keep(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, gbgpu_sta
 }
 
 int gbgpu_kept_answer(const gbgpu_mat_t* mat) {
-    return g_kept.plan && g_kept.mat == mat && mat && g_kept.np == mat->np ? 1 : 0;
+    return (g_kept.plan || g_kept.host) && g_kept.mat == mat && mat && g_kept.np == mat->np ? 1
+                                                                                            : 0;
 }
 
 int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
@@ -487,7 +519,7 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
         return GBGPU_EINVAL;
     }
     const double ct0 = cpu_seconds(), rt0 = wall_seconds();
-    const KeptAnswer ka = g_kept;
+    const KeptAnswer& ka = g_kept;  // dropped at the end
     const int bits = ka.bits;
     int rc;
     // room for the new elements and for every entry's monomial
@@ -496,8 +528,13 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
     if ((rc = grow_hash_table(bht, ka.nnz))) return rc;
     // the right columns by their first entry in the answer: the order in
     // which the reference meets (and inserts) their monomials
-    std::vector<int64_t> first((size_t)std::max(ka.ncr, 1));
-    if ((rc = gbgpu_plan_first_entry(ka.plan, first.data(), ka.ncr))) return rc;
+    std::vector<int64_t> first((size_t)std::max(ka.ncr, 1), -1);
+    if (ka.host) {
+        for (int64_t e = (int64_t)ka.hcols.size() - 1; e >= 0; --e)
+            first[ka.hcols[e] - ka.ncl] = e;
+    } else if ((rc = gbgpu_plan_first_entry(ka.plan, first.data(), ka.ncr))) {
+        return rc;
+    }
     std::vector<int32_t> order;
     order.reserve((size_t)ka.ncr);
     for (int32_t j = 0; j < ka.ncr; ++j)
@@ -509,9 +546,25 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
         const int32_t h = hcm[ka.ncl + j];  // the column's monomial in the secondary table
         map[j] = table_index(bht, sht->ev[h], sht->hd[h].val, sht->hd[h].deg, sht->hd[h].sdm);
     }
-    if ((rc = gbgpu_plan_map_columns(ka.plan, map.data(), ka.ncr))) return rc;
+    // the answer with its entries mapped: rewritten on the device (plan), or
+    // here for an answer already in host memory
     gbgpu_rows out{};
-    if ((rc = gbgpu_plan_result(ka.plan, &out))) return rc;
+    std::vector<int32_t> hmapped;
+    if (ka.host) {
+        hmapped.resize(ka.hcols.size());
+        for (size_t e = 0; e < ka.hcols.size(); ++e) hmapped[e] = map[ka.hcols[e] - ka.ncl];
+        out.np = ka.np;
+        out.nnz = ka.nnz;
+        out.row_ptr = const_cast<int64_t*>(ka.hptr.data());
+        out.cols = hmapped.data();
+        out.vals = const_cast<int32_t*>(ka.hvals.data());
+    } else {
+        if ((rc = gbgpu_plan_map_columns(ka.plan, map.data(), ka.ncr))) return rc;
+        if ((rc = gbgpu_plan_result(ka.plan, &out))) return rc;
+    }
+    auto release_out = [&]() {
+        if (!ka.host) gbgpu_rows_free(&out);
+    };
     // the rows join the basis at bs->ld + i (src/convert.c:225-236); mat keeps
     // the pointer arrays the la would have left
     const int32_t bl = bs->ld, np = out.np;
@@ -521,7 +574,7 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
     if (!cf || !r) {
         free(cf);
         free(r);
-        gbgpu_rows_free(&out);
+        release_out();
         return GBGPU_ENOMEM;
     }
     std::atomic<bool> oom{false};
@@ -554,7 +607,7 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
         else bs->cf_32[bl + i] = (int32_t*)c;
       }
     });
-    gbgpu_rows_free(&out);
+    release_out();
     if (oom) return GBGPU_ENOMEM;
     free(mat->r);
     mat->r = r;
