@@ -112,3 +112,35 @@ def test_integration_recipe_build_links_to_library():
     undefined = set(re.findall(r" U (gbgpu_\w+)", out))
     assert undefined == {"gbgpu_linear_algebra", "gbgpu_interreduce_matrix_rows"}
     assert re.search(r" T f4_julia\b", out)
+
+
+def test_steps_around_the_la_reject_bad_calls_before_any_device_work():
+    """The basis conversion needs the kept answer of gbgpu_linear_algebra_keep
+    for the same matrix, and symbolic preprocessing tables over the same
+    variables with a power-of-two map: both refuse otherwise, with
+    GBGPU_EINVAL, before touching the device."""
+    import ctypes as C
+    lib = _lib.load()
+    mat = (C.c_uint8 * 256)()
+    bs = (C.c_uint8 * 256)()
+    st = (C.c_uint8 * 1024)()
+    bht = (C.c_int32 * 32)()
+    sht = (C.c_int32 * 32)()
+    hcm = (C.c_int32 * 4)()
+    lib.gbgpu_kept_answer.argtypes = [C.c_void_p]
+    assert lib.gbgpu_kept_answer(C.addressof(mat)) == 0
+    f = lib.gbgpu_convert_sparse_matrix_rows_to_basis_elements_status
+    f.argtypes = [C.c_void_p] * 6
+    assert f(C.addressof(mat), C.addressof(bs), C.addressof(bht), C.addressof(sht),
+             C.addressof(hcm), C.addressof(st)) == -22
+    # ht_t: 3 pointers (6 int32 slots), then eld, esz, hsz, nv
+    sht[6:10] = [1, 8, 16, 3]
+    bht[6:10] = [1, 8, 16, 4]
+    g = lib.gbgpu_symbolic_preprocessing_status
+    g.argtypes = [C.c_void_p] * 5
+    assert g(C.addressof(mat), C.addressof(bs), C.addressof(st), C.addressof(sht),
+             C.addressof(bht)) == -22
+    bht[9] = 3
+    sht[8] = 12  # not a power of two
+    assert g(C.addressof(mat), C.addressof(bs), C.addressof(st), C.addressof(sht),
+             C.addressof(bht)) == -22
