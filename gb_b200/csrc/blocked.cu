@@ -88,25 +88,11 @@ __global__ void k_densify(int32_t n, const int32_t* __restrict__ rows,
 // stride is 0); columns left of from_i are not written.  Each CTA assembles
 // DS_COLS-column segments of a row in shared memory and writes them whole
 // with 16-byte stores (ld a multiple of 4, out 16-byte aligned).
-//
-// With split > 0 (the known pivots P = [A | B] of the tensor form, whose
-// readers need less) only two column intervals of row i are written:
-//   [from_i, e1), e1 = min(split, max(from_i + stride, span[i / stride] + 1)):
-//       the diagonal block and the left columns the block's rows reach;
-//   [split + lo, split + hi): the right columns of row group i / 128, from
-//       brange[i / 128] = (first, last) nonzero right column of the group,
-//       widened to 64-column boundaries (the limb split reads whole
-//       64-column blocks); nothing when the group's right part is zero.
-// Everything else in the row is left as it was: its readers (the block
-// inverses, the block solves and the limb split of the Schur product's B)
-// never look there.
 constexpr int DS_COLS = 16384;
 __global__ void __launch_bounds__(512)
 k_densify_seg(int32_t n, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_ptr,
               const int32_t* __restrict__ cols, const uint32_t* __restrict__ vals, int32_t nc,
-              int32_t stride, uint32_t* out, int64_t ld, int32_t split = 0,
-              const int32_t* __restrict__ span = nullptr,
-              const int2* __restrict__ brange = nullptr) {
+              int32_t stride, uint32_t* out, int64_t ld) {
     extern __shared__ uint4 ds_smem[];
     uint32_t* seg = (uint32_t*)ds_smem;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
@@ -114,44 +100,20 @@ k_densify_seg(int32_t n, const int32_t* __restrict__ rows, const int64_t* __rest
         const int64_t b = row_ptr[r], e = row_ptr[r + 1];
         const int32_t from = stride ? (i / stride) * stride : 0;
         uint32_t* o = out + (size_t)i * ld;
-        // the (one or two) intervals of this row
-        int32_t iv[2][2] = {{from, nc}, {0, 0}};
-        int n_iv = 1;
-        if (split > 0) {
-            int32_t e1 = split;
-            if (span && stride) e1 = min(split, max(from + stride, span[i / stride] + 1));
-            iv[0][1] = e1;
-            const int2 br = brange[i / 128];
-            if (br.y >= br.x) {
-                const int32_t lo = split + (br.x / 64) * 64;
-                const int32_t hi = min(nc, split + (br.y / 64 + 1) * 64);
-                const int32_t s = lo & ~3;
-                if (s <= e1) {
-                    iv[0][1] = max(e1, hi);
-                } else {
-                    iv[1][0] = s;
-                    iv[1][1] = hi;
-                    n_iv = 2;
-                }
+        for (int32_t s0 = from; s0 < nc; s0 += DS_COLS) {
+            const int32_t w = min(DS_COLS, nc - s0);
+            for (int j = threadIdx.x; j < (w + 3) / 4; j += blockDim.x)
+                ds_smem[j] = make_uint4(0u, 0u, 0u, 0u);
+            __syncthreads();
+            for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
+                const int32_t c = cols[k] - s0;
+                if (c >= 0 && c < w) seg[c] = vals[k];
             }
-        }
-        for (int q = 0; q < n_iv; ++q) {
-            const int32_t a0 = iv[q][0], a1 = iv[q][1];
-            for (int32_t s0 = a0; s0 < a1; s0 += DS_COLS) {
-                const int32_t w = min(DS_COLS, a1 - s0);
-                for (int j = threadIdx.x; j < (w + 3) / 4; j += blockDim.x)
-                    ds_smem[j] = make_uint4(0u, 0u, 0u, 0u);
-                __syncthreads();
-                for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
-                    const int32_t c = cols[k] - s0;
-                    if (c >= 0 && c < w) seg[c] = vals[k];
-                }
-                __syncthreads();
-                uint4* o4 = (uint4*)(o + s0);
-                for (int j = threadIdx.x; j < w / 4; j += blockDim.x) o4[j] = ds_smem[j];
-                for (int j = (w / 4) * 4 + threadIdx.x; j < w; j += blockDim.x) o[s0 + j] = seg[j];
-                __syncthreads();
-            }
+            __syncthreads();
+            uint4* o4 = (uint4*)(o + s0);
+            for (int j = threadIdx.x; j < w / 4; j += blockDim.x) o4[j] = ds_smem[j];
+            for (int j = (w / 4) * 4 + threadIdx.x; j < w; j += blockDim.x) o[s0 + j] = seg[j];
+            __syncthreads();
         }
     }
 }
