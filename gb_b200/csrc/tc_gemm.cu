@@ -208,6 +208,7 @@ struct TcParams {
     const uint8_t* fb;
     unsigned long long* steps;  // optional: K steps executed, summed over tiles
     uint32_t p, pneg_inv;
+    uint32_t mu;     // floor(2^32 / p)
     uint32_t cw[7];  // 2^(8w) R mod p
     int32_t* err;
     long long budget;
@@ -529,22 +530,48 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     // D values of the later blocks, issued before the fold
                     if (!EARLY_D || c0 != cbeg) load_d(c0, dv);
                     uint32_t v[32];
+                    if constexpr (L <= 3) {
+                        // one Montgomery reduction of the weighted sum:
+                        // T = sum_w S_w (2^(8w) R mod p) < (2L - 1) 2^31 p, so
+                        // (T + q p) / 2^32 < 2^32, then one Barrett step
+                        uint64_t T[32];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] = 0;
+                        for (int w = 0; w < C::NW; ++w) {
+                            uint32_t a[32];
+                            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + acc_base +
+                                          (uint32_t)(w * C::BN + c0),
+                                      a);
+                            const uint32_t cw = prm.cw[w];
 #pragma unroll
-                    for (int w = 0; w < C::NW; ++w) {
-                        uint32_t a[32];
-                        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + acc_base + (uint32_t)(w * C::BN + c0),
-                                  a);
-                        const uint32_t cw = prm.cw[w];
+                            for (int j = 0; j < 32; ++j)
+                                T[j] = (w == 0 ? 0ull : T[j]) + (uint64_t)a[j] * cw;
+                        }
 #pragma unroll
                         for (int j = 0; j < 32; ++j) {
-                            const uint64_t T = (uint64_t)a[j] * cw;
-                            const uint32_t qq = (uint32_t)T * prm.pneg_inv;
-                            uint32_t r = (uint32_t)((T + (uint64_t)qq * p) >> 32);
-                            r = r >= p ? r - p : r;
-                            const uint32_t sum = v[j] + r;
-                            v[j] = sum >= p ? sum - p : sum;
+                            const uint32_t qq = (uint32_t)T[j] * prm.pneg_inv;
+                            const uint32_t t = (uint32_t)((T[j] + (uint64_t)qq * p) >> 32);
+                            const uint32_t r = t - __umulhi(t, prm.mu) * p;
+                            v[j] = r >= p ? r - p : r;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) v[j] = 0;
+#pragma unroll
+                        for (int w = 0; w < C::NW; ++w) {
+                            uint32_t a[32];
+                            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + acc_base +
+                                          (uint32_t)(w * C::BN + c0),
+                                      a);
+                            const uint32_t cw = prm.cw[w];
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const uint64_t T = (uint64_t)a[j] * cw;
+                                const uint32_t qq = (uint32_t)T * prm.pneg_inv;
+                                uint32_t r = (uint32_t)((T + (uint64_t)qq * p) >> 32);
+                                r = r >= p ? r - p : r;
+                                const uint32_t sum = v[j] + r;
+                                v[j] = sum >= p ? sum - p : sum;
+                            }
                         }
                     }
                     // stage (row lane, column j) at [lane][j ^ lane]
@@ -971,6 +998,7 @@ static int tc_run(const TcGemmArgs& g, uint8_t* planes, cudaStream_t s, int32_t*
     const FieldMont f = FieldMont::make(g.p);
     prm.p = g.p;
     prm.pneg_inv = f.pneg_inv;
+    prm.mu = (uint32_t)((((uint64_t)1) << 32) / g.p);
     const uint64_t R = ((uint64_t)1 << 32) % g.p;
     uint64_t pw = 1;
     for (int w = 0; w < 7; ++w) {
