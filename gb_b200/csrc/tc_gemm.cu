@@ -412,6 +412,11 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                     }
                     tc_fence_after();
                     const uint32_t st = base + s * C::STAGE_BYTES;
+                    // the descriptors of the stage's operands: the start address
+                    // field holds address / 16 in its low 14 bits, and every
+                    // operand of the stage lies below 2^18 bytes, so an offset
+                    // adds to the descriptor without a carry out of the field
+                    const uint64_t dst = umma_desc_sw128(st);
 #pragma unroll
                     for (int i = 0; i < L; ++i) {
 #pragma unroll
@@ -420,9 +425,9 @@ k_tc_submul(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                             const bool first_pair = (i == (w > L - 1 ? w - (L - 1) : 0));
 #pragma unroll
                             for (int kk = 0; kk < C::BK / 32; ++kk) {
-                                const uint64_t ad = umma_desc_sw128(st + i * C::A_BYTES + kk * 32);
-                                const uint64_t bd = umma_desc_sw128(
-                                    st + L * C::A_BYTES + jj * C::B_BYTES + kk * 32);
+                                const uint64_t ad = dst + (uint64_t)((i * C::A_BYTES + kk * 32) >> 4);
+                                const uint64_t bd =
+                                    dst + (uint64_t)((L * C::A_BYTES + jj * C::B_BYTES + kk * 32) >> 4);
                                 const uint32_t acc = (pk == 0 && kk == 0 && first_pair) ? 0u : 1u;
                                 tc_mma_i8(tmem + (uint32_t)(ab * C::NW * C::BN + w * C::BN), ad, bd,
                                           C::IDESC, acc);
