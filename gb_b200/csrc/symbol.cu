@@ -205,13 +205,17 @@ int gbgpu_symbolic_preprocessing_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, 
     int rc;
     // the basis leads, in the order of the lead-monomial list
     // capacities in entries: the variable count differs from one system to the next
+    // (a capacity is cleared before its buffers are replaced, so that a failed
+    // allocation leaves nothing that a later call would take for a buffer)
     if ((size_t)lml > g.lcap) {
         const size_t cap = std::max<size_t>((size_t)lml, 2 * g.lcap);
+        g.lcap = 0;
         if ((rc = grow_device(&g.lsdm, cap)) || (rc = grow_device(&g.ldeg, cap))) return rc;
         g.lcap = cap;
     }
     if ((size_t)lml * nv > g.lecap) {
         const size_t cap = std::max<size_t>((size_t)lml * nv, 2 * g.lecap);
+        g.lecap = 0;
         if ((rc = grow_device(&g.lexp, cap))) return rc;
         g.lecap = cap;
     }
@@ -245,6 +249,7 @@ int gbgpu_symbolic_preprocessing_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, 
         int r;
         if ((size_t)n > g.mcap) {
             const size_t cap = std::max<size_t>((size_t)n, 2 * g.mcap);
+            g.mcap = 0;
             if ((r = grow_device(&g.msdm, cap)) || (r = grow_device(&g.mdeg, cap)) ||
                 (r = grow_device(&g.red, cap)))
                 return r;
@@ -252,6 +257,7 @@ int gbgpu_symbolic_preprocessing_status(gbgpu_mat_t* mat, const gbgpu_bs_t* bs, 
         }
         if ((size_t)n * nv > g.mecap) {
             const size_t cap = std::max<size_t>((size_t)n * nv, 2 * g.mecap);
+            g.mecap = 0;
             if ((r = grow_device(&g.mexp, cap))) return r;
             g.mecap = cap;
         }
