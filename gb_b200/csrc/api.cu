@@ -211,6 +211,9 @@ struct Plan {
     // answer streamed to host arrays during the run (gbgpu_plan_run_into_v)
     StreamOut* stream_req = nullptr;
     bool streamed = false;
+    // the answer's columns were rewritten by plan_map_columns: they are the
+    // caller's table indices and no longer count from ncl
+    bool mapped = false;
     cudaStream_t s_out = nullptr;
     gbgpu_stats stats{};
     cudaEvent_t ev[8] = {};
@@ -686,6 +689,7 @@ int settle(Plan* P) {
 int plan_run(Plan* P) {
     P->launches = 0;
     P->streamed = false;
+    P->mapped = false;
     int rc;
     GemmProfile prof;
     if (P->profile) {
@@ -824,9 +828,9 @@ __global__ void k_map_columns(int64_t nnz, int32_t* cols, int32_t shift,
 
 int plan_first_entry(Plan* P, int64_t* first, int32_t n) {
     if (int rc = settle(P)) return rc;
-    if (P->mode != 0 || P->streamed || n != P->ncr) {
-        set_error("first entries: a linear_algebra plan whose answer is on the device, "
-                  "n = ncr");
+    if (P->mode != 0 || P->streamed || P->mapped || n != P->ncr) {
+        set_error("first entries: a linear_algebra plan whose answer is on the device and "
+                  "not mapped yet, n = ncr");
         return GBGPU_EINVAL;
     }
     if (n == 0) return GBGPU_OK;
@@ -847,11 +851,15 @@ int plan_first_entry(Plan* P, int64_t* first, int32_t n) {
 
 int plan_map_columns(Plan* P, const int32_t* map, int32_t n) {
     if (int rc = settle(P)) return rc;
-    if (P->mode != 0 || P->streamed || n != P->ncr) {
-        set_error("column map: a linear_algebra plan whose answer is on the device, n = ncr");
+    if (P->mode != 0 || P->streamed || P->mapped || n != P->ncr) {
+        set_error("column map: a linear_algebra plan whose answer is on the device and not "
+                  "mapped yet, n = ncr");
         return GBGPU_EINVAL;
     }
-    if (P->onnz == 0) return GBGPU_OK;
+    if (P->onnz == 0) {
+        P->mapped = true;
+        return GBGPU_OK;
+    }
     int32_t* d = nullptr;
     if (int rc = P->alloc(&d, (size_t)n)) return rc;
     cudaStream_t s = P->stream;
@@ -862,6 +870,7 @@ int plan_map_columns(Plan* P, const int32_t* map, int32_t n) {
     // the answer's columns are indices of the caller's table from now on:
     // they no longer count from ncl
     GB_CUDA(cudaStreamSynchronize(s));
+    P->mapped = true;
     return GBGPU_OK;
 }
 

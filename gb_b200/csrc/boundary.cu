@@ -608,7 +608,14 @@ int gbgpu_convert_sparse_matrix_rows_to_basis_elements_status(
       }
     });
     release_out();
-    if (oom) return GBGPU_ENOMEM;
+    if (oom) {
+        // the rows made so far are the basis's (bs->hm, bs->cf_*); the
+        // pointer arrays meant for mat are not handed over
+        free(cf);
+        free(r);
+        set_error("basis conversion: host allocation failed");
+        return GBGPU_ENOMEM;
+    }
     free(mat->r);
     mat->r = r;
     if (bits == 8) {

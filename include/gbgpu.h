@@ -317,7 +317,9 @@ int gbgpu_plan_first_entry(gbgpu_plan *plan, int64_t *first, int32_t n);
 /* Rewrites every entry of the plan's answer on the device: column ncl + j
  * becomes map[j] (n = ncr entries; the basis hash table's indices for the
  * conversion of src/convert.c:137-280).  The gbgpu_plan_result* calls then
- * return the mapped entries. */
+ * return the mapped entries.  Once mapped, the answer's columns no longer
+ * count from ncl: a second map or a gbgpu_plan_first_entry call returns
+ * GBGPU_EINVAL until the plan runs again. */
 int gbgpu_plan_map_columns(gbgpu_plan *plan, const int32_t *map, int32_t n);
 void gbgpu_plan_destroy(gbgpu_plan *plan);
 

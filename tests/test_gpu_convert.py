@@ -112,6 +112,16 @@ def test_plan_first_entry_and_column_map(p, form):
     assert np.array_equal(mapped.vals, rr.vals)
     want = mapping[np.asarray(rr.cols, dtype=np.int64) - m.ncl]
     assert np.array_equal(np.asarray(mapped.cols), want)
+    # the mapped answer no longer counts from ncl: a second map or a first-
+    # entry query is refused, and the answer stays as mapped
+    with pytest.raises(_lib.GbgpuError):
+        plan.map_columns(mapping)
+    with pytest.raises(_lib.GbgpuError):
+        plan.first_entry()
+    assert np.array_equal(np.asarray(plan.result().cols), want)
+    # a new run starts from ncl-based columns again
+    plan.run()
+    assert plan.first_entry().tolist() == first.tolist()
     plan.close()
 
 
