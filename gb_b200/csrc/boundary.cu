@@ -666,6 +666,15 @@ int gbgpu_reduce_batch(int32_t n, const gbgpu_csr* ms, const gbgpu_options* opt,
         memset(&outs[i], 0, sizeof(gbgpu_rows));
         status[i] = GBGPU_OK;
     }
+    if (n == 0) return GBGPU_OK;
+    {
+        // no usable device: no matrix runs, each one says why
+        DeviceInfo info;
+        if (int rc = device_init(opt ? opt->device : 0, &info)) {
+            for (int32_t i = 0; i < n; ++i) status[i] = rc;
+            return rc;
+        }
+    }
     // The small matrices of the batch go to ONE persistent launch (small.cu,
     // a device work queue over the matrices); the others are reduced by a few
     // host workers, each one matrix at a time on a stream of its own, so

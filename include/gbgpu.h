@@ -325,7 +325,9 @@ void gbgpu_plan_destroy(gbgpu_plan *plan);
 
 /* Batched reduction of n independent matrices (different sizes and primes)
  * in one pass: status[i] receives each matrix's own status, so one bad
- * matrix does not fail the others.  Returns GBGPU_OK if the batch ran.
+ * matrix does not fail the others.  Returns GBGPU_OK if the batch ran;
+ * without a usable device none runs and the call and every status[i]
+ * return the device error (GBGPU_ENODEV).
  * GBGPU_BATCH_WORKERS (default 4) matrices are in flight at once, each on a
  * stream of its own (opt->stream is not used). */
 int gbgpu_reduce_batch(int32_t n, const gbgpu_csr *ms,
