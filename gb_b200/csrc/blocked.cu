@@ -759,15 +759,15 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
     my_lead = min(my_lead, __shfl_xor_sync(0xffffffffu, my_lead, 4));
     int k = 0;
     for (int step = 0; step < KB; ++step) {
-        int key = (g == 0 && !my_piv && my_lead != INT_MAX) ? my_lead * KB + r : INT_MAX;
-        for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+        // warp minima by the warp-wide integer reduction (one redux.sync each)
+        const int key = __reduce_min_sync(
+            0xffffffffu, (g == 0 && !my_piv && my_lead != INT_MAX) ? my_lead * KB + r : INT_MAX);
         int* sm = s_min[step & 1];
         if (lane == 0) sm[warp] = key;
         __syncthreads();  // also: the previous step's updates are visible
         // the 32 warp minima: one read per lane, then a warp reduction
         static_assert(KB * PF_GROUPS / 32 == 32, "one warp minimum per lane");
-        int best = sm[lane];
-        for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+        const int best = __reduce_min_sync(0xffffffffu, sm[lane]);
         if (best == INT_MAX) break;  // uniform: no pivot left in the panel
         const int c = best / KB, i = best % KB;
         if (tid == 0) {
@@ -820,10 +820,8 @@ k_panel_factor(const uint32_t* __restrict__ Dp, int64_t ld, const int32_t* __res
             }
             __syncwarp(grp);  // the row's lanes have read its old support
             if (g < 4) s_emask[r][g] = g == 0 ? U[0] : g == 1 ? U[1] : g == 2 ? U[2] : U[3];
-            nl = min(nl, __shfl_xor_sync(grp, nl, 1));
-            nl = min(nl, __shfl_xor_sync(grp, nl, 2));
-            nl = min(nl, __shfl_xor_sync(grp, nl, 4));
-            my_lead = nl;
+            // the row's eight lanes (all of them take this branch together)
+            my_lead = __reduce_min_sync(grp, nl);
         }
         ++k;
     }
